@@ -1,0 +1,389 @@
+"""Benchmark of the supermesh hot path: clipped element pairs per second.
+
+One step = one pass of the hot path over one pair of meshes: candidate
+search (LBVH build + traversal), intersection of every candidate pair, and
+the compensated measure reduction, through libsupermesh_gpu_supermesh.
+
+Workload (default): 3D plain supermesh, target 27^3 x 6 = 118,098 Kuhn tets
+(seed 3) against source 32^3 x 6 = 196,608 tets (seed 2), jitter 0.25h,
+FP64.  The unit of work is one candidate pair of the strict-AABB candidate
+set (the tree finder's set); pairs/s = candidates / step time.
+
+  value      device-resident inputs (positions/enlists already in HBM)
+  e2e        the same call with host (pinned) inputs: H2D of positions and
+             element lists and D2H of the per-element measure in the timed
+             region
+  roofline   the dominant kernel (tet clipping), timed alone over the same
+             candidates, against the measured FP64 DADD/DMUL issue rate
+  cpu_baseline  the oracle restatement of the reference algorithm
+             (quadtree/octree + breadth-first clipping), one thread, full
+             workload, on this host
+
+Multi-GPU: the workload is replicated per rank (independent replicas, no
+collective on the data path); value = all ranks' pairs / max step time.
+
+`--impl reference` times the reference algorithm on the host CPU (the oracle
+restatement, all host threads; the Fortran reference cannot be built here).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "clipped element-pairs/sec"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", default="tet3d_27x32")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--kernel-only", action="store_true",
+                   help="run only warm-up + timed steps (for profiler launch lists)")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.lines = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(gpus: int):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def all_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def load_probe():
+    from libsupermesh_b200 import build
+
+    L = ctypes.CDLL(str(build.build_probe()))
+    L.lsm_probe_fp64_rate.restype = ctypes.c_double
+    L.lsm_probe_fp64_rate.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.lsm_probe_flush_l2.restype = ctypes.c_int
+    L.lsm_probe_flush_l2.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+    return L
+
+
+def profile_traffic(kernel: str, workload: str):
+    """dram bytes per launch from the committed ncu summary, if present."""
+    f = ROOT / "profiles" / f"{kernel}_{workload}.md"
+    if not f.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
+def measured_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return json.loads(f.read_text())
+        except ValueError:
+            return {}
+    return {}
+
+
+def cpu_baseline(dim, A, B, threads: int = 1):
+    """Oracle (reference algorithm) on this host: full pipeline as the C API
+    caller drives it.  Returns (pairs/s, seconds, stats, flops)."""
+    import oracle
+
+    t0 = time.perf_counter()
+    st = oracle.supermesh(dim, A, B, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return st.n_candidates / dt, dt, st
+
+
+def algorithmic_flops(dim, A, B):
+    """Algorithmic FP64 operations of the narrow phase (per-pair clipping and
+    measures plus per-element setup), counted by the oracle."""
+    import oracle
+
+    ip, ind = oracle.tree_finder(dim, A, B)
+    n = os.cpu_count() or 1
+    _, _, _, st = oracle.narrow(dim, A, B, ip, ind, nthreads=n, count_flops=True)
+    return st.flops, st
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from libsupermesh_b200 import meshes as M
+
+    dim, A, B = M.config_meshes(args.workload)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_baseline(dim, A, B, threads)
+    times, st = [], None
+    for _ in range(args.steps):
+        _, dt, st = cpu_baseline(dim, A, B, threads)
+        times.append(dt)
+    total = sum(times)
+    value = st.n_candidates * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "candidates": st.n_candidates},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
+                         "sample": "full workload per step: oracle quadtree/octree finder (1 thread) + "
+                                   "breadth-first clipping (OpenMP over A rows)"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "total_measure": st.total,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import libsupermesh_b200 as lsm
+    from libsupermesh_b200 import meshes as M
+
+    dim, A, B = M.config_meshes(args.workload)
+    dev = torch.device("cuda", local)
+    ctx = lsm.Context(local)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    probe = load_probe()
+    flush_buf = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def flush():
+        probe.lsm_probe_flush_l2(flush_buf.data_ptr(), L2_FLUSH_BYTES, sp)
+
+    tA = (torch.from_numpy(A[0]).to(dev), torch.from_numpy(A[1]).to(dev))
+    tB = (torch.from_numpy(B[0]).to(dev), torch.from_numpy(B[1]).to(dev))
+    em_dev = torch.zeros(len(A[1]), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    def step_device():
+        return ctx.supermesh(tA, tB, elem_measure=True, on_device=True, out=em_dev, stream=sp)[0]
+
+    # pinned host inputs for the end-to-end leg
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        return t.numpy()
+
+    hA = (pinned(A[0]), pinned(A[1]))
+    hB = (pinned(B[0]), pinned(B[1]))
+    em_host = pinned(np.zeros(len(A[1])))
+    h2d = A[0].nbytes + A[1].nbytes + B[0].nbytes + B[1].nbytes
+    d2h = em_host.nbytes + 32
+
+    def step_e2e():
+        return ctx.supermesh(hA, hB, elem_measure=True, on_device=False, out=em_host, stream=sp)[0]
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        st = None
+        for e0, e1 in evs:
+            flush()
+            e0.record(stream)
+            st = fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+        return ms, st
+
+    launches0 = lsm.kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_dev, st = timed(step_device, args.steps, args.warmup)
+    clock_rec = clocks.stop()
+    launches = lsm.kernel_launches() - launches0
+    per_step_launches = launches // (args.steps + args.warmup)
+    ms_dev = all_max(ms_dev, world)
+    n_cand = st.n_candidates
+    value = n_cand * args.steps * world / (ms_dev * 1e-3)
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "kernel_only": True}), flush=True)
+        return
+
+    ms_e2e, st_e2e = timed(step_e2e, args.steps, max(3, args.warmup // 2))
+    ms_e2e = all_max(ms_e2e, world)
+    e2e = n_cand * args.steps * world / (ms_e2e * 1e-3)
+    assert st_e2e.n_candidates == n_cand and st_e2e.total_measure == st.total_measure
+
+    # dominant kernel alone: the clipping launch over the same candidates
+    step_device()
+    ms_clip, _ = timed(lambda: ctx.clip_candidates(stream=sp), args.steps, 3)
+    clip_ms = ms_clip / args.steps
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "dim": dim, "elements_a": int(len(A[1])),
+                   "elements_b": int(len(B[1])), "candidates": n_cand,
+                   "intersecting": st.n_intersecting, "out_simplices": st.n_out_simplices,
+                   "l2": "flushed before every timed step (256 MiB write, outside the events)",
+                   "parallelism": f"replicas x{world}"},
+        "total_measure": st.total_measure,
+        "measure_err_vs_domain": abs(st.total_measure - 1.0),
+        "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": ms_e2e / args.steps},
+        "gpu_launches": per_step_launches * args.steps,
+        "clocks": clock_rec,
+    }
+    if rank == 0:
+        peak_rate = probe.lsm_probe_fp64_rate(0, 5)
+        fma_rate = probe.lsm_probe_fp64_rate(1, 5)
+        flops = None
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            flops, _ = algorithmic_flops(dim, A, B)
+            v, dt, st_cpu = cpu_baseline(dim, A, B, 1)
+            cpu = {"value": v, "unit": "pairs/s", "cores": 1, "kind": "port",
+                   "sample": f"full workload ({st_cpu.n_candidates} candidates), oracle quadtree/octree "
+                             f"finder + breadth-first clipping, 1 thread, {dt:.2f} s"}
+            assert st_cpu.n_candidates == n_cand
+            line["cpu_total_measure"] = st_cpu.total
+        achieved = flops / (clip_ms * 1e-3) / 1e12 if flops else None
+        peak = peak_rate / 1e12 if peak_rate > 0 else None
+        line["roofline"] = {
+            "kernel": "k_clip_tets" if dim == 3 else "k_clip_tris",
+            "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if (achieved and peak) else None,
+            "traffic": profile_traffic("k_clip_tets" if dim == 3 else "k_clip_tris", args.workload),
+            "launch_ms": clip_ms,
+            "flops_per_launch": flops,
+            "peak_source": "measured in-run: DADD+DMUL issue rate, 1 op each (the clipper is FMA-free); "
+                           f"DFMA rate for context {fma_rate / 1e12:.1f} TFLOP/s",
+        }
+        pk = measured_peaks()
+        line["roofline"]["hbm_peak_gbs"] = pk.get("hbm_gbs")
+        line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

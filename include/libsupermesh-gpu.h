@@ -1,0 +1,141 @@
+/*
+ * libsupermesh GPU extension: batched and device-resident entry points of
+ * the B200 supermesh library, declared beside the drop-in C API of
+ * libsupermesh-c.h.  None of these has a single counterpart in the
+ * reference; each comment names the reference routines whose work it
+ * performs (paths within firedrakeproject/libsupermesh).
+ *
+ * Conventions
+ *   - meshes: positions [nnodes][dim] float64, enlist [nelements][loc]
+ *     0-based (int32 or int64), row-major -- the layout of
+ *     libsupermesh_tree_intersection_finder_set_input.
+ *   - A is the target (query) mesh whose elements are the CSR rows; B is the
+ *     source mesh the search structure is built on.
+ *   - on_device = 0: every pointer of the call is host memory (pinned for
+ *     asynchronous copies); on_device = 1: every pointer is device memory of
+ *     the context's GPU.  Outputs follow the inputs' memory space.
+ *   - every function returns an lsm_status; the context keeps the message
+ *     of the last failure (libsupermesh_gpu_last_error).
+ *   - stream: a cudaStream_t (NULL = the context's own stream).  Calls are
+ *     synchronous with respect to the host unless stated otherwise.
+ */
+#ifndef LIBSUPERMESH_GPU_H
+#define LIBSUPERMESH_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  LSM_SUCCESS = 0,
+  LSM_ERROR_INVALID_ARGUMENT = 1,
+  LSM_ERROR_OUT_OF_MEMORY = 2,
+  LSM_ERROR_CAPACITY = 3,
+  LSM_ERROR_TIMEOUT = 4,
+  LSM_ERROR_CUDA = 5,
+  LSM_ERROR_STATE = 6
+} lsm_status;
+
+typedef struct lsm_gpu_context lsm_gpu_context;
+
+typedef struct {
+  int dim;               /* 2 or 3 */
+  int loc;               /* dim + 1 (simplices) */
+  int64_t nnodes;
+  int64_t nelements;
+  const double *positions; /* [nnodes][dim] */
+  const void *enlist;      /* [nelements][loc], 0-based */
+  int index_bytes;         /* 4 (int32) or 8 (int64) */
+} lsm_gpu_mesh;
+
+typedef struct {
+  int64_t n_candidates;    /* strict-AABB candidate pairs (tree finder set) */
+  int64_t n_intersecting;  /* pairs with at least one output simplex */
+  int64_t n_out_simplices; /* supermesh elements */
+  double total_measure;    /* compensated sum of all supermesh measures */
+  double total_measure_err;/* its compensation term */
+} lsm_gpu_stats;
+
+/* Context on one CUDA device.  Owns a stream and grow-only device buffers
+ * that are reused by later calls. */
+int libsupermesh_gpu_context_create(int device, lsm_gpu_context **ctx);
+int libsupermesh_gpu_context_destroy(lsm_gpu_context *ctx);
+const char *libsupermesh_gpu_status_string(int status);
+const char *libsupermesh_gpu_last_error(const lsm_gpu_context *ctx);
+/* Bytes of device memory currently held by the context. */
+int64_t libsupermesh_gpu_context_bytes(const lsm_gpu_context *ctx);
+/* Kernel launches issued by this library in this process so far. */
+int64_t libsupermesh_gpu_kernel_launches(void);
+
+/* Candidate search only (tree finder): the work of
+ * tree_intersection_finder_set_input_c (C_bindings.F90:346-366) on the GPU.
+ * Results stay in the context; read them with
+ * libsupermesh_gpu_get_candidates. */
+int libsupermesh_gpu_find_candidates(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
+                                     const lsm_gpu_mesh *b, int on_device,
+                                     int64_t *n_candidates, void *stream);
+
+/* Copy the last candidate CSR out: ind_ptr[nelements_a + 1] (0-based, starts
+ * at 0) and indices[n_candidates] (0-based B elements; within a row in
+ * LBVH traversal order).  on_device selects the destination memory. */
+int libsupermesh_gpu_get_candidates(lsm_gpu_context *ctx, int64_t *ind_ptr,
+                                    int64_t *indices, int on_device, void *stream);
+
+/* Whole supermesh of one mesh pair: candidate search, intersect every
+ * candidate (intersect_tris_real / intersect_tets_real semantics), and sum
+ * the libsupermesh_triangle_area / tetrahedron_volume of every output
+ * simplex.  elem_measure_a (optional, [nelements_a]) receives per A element
+ * the supermesh measure inside it; stats (optional) the totals. */
+int libsupermesh_gpu_supermesh(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
+                               const lsm_gpu_mesh *b, int on_device,
+                               double *elem_measure_a, lsm_gpu_stats *stats,
+                               void *stream);
+
+/* Narrow phase alone: intersect and measure every candidate of the last
+ * libsupermesh_gpu_find_candidates / libsupermesh_gpu_supermesh call on
+ * this context (simplex meshes), as libsupermesh_gpu_supermesh does after
+ * its search.  Lets callers time or repeat the clipping without the
+ * search. */
+int libsupermesh_gpu_clip_candidates(lsm_gpu_context *ctx, lsm_gpu_stats *stats, void *stream);
+
+/* Per-pair results of the last libsupermesh_gpu_supermesh call, in CSR
+ * order: measure[n_candidates] and n_out[n_candidates]. */
+int libsupermesh_gpu_get_pair_results(lsm_gpu_context *ctx, double *measure,
+                                      int32_t *n_out, int on_device, void *stream);
+
+/* Batched form of the per-pair C API.  tri: a, b [n][3][2]; tet: a, b
+ * [n][4][3].  measure[n] = sum of output simplex measures, n_out[n] = number
+ * of output simplices; elems (optional) [n][22][3][2] or [n][81][4][3] in
+ * the reference's output order. */
+int libsupermesh_gpu_intersect_pairs(lsm_gpu_context *ctx, int dim, int64_t n,
+                                     const double *a, const double *b,
+                                     double *measure, int32_t *n_out,
+                                     double *elems, int on_device, void *stream);
+
+/* P1-P1 mixed mass matrix over the supermesh of A and B: per candidate pair
+ * the local block M[i][j] = sum_c |c| sum_q w_q phi_i^A(x_q) phi_j^B(x_q)
+ * (blocks, optional, [n_candidates][loc][loc], device memory only when
+ * on_device), and integral = u_a^T M v_b (u_a [nnodes_a], v_b [nnodes_b],
+ * optional).  Quadrature as test_parallel_p1_inner_product_{2d,3d}.F90. */
+int libsupermesh_gpu_p1_mass(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
+                             const lsm_gpu_mesh *b, const double *u_a,
+                             const double *v_b, double *blocks, double *integral,
+                             int on_device, void *stream);
+
+/* Many independent mesh pairs in one call.  totals[npairs] receives each
+ * pair's supermesh measure
+ * and n_candidates[npairs] / n_intersecting[npairs] (optional) its counts.
+ * All meshes live in the memory space given by on_device. */
+int libsupermesh_gpu_supermesh_batched(lsm_gpu_context *ctx, int npairs,
+                                       const lsm_gpu_mesh *a, const lsm_gpu_mesh *b,
+                                       int on_device, double *totals,
+                                       int64_t *n_candidates, int64_t *n_intersecting,
+                                       void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,341 @@
+"""B200-native supermesh library: Python binding of lib/libsupermesh.so.
+
+The shared library exports the drop-in C API of libsupermesh
+(include/libsupermesh-c.h) and the GPU extension (include/libsupermesh-gpu.h).
+``get_library`` / ``get_include`` / ``load`` mirror the loader of the
+reference's Python package (src/supermesh/__init__.py:8-22 upstream).  The
+classes below are thin ctypes wrappers over those C entry points; all work
+runs on the GPU, and nothing here falls back to the CPU: if the CUDA library
+is missing, ``load`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+__all__ = [
+    "get_library", "get_include", "load", "Context", "LsmError", "Stats",
+    "tree_intersection_finder", "intersect_tris_real", "intersect_tets_real",
+    "triangle_area", "tetrahedron_volume", "TRI_BUF_SIZE", "TET_BUF_SIZE",
+]
+
+_PKG = Path(__file__).resolve().parent
+_LIB = _PKG / "lib" / "libsupermesh.so"
+TRI_BUF_SIZE = 22
+TET_BUF_SIZE = 81
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_lp = ctypes.POINTER(ctypes.c_long)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def get_library() -> str:
+    """Path of the shared library."""
+    return str(_LIB)
+
+
+def get_include() -> str:
+    """Directory holding libsupermesh-c.h, libsupermesh.h, libsupermesh-gpu.h."""
+    return str(_PKG.parent / "include")
+
+
+class LsmError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"libsupermesh GPU call failed ({status}): {message}")
+        self.status = status
+
+
+class Mesh(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int),
+        ("loc", ctypes.c_int),
+        ("nnodes", ctypes.c_int64),
+        ("nelements", ctypes.c_int64),
+        ("positions", ctypes.c_void_p),
+        ("enlist", ctypes.c_void_p),
+        ("index_bytes", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("n_candidates", ctypes.c_int64),
+        ("n_intersecting", ctypes.c_int64),
+        ("n_out_simplices", ctypes.c_int64),
+        ("total_measure", ctypes.c_double),
+        ("total_measure_err", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB.exists():
+        raise RuntimeError(
+            f"{_LIB} is missing: build it with `python libsupermesh_b200/build.py` "
+            "(there is no CPU implementation to fall back to)")
+    L = ctypes.CDLL(str(_LIB))
+    vp = ctypes.c_void_p
+    L.libsupermesh_gpu_context_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+    L.libsupermesh_gpu_context_destroy.argtypes = [vp]
+    L.libsupermesh_gpu_status_string.restype = ctypes.c_char_p
+    L.libsupermesh_gpu_status_string.argtypes = [ctypes.c_int]
+    L.libsupermesh_gpu_last_error.restype = ctypes.c_char_p
+    L.libsupermesh_gpu_last_error.argtypes = [vp]
+    L.libsupermesh_gpu_context_bytes.restype = ctypes.c_int64
+    L.libsupermesh_gpu_context_bytes.argtypes = [vp]
+    L.libsupermesh_gpu_kernel_launches.restype = ctypes.c_int64
+    L.libsupermesh_gpu_kernel_launches.argtypes = []
+    mp = ctypes.POINTER(Mesh)
+    L.libsupermesh_gpu_find_candidates.argtypes = [vp, mp, mp, ctypes.c_int, _i64p, vp]
+    L.libsupermesh_gpu_get_candidates.argtypes = [vp, vp, vp, ctypes.c_int, vp]
+    L.libsupermesh_gpu_supermesh.argtypes = [vp, mp, mp, ctypes.c_int, vp, ctypes.POINTER(Stats), vp]
+    L.libsupermesh_gpu_get_pair_results.argtypes = [vp, vp, vp, ctypes.c_int, vp]
+    L.libsupermesh_gpu_clip_candidates.argtypes = [vp, ctypes.POINTER(Stats), vp]
+    L.libsupermesh_gpu_intersect_pairs.argtypes = [vp, ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp, vp,
+                                                   ctypes.c_int, vp]
+    L.libsupermesh_gpu_p1_mass.argtypes = [vp, mp, mp, vp, vp, vp, _dp, ctypes.c_int, vp]
+    L.libsupermesh_gpu_supermesh_batched.argtypes = [vp, ctypes.c_int, mp, mp, ctypes.c_int, vp, vp, vp, vp]
+    for name in ("libsupermesh_gpu_context_create", "libsupermesh_gpu_context_destroy",
+                 "libsupermesh_gpu_find_candidates", "libsupermesh_gpu_get_candidates",
+                 "libsupermesh_gpu_supermesh", "libsupermesh_gpu_get_pair_results",
+                 "libsupermesh_gpu_clip_candidates",
+                 "libsupermesh_gpu_intersect_pairs", "libsupermesh_gpu_p1_mass",
+                 "libsupermesh_gpu_supermesh_batched"):
+        getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _ptr(a) -> int | None:
+    """Address of a numpy array or of anything exposing data_ptr() (torch)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def _mesh(pos, en, on_device: bool) -> Mesh:
+    if on_device:
+        nnodes, dim = pos.shape
+        nel, loc = en.shape
+        ib = en.element_size()
+        return Mesh(dim, loc, nnodes, nel, _ptr(pos), _ptr(en), ib)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    if en.dtype not in (np.int32, np.int64):
+        en = en.astype(np.int64)
+    en = np.ascontiguousarray(en)
+    m = Mesh(pos.shape[1], en.shape[1], pos.shape[0], en.shape[0], pos.ctypes.data, en.ctypes.data,
+             en.dtype.itemsize)
+    m._keep = (pos, en)  # keep the arrays alive with the struct
+    return m
+
+
+class Context:
+    """A GPU context (one device, one stream, reusable device buffers)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        self._h = ctypes.c_void_p()
+        st = self.lib.libsupermesh_gpu_context_create(device, ctypes.byref(self._h))
+        if st != 0:
+            raise LsmError(st, self.lib.libsupermesh_gpu_status_string(st).decode())
+
+    def close(self):
+        if self._h:
+            self.lib.libsupermesh_gpu_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = self.lib.libsupermesh_gpu_last_error(self._h).decode()
+            raise LsmError(st, msg)
+
+    @property
+    def device_bytes(self) -> int:
+        return self.lib.libsupermesh_gpu_context_bytes(self._h)
+
+    # -- candidate search -------------------------------------------------
+    def find_candidates(self, mesh_a, mesh_b, on_device: bool = False, stream: int | None = None):
+        ma, mb = _mesh(*mesh_a, on_device), _mesh(*mesh_b, on_device)
+        n = ctypes.c_int64(0)
+        self._check(self.lib.libsupermesh_gpu_find_candidates(self._h, ctypes.byref(ma), ctypes.byref(mb),
+                                                              int(on_device), ctypes.byref(n), stream))
+        return n.value
+
+    def get_candidates(self, nel_a: int, n: int):
+        indptr = np.zeros(nel_a + 1, dtype=np.int64)
+        indices = np.zeros(max(n, 1), dtype=np.int64)
+        self._check(self.lib.libsupermesh_gpu_get_candidates(self._h, indptr.ctypes.data, indices.ctypes.data,
+                                                             0, None))
+        return indptr, indices[:n]
+
+    # -- whole supermesh --------------------------------------------------
+    def supermesh(self, mesh_a, mesh_b, elem_measure: bool = False, on_device: bool = False,
+                  out=None, stream: int | None = None):
+        """Returns (Stats, elem_measure or None)."""
+        ma, mb = _mesh(*mesh_a, on_device), _mesh(*mesh_b, on_device)
+        em = None
+        if elem_measure:
+            em = out if out is not None else np.zeros(ma.nelements, dtype=np.float64)
+        st = Stats()
+        self._check(self.lib.libsupermesh_gpu_supermesh(self._h, ctypes.byref(ma), ctypes.byref(mb),
+                                                        int(on_device), _ptr(em), ctypes.byref(st), stream))
+        return st, em
+
+    def clip_candidates(self, stream: int | None = None) -> Stats:
+        """Re-run the narrow phase over the last candidate set."""
+        st = Stats()
+        self._check(self.lib.libsupermesh_gpu_clip_candidates(self._h, ctypes.byref(st), stream))
+        return st
+
+    def pair_results(self, n: int):
+        m = np.zeros(max(n, 1), dtype=np.float64)
+        k = np.zeros(max(n, 1), dtype=np.int32)
+        self._check(self.lib.libsupermesh_gpu_get_pair_results(self._h, m.ctypes.data, k.ctypes.data, 0, None))
+        return m[:n], k[:n]
+
+    def intersect_pairs(self, dim: int, a, b, want_elems: bool = False):
+        per = 6 if dim == 2 else 12
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, per)
+        b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, per)
+        n = a.shape[0]
+        m = np.zeros(max(n, 1))
+        k = np.zeros(max(n, 1), dtype=np.int32)
+        e = None
+        if want_elems:
+            e = np.zeros((max(n, 1), 22, 3, 2) if dim == 2 else (max(n, 1), 81, 4, 3))
+        self._check(self.lib.libsupermesh_gpu_intersect_pairs(self._h, dim, n, a.ctypes.data, b.ctypes.data,
+                                                              m.ctypes.data, k.ctypes.data, _ptr(e), 0, None))
+        return m[:n], k[:n], (e[:n] if e is not None else None)
+
+    def p1_mass(self, mesh_a, mesh_b, u_a=None, v_b=None, want_blocks: bool = False):
+        """Returns (u^T M v or None, blocks or None) for host meshes."""
+        ma, mb = _mesh(*mesh_a, False), _mesh(*mesh_b, False)
+        if ma.index_bytes != mb.index_bytes:
+            raise ValueError("A and B must use the same index width")
+        u = np.ascontiguousarray(u_a, dtype=np.float64) if u_a is not None else None
+        v = np.ascontiguousarray(v_b, dtype=np.float64) if v_b is not None else None
+        blocks, n = None, 0
+        if want_blocks:
+            n = self.find_candidates(mesh_a, mesh_b)
+            loc = ma.dim + 1
+            blocks = np.zeros((max(n, 1), loc, loc))
+        integral = ctypes.c_double(0.0)
+        self._check(self.lib.libsupermesh_gpu_p1_mass(self._h, ctypes.byref(ma), ctypes.byref(mb), _ptr(u),
+                                                      _ptr(v), _ptr(blocks), ctypes.byref(integral), 0, None))
+        return (integral.value if u is not None else None), (blocks[:n] if blocks is not None else None)
+
+    def supermesh_batched(self, pairs, on_device: bool = False):
+        """pairs: list of (mesh_a, mesh_b).  Returns (totals, n_candidates,
+        n_intersecting) as numpy arrays."""
+        n = len(pairs)
+        A = (Mesh * max(n, 1))()
+        B = (Mesh * max(n, 1))()
+        keep = []
+        for i, (ma, mb) in enumerate(pairs):
+            a, b = _mesh(*ma, on_device), _mesh(*mb, on_device)
+            keep.append((a, b))
+            A[i], B[i] = a, b
+        totals = np.zeros(max(n, 1))
+        nc = np.zeros(max(n, 1), dtype=np.int64)
+        ni = np.zeros(max(n, 1), dtype=np.int64)
+        self._check(self.lib.libsupermesh_gpu_supermesh_batched(self._h, n, A, B, int(on_device), totals.ctypes.data,
+                                                                nc.ctypes.data, ni.ctypes.data, None))
+        return totals[:n], nc[:n], ni[:n]
+
+
+def kernel_launches() -> int:
+    """Kernel launches this library has issued in this process."""
+    return load().libsupermesh_gpu_kernel_launches()
+
+
+# -- drop-in C API (libsupermesh-c.h) --------------------------------------
+
+def _long(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def tree_intersection_finder(pos_a, en_a, pos_b, en_b):
+    """set_input -> query_output -> get_output through the C API."""
+    L = load()
+    pa = np.ascontiguousarray(pos_a, dtype=np.float64)
+    pb = np.ascontiguousarray(pos_b, dtype=np.float64)
+    ea, eb = _long(en_a), _long(en_b)
+    c_long, c_int = ctypes.c_long, ctypes.c_int
+    args = [c_long(pa.shape[0]), c_int(pa.shape[1]), c_long(ea.shape[0]), c_int(ea.shape[1]),
+            c_long(pb.shape[0]), c_int(pb.shape[1]), c_long(eb.shape[0]), c_int(eb.shape[1])]
+    L.libsupermesh_tree_intersection_finder_set_input(
+        *[ctypes.byref(x) for x in args], pa.ctypes.data_as(_dp), ea.ctypes.data_as(_lp),
+        pb.ctypes.data_as(_dp), eb.ctypes.data_as(_lp))
+    n = c_long(0)
+    L.libsupermesh_tree_intersection_finder_query_output(ctypes.byref(n))
+    indices = np.zeros(max(n.value, 1), dtype=np.int64)
+    indptr = np.zeros(ea.shape[0] + 1, dtype=np.int64)
+    nel = c_long(ea.shape[0])
+    L.libsupermesh_tree_intersection_finder_get_output(ctypes.byref(nel), ctypes.byref(n),
+                                                       indices.ctypes.data_as(_lp), indptr.ctypes.data_as(_lp))
+    return indptr, indices[: n.value]
+
+
+def intersect_tris_real(tri_a, tri_b):
+    L = load()
+    a = np.ascontiguousarray(tri_a, dtype=np.float64).reshape(3, 2)
+    b = np.ascontiguousarray(tri_b, dtype=np.float64).reshape(3, 2)
+    out = np.zeros((TRI_BUF_SIZE, 3, 2))
+    n = ctypes.c_int(0)
+    L.libsupermesh_intersect_tris_real(a.ctypes.data_as(_dp), b.ctypes.data_as(_dp), out.ctypes.data_as(_dp),
+                                       ctypes.byref(n))
+    return out[: n.value].copy()
+
+
+def intersect_tets_real(tet_a, tet_b):
+    L = load()
+    a = np.ascontiguousarray(tet_a, dtype=np.float64).reshape(4, 3)
+    b = np.ascontiguousarray(tet_b, dtype=np.float64).reshape(4, 3)
+    out = np.zeros((TET_BUF_SIZE, 4, 3))
+    n = ctypes.c_int(0)
+    L.libsupermesh_intersect_tets_real(a.ctypes.data_as(_dp), b.ctypes.data_as(_dp), out.ctypes.data_as(_dp),
+                                       ctypes.byref(n))
+    return out[: n.value].copy()
+
+
+def triangle_area(tri) -> float:
+    L = load()
+    t = np.ascontiguousarray(tri, dtype=np.float64).reshape(6)
+    r = ctypes.c_double(0.0)
+    L.libsupermesh_triangle_area(t.ctypes.data_as(_dp), ctypes.byref(r))
+    return r.value
+
+
+def tetrahedron_volume(tet) -> float:
+    L = load()
+    t = np.ascontiguousarray(tet, dtype=np.float64).reshape(12)
+    r = ctypes.c_double(0.0)
+    L.libsupermesh_tetrahedron_volume(t.ctypes.data_as(_dp), ctypes.byref(r))
+    return r.value

@@ -1,0 +1,745 @@
+// C-ABI of the B200 supermesh library: the drop-in entries of
+// include/libsupermesh-c.h and the GPU extension of include/libsupermesh-gpu.h.
+//
+// Pipeline per mesh pair (all on one stream):
+//   prep A, prep B            gather coords, boxes, tolerances, B clip setup
+//   root box, Morton, sort    LBVH leaves in Morton order
+//   LBVH build + refit
+//   query (count) -> scan -> [host reads n_candidates] -> query (fill)
+//   clip (+ overflow re-run) -> finalize (compensated totals, counts)
+// The only host synchronisation inside the pipeline is the read of the
+// candidate count, needed to size the pair arrays.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/libsupermesh-c.h"
+#include "../../include/libsupermesh-gpu.h"
+#include "lsm_kernels.h"
+
+namespace {
+
+// ------------------------------------------------------------------ buffers
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  int64_t bytes = 0;
+
+  // mesh A (query side)
+  DevBuf a_pos, a_en, a_coords, a_box64, a_tol;
+  // mesh B (tree side)
+  DevBuf b_pos, b_en, b_coords, b_box64, b_box32, b_setup;
+  // tree
+  DevBuf keys, vals, keys_tmp, vals_tmp, hist, root_partial, rootbox, bvh_lo, bvh_hi, bvh_work;
+  // candidates
+  DevBuf counts, offsets, scan_tmp, pair_a, pair_b, i64_tmp;
+  // narrow phase
+  DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals;
+  // explicit pairs / p1 / batched
+  DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
+  // pinned host scalars
+  void* host_scalars = nullptr;
+
+  // state of the last candidate search
+  int dim = 0;
+  int loc_a = 0, loc_b = 0;
+  int64_t nel_a = 0, nel_b = 0;
+  int64_t ncand = -1;
+  bool have_pairs = false;
+  bool simplex_prep = false;  // A coords/tol and B clip setup are current
+};
+
+struct Fail {
+  int status;
+};
+
+void set_error(Ctx* c, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  c->last_error = buf;
+}
+
+#define CU(call)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      set_error(c, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                __LINE__);                                                           \
+      throw Fail{e_ == cudaErrorMemoryAllocation ? LSM_ERROR_OUT_OF_MEMORY           \
+                                                 : LSM_ERROR_CUDA};                  \
+    }                                                                                \
+  } while (0)
+
+#define REQUIRE(cond, ...)         \
+  do {                             \
+    if (!(cond)) {                 \
+      set_error(c, __VA_ARGS__);   \
+      throw Fail{LSM_ERROR_INVALID_ARGUMENT}; \
+    }                              \
+  } while (0)
+
+template <class T>
+T* ensure(Ctx* c, DevBuf& b, int64_t count) {
+  size_t need = sizeof(T) * (size_t)(count > 0 ? count : 1);
+  need = (need + 255) & ~(size_t)255;
+  if (b.cap < need) {
+    if (b.p) {
+      cudaFree(b.p);
+      c->bytes -= (int64_t)b.cap;
+      b.p = nullptr;
+      b.cap = 0;
+    }
+    size_t want = need + need / 4;  // growth headroom
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      want = need;
+      e = cudaMalloc(&b.p, want);
+    }
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      set_error(c, "cudaMalloc of %zu bytes failed: %s", want, cudaGetErrorString(e));
+      throw Fail{LSM_ERROR_OUT_OF_MEMORY};
+    }
+    b.cap = want;
+    c->bytes += (int64_t)want;
+  }
+  return static_cast<T*>(b.p);
+}
+
+void free_buf(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int init_ctx(int device, Ctx* c) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    (void)cudaGetLastError();
+    return LSM_ERROR_CUDA;
+  }
+  if (device < 0 || device >= n) return LSM_ERROR_INVALID_ARGUMENT;
+  DeviceGuard g(device);
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMallocHost(&c->host_scalars, 4096) != cudaSuccess || lsm::init_device_attributes() != cudaSuccess) {
+    (void)cudaGetLastError();
+    return LSM_ERROR_CUDA;
+  }
+  return LSM_SUCCESS;
+}
+
+void fini_ctx(Ctx* c) {
+  DeviceGuard g(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  DevBuf* all[] = {&c->a_pos, &c->a_en, &c->a_coords, &c->a_box64, &c->a_tol, &c->b_pos, &c->b_en,
+                   &c->b_coords, &c->b_box64, &c->b_box32, &c->b_setup, &c->keys, &c->vals,
+                   &c->keys_tmp, &c->vals_tmp, &c->hist, &c->root_partial, &c->rootbox, &c->bvh_lo,
+                   &c->bvh_hi, &c->bvh_work, &c->counts, &c->offsets, &c->scan_tmp, &c->pair_a,
+                   &c->pair_b, &c->i64_tmp, &c->pair_measure, &c->pair_nout, &c->partials,
+                   &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->x_a, &c->x_b, &c->x_measure,
+                   &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks};
+  for (DevBuf* b : all) free_buf(*b);
+  if (c->host_scalars) cudaFreeHost(c->host_scalars);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->host_scalars = nullptr;
+  c->stream = nullptr;
+}
+
+cudaStream_t pick(Ctx* c, void* s) { return s ? static_cast<cudaStream_t>(s) : c->stream; }
+
+// ------------------------------------------------------------- mesh upload
+struct MeshDev {
+  int dim, loc, idx_bytes;
+  int64_t nnodes, nel;
+  const double* pos;
+  const void* en;
+};
+
+void check_mesh(Ctx* c, const lsm_gpu_mesh* m, const char* name, bool simplex) {
+  REQUIRE(m != nullptr, "mesh %s is NULL", name);
+  REQUIRE(m->dim == 2 || m->dim == 3, "Invalid dimension %d for mesh %s", m->dim, name);
+  if (simplex)
+    REQUIRE(m->loc == m->dim + 1, "mesh %s: loc %d is not a simplex of dimension %d", name, m->loc, m->dim);
+  else
+    REQUIRE(m->loc == m->dim + 1 || m->loc == (1 << m->dim), "mesh %s: unsupported loc %d", name, m->loc);
+  REQUIRE(m->index_bytes == 4 || m->index_bytes == 8, "mesh %s: index_bytes must be 4 or 8", name);
+  REQUIRE(m->nnodes >= 0 && m->nelements >= 0, "mesh %s: negative size", name);
+  REQUIRE(m->nelements < (int64_t)0x7fffffff, "mesh %s: more than 2^31-1 elements", name);
+  REQUIRE(m->nelements == 0 || (m->positions && m->enlist), "mesh %s: NULL arrays", name);
+  REQUIRE(m->nelements == 0 || m->nnodes > 0, "mesh %s: No nodes", name);
+}
+
+MeshDev upload(Ctx* c, const lsm_gpu_mesh* m, int on_device, DevBuf& pos, DevBuf& en, cudaStream_t s) {
+  MeshDev d{m->dim, m->loc, m->index_bytes, m->nnodes, m->nelements, m->positions, m->enlist};
+  if (!on_device && m->nelements > 0) {
+    double* p = ensure<double>(c, pos, m->nnodes * m->dim);
+    CU(cudaMemcpyAsync(p, m->positions, sizeof(double) * m->nnodes * m->dim, cudaMemcpyHostToDevice, s));
+    char* e = ensure<char>(c, en, m->nelements * m->loc * m->index_bytes);
+    CU(cudaMemcpyAsync(e, m->enlist, (size_t)m->nelements * m->loc * m->index_bytes, cudaMemcpyHostToDevice, s));
+    d.pos = p;
+    d.en = e;
+  }
+  return d;
+}
+
+int* bad_flag(Ctx* c) { return ensure<int>(c, c->misc, 64); }
+
+// prep of the query mesh A: coords (simplices only), box64, tol
+void prep_a(Ctx* c, const MeshDev& a, bool simplex, cudaStream_t s) {
+  double* coords = simplex ? ensure<double>(c, c->a_coords, a.nel * a.loc * a.dim) : nullptr;
+  double* box = ensure<double>(c, c->a_box64, a.nel * 2 * a.dim);
+  double* tol = simplex ? ensure<double>(c, c->a_tol, a.nel) : nullptr;
+  CU(lsm::launch_prep(a.dim, a.loc, a.nel, a.pos, a.en, a.idx_bytes, coords, box, nullptr, tol, nullptr,
+                      bad_flag(c), a.nnodes, s));
+}
+
+void prep_b(Ctx* c, const MeshDev& b, bool simplex, bool want_coords, cudaStream_t s) {
+  double* coords = want_coords ? ensure<double>(c, c->b_coords, b.nel * b.loc * b.dim) : nullptr;
+  double* box = ensure<double>(c, c->b_box64, b.nel * 2 * b.dim);
+  float* box32 = ensure<float>(c, c->b_box32, b.nel * 8);
+  double* setup = nullptr;
+  if (simplex) setup = ensure<double>(c, c->b_setup, b.nel * (b.dim == 2 ? lsm::kSetup2 : lsm::kSetup3));
+  CU(lsm::launch_prep(b.dim, b.loc, b.nel, b.pos, b.en, b.idx_bytes, coords, box, box32, nullptr, setup,
+                      bad_flag(c), b.nnodes, s));
+}
+
+lsm::BVH build_tree(Ctx* c, const MeshDev& b, cudaStream_t s) {
+  const int64_t n = b.nel;
+  lsm::BVH bvh;
+  bvh.n = (int)n;
+  if (n == 0) return bvh;
+  const int dim = b.dim;
+  uint32_t* keys = ensure<uint32_t>(c, c->keys, n);
+  int32_t* vals = ensure<int32_t>(c, c->vals, n);
+  uint32_t* kt = ensure<uint32_t>(c, c->keys_tmp, n);
+  int32_t* vt = ensure<int32_t>(c, c->vals_tmp, n);
+  uint32_t* hist = ensure<uint32_t>(c, c->hist, lsm::radix_hist_entries(n));
+  const int pcap = 4096;
+  double* part = ensure<double>(c, c->root_partial, (int64_t)pcap * 2 * dim);
+  double* root = ensure<double>(c, c->rootbox, 2 * dim);
+  CU(lsm::launch_root_box(dim, n, static_cast<double*>(c->b_box64.p), part, pcap, root, s));
+  CU(lsm::launch_morton(dim, n, static_cast<double*>(c->b_box64.p), root, keys, vals, s));
+  CU(lsm::radix_sort_pairs(n, dim == 2 ? 32 : 30, keys, vals, kt, vt, hist, s));
+  bvh.lo_left = ensure<float4>(c, c->bvh_lo, 2 * n - 1);
+  bvh.hi_esc = ensure<float4>(c, c->bvh_hi, 2 * n - 1);
+  int* work = ensure<int>(c, c->bvh_work, 8 * n);
+  CU(lsm::launch_bvh_build(dim, (int)n, keys, vals, static_cast<float*>(c->b_box32.p), bvh, work, s));
+  return bvh;
+}
+
+// Broad phase: candidates as CSR (offsets) + pair arrays.
+void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int on_device, bool simplex,
+                     bool want_b_coords, cudaStream_t s) {
+  check_mesh(c, ma, "A", simplex);
+  check_mesh(c, mb, "B", simplex);
+  REQUIRE(ma->dim == mb->dim, "Invalid dimension: A is %dD, B is %dD", ma->dim, mb->dim);
+  c->have_pairs = false;
+  c->ncand = -1;
+  c->simplex_prep = false;
+  simplex = simplex || (ma->loc == ma->dim + 1 && mb->loc == mb->dim + 1);
+  MeshDev a = upload(c, ma, on_device, c->a_pos, c->a_en, s);
+  MeshDev b = upload(c, mb, on_device, c->b_pos, c->b_en, s);
+  CU(cudaMemsetAsync(bad_flag(c), 0, sizeof(int) * 64, s));
+  prep_a(c, a, simplex, s);
+  prep_b(c, b, simplex, want_b_coords, s);
+  const int64_t nel_a = a.nel;
+  int64_t* offsets = ensure<int64_t>(c, c->offsets, nel_a + 1);
+  int* counts = ensure<int>(c, c->counts, nel_a);
+  int64_t* stmp = ensure<int64_t>(c, c->scan_tmp, lsm::scan_tmp_entries(nel_a) + 1);
+  lsm::BVH bvh{};
+  if (b.nel > 0 && nel_a > 0) {
+    bvh = build_tree(c, b, s);
+    CU(lsm::launch_query(a.dim, false, nel_a, static_cast<double*>(c->a_box64.p), bvh,
+                         static_cast<double*>(c->b_box64.p), counts, nullptr, nullptr, nullptr, s));
+  } else if (nel_a > 0) {
+    CU(cudaMemsetAsync(counts, 0, sizeof(int) * nel_a, s));
+  }
+  CU(lsm::launch_scan(nel_a, counts, offsets, stmp, s));
+  int64_t* h = static_cast<int64_t*>(c->host_scalars) + 8;
+  CU(cudaMemcpyAsync(h, offsets + nel_a, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  int* hb = static_cast<int*>(c->host_scalars);
+  CU(cudaMemcpyAsync(hb, c->misc.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  REQUIRE(hb[0] == 0, "Invalid node index in an element list");
+  const int64_t nnz = *h;
+  int32_t* pa = ensure<int32_t>(c, c->pair_a, nnz);
+  int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);
+  if (nnz > 0)
+    CU(lsm::launch_query(a.dim, true, nel_a, static_cast<double*>(c->a_box64.p), bvh,
+                         static_cast<double*>(c->b_box64.p), nullptr, offsets, pa, pb, s));
+  c->dim = a.dim;
+  c->loc_a = a.loc;
+  c->loc_b = b.loc;
+  c->nel_a = a.nel;
+  c->nel_b = b.nel;
+  c->ncand = nnz;
+  c->simplex_prep = simplex;
+}
+
+// Narrow phase over the current candidates.  Leaves the merged totals in
+// c->totals (one lsm::Partial).
+void narrow(Ctx* c, cudaStream_t s) {
+  const int64_t nnz = c->ncand;
+  double* pm = ensure<double>(c, c->pair_measure, nnz);
+  int32_t* pn = ensure<int32_t>(c, c->pair_nout, nnz);
+  const int nblk = lsm::clip_grid_blocks(c->dim);
+  lsm::Partial* part = ensure<lsm::Partial>(c, c->partials, nblk + 1);
+  lsm::Partial* tot = ensure<lsm::Partial>(c, c->totals, 1);
+  int32_t* ovf = nullptr;
+  int* ovf_count = bad_flag(c) + 2;
+  if (c->dim == 2) {
+    ovf = ensure<int32_t>(c, c->ovf_list, nnz);
+    CU(cudaMemsetAsync(ovf_count, 0, sizeof(int), s));
+  }
+  CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+                      static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
+                      static_cast<double*>(c->b_setup.p), pm, pn, part, ovf, ovf_count, s));
+  int np = nblk;
+  if (c->dim == 2) {
+    CU(lsm::launch_clip_tris_wide(ovf, ovf_count, nnz, static_cast<int32_t*>(c->pair_a.p),
+                                  static_cast<int32_t*>(c->pair_b.p), static_cast<double*>(c->a_coords.p),
+                                  static_cast<double*>(c->a_tol.p), static_cast<double*>(c->b_setup.p), pm,
+                                  pn, part + nblk, s));
+    np = nblk + 1;
+  }
+  CU(lsm::launch_finalize(part, np, tot, s));
+  c->have_pairs = true;
+}
+
+void read_stats(Ctx* c, lsm_gpu_stats* st, cudaStream_t s) {
+  lsm::Partial* h = reinterpret_cast<lsm::Partial*>(static_cast<char*>(c->host_scalars) + 256);
+  CU(cudaMemcpyAsync(h, c->totals.p, sizeof(lsm::Partial), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (st) {
+    st->n_candidates = c->ncand;
+    st->total_measure = h->sum;
+    st->total_measure_err = h->err;
+    st->n_intersecting = (int64_t)h->n_int;
+    st->n_out_simplices = (int64_t)h->n_out;
+  }
+}
+
+template <class F>
+int guarded(Ctx* c, F&& f) {
+  if (!c) return LSM_ERROR_INVALID_ARGUMENT;
+  try {
+    DeviceGuard g(c->device);
+    f();
+    return LSM_SUCCESS;
+  } catch (const Fail& e) {
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    set_error(c, "host allocation failed");
+    return LSM_ERROR_OUT_OF_MEMORY;
+  }
+}
+
+// ------------------------------------------------------------- legacy API
+std::mutex g_mutex;
+Ctx* g_ctx = nullptr;
+bool g_tree_state = false;
+
+[[noreturn]] void legacy_abort(const char* what) {
+  fprintf(stderr, "libsupermesh (B200) error: %s\n", what);
+  fflush(stderr);
+  exit(1);
+}
+
+Ctx* legacy_ctx() {
+  if (!g_ctx) {
+    int dev = 0;
+    const char* env = getenv("LIBSUPERMESH_CUDA_DEVICE");
+    if (env && *env) dev = atoi(env);
+    g_ctx = new Ctx();
+    const int st = init_ctx(dev, g_ctx);
+    if (st != LSM_SUCCESS) legacy_abort("no usable CUDA device for libsupermesh");
+  }
+  return g_ctx;
+}
+
+void legacy_check(Ctx* c, int st) {
+  if (st != LSM_SUCCESS) legacy_abort(c->last_error.empty() ? "CUDA failure" : c->last_error.c_str());
+}
+
+void single_pair(int dim, const double* a, const double* b, double* out_elems, int* n_out) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  Ctx* c = legacy_ctx();
+  const int per = dim == 2 ? 6 : 12;
+  const int cap = dim == 2 ? 22 : 81;
+  legacy_check(c, guarded(c, [&] {
+    cudaStream_t s = c->stream;
+    double* da = ensure<double>(c, c->x_a, per);
+    double* db = ensure<double>(c, c->x_b, per);
+    int32_t* dn = ensure<int32_t>(c, c->x_nout, 1);
+    double* de = ensure<double>(c, c->x_elems, (int64_t)cap * per);
+    CU(cudaMemcpyAsync(da, a, sizeof(double) * per, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(db, b, sizeof(double) * per, cudaMemcpyHostToDevice, s));
+    CU(lsm::launch_pairs_explicit(dim, 1, da, db, nullptr, dn, de, s));
+    int32_t* hn = static_cast<int32_t*>(c->host_scalars);
+    CU(cudaMemcpyAsync(hn, dn, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    *n_out = hn[0];
+    if (hn[0] > 0) {
+      CU(cudaMemcpyAsync(out_elems, de, sizeof(double) * per * hn[0], cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+    }
+  }));
+}
+
+double single_measure(int dim, const double* e) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  Ctx* c = legacy_ctx();
+  const int per = dim == 2 ? 6 : 12;
+  double r = 0.0;
+  legacy_check(c, guarded(c, [&] {
+    cudaStream_t s = c->stream;
+    double* de = ensure<double>(c, c->x_a, per);
+    double* dm = ensure<double>(c, c->x_measure, 1);
+    CU(cudaMemcpyAsync(de, e, sizeof(double) * per, cudaMemcpyHostToDevice, s));
+    CU(lsm::launch_measure_explicit(dim, 1, de, dm, s));
+    double* h = static_cast<double*>(c->host_scalars);
+    CU(cudaMemcpyAsync(h, dm, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    r = h[0];
+  }));
+  return r;
+}
+
+}  // namespace
+
+struct lsm_gpu_context {
+  Ctx c;
+};
+
+static Ctx* C(lsm_gpu_context* p) { return p ? &p->c : nullptr; }
+
+extern "C" {
+
+// ---------------------------------------------------------------- legacy
+void libsupermesh_tree_intersection_finder_set_input(long* nnodes_a, int* dim_a, long* nelements_a, int* loc_a,
+                                                     long* nnodes_b, int* dim_b, long* nelements_b, int* loc_b,
+                                                     double* positions_a, long* enlist_a, double* positions_b,
+                                                     long* enlist_b) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  if (g_tree_state) legacy_abort("tree intersection finder: set_input called again before get_output");
+  if (*dim_a != 2 && *dim_a != 3) legacy_abort("Invalid dimension");
+  if (*dim_b != *dim_a) legacy_abort("Invalid dimension");
+  Ctx* c = legacy_ctx();
+  lsm_gpu_mesh a{*dim_a, *loc_a, (int64_t)*nnodes_a, (int64_t)*nelements_a, positions_a, enlist_a, (int)sizeof(long)};
+  lsm_gpu_mesh b{*dim_b, *loc_b, (int64_t)*nnodes_b, (int64_t)*nelements_b, positions_b, enlist_b, (int)sizeof(long)};
+  legacy_check(c, guarded(c, [&] { find_candidates(c, &a, &b, 0, false, false, c->stream); }));
+  g_tree_state = true;
+}
+
+void libsupermesh_tree_intersection_finder_query_output(long* nindices) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  if (!g_tree_state) legacy_abort("tree intersection finder: query_output without set_input");
+  *nindices = (long)g_ctx->ncand;
+}
+
+void libsupermesh_tree_intersection_finder_get_output(long* nelements, long* nindices, long* indices, long* ind_ptr) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  if (!g_tree_state) legacy_abort("tree intersection finder: get_output without set_input");
+  Ctx* c = g_ctx;
+  if (*nelements != (long)c->nel_a || *nindices != (long)c->ncand)
+    legacy_abort("tree intersection finder: get_output sizes do not match set_input");
+  legacy_check(c, guarded(c, [&] {
+    cudaStream_t s = c->stream;
+    const int64_t nnz = c->ncand;
+    if (nnz > 0) {
+      int64_t* tmp = ensure<int64_t>(c, c->i64_tmp, nnz);
+      CU(lsm::launch_i32_to_i64(nnz, static_cast<int32_t*>(c->pair_b.p), tmp, s));
+      CU(cudaMemcpyAsync(indices, tmp, sizeof(int64_t) * nnz, cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaMemcpyAsync(ind_ptr, c->offsets.p, sizeof(int64_t) * (c->nel_a + 1), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+  }));
+  g_tree_state = false;
+}
+
+void libsupermesh_intersect_tris_real(double* tri_a, double* tri_b, double* tris_c, int* n_tris_c) {
+  single_pair(2, tri_a, tri_b, tris_c, n_tris_c);
+}
+
+void libsupermesh_intersect_tets_real(double* tet_a, double* tet_b, double* tets_c, int* n_tets_c) {
+  single_pair(3, tet_a, tet_b, tets_c, n_tets_c);
+}
+
+void libsupermesh_triangle_area(double* tri, double* area) { *area = single_measure(2, tri); }
+
+void libsupermesh_tetrahedron_volume(double* tet, double* volume) { *volume = single_measure(3, tet); }
+
+void libsupermesh_sort_intersection_finder_set_input(long*, int*, long*, int*, long*, int*, long*, int*, double*,
+                                                     long*, double*, long*) {
+  legacy_abort("libsupermesh_sort_intersection_finder_set_input is not provided by the GPU build");
+}
+void libsupermesh_sort_intersection_finder_query_output(long*) {
+  legacy_abort("libsupermesh_sort_intersection_finder_query_output is not provided by the GPU build");
+}
+void libsupermesh_sort_intersection_finder_get_output(long*, long*, long*, long*) {
+  legacy_abort("libsupermesh_sort_intersection_finder_get_output is not provided by the GPU build");
+}
+void libsupermesh_interval_size(double*, double*) {
+  legacy_abort("libsupermesh_interval_size is not provided by the GPU build");
+}
+void libsupermesh_intersect_intervals(double*, double*, double*, int*) {
+  legacy_abort("libsupermesh_intersect_intervals is not provided by the GPU build");
+}
+void libsupermesh_intersect_tet_hex(double*, double*, double*, int*) {
+  legacy_abort("libsupermesh_intersect_tet_hex is not provided by the GPU build");
+}
+void libsupermesh_intersect_tri_quad(double*, double*, double*, int*) {
+  legacy_abort("libsupermesh_intersect_tri_quad is not provided by the GPU build");
+}
+
+// ------------------------------------------------------------- GPU API
+int libsupermesh_gpu_context_create(int device, lsm_gpu_context** ctx) {
+  if (!ctx) return LSM_ERROR_INVALID_ARGUMENT;
+  *ctx = nullptr;
+  lsm_gpu_context* p = new lsm_gpu_context();
+  const int st = init_ctx(device, &p->c);
+  if (st != LSM_SUCCESS) {
+    fini_ctx(&p->c);
+    delete p;
+    return st;
+  }
+  *ctx = p;
+  return LSM_SUCCESS;
+}
+
+int libsupermesh_gpu_context_destroy(lsm_gpu_context* ctx) {
+  if (!ctx) return LSM_ERROR_INVALID_ARGUMENT;
+  fini_ctx(&ctx->c);
+  delete ctx;
+  return LSM_SUCCESS;
+}
+
+const char* libsupermesh_gpu_status_string(int status) {
+  switch (status) {
+    case LSM_SUCCESS: return "success";
+    case LSM_ERROR_INVALID_ARGUMENT: return "invalid argument";
+    case LSM_ERROR_OUT_OF_MEMORY: return "out of device memory";
+    case LSM_ERROR_CAPACITY: return "output capacity exceeded";
+    case LSM_ERROR_TIMEOUT: return "timed out";
+    case LSM_ERROR_CUDA: return "CUDA error";
+    case LSM_ERROR_STATE: return "invalid call sequence";
+    default: return "unknown status";
+  }
+}
+
+const char* libsupermesh_gpu_last_error(const lsm_gpu_context* ctx) {
+  return ctx ? ctx->c.last_error.c_str() : "NULL context";
+}
+
+int64_t libsupermesh_gpu_context_bytes(const lsm_gpu_context* ctx) {
+  return ctx ? ctx->c.bytes : 0;
+}
+
+int64_t libsupermesh_gpu_kernel_launches(void) { return (int64_t)lsm::launches(); }
+
+int libsupermesh_gpu_find_candidates(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b,
+                                     int on_device, int64_t* n_candidates, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    find_candidates(c, a, b, on_device, false, false, pick(c, stream));
+    if (n_candidates) *n_candidates = c->ncand;
+  });
+}
+
+int libsupermesh_gpu_get_candidates(lsm_gpu_context* ctx, int64_t* ind_ptr, int64_t* indices, int on_device,
+                                    void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    if (c->ncand < 0) {
+      set_error(c, "no candidate search has run on this context");
+      throw Fail{LSM_ERROR_STATE};
+    }
+    cudaStream_t s = pick(c, stream);
+    const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (indices && c->ncand > 0) {
+      if (on_device) {
+        CU(lsm::launch_i32_to_i64(c->ncand, static_cast<int32_t*>(c->pair_b.p), indices, s));
+      } else {
+        int64_t* tmp = ensure<int64_t>(c, c->i64_tmp, c->ncand);
+        CU(lsm::launch_i32_to_i64(c->ncand, static_cast<int32_t*>(c->pair_b.p), tmp, s));
+        CU(cudaMemcpyAsync(indices, tmp, sizeof(int64_t) * c->ncand, k, s));
+      }
+    }
+    if (ind_ptr) CU(cudaMemcpyAsync(ind_ptr, c->offsets.p, sizeof(int64_t) * (c->nel_a + 1), k, s));
+    CU(cudaStreamSynchronize(s));
+  });
+}
+
+int libsupermesh_gpu_supermesh(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b, int on_device,
+                               double* elem_measure_a, lsm_gpu_stats* stats, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    cudaStream_t s = pick(c, stream);
+    find_candidates(c, a, b, on_device, true, false, s);
+    narrow(c, s);
+    if (elem_measure_a && c->nel_a > 0) {
+      double* em = on_device ? elem_measure_a : ensure<double>(c, c->elem_measure, c->nel_a);
+      CU(lsm::launch_row_sums(c->nel_a, static_cast<int64_t*>(c->offsets.p), static_cast<double*>(c->pair_measure.p),
+                              em, s));
+      if (!on_device)
+        CU(cudaMemcpyAsync(elem_measure_a, em, sizeof(double) * c->nel_a, cudaMemcpyDeviceToHost, s));
+    }
+    read_stats(c, stats, s);
+  });
+}
+
+int libsupermesh_gpu_clip_candidates(lsm_gpu_context* ctx, lsm_gpu_stats* stats, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    if (c->ncand < 0 || !c->simplex_prep) {
+      set_error(c, "no simplex candidate search has run on this context");
+      throw Fail{LSM_ERROR_STATE};
+    }
+    cudaStream_t s = pick(c, stream);
+    narrow(c, s);
+    read_stats(c, stats, s);
+  });
+}
+
+int libsupermesh_gpu_get_pair_results(lsm_gpu_context* ctx, double* measure, int32_t* n_out, int on_device,
+                                      void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    if (!c->have_pairs) {
+      set_error(c, "no supermesh has run on this context");
+      throw Fail{LSM_ERROR_STATE};
+    }
+    cudaStream_t s = pick(c, stream);
+    const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (measure && c->ncand > 0)
+      CU(cudaMemcpyAsync(measure, c->pair_measure.p, sizeof(double) * c->ncand, k, s));
+    if (n_out && c->ncand > 0) CU(cudaMemcpyAsync(n_out, c->pair_nout.p, sizeof(int32_t) * c->ncand, k, s));
+    CU(cudaStreamSynchronize(s));
+  });
+}
+
+int libsupermesh_gpu_intersect_pairs(lsm_gpu_context* ctx, int dim, int64_t n, const double* a, const double* b,
+                                     double* measure, int32_t* n_out, double* elems, int on_device, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(dim == 2 || dim == 3, "Invalid dimension %d", dim);
+    REQUIRE(n >= 0, "negative pair count");
+    if (n == 0) return;
+    REQUIRE(a && b, "NULL element arrays");
+    cudaStream_t s = pick(c, stream);
+    const int per = dim == 2 ? 6 : 12;
+    const int64_t cap = dim == 2 ? 22 : 81;
+    const double *da = a, *db = b;
+    double* dm = measure;
+    int32_t* dn = n_out;
+    double* de = elems;
+    if (!on_device) {
+      double* ta = ensure<double>(c, c->x_a, n * per);
+      double* tb = ensure<double>(c, c->x_b, n * per);
+      CU(cudaMemcpyAsync(ta, a, sizeof(double) * n * per, cudaMemcpyHostToDevice, s));
+      CU(cudaMemcpyAsync(tb, b, sizeof(double) * n * per, cudaMemcpyHostToDevice, s));
+      da = ta;
+      db = tb;
+      dm = measure ? ensure<double>(c, c->x_measure, n) : nullptr;
+      dn = n_out ? ensure<int32_t>(c, c->x_nout, n) : nullptr;
+      de = elems ? ensure<double>(c, c->x_elems, n * cap * per) : nullptr;
+    }
+    CU(lsm::launch_pairs_explicit(dim, n, da, db, dm, dn, de, s));
+    if (!on_device) {
+      if (measure) CU(cudaMemcpyAsync(measure, dm, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      if (n_out) CU(cudaMemcpyAsync(n_out, dn, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+      if (elems) CU(cudaMemcpyAsync(elems, de, sizeof(double) * n * cap * per, cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaStreamSynchronize(s));
+  });
+}
+
+int libsupermesh_gpu_p1_mass(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b, const double* u_a,
+                             const double* v_b, double* blocks, double* integral, int on_device, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    cudaStream_t s = pick(c, stream);
+    REQUIRE(a && b && a->index_bytes == b->index_bytes, "A and B must use the same index width");
+    find_candidates(c, a, b, on_device, true, true, s);
+    const int64_t nnz = c->ncand;
+    const int loc = c->dim + 1;
+    const double *du = u_a, *dv = v_b;
+    if (!on_device && u_a && v_b) {
+      double* tu = ensure<double>(c, c->u_a, a->nnodes);
+      double* tv = ensure<double>(c, c->v_b, b->nnodes);
+      CU(cudaMemcpyAsync(tu, u_a, sizeof(double) * a->nnodes, cudaMemcpyHostToDevice, s));
+      CU(cudaMemcpyAsync(tv, v_b, sizeof(double) * b->nnodes, cudaMemcpyHostToDevice, s));
+      du = tu;
+      dv = tv;
+    }
+    double* dbk = blocks;
+    if (blocks && !on_device) dbk = ensure<double>(c, c->blocks, nnz * loc * loc);
+    const int nblk = lsm::p1_grid_blocks(c->dim);
+    lsm::Partial* part = ensure<lsm::Partial>(c, c->partials, nblk + 1);
+    lsm::Partial* tot = ensure<lsm::Partial>(c, c->totals, 1);
+    const void* en_a = on_device ? a->enlist : c->a_en.p;
+    const void* en_b = on_device ? b->enlist : c->b_en.p;
+    CU(lsm::launch_p1_mass(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+                           static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
+                           static_cast<double*>(c->b_coords.p), static_cast<double*>(c->b_setup.p), en_a, en_b,
+                           a->index_bytes, du, dv, dbk, part, s));
+    CU(lsm::launch_finalize(part, nblk, tot, s));
+    double* h = static_cast<double*>(c->host_scalars) + 64;
+    CU(cudaMemcpyAsync(h, tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (blocks && !on_device && nnz > 0)
+      CU(cudaMemcpyAsync(blocks, dbk, sizeof(double) * nnz * loc * loc, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (integral) *integral = h[0];
+  });
+}
+
+int libsupermesh_gpu_supermesh_batched(lsm_gpu_context* ctx, int npairs, const lsm_gpu_mesh* a,
+                                       const lsm_gpu_mesh* b, int on_device, double* totals,
+                                       int64_t* n_candidates, int64_t* n_intersecting, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(npairs >= 0 && (npairs == 0 || (a && b)), "invalid batch");
+    cudaStream_t s = pick(c, stream);
+    for (int i = 0; i < npairs; ++i) {
+      find_candidates(c, &a[i], &b[i], on_device, true, false, s);
+      narrow(c, s);
+      lsm_gpu_stats st{};
+      read_stats(c, &st, s);
+      if (totals) totals[i] = st.total_measure;
+      if (n_candidates) n_candidates[i] = st.n_candidates;
+      if (n_intersecting) n_intersecting[i] = st.n_intersecting;
+    }
+  });
+}
+
+}  // extern "C"

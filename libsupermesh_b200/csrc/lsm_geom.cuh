@@ -1,0 +1,416 @@
+// Device geometry for the supermesh narrow phase: FP64, FMA-free (the whole
+// library is compiled with -fmad=false), evaluated in libsupermesh's order so
+// that every clipped vertex, area and volume is bit-identical to the
+// reference algorithm.
+//
+// Reference routines (firedrakeproject/libsupermesh):
+//   src/Triangle_Intersection.F90   clip_buf :282-335, get_lines_tri
+//                                   :395-420, triangle_area :453-477,
+//                                   intersect_tris_tri :144-185
+//   src/Tetrahedron_Intersection.F90 clip_buf :244-436, get_planes_tet
+//                                   :634-667, unit_cross :669-677,
+//                                   distances_to_plane :679-688,
+//                                   tetrahedron_volume_{real,tet} :690-725,
+//                                   intersect_tets_planes :137-179
+#pragma once
+
+#include <cstdint>
+
+namespace lsm {
+
+// Fortran EPSILON(1.0_real64) = 2**-52.
+constexpr double kEps = 2.220446049250313080847263336181640625e-16;
+constexpr double kTiny = 2.2250738585072013830902327173324040642e-308;  // 2**-1022
+
+// Fortran SPACING for real64: 2**(exponent(x)-53), TINY when that is not a
+// normal number (x == 0, subnormal x, or |x| < 2**-969).
+__device__ __forceinline__ double spacing(double x) {
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffULL;
+  const int e = (int)(bits >> 52);  // biased exponent of |x|
+  const int es = e - 52;            // biased exponent of the spacing
+  if (e == 0 || es < 1) return kTiny;
+  return __longlong_as_double((long long)es << 52);
+}
+
+// gfortran's inline NORM2 of a 3-vector (scaled sum of squares).
+__device__ __forceinline__ double norm2_3(double a, double b, double c) {
+  double scale = 0.0, result = 1.0;
+  const double v[3] = {a, b, c};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (v[i] != 0.0) {
+      const double ax = fabs(v[i]);
+      if (scale < ax) {
+        const double val = scale / ax;
+        result = 1.0 + result * (val * val);
+        scale = ax;
+      } else {
+        const double val = ax / scale;
+        result = result + val * val;
+      }
+    }
+  }
+  return sqrt(result) * scale;
+}
+
+// ---------------------------------------------------------------- measures
+// tri: vertices (x0,y0),(x1,y1),(x2,y2).  0.5*|u2 v1 - u1 v2| with u = v3-v1,
+// v = v2-v1.
+__device__ __forceinline__ double tri_area(double x0, double y0, double x1, double y1,
+                                           double x2, double y2) {
+  const double u0 = x2 - x0, u1 = y2 - y0;
+  const double w0 = x1 - x0, w1 = y1 - y0;
+  return 0.5 * fabs(u1 * w0 - u0 * w1);
+}
+
+struct Tet {
+  double x[4], y[4], z[4];
+};
+
+// Vertex-1 based volume (the C API's libsupermesh_tetrahedron_volume).
+__device__ __forceinline__ double tet_volume_v1(const Tet& t) {
+  const double e1x = t.x[1] - t.x[0], e1y = t.y[1] - t.y[0], e1z = t.z[1] - t.z[0];
+  const double e2x = t.x[2] - t.x[0], e2y = t.y[2] - t.y[0], e2z = t.z[2] - t.z[0];
+  const double e3x = t.x[3] - t.x[0], e3y = t.y[3] - t.y[0], e3z = t.z[3] - t.z[0];
+  double s = e1x * (e2y * e3z - e2z * e3y) + e1y * (e2z * e3x - e2x * e3z);
+  s = s + e1z * (e2x * e3y - e2y * e3x);
+  return (1.0 / 6.0) * fabs(s);
+}
+
+// Vertex-4 based volume (used for the clipping tolerance).
+__device__ __forceinline__ double tet_volume_v4(const Tet& t) {
+  const double ax = t.x[0] - t.x[3], ay = t.y[0] - t.y[3], az = t.z[0] - t.z[3];
+  const double bx = t.x[1] - t.x[3], by = t.y[1] - t.y[3], bz = t.z[1] - t.z[3];
+  const double cx = t.x[2] - t.x[3], cy = t.y[2] - t.y[3], cz = t.z[2] - t.z[3];
+  const double xx = by * cz - bz * cy;
+  const double xy = bz * cx - bx * cz;
+  const double xz = bx * cy - by * cx;
+  const double d = (ax * xx + ay * xy) + az * xz;
+  return fabs(d) / 6.0;
+}
+
+// ------------------------------------------------------------- tri setup
+// Three edge lines of triangle B: (normal, point), normals not normalised,
+// orientation fixed so that the inside has negative distance.
+struct Lines {
+  double nx[3], ny[3], px[3], py[3];
+};
+
+__device__ __forceinline__ void tri_lines(const double* v, Lines& L) {
+  L.nx[0] = -(v[3] - v[1]);
+  L.ny[0] = (v[2] - v[0]);
+  L.px[0] = v[0];
+  L.py[0] = v[1];
+  L.nx[1] = -(v[5] - v[3]);
+  L.ny[1] = (v[4] - v[2]);
+  L.px[1] = v[2];
+  L.py[1] = v[3];
+  L.nx[2] = -(v[1] - v[5]);
+  L.ny[2] = (v[0] - v[4]);
+  L.px[2] = v[4];
+  L.py[2] = v[5];
+  const double dot = (v[2] - v[0]) * L.nx[2] + (v[3] - v[1]) * L.ny[2];
+  if (dot > 0.0) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      L.nx[i] = -L.nx[i];
+      L.ny[i] = -L.ny[i];
+    }
+  }
+}
+
+// ------------------------------------------------------------- tet setup
+struct Planes {
+  double nx[4], ny[4], nz[4], c[4];
+};
+
+__device__ __forceinline__ void unit_cross(double ax, double ay, double az, double bx,
+                                           double by, double bz, double& ox, double& oy,
+                                           double& oz) {
+  ox = ay * bz - az * by;
+  oy = az * bx - ax * bz;
+  oz = ax * by - ay * bx;
+  const double n = norm2_3(ox, oy, oz);
+  ox = ox / n;
+  oy = oy / n;
+  oz = oz / n;
+}
+
+__device__ __forceinline__ void tet_planes(const Tet& t, Planes& P) {
+  const double e10x = t.x[1] - t.x[0], e10y = t.y[1] - t.y[0], e10z = t.z[1] - t.z[0];
+  const double e20x = t.x[2] - t.x[0], e20y = t.y[2] - t.y[0], e20z = t.z[2] - t.z[0];
+  const double e30x = t.x[3] - t.x[0], e30y = t.y[3] - t.y[0], e30z = t.z[3] - t.z[0];
+  const double e21x = t.x[2] - t.x[1], e21y = t.y[2] - t.y[1], e21z = t.z[2] - t.z[1];
+  const double e31x = t.x[3] - t.x[1], e31y = t.y[3] - t.y[1], e31z = t.z[3] - t.z[1];
+  unit_cross(e20x, e20y, e20z, e10x, e10y, e10z, P.nx[0], P.ny[0], P.nz[0]);
+  unit_cross(e10x, e10y, e10z, e30x, e30y, e30z, P.nx[1], P.ny[1], P.nz[1]);
+  unit_cross(e30x, e30y, e30z, e20x, e20y, e20z, P.nx[2], P.ny[2], P.nz[2]);
+  unit_cross(e21x, e21y, e21z, e31x, e31y, e31z, P.nx[3], P.ny[3], P.nz[3]);
+  const double det = (e10x * P.nx[3] + e10y * P.ny[3]) + e10z * P.nz[3];
+  if (det < 0.0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      P.nx[i] = -P.nx[i];
+      P.ny[i] = -P.ny[i];
+      P.nz[i] = -P.nz[i];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) P.c[i] = (t.x[i] * P.nx[i] + t.y[i] * P.ny[i]) + t.z[i] * P.nz[i];
+}
+
+// ------------------------------------------------------------ tri clipping
+// Polygon storage is supplied by the caller through an accessor so that the
+// same code runs on shared-memory slots (fast path) or local arrays.
+// clip_stage: one Sutherland-Hodgman pass of polygon `in` (n vertices)
+// against line (nx,ny,px,py), writing to `out`; returns the output count or
+// -1 when it would exceed `cap` slots.
+template <class Poly>
+__device__ __forceinline__ int clip_stage(const Poly& in, Poly& out, int n, int cap, double nx,
+                                          double ny, double px, double py) {
+  const double x0 = in.x(0), y0 = in.y(0);
+  const double d0 = nx * (x0 - px) + ny * (y0 - py);
+  double x1 = x0, y1 = y0, d1 = d0;
+  int m = 0;
+  for (int i = 0; i < n; ++i) {
+    double x2, y2, d2;
+    if (i == n - 1) {
+      x2 = x0;
+      y2 = y0;
+      d2 = d0;
+    } else {
+      x2 = in.x(i + 1);
+      y2 = in.y(i + 1);
+      d2 = nx * (x2 - px) + ny * (y2 - py);
+    }
+    if (d1 < 0.0) {
+      if (m + (d2 <= 0.0 ? 1 : 2) > cap) return -1;
+      out.set(m++, x1, y1);
+      if (!(d2 <= 0.0)) {
+        double f = fabs(d1) / (fabs(d1) + fabs(d2));
+        f = fmax(fmin(f, 1.0), 0.0);
+        out.set(m++, x1 + f * (x2 - x1), y1 + f * (y2 - y1));
+      }
+    } else if (d1 == 0.0) {
+      if (m + 1 > cap) return -1;
+      out.set(m++, x1, y1);
+    } else if (d2 < 0.0) {
+      if (m + 1 > cap) return -1;
+      double f = fabs(d1) / (fabs(d1) + fabs(d2));
+      f = fmax(fmin(f, 1.0), 0.0);
+      out.set(m++, x1 + f * (x2 - x1), y1 + f * (y2 - y1));
+    }
+    x1 = x2;
+    y1 = y2;
+    d1 = d2;
+  }
+  return m;
+}
+
+// Full tri-tri clip.  Returns the number of kept fan triangles, or -1 on
+// buffer overflow (caller retries with larger buffers).  `measure` receives
+// the sum of kept fan-triangle areas in fan order.  If `emit` is non-null
+// it is called as emit(k, x0,y0, x1,y1, x2,y2) for each kept triangle.
+template <class Poly, class Emit>
+__device__ __forceinline__ int clip_tri(double ax0, double ay0, double ax1, double ay1,
+                                        double ax2, double ay2, const Lines& L, double tol,
+                                        Poly& p, Poly& q, int cap, double& measure,
+                                        Emit emit) {
+  measure = 0.0;
+  p.set(0, ax0, ay0);
+  p.set(1, ax1, ay1);
+  p.set(2, ax2, ay2);
+  int n = clip_stage(p, q, 3, cap, L.nx[0], L.ny[0], L.px[0], L.py[0]);
+  if (n < 0) return -1;
+  if (n < 3) return 0;
+  n = clip_stage(q, p, n, cap, L.nx[1], L.ny[1], L.px[1], L.py[1]);
+  if (n < 0) return -1;
+  if (n < 3) return 0;
+  n = clip_stage(p, q, n, cap, L.nx[2], L.ny[2], L.px[2], L.py[2]);
+  if (n < 0) return -1;
+  if (n < 3) return 0;
+  const double x0 = q.x(0), y0 = q.y(0);
+  int kept = 0;
+  double xi = q.x(1), yi = q.y(1);
+  for (int i = 1; i < n - 1; ++i) {
+    const double xj = q.x(i + 1), yj = q.y(i + 1);
+    const double ar = tri_area(x0, y0, xi, yi, xj, yj);
+    if (!(ar < tol)) {
+      measure = measure + ar;
+      emit(kept, x0, y0, xi, yi, xj, yj);
+      ++kept;
+    }
+    xi = xj;
+    yi = yj;
+  }
+  return kept;
+}
+
+// ------------------------------------------------------------ tet clipping
+// Dynamic-index helpers (selects keep the tet in registers).
+__device__ __forceinline__ double sel4(int k, double a0, double a1, double a2, double a3) {
+  double r = a3;
+  r = (k == 2) ? a2 : r;
+  r = (k == 1) ? a1 : r;
+  r = (k == 0) ? a0 : r;
+  return r;
+}
+
+struct V3 {
+  double x, y, z;
+};
+
+__device__ __forceinline__ V3 vget(const Tet& t, int k) {
+  return V3{sel4(k, t.x[0], t.x[1], t.x[2], t.x[3]), sel4(k, t.y[0], t.y[1], t.y[2], t.y[3]),
+            sel4(k, t.z[0], t.z[1], t.z[2], t.z[3])};
+}
+
+__device__ __forceinline__ void vset(Tet& t, int k, const V3& v) {
+  t.x[k] = v.x;
+  t.y[k] = v.y;
+  t.z[k] = v.z;
+}
+
+// w0 * vp + w1 * vn, invdiff = 1/(dp - dn), w0 = -dn*invdiff, w1 = dp*invdiff
+__device__ __forceinline__ V3 interp(const V3& vp, const V3& vn, double dp, double dn) {
+  const double invdiff = __drcp_rn(dp - dn);
+  const double w0 = -dn * invdiff;
+  const double w1 = dp * invdiff;
+  return V3{w0 * vp.x + w1 * vn.x, w0 * vp.y + w1 * vn.y, w0 * vp.z + w1 * vn.z};
+}
+
+// Result of clipping one tet by one plane: up to three children.
+// c0 is written in place of the input; c1, c2 are returned separately.
+struct Split {
+  int k;  // number of children (0..3)
+};
+
+// Clip tet `t` by plane (nx,ny,nz,c).  On return t holds child 0 (if any)
+// and c1/c2 hold children 1/2, in the reference's output order.
+__device__ __forceinline__ int clip_tet_plane(Tet& t, double nx, double ny, double nz, double c,
+                                              Tet& c1, Tet& c2) {
+  double d[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) d[i] = ((nx * t.x[i] + ny * t.y[i]) + nz * t.z[i]) - c;
+  // Classify: index lists packed 2 bits per entry, in ascending vertex order.
+  unsigned negl = 0, posl = 0, zerl = 0;
+  int nn = 0, np = 0, nz0 = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (fabs(d[i]) < kEps) {
+      zerl |= (unsigned)i << (2 * nz0);
+      ++nz0;
+    } else if (d[i] < 0.0) {
+      negl |= (unsigned)i << (2 * nn);
+      ++nn;
+    } else if (d[i] > 0.0) {
+      posl |= (unsigned)i << (2 * np);
+      ++np;
+    }
+  }
+  if (nn == 0) return 0;
+  if (np == 0) return 1;
+  const int n0 = negl & 3;
+  const V3 vn0 = vget(t, n0);
+  const double dn0 = sel4(n0, d[0], d[1], d[2], d[3]);
+  if (nn == 1) {
+    // +++-, ++-0, +-00: every positive vertex slides towards the negative one
+    Tet o = t;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (d[k] > 0.0 && !(fabs(d[k]) < kEps)) {
+        const V3 p = interp(V3{t.x[k], t.y[k], t.z[k]}, vn0, d[k], dn0);
+        o.x[k] = p.x;
+        o.y[k] = p.y;
+        o.z[k] = p.z;
+      }
+    }
+    t = o;
+    return 1;
+  }
+  const int p0 = posl & 3;
+  const V3 vp0 = vget(t, p0);
+  const double dp0 = sel4(p0, d[0], d[1], d[2], d[3]);
+  const int n1 = (negl >> 2) & 3;
+  const V3 vn1 = vget(t, n1);
+  const double dn1 = sel4(n1, d[0], d[1], d[2], d[3]);
+  if (np == 2) {
+    // ++--
+    const int p1 = (posl >> 2) & 3;
+    const V3 vp1 = vget(t, p1);
+    const double dp1 = sel4(p1, d[0], d[1], d[2], d[3]);
+    const V3 t0 = interp(vp0, vn0, dp0, dn0);
+    const V3 t1 = interp(vp1, vn0, dp1, dn0);
+    const V3 t2 = interp(vp0, vn1, dp0, dn1);
+    const V3 t3 = interp(vp1, vn1, dp1, dn1);
+    // child 1: (v[n1], t3, t2, t1); child 2: (v[n0], t0, t1, t2)
+    vset(c1, 0, vn1);
+    vset(c1, 1, t3);
+    vset(c1, 2, t2);
+    vset(c1, 3, t1);
+    vset(c2, 0, vn0);
+    vset(c2, 1, t0);
+    vset(c2, 2, t1);
+    vset(c2, 3, t2);
+    // child 0: tet with v[p0] = t2, v[p1] = t1
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k == p0) {
+        t.x[k] = t2.x;
+        t.y[k] = t2.y;
+        t.z[k] = t2.z;
+      } else if (k == p1) {
+        t.x[k] = t1.x;
+        t.y[k] = t1.y;
+        t.z[k] = t1.z;
+      }
+    }
+    return 3;
+  }
+  // np == 1
+  const V3 t0 = interp(vp0, vn0, dp0, dn0);
+  const V3 t1 = interp(vp0, vn1, dp0, dn1);
+  if (nn == 3) {
+    // +---
+    const int n2 = (negl >> 4) & 3;
+    const V3 vn2 = vget(t, n2);
+    const double dn2 = sel4(n2, d[0], d[1], d[2], d[3]);
+    const V3 t2 = interp(vp0, vn2, dp0, dn2);
+    // child 1: (t0, v[n1], v[n2], t1); child 2: (v[n2], t1, t2, t0)
+    vset(c1, 0, t0);
+    vset(c1, 1, vn1);
+    vset(c1, 2, vn2);
+    vset(c1, 3, t1);
+    vset(c2, 0, vn2);
+    vset(c2, 1, t1);
+    vset(c2, 2, t2);
+    vset(c2, 3, t0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k == p0) {
+        t.x[k] = t0.x;
+        t.y[k] = t0.y;
+        t.z[k] = t0.z;
+      }
+    }
+    return 3;
+  }
+  // +--0: child 1: (t1, v[z0], v[n1], t0)
+  const int z0 = zerl & 3;
+  const V3 vz0 = vget(t, z0);
+  vset(c1, 0, t1);
+  vset(c1, 1, vz0);
+  vset(c1, 2, vn1);
+  vset(c1, 3, t0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k == p0) {
+      t.x[k] = t0.x;
+      t.y[k] = t0.y;
+      t.z[k] = t0.z;
+    }
+  }
+  return 2;
+}
+
+}  // namespace lsm

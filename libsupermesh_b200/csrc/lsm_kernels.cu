@@ -1,0 +1,1470 @@
+// Supermesh kernels for sm_100a.
+//
+//   K1  k_prep          element gather, FP64/FP32 boxes, measures, tolerances,
+//                       B-element clip setup (lines / unit-normal planes)
+//   K1b k_root_*        root box reduction;  k_morton  Morton keys
+//   K2  radix sort      stable LSD, 8-bit digits, warp-match ranking
+//   K3  k_bvh_internal  Karras LBVH hierarchy + rope table;
+//       k_bvh_refit     bottom-up FP32 box refit, escape links
+//   K4  k_query         stackless LBVH traversal per A element (FP32,
+//                       outward-rounded boxes) + exact strict FP64 box test
+//   K5  k_clip_tris     one candidate pair per thread, polygon in shared
+//                       memory, FP64 Sutherland-Hodgman
+//   K6  k_clip_tets     one candidate pair per thread, depth-first plane
+//                       clipping with a shared-memory tet stack
+//   K7  compensated reductions (per-block (sum, err), then final)
+//   K8  k_p1_mass       P1-P1 mixed mass blocks + u^T M v
+//
+// Everything FP64 is compiled with -fmad=false so that each +,-,*,/ is a
+// separately rounded IEEE operation, matching libsupermesh's gfortran build.
+#include "lsm_geom.cuh"
+#include "lsm_kernels.h"
+
+#include <cfloat>
+#include <cstdio>
+
+namespace lsm {
+
+namespace {
+unsigned long long g_launches = 0;
+}  // namespace
+
+unsigned long long launches() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+namespace {
+
+inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+
+int sm_count() {
+  static int cached = -1;
+  if (cached < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cached = n;
+  }
+  return cached;
+}
+
+int grid_for(int64_t n, int block, int per_sm) {
+  int64_t need = (n + block - 1) / block;
+  int64_t cap = (int64_t)sm_count() * per_sm;
+  if (need < 1) need = 1;
+  return (int)(need < cap ? need : cap);
+}
+
+// Compensated (sum, err) pair helpers: TwoSum-based merge.
+__device__ __forceinline__ void cs_add(double& sum, double& err, double x) {
+  // Kahan step (Precision.F90:89-95)
+  const double cx = err + x;
+  const double s = sum + cx;
+  err = (sum - s) + cx;
+  sum = s;
+}
+
+__device__ __forceinline__ void two_sum_merge(double& s, double& e, double s2, double e2) {
+  const double t = s + s2;
+  const double bp = t - s;
+  const double err = (s - (t - bp)) + (s2 - bp);
+  s = t;
+  e = e + e2 + err;
+}
+
+template <int BLOCK>
+__device__ void block_reduce_partial(double sum, double err, unsigned long long ni, unsigned long long no,
+                                     Partial* out) {
+  __shared__ double ss[BLOCK / 32], se[BLOCK / 32];
+  __shared__ unsigned long long si[BLOCK / 32], so[BLOCK / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double s2 = __shfl_down_sync(0xffffffffu, sum, o);
+    const double e2 = __shfl_down_sync(0xffffffffu, err, o);
+    two_sum_merge(sum, err, s2, e2);
+    ni += __shfl_down_sync(0xffffffffu, ni, o);
+    no += __shfl_down_sync(0xffffffffu, no, o);
+  }
+  if (lane == 0) {
+    ss[wid] = sum;
+    se[wid] = err;
+    si[wid] = ni;
+    so[wid] = no;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Partial p{ss[0], se[0], si[0], so[0]};
+    for (int w = 1; w < BLOCK / 32; ++w) {
+      two_sum_merge(p.sum, p.err, ss[w], se[w]);
+      p.n_int += si[w];
+      p.n_out += so[w];
+    }
+    *out = p;
+  }
+}
+
+}  // namespace
+
+// ======================================================================
+// K1: element prep
+// ======================================================================
+// LOC = DIM + 1 for simplices; other LOC (quads, hexes) only get boxes,
+// which is all the candidate search needs.
+template <int DIM, int LOC, typename IDX>
+__global__ void k_prep(int64_t nel, const double* __restrict__ pos, const IDX* __restrict__ en,
+                       double* coords, double* box64, float* box32, double* tolv, double* setup,
+                       int* bad, int64_t nnodes) {
+  constexpr bool SIMPLEX = LOC == DIM + 1;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    double v[LOC * DIM];
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < LOC; ++k) {
+      int64_t node = (int64_t)en[e * LOC + k];
+      if (node < 0 || node >= nnodes) {
+        ok = false;
+        node = 0;
+      }
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) v[k * DIM + c] = pos[node * DIM + c];
+    }
+    if (!ok) atomicExch(bad, 1);
+    if (coords) {
+#pragma unroll
+      for (int j = 0; j < LOC * DIM; ++j) coords[e * LOC * DIM + j] = v[j];
+    }
+    double lo[DIM], hi[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) lo[c] = hi[c] = v[c];
+#pragma unroll
+    for (int k = 1; k < LOC; ++k)
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        lo[c] = fmin(lo[c], v[k * DIM + c]);
+        hi[c] = fmax(hi[c], v[k * DIM + c]);
+      }
+    if (box64) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        box64[e * 2 * DIM + c] = lo[c];
+        box64[e * 2 * DIM + DIM + c] = hi[c];
+      }
+    }
+    if (box32) {
+      float4 l = make_float4(0.f, 0.f, 0.f, 0.f), h = make_float4(0.f, 0.f, 0.f, 0.f);
+      l.x = __double2float_rd(lo[0]);
+      l.y = __double2float_rd(lo[1]);
+      h.x = __double2float_ru(hi[0]);
+      h.y = __double2float_ru(hi[1]);
+      if (DIM == 3) {
+        l.z = __double2float_rd(lo[DIM - 1]);
+        h.z = __double2float_ru(hi[DIM - 1]);
+      }
+      reinterpret_cast<float4*>(box32)[2 * e] = l;
+      reinterpret_cast<float4*>(box32)[2 * e + 1] = h;
+    }
+    if (!SIMPLEX) continue;
+    double meas;
+    Tet t;
+    if (DIM == 2) {
+      meas = tri_area(v[0], v[1], v[2], v[3], v[4], v[5]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        t.x[k] = v[k * DIM + 0];
+        t.y[k] = v[k * DIM + 1];
+        t.z[k] = v[k * DIM + DIM - 1];
+      }
+      meas = tet_volume_v4(t);
+    }
+    const double tol = 10.0 * spacing(meas);
+    if (tolv) tolv[e] = tol;
+    if (setup) {
+      if (DIM == 2) {
+        Lines L;
+        tri_lines(v, L);
+        double* o = setup + e * kSetup2;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          o[4 * i + 0] = L.nx[i];
+          o[4 * i + 1] = L.ny[i];
+          o[4 * i + 2] = L.px[i];
+          o[4 * i + 3] = L.py[i];
+        }
+        o[12] = tol;
+      } else {
+        Planes P;
+        tet_planes(t, P);
+        double* o = setup + e * kSetup3;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          o[4 * i + 0] = P.nx[i];
+          o[4 * i + 1] = P.ny[i];
+          o[4 * i + 2] = P.nz[i];
+          o[4 * i + 3] = P.c[i];
+        }
+        o[16] = tol;
+      }
+    }
+  }
+}
+
+template <int DIM, int LOC>
+static void prep_dispatch_idx(int g, int B, cudaStream_t s, int64_t nel, const double* pos,
+                              const void* enlist, int idx_bytes, double* coords, double* box64,
+                              float* box32, double* tolv, double* setup, int* bad, int64_t nnodes) {
+  count_launch();
+  if (idx_bytes == 4)
+    k_prep<DIM, LOC, int32_t><<<g, B, 0, s>>>(nel, pos, (const int32_t*)enlist, coords, box64, box32, tolv, setup, bad, nnodes);
+  else
+    k_prep<DIM, LOC, int64_t><<<g, B, 0, s>>>(nel, pos, (const int64_t*)enlist, coords, box64, box32, tolv, setup, bad, nnodes);
+}
+
+cudaError_t launch_prep(int dim, int loc, int64_t nel, const double* pos, const void* enlist, int idx_bytes,
+                        double* coords, double* box64, float* box32, double* tolv, double* setup,
+                        int* bad_index, int64_t nnodes, cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  const int B = 256;
+  const int g = grid_for(nel, B, 8);
+  if (dim == 2 && loc == 3)
+    prep_dispatch_idx<2, 3>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes);
+  else if (dim == 2 && loc == 4)
+    prep_dispatch_idx<2, 4>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes);
+  else if (dim == 3 && loc == 4)
+    prep_dispatch_idx<3, 4>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes);
+  else if (dim == 3 && loc == 8)
+    prep_dispatch_idx<3, 8>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// K1b: root box and Morton keys
+// ======================================================================
+template <int DIM>
+__global__ void k_root_partial(int64_t nel, const double* __restrict__ box64, double* partial) {
+  double lo[DIM], hi[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    lo[c] = DBL_MAX;
+    hi[c] = -DBL_MAX;
+  }
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
+       e += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      lo[c] = fmin(lo[c], box64[e * 2 * DIM + c]);
+      hi[c] = fmax(hi[c], box64[e * 2 * DIM + DIM + c]);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      lo[c] = fmin(lo[c], __shfl_down_sync(0xffffffffu, lo[c], o));
+      hi[c] = fmax(hi[c], __shfl_down_sync(0xffffffffu, hi[c], o));
+    }
+  __shared__ double sl[32][DIM], sh[32][DIM];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      sl[wid][c] = lo[c];
+      sh[wid][c] = hi[c];
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        lo[c] = fmin(lo[c], sl[w][c]);
+        hi[c] = fmax(hi[c], sh[w][c]);
+      }
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      partial[blockIdx.x * 2 * DIM + c] = lo[c];
+      partial[blockIdx.x * 2 * DIM + DIM + c] = hi[c];
+    }
+  }
+}
+
+template <int DIM>
+__global__ void k_root_final(int np, const double* partial, double* root) {
+  if (threadIdx.x != 0) return;
+  double lo[DIM], hi[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    lo[c] = DBL_MAX;
+    hi[c] = -DBL_MAX;
+  }
+  for (int b = 0; b < np; ++b)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      lo[c] = fmin(lo[c], partial[b * 2 * DIM + c]);
+      hi[c] = fmax(hi[c], partial[b * 2 * DIM + DIM + c]);
+    }
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    root[c] = lo[c];
+    root[DIM + c] = hi[c];
+  }
+}
+
+cudaError_t launch_root_box(int dim, int64_t nel, const double* box64, double* partial,
+                            int partial_cap, double* rootbox, cudaStream_t s) {
+  const int B = 256;
+  int g = grid_for(nel, B, 2);
+  if (g > partial_cap) g = partial_cap;
+  count_launch(2);
+  if (dim == 2) {
+    k_root_partial<2><<<g, B, 0, s>>>(nel, box64, partial);
+    k_root_final<2><<<1, 32, 0, s>>>(g, partial, rootbox);
+  } else {
+    k_root_partial<3><<<g, B, 0, s>>>(nel, box64, partial);
+    k_root_final<3><<<1, 32, 0, s>>>(g, partial, rootbox);
+  }
+  return cudaGetLastError();
+}
+
+__device__ __forceinline__ uint32_t spread2(uint32_t x) {  // 16 bits -> even bits
+  x &= 0xffffu;
+  x = (x | (x << 8)) & 0x00ff00ffu;
+  x = (x | (x << 4)) & 0x0f0f0f0fu;
+  x = (x | (x << 2)) & 0x33333333u;
+  x = (x | (x << 1)) & 0x55555555u;
+  return x;
+}
+
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {  // 10 bits -> every 3rd bit
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+template <int DIM>
+__global__ void k_morton(int64_t nel, const double* __restrict__ box64, const double* __restrict__ root,
+                         uint32_t* keys, int32_t* vals) {
+  constexpr double kScale = DIM == 2 ? 65536.0 : 1024.0;
+  constexpr uint32_t kMax = DIM == 2 ? 65535u : 1023u;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t q[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      const double mid = 0.5 * (box64[e * 2 * DIM + c] + box64[e * 2 * DIM + DIM + c]);
+      const double ext = root[DIM + c] - root[c];
+      double u = ext > 0.0 ? (mid - root[c]) / ext : 0.0;
+      u = fmin(fmax(u, 0.0), 1.0);
+      const double f = u * kScale;
+      q[c] = f >= (double)kMax ? kMax : (uint32_t)f;
+    }
+    uint32_t key;
+    if (DIM == 2)
+      key = (spread2(q[1]) << 1) | spread2(q[0]);
+    else
+      key = (spread3(q[DIM - 1]) << 2) | (spread3(q[1]) << 1) | spread3(q[0]);
+    keys[e] = key;
+    vals[e] = (int32_t)e;
+  }
+}
+
+cudaError_t launch_morton(int dim, int64_t nel, const double* box64, const double* rootbox,
+                          uint32_t* keys, int32_t* vals, cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  const int B = 256;
+  const int g = grid_for(nel, B, 8);
+  count_launch();
+  if (dim == 2)
+    k_morton<2><<<g, B, 0, s>>>(nel, box64, rootbox, keys, vals);
+  else
+    k_morton<3><<<g, B, 0, s>>>(nel, box64, rootbox, keys, vals);
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// K2: stable LSD radix sort (8-bit digits)
+// ======================================================================
+namespace {
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 8;                           // per thread
+constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per block
+constexpr int kWarpTile = 32 * kSortItems;             // contiguous per warp
+}  // namespace
+
+int64_t radix_hist_entries(int64_t n) {
+  const int64_t nb = (n + kSortTile - 1) / kSortTile;
+  return 256 * (nb > 0 ? nb : 1);
+}
+
+// Histogram of one digit per block: hist[d * nblocks + block].
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(int64_t n, int shift, const uint32_t* __restrict__ keys,
+                                                             uint32_t* hist) {
+  __shared__ uint32_t h[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kSortTile;
+  for (int r = 0; r < kSortItems; ++r) {
+    const int64_t i = base + (int64_t)r * kSortThreads + threadIdx.x;
+    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[(int64_t)d * gridDim.x + blockIdx.x] = h[d];
+}
+
+// Exclusive scan of `count` uint32 entries in place by one block of 1024.
+__global__ void __launch_bounds__(1024) k_scan_u32_single(int64_t count, uint32_t* data) {
+  __shared__ uint32_t warp_tot[32];
+  const int64_t per = (count + blockDim.x - 1) / blockDim.x;
+  const int64_t beg = (int64_t)threadIdx.x * per;
+  const int64_t end = beg + per < count ? beg + per : count;
+  uint32_t local = 0;
+  for (int64_t i = beg; i < end; ++i) local += data[i];
+  // block exclusive scan of `local`
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t inc = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) warp_tot[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = warp_tot[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    warp_tot[lane] = w;
+  }
+  __syncthreads();
+  uint32_t run = inc - local + (wid > 0 ? warp_tot[wid - 1] : 0u);
+  for (int64_t i = beg; i < end; ++i) {
+    const uint32_t v = data[i];
+    data[i] = run;
+    run += v;
+  }
+}
+
+// Stable scatter: each warp owns a contiguous 256-key sub-tile.
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(int64_t n, int shift, const uint32_t* __restrict__ keys_in,
+                                                                const int32_t* __restrict__ vals_in,
+                                                                uint32_t* keys_out, int32_t* vals_out,
+                                                                const uint32_t* __restrict__ hist) {
+  __shared__ uint32_t wh[kSortWarps][256];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int i = lane; i < 256; i += 32) wh[wid][i] = 0;
+  __syncwarp();
+  const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)wid * kWarpTile;
+  uint32_t k[kSortItems];
+  int dg[kSortItems];
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const int64_t i = base + r * 32 + lane;
+    k[r] = i < n ? keys_in[i] : 0u;
+    dg[r] = i < n ? (int)((k[r] >> shift) & 255u) : 256;
+    const unsigned peers = __match_any_sync(0xffffffffu, dg[r]);
+    if (dg[r] < 256 && (peers & lt) == 0) wh[wid][dg[r]] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // cross-warp exclusive offsets per digit, plus the global digit/block base
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) {
+    uint32_t run = hist[(int64_t)d * gridDim.x + blockIdx.x];
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = wh[w][d];
+      wh[w][d] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const int64_t i = base + r * 32 + lane;
+    const unsigned peers = __match_any_sync(0xffffffffu, dg[r]);
+    if (dg[r] < 256) {
+      const uint32_t pos = wh[wid][dg[r]] + __popc(peers & lt);
+      keys_out[pos] = k[r];
+      vals_out[pos] = vals_in[i];
+    }
+    __syncwarp();
+    if (dg[r] < 256 && (peers & lt) == 0) wh[wid][dg[r]] += __popc(peers);
+    __syncwarp();
+  }
+}
+
+cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals, uint32_t* keys_tmp,
+                             int32_t* vals_tmp, uint32_t* hist, cudaStream_t s) {
+  if (n <= 1) return cudaSuccess;
+  const int nb = (int)((n + kSortTile - 1) / kSortTile);
+  const int passes = (bits + 7) / 8;
+  uint32_t *ki = keys, *ko = keys_tmp;
+  int32_t *vi = vals, *vo = vals_tmp;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = 8 * p;
+    count_launch(3);
+    k_radix_hist<<<nb, kSortThreads, 0, s>>>(n, shift, ki, hist);
+    k_scan_u32_single<<<1, 1024, 0, s>>>((int64_t)256 * nb, hist);
+    k_radix_scatter<<<nb, kSortThreads, 0, s>>>(n, shift, ki, vi, ko, vo, hist);
+    uint32_t* tk = ki;
+    ki = ko;
+    ko = tk;
+    int32_t* tv = vi;
+    vi = vo;
+    vo = tv;
+  }
+  if (ki != keys) {
+    cudaMemcpyAsync(keys, ki, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(vals, vi, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s);
+  }
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// K3: LBVH (Karras 2012) + ropes + refit
+// ======================================================================
+// Node ids: internal i in [0, n-2]; leaf k -> (n-1) + k.  Root = node 0.
+__device__ __forceinline__ int bvh_delta(const uint32_t* __restrict__ codes, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  const uint32_t a = codes[i], b = codes[j];
+  if (a != b) return __clz(a ^ b);
+  return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+}
+
+// work layout (ints): parent[2n-1] | rope[n] | visit[n] | last[n] | left[n] | right[n]
+__global__ void k_bvh_internal(int n, const uint32_t* __restrict__ codes, int* parent, int* rope,
+                               int* last, int* left, int* right) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int d = (bvh_delta(codes, n, i, i + 1) - bvh_delta(codes, n, i, i - 1)) >= 0 ? 1 : -1;
+  const int dmin = bvh_delta(codes, n, i, i - d);
+  int lmax = 2;
+  while (bvh_delta(codes, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (bvh_delta(codes, n, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int dnode = bvh_delta(codes, n, i, j);
+  int s = 0;
+  int t = l;
+  do {
+    t = (t + 1) >> 1;
+    if (bvh_delta(codes, n, i, i + (s + t) * d) > dnode) s += t;
+  } while (t > 1);
+  const int gamma = i + s * d + (d < 0 ? -1 : 0);
+  const int first = i < j ? i : j;
+  const int lst = i < j ? j : i;
+  const int lc = (first == gamma) ? (n - 1) + gamma : gamma;
+  const int rc = (lst == gamma + 1) ? (n - 1) + gamma + 1 : gamma + 1;
+  left[i] = lc;
+  right[i] = rc;
+  parent[lc] = i;
+  parent[rc] = i;
+  rope[gamma + 1] = rc;
+  last[i] = lst;
+}
+
+__device__ __forceinline__ int bvh_escape(int n, int node, const int* __restrict__ rope, const int* __restrict__ last) {
+  const int r = node >= n - 1 ? node - (n - 1) : last[node];
+  return r == n - 1 ? -1 : rope[r + 1];
+}
+
+__global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, const float4* __restrict__ box32,
+                            const int* __restrict__ parent, const int* __restrict__ rope,
+                            const int* __restrict__ last, const int* __restrict__ left,
+                            const int* __restrict__ right, int* visit, float4* lo_left, float4* hi_esc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int elem = sorted_vals[k];
+  int node = (n - 1) + k;
+  float4 lo = box32[2 * elem], hi = box32[2 * elem + 1];
+  lo.w = __int_as_float(elem);
+  hi.w = __int_as_float(bvh_escape(n, node, rope, last));
+  lo_left[node] = lo;
+  hi_esc[node] = hi;
+  if (n == 1) return;
+  int p = parent[node];
+  for (int guard = 0; guard < 128 && p >= 0; ++guard) {
+    __threadfence();
+    if (atomicAdd(&visit[p], 1) == 0) return;  // sibling not done yet
+    __threadfence();
+    const int lc = left[p], rc = right[p];
+    const float4 a0 = __ldcg(&lo_left[lc]), a1 = __ldcg(&hi_esc[lc]);
+    const float4 b0 = __ldcg(&lo_left[rc]), b1 = __ldcg(&hi_esc[rc]);
+    float4 l, h;
+    l.x = fminf(a0.x, b0.x);
+    l.y = fminf(a0.y, b0.y);
+    l.z = fminf(a0.z, b0.z);
+    l.w = __int_as_float(lc);
+    h.x = fmaxf(a1.x, b1.x);
+    h.y = fmaxf(a1.y, b1.y);
+    h.z = fmaxf(a1.z, b1.z);
+    h.w = __int_as_float(bvh_escape(n, p, rope, last));
+    __stcg(&lo_left[p], l);
+    __stcg(&hi_esc[p], h);
+    if (p == 0) return;
+    p = parent[p];
+  }
+}
+
+cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const int32_t* sorted_vals,
+                             const float* box32, BVH bvh, int* work, cudaStream_t s) {
+  (void)dim;
+  if (n <= 0) return cudaSuccess;
+  int* parent = work;
+  int* rope = parent + (2 * n - 1);
+  int* visit = rope + n;
+  int* last = visit + n;
+  int* left = last + n;
+  int* right = left + n;
+  cudaMemsetAsync(visit, 0, sizeof(int) * n, s);
+  cudaMemsetAsync(rope, 0xff, sizeof(int) * n, s);  // unset ropes read as "end"
+  count_launch(n > 1 ? 2 : 1);
+  if (n > 1) {
+    k_bvh_internal<<<(n - 1 + 255) / 256, 256, 0, s>>>(n, sorted_keys, parent, rope, last, left, right);
+  }
+  cudaMemsetAsync(parent, 0xff, sizeof(int), s);  // parent[root] = -1
+  k_bvh_refit<<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
+                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc);
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// K4: candidate search
+// ======================================================================
+template <int DIM, bool FILL>
+__global__ void __launch_bounds__(128) k_query(int64_t nel_a, const double* __restrict__ box64_a,
+                                               const float4* __restrict__ lo_left,
+                                               const float4* __restrict__ hi_esc, int n,
+                                               const double* __restrict__ box64_b, int* counts,
+                                               const int64_t* __restrict__ offsets, int32_t* pair_a,
+                                               int32_t* pair_b) {
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < nel_a;
+       a += (int64_t)gridDim.x * blockDim.x) {
+    double lo[DIM], hi[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      lo[c] = box64_a[a * 2 * DIM + c];
+      hi[c] = box64_a[a * 2 * DIM + DIM + c];
+    }
+    float ql[3], qh[3];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      ql[c] = __double2float_rd(lo[c]);
+      qh[c] = __double2float_ru(hi[c]);
+    }
+    int cnt = 0;
+    int64_t out = FILL ? offsets[a] : 0;
+    int node = 0;
+    // Each step moves forward in depth-first order; 2n-1 nodes bound it.
+    const int nodes = 2 * n - 1;
+    for (int guard = 0; node >= 0 && guard < 2 * n + 1; ++guard) {
+      if (node >= nodes) break;  // never taken for a well-formed hierarchy
+      const float4 L = __ldg(&lo_left[node]);
+      const float4 H = __ldg(&hi_esc[node]);
+      bool ov = H.x > ql[0] && L.x < qh[0] && H.y > ql[1] && L.y < qh[1];
+      if (DIM == 3) ov = ov && H.z > ql[2] && L.z < qh[2];
+      if (ov) {
+        const int w = __float_as_int(L.w);
+        if (node < n - 1) {
+          node = w;
+          continue;
+        }
+        const double* bb = box64_b + (int64_t)w * 2 * DIM;
+        bool ex = true;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) ex = ex && (hi[c] > bb[c]) && (lo[c] < bb[DIM + c]);
+        if (ex) {
+          if (FILL) {
+            pair_a[out + cnt] = (int32_t)a;
+            pair_b[out + cnt] = w;
+          }
+          ++cnt;
+        }
+      }
+      node = __float_as_int(H.w);
+    }
+    if (!FILL) counts[a] = cnt;
+  }
+}
+
+cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_a, BVH bvh,
+                         const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
+                         int32_t* pair_b, cudaStream_t s) {
+  if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
+  const int B = 128;
+  const int g = grid_for(nel_a, B, 16);
+  count_launch();
+  if (dim == 2) {
+    if (fill)
+      k_query<2, true><<<g, B, 0, s>>>(nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+    else
+      k_query<2, false><<<g, B, 0, s>>>(nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+  } else {
+    if (fill)
+      k_query<3, true><<<g, B, 0, s>>>(nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+    else
+      k_query<3, false><<<g, B, 0, s>>>(nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+  }
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// Scan of int32 counts -> int64 offsets
+// ======================================================================
+namespace {
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+}  // namespace
+
+int64_t scan_tmp_entries(int64_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
+
+template <int BLOCK>
+__device__ int64_t block_excl_scan(int64_t v, int64_t* total) {
+  __shared__ int64_t wt[BLOCK / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int64_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) wt[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    int64_t w = lane < BLOCK / 32 ? wt[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    if (lane < BLOCK / 32) wt[lane] = w;
+  }
+  __syncthreads();
+  const int64_t r = inc - v + (wid > 0 ? wt[wid - 1] : 0);
+  if (total) *total = wt[BLOCK / 32 - 1];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(int64_t n, const int* __restrict__ counts, int64_t* tmp) {
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i)
+    if (base + i < n) s += counts[base + i];
+  int64_t tot;
+  block_excl_scan<kScanThreads>(s, &tot);
+  if (threadIdx.x == 0) tmp[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_top(int nb, int64_t* tmp) {
+  // exclusive scan of tmp[0..nb) in place; tmp[nb] = total
+  __shared__ int64_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int64_t v = i < nb ? tmp[i] : 0;
+    int64_t tot;
+    const int64_t ex = block_excl_scan<1024>(v, &tot);
+    if (i < nb) tmp[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) tmp[nb] = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_down(int64_t n, const int* __restrict__ counts,
+                                                            const int64_t* __restrict__ tmp, int64_t* out,
+                                                            int nb) {
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = base + i < n ? counts[base + i] : 0;
+    s += v[i];
+  }
+  int64_t run = block_excl_scan<kScanThreads>(s, nullptr) + tmp[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i < n) out[base + i] = run;
+    run += v[i];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tmp[nb];
+}
+
+cudaError_t launch_scan(int64_t n, const int* counts, int64_t* offsets, int64_t* tmp, cudaStream_t s) {
+  if (n <= 0) {
+    cudaMemsetAsync(offsets, 0, sizeof(int64_t), s);
+    return cudaGetLastError();
+  }
+  const int nb = (int)((n + kScanTile - 1) / kScanTile);
+  count_launch(3);
+  k_scan_reduce<<<nb, kScanThreads, 0, s>>>(n, counts, tmp);
+  k_scan_top<<<1, 1024, 0, s>>>(nb, tmp);
+  k_scan_down<<<nb, kScanThreads, 0, s>>>(n, counts, tmp, offsets, nb);
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// K5: triangle clipping
+// ======================================================================
+namespace {
+constexpr int kTriBlock = 128;
+constexpr int kTriCap = 8;  // fast-path polygon slots (geometric max is 6)
+constexpr int kTriWideCap = 24;
+constexpr int kTetBlock = 128;
+constexpr int kTetStack = 6;  // max pending tets: 2 per level for planes 1-3
+}  // namespace
+
+// Polygon in shared memory: slot i, coord c at base[(2*i + c) * BLOCK].
+template <int BLOCK>
+struct SmemPoly {
+  double* base;
+  __device__ __forceinline__ double x(int i) const { return base[(2 * i) * BLOCK]; }
+  __device__ __forceinline__ double y(int i) const { return base[(2 * i + 1) * BLOCK]; }
+  __device__ __forceinline__ void set(int i, double px, double py) {
+    base[(2 * i) * BLOCK] = px;
+    base[(2 * i + 1) * BLOCK] = py;
+  }
+};
+
+template <int CAP>
+struct LocalPoly {
+  double px[CAP], py[CAP];
+  __device__ __forceinline__ double x(int i) const { return px[i]; }
+  __device__ __forceinline__ double y(int i) const { return py[i]; }
+  __device__ __forceinline__ void set(int i, double a, double b) {
+    px[i] = a;
+    py[i] = b;
+  }
+};
+
+struct NoEmit {
+  __device__ __forceinline__ void operator()(int, double, double, double, double, double, double) const {}
+};
+
+__device__ __forceinline__ void load_lines(const double* __restrict__ o, Lines& L, double& tol) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    L.nx[i] = o[4 * i + 0];
+    L.ny[i] = o[4 * i + 1];
+    L.px[i] = o[4 * i + 2];
+    L.py[i] = o[4 * i + 3];
+  }
+  tol = o[12];
+}
+
+__global__ void __launch_bounds__(kTriBlock) k_clip_tris(int64_t npairs, const int32_t* __restrict__ pa,
+                                                         const int32_t* __restrict__ pb,
+                                                         const double* __restrict__ coords_a,
+                                                         const double* __restrict__ tol_a,
+                                                         const double* __restrict__ setup_b,
+                                                         double* pair_measure, int32_t* pair_nout,
+                                                         Partial* partials, int32_t* ovf_list,
+                                                         int* ovf_count) {
+  __shared__ double poly[2 * 2 * kTriCap * kTriBlock];
+  SmemPoly<kTriBlock> p{poly + threadIdx.x}, q{poly + 2 * kTriCap * kTriBlock + threadIdx.x};
+  double sum = 0.0, err = 0.0;
+  unsigned long long ni = 0, no = 0;
+  for (int64_t i = (int64_t)blockIdx.x * kTriBlock + threadIdx.x; i < npairs;
+       i += (int64_t)gridDim.x * kTriBlock) {
+    const int a = pa[i], b = pb[i];
+    const double* va = coords_a + (int64_t)a * 6;
+    Lines L;
+    double tolb;
+    load_lines(setup_b + (int64_t)b * kSetup2, L, tolb);
+    const double tol = fmin(tol_a[a], tolb);
+    double m;
+    const int n = clip_tri(va[0], va[1], va[2], va[3], va[4], va[5], L, tol, p, q, kTriCap, m, NoEmit{});
+    if (n < 0) {
+      const int k = atomicAdd(ovf_count, 1);
+      ovf_list[k] = (int32_t)i;
+      continue;
+    }
+    pair_measure[i] = m;
+    pair_nout[i] = n;
+    cs_add(sum, err, m);
+    ni += n > 0;
+    no += n;
+  }
+  block_reduce_partial<kTriBlock>(sum, err, ni, no, &partials[blockIdx.x]);
+}
+
+__global__ void __launch_bounds__(32) k_clip_tris_wide(const int32_t* __restrict__ list, const int* __restrict__ count,
+                                                       int64_t cap, const int32_t* __restrict__ pa,
+                                                       const int32_t* __restrict__ pb,
+                                                       const double* __restrict__ coords_a,
+                                                       const double* __restrict__ tol_a,
+                                                       const double* __restrict__ setup_b,
+                                                       double* pair_measure, int32_t* pair_nout,
+                                                       Partial* partial) {
+  double sum = 0.0, err = 0.0;
+  unsigned long long ni = 0, no = 0;
+  int64_t nl = *count;
+  if (nl > cap) nl = cap;
+  for (int64_t j = threadIdx.x; j < nl; j += 32) {
+    const int64_t i = list[j];
+    const int a = pa[i], b = pb[i];
+    const double* va = coords_a + (int64_t)a * 6;
+    Lines L;
+    double tolb;
+    load_lines(setup_b + (int64_t)b * kSetup2, L, tolb);
+    const double tol = fmin(tol_a[a], tolb);
+    LocalPoly<kTriWideCap> p, q;
+    double m;
+    int n = clip_tri(va[0], va[1], va[2], va[3], va[4], va[5], L, tol, p, q, kTriWideCap, m, NoEmit{});
+    if (n < 0) {  // cannot happen: 3 -> 6 -> 12 -> 24 vertices at most
+      n = 0;
+      m = 0.0;
+    }
+    pair_measure[i] = m;
+    pair_nout[i] = n;
+    cs_add(sum, err, m);
+    ni += n > 0;
+    no += n;
+  }
+  block_reduce_partial<32>(sum, err, ni, no, partial);
+}
+
+// ======================================================================
+// K6: tetrahedron clipping, depth-first
+// ======================================================================
+template <int BLOCK>
+struct TetStack {
+  double* base;  // slot s, component j at base[(s*12 + j) * BLOCK]
+  __device__ __forceinline__ void store(int s, const Tet& t) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      base[(s * 12 + 3 * k + 0) * BLOCK] = t.x[k];
+      base[(s * 12 + 3 * k + 1) * BLOCK] = t.y[k];
+      base[(s * 12 + 3 * k + 2) * BLOCK] = t.z[k];
+    }
+  }
+  __device__ __forceinline__ void load(int s, Tet& t) const {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      t.x[k] = base[(s * 12 + 3 * k + 0) * BLOCK];
+      t.y[k] = base[(s * 12 + 3 * k + 1) * BLOCK];
+      t.z[k] = base[(s * 12 + 3 * k + 2) * BLOCK];
+    }
+  }
+};
+
+struct TetStackLocal {
+  Tet slot[kTetStack];
+  __device__ __forceinline__ void store(int s, const Tet& t) { slot[s] = t; }
+  __device__ __forceinline__ void load(int s, Tet& t) const { t = slot[s]; }
+};
+
+// Depth-first clip of tet `t` by planes P; visits kept output tets in the
+// reference's (breadth-first) order.  `leaf(t)` is called for each final
+// tet with vol_v4 >= tol.  Returns the number of kept tets.
+template <class Stack, class Leaf>
+__device__ __forceinline__ int clip_tet_dfs(Tet t, const Planes& P, double tol, Stack& stk, Leaf leaf) {
+  int sp = 0;
+  unsigned levels = 0;  // 2 bits per stack slot
+  int L = 0;
+  int kept = 0;
+  for (int guard = 0; guard < 200; ++guard) {
+    const double nx = sel4(L, P.nx[0], P.nx[1], P.nx[2], P.nx[3]);
+    const double ny = sel4(L, P.ny[0], P.ny[1], P.ny[2], P.ny[3]);
+    const double nz = sel4(L, P.nz[0], P.nz[1], P.nz[2], P.nz[3]);
+    const double c = sel4(L, P.c[0], P.c[1], P.c[2], P.c[3]);
+    Tet c1, c2;
+    const int k = clip_tet_plane(t, nx, ny, nz, c, c1, c2);
+    if (L == 3) {
+      if (k >= 1 && tet_volume_v4(t) >= tol) {
+        leaf(t);
+        ++kept;
+      }
+      if (k >= 2 && tet_volume_v4(c1) >= tol) {
+        leaf(c1);
+        ++kept;
+      }
+      if (k >= 3 && tet_volume_v4(c2) >= tol) {
+        leaf(c2);
+        ++kept;
+      }
+    } else if (k > 0) {
+      if (k == 3) {
+        stk.store(sp, c2);
+        levels |= (unsigned)(L + 1) << (2 * sp);
+        ++sp;
+      }
+      if (k >= 2) {
+        stk.store(sp, c1);
+        levels |= (unsigned)(L + 1) << (2 * sp);
+        ++sp;
+      }
+      ++L;
+      continue;
+    }
+    if (sp == 0) break;
+    --sp;
+    stk.load(sp, t);
+    L = (int)((levels >> (2 * sp)) & 3u);
+    levels &= ~(3u << (2 * sp));
+  }
+  return kept;
+}
+
+__device__ __forceinline__ void load_planes(const double* __restrict__ o, Planes& P, double& tol) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    P.nx[i] = o[4 * i + 0];
+    P.ny[i] = o[4 * i + 1];
+    P.nz[i] = o[4 * i + 2];
+    P.c[i] = o[4 * i + 3];
+  }
+  tol = o[16];
+}
+
+__device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    t.x[k] = v[3 * k + 0];
+    t.y[k] = v[3 * k + 1];
+    t.z[k] = v[3 * k + 2];
+  }
+}
+
+__global__ void __launch_bounds__(kTetBlock) k_clip_tets(int64_t npairs, const int32_t* __restrict__ pa,
+                                                         const int32_t* __restrict__ pb,
+                                                         const double* __restrict__ coords_a,
+                                                         const double* __restrict__ tol_a,
+                                                         const double* __restrict__ setup_b,
+                                                         double* pair_measure, int32_t* pair_nout,
+                                                         Partial* partials) {
+  extern __shared__ double stack_mem[];
+  TetStack<kTetBlock> stk{stack_mem + threadIdx.x};
+  double sum = 0.0, err = 0.0;
+  unsigned long long ni = 0, no = 0;
+  for (int64_t i = (int64_t)blockIdx.x * kTetBlock + threadIdx.x; i < npairs;
+       i += (int64_t)gridDim.x * kTetBlock) {
+    const int a = pa[i], b = pb[i];
+    Tet t;
+    load_tet(coords_a + (int64_t)a * 12, t);
+    Planes P;
+    double tolb;
+    load_planes(setup_b + (int64_t)b * kSetup3, P, tolb);
+    const double tol = fmin(tol_a[a], tolb);
+    double m = 0.0;
+    const int n = clip_tet_dfs(t, P, tol, stk, [&](const Tet& o) { m = m + tet_volume_v1(o); });
+    pair_measure[i] = m;
+    pair_nout[i] = n;
+    cs_add(sum, err, m);
+    ni += n > 0;
+    no += n;
+  }
+  block_reduce_partial<kTetBlock>(sum, err, ni, no, &partials[blockIdx.x]);
+}
+
+int clip_grid_blocks(int dim) {
+  if (dim == 2) return sm_count() * 8;
+  return sm_count() * 3;
+}
+
+cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
+                        const double* coords_a, const double* tol_a, const double* setup_b,
+                        double* pair_measure, int32_t* pair_nout, Partial* partials,
+                        int32_t* overflow_list, int* overflow_count, cudaStream_t s) {
+  const int g = clip_grid_blocks(dim);
+  count_launch();
+  if (dim == 2) {
+    k_clip_tris<<<g, kTriBlock, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure,
+                                        pair_nout, partials, overflow_list, overflow_count);
+  } else {
+    const size_t smem = sizeof(double) * kTetStack * 12 * kTetBlock;
+    k_clip_tets<<<g, kTetBlock, smem, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure,
+                                           pair_nout, partials);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t init_device_attributes() {
+  const int smem = (int)(sizeof(double) * kTetStack * 12 * kTetBlock);
+  return cudaFuncSetAttribute(k_clip_tets, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
+                                  const int32_t* pair_a, const int32_t* pair_b,
+                                  const double* coords_a, const double* tol_a,
+                                  const double* setup_b, double* pair_measure, int32_t* pair_nout,
+                                  Partial* partial, cudaStream_t s) {
+  count_launch();
+  k_clip_tris_wide<<<1, 32, 0, s>>>(overflow_list, overflow_count, cap, pair_a, pair_b, coords_a, tol_a,
+                                    setup_b, pair_measure, pair_nout, partial);
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// K7: finalize totals and per-row sums
+// ======================================================================
+__global__ void k_finalize(const Partial* __restrict__ partials, int np, Partial* out) {
+  if (threadIdx.x != 0) return;
+  Partial p{0.0, 0.0, 0ull, 0ull};
+  for (int b = 0; b < np; ++b) {
+    two_sum_merge(p.sum, p.err, partials[b].sum, partials[b].err);
+    p.n_int += partials[b].n_int;
+    p.n_out += partials[b].n_out;
+  }
+  p.sum = p.sum + p.err;
+  *out = p;
+}
+
+cudaError_t launch_finalize(const Partial* partials, int npartials, Partial* out, cudaStream_t s) {
+  count_launch();
+  k_finalize<<<1, 32, 0, s>>>(partials, npartials, out);
+  return cudaGetLastError();
+}
+
+__global__ void k_row_sums(int64_t nel_a, const int64_t* __restrict__ off, const double* __restrict__ pm,
+                           double* em) {
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < nel_a;
+       a += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int64_t p = off[a]; p < off[a + 1]; ++p) s = s + pm[p];
+    em[a] = s;
+  }
+}
+
+cudaError_t launch_row_sums(int64_t nel_a, const int64_t* offsets, const double* pair_measure,
+                            double* elem_measure, cudaStream_t s) {
+  if (nel_a <= 0) return cudaSuccess;
+  count_launch();
+  k_row_sums<<<grid_for(nel_a, 256, 8), 256, 0, s>>>(nel_a, offsets, pair_measure, elem_measure);
+  return cudaGetLastError();
+}
+
+__global__ void k_i32_to_i64(int64_t n, const int32_t* __restrict__ in, int64_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+
+cudaError_t launch_i32_to_i64(int64_t n, const int32_t* in, int64_t* out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launch();
+  k_i32_to_i64<<<grid_for(n, 256, 8), 256, 0, s>>>(n, in, out);
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// Explicit element pairs (the single-pair C API and its batched form)
+// ======================================================================
+struct TriEmit {
+  double* out;  // [22][3][2] for this pair, or nullptr
+  __device__ __forceinline__ void operator()(int k, double x0, double y0, double x1, double y1, double x2,
+                                             double y2) const {
+    if (!out || k >= 22) return;
+    double* o = out + 6 * k;
+    o[0] = x0;
+    o[1] = y0;
+    o[2] = x1;
+    o[3] = y1;
+    o[4] = x2;
+    o[5] = y2;
+  }
+};
+
+__global__ void k_pairs_tris(int64_t n, const double* __restrict__ A, const double* __restrict__ B,
+                             double* measure, int32_t* nout, double* out_elems) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* va = A + 6 * i;
+    const double* vb = B + 6 * i;
+    Lines L;
+    tri_lines(vb, L);
+    const double tol = 10.0 * fmin(spacing(tri_area(va[0], va[1], va[2], va[3], va[4], va[5])),
+                                   spacing(tri_area(vb[0], vb[1], vb[2], vb[3], vb[4], vb[5])));
+    LocalPoly<kTriWideCap> p, q;
+    double m;
+    int k = clip_tri(va[0], va[1], va[2], va[3], va[4], va[5], L, tol, p, q, kTriWideCap, m,
+                     TriEmit{out_elems ? out_elems + 22 * 6 * i : nullptr});
+    if (k < 0) {
+      k = 0;
+      m = 0.0;
+    }
+    if (measure) measure[i] = m;
+    if (nout) nout[i] = k;
+  }
+}
+
+__global__ void k_pairs_tets(int64_t n, const double* __restrict__ A, const double* __restrict__ B,
+                             double* measure, int32_t* nout, double* out_elems) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    Tet ta, tb;
+    load_tet(A + 12 * i, ta);
+    load_tet(B + 12 * i, tb);
+    Planes P;
+    tet_planes(tb, P);
+    const double tol = 10.0 * fmin(spacing(tet_volume_v4(ta)), spacing(tet_volume_v4(tb)));
+    TetStackLocal stk;
+    double m = 0.0;
+    int idx = 0;
+    double* o = out_elems ? out_elems + (int64_t)81 * 12 * i : nullptr;
+    const int k = clip_tet_dfs(ta, P, tol, stk, [&](const Tet& t) {
+      m = m + tet_volume_v1(t);
+      if (o && idx < 81) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          o[12 * idx + 3 * v + 0] = t.x[v];
+          o[12 * idx + 3 * v + 1] = t.y[v];
+          o[12 * idx + 3 * v + 2] = t.z[v];
+        }
+      }
+      ++idx;
+    });
+    if (measure) measure[i] = m;
+    if (nout) nout[i] = k;
+  }
+}
+
+cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const double* b,
+                                  double* measure, int32_t* nout, double* out_elems,
+                                  cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int B = 128;
+  const int g = grid_for(n, B, 8);
+  count_launch();
+  if (dim == 2)
+    k_pairs_tris<<<g, B, 0, s>>>(n, a, b, measure, nout, out_elems);
+  else
+    k_pairs_tets<<<g, B, 0, s>>>(n, a, b, measure, nout, out_elems);
+  return cudaGetLastError();
+}
+
+__global__ void k_measure_explicit(int dim, int64_t n, const double* __restrict__ e, double* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (dim == 2) {
+      const double* v = e + 6 * i;
+      out[i] = tri_area(v[0], v[1], v[2], v[3], v[4], v[5]);
+    } else {
+      Tet t;
+      load_tet(e + 12 * i, t);
+      out[i] = tet_volume_v1(t);
+    }
+  }
+}
+
+cudaError_t launch_measure_explicit(int dim, int64_t n, const double* elems, double* out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launch();
+  k_measure_explicit<<<grid_for(n, 256, 8), 256, 0, s>>>(dim, n, elems, out);
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// K8: P1-P1 mixed mass matrix
+// ======================================================================
+// P1 basis on a triangle (test_parallel_p1_inner_product_2d.F90:206-229).
+__device__ __forceinline__ void p1_basis_2d(const double* cc, double x, double y, double f[3]) {
+  const double e1x = cc[2] - cc[0], e1y = cc[3] - cc[1];
+  const double e2x = cc[4] - cc[0], e2y = cc[5] - cc[1];
+  double j11 = e2y, j12 = -e2x, j21 = -e1y, j22 = e1x;
+  const double det = j11 * j22 - j12 * j21;
+  j11 = j11 / det;
+  j12 = j12 / det;
+  j21 = j21 / det;
+  j22 = j22 / det;
+  const double dx = x - cc[0], dy = y - cc[1];
+  f[1] = j11 * dx + j12 * dy;
+  f[2] = j21 * dx + j22 * dy;
+  f[0] = 1.0 - f[1] - f[2];
+}
+
+// P1 basis on a tetrahedron: Gaussian elimination with partial pivoting in
+// the order of test_parallel_p1_inner_product_3d.F90:215-250.
+__device__ __forceinline__ void p1_basis_3d(const double* cc, double x, double y, double z, double f[4]) {
+  double m[3][4];
+  const double xx[3] = {x, y, z};
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m[r][c] = cc[3 * (c + 1) + r] - cc[r];
+    m[r][3] = xx[r] - cc[r];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    int j = i;
+    double best = fabs(m[i][i]);
+#pragma unroll
+    for (int k = i + 1; k < 3; ++k)
+      if (fabs(m[k][i]) > best) {
+        best = fabs(m[k][i]);
+        j = k;
+      }
+    // swap rows i and j (registers: select-based)
+#pragma unroll
+    for (int k = i + 1; k < 3; ++k) {
+      if (j == k) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const double t = m[i][c];
+          m[i][c] = m[k][c];
+          m[k][c] = t;
+        }
+      }
+    }
+    const double piv = m[i][i];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) m[i][c] = m[i][c] / piv;
+#pragma unroll
+    for (int k = i + 1; k < 3; ++k) {
+      const double fk = m[k][i];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) m[k][c] = m[k][c] - fk * m[i][c];
+    }
+  }
+#pragma unroll
+  for (int i = 2; i >= 0; --i)
+#pragma unroll
+    for (int k = i - 1; k >= 0; --k) {
+      const double fk = m[k][i];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) m[k][c] = m[k][c] - fk * m[i][c];
+    }
+  f[1] = m[0][3];
+  f[2] = m[1][3];
+  f[3] = m[2][3];
+  f[0] = 1.0 - f[1] - f[2] - f[3];
+}
+
+template <typename IDX>
+__device__ __forceinline__ int64_t node_of(const void* en, int64_t e, int loc, int k) {
+  return (int64_t)((const IDX*)en)[e * loc + k];
+}
+
+template <int DIM, typename IDX>
+__global__ void __launch_bounds__(128) k_p1_mass(int64_t npairs, const int32_t* __restrict__ pa,
+                                                 const int32_t* __restrict__ pb,
+                                                 const double* __restrict__ coords_a,
+                                                 const double* __restrict__ tol_a,
+                                                 const double* __restrict__ coords_b,
+                                                 const double* __restrict__ setup_b, const void* en_a,
+                                                 const void* en_b, const double* __restrict__ u_a,
+                                                 const double* __restrict__ v_b, double* blocks,
+                                                 Partial* partials) {
+  constexpr int LOC = DIM + 1;
+  double sum = 0.0, err = 0.0;
+  unsigned long long ni = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npairs;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int a = pa[i], b = pb[i];
+    const double* ca = coords_a + (int64_t)a * LOC * DIM;
+    const double* cb = coords_b + (int64_t)b * LOC * DIM;
+    double blk[LOC * LOC];
+#pragma unroll
+    for (int j = 0; j < LOC * LOC; ++j) blk[j] = 0.0;
+    if (DIM == 2) {
+      Lines L;
+      double tolb;
+      load_lines(setup_b + (int64_t)b * kSetup2, L, tolb);
+      const double tol = fmin(tol_a[a], tolb);
+      LocalPoly<kTriWideCap> p, q;
+      double m;
+      const double qp0 = 4.0 / 6.0, qp1 = 1.0 / 6.0;
+      clip_tri(ca[0], ca[1], ca[2], ca[3], ca[4], ca[5], L, tol, p, q, kTriWideCap, m,
+               [&](int, double x0, double y0, double x1, double y1, double x2, double y2) {
+                 const double meas = tri_area(x0, y0, x1, y1, x2, y2);
+                 const double w = (1.0 / 3.0) * meas;
+#pragma unroll
+                 for (int qq = 0; qq < 3; ++qq) {
+                   const double w0 = qq == 0 ? qp0 : qp1;
+                   const double w1 = qq == 1 ? qp0 : qp1;
+                   const double w2 = qq == 2 ? qp0 : qp1;
+                   const double x = (w0 * x0 + w1 * x1) + w2 * x2;
+                   const double y = (w0 * y0 + w1 * y1) + w2 * y2;
+                   double fa[3], fb[3];
+                   p1_basis_2d(ca, x, y, fa);
+                   p1_basis_2d(cb, x, y, fb);
+#pragma unroll
+                   for (int r = 0; r < 3; ++r)
+#pragma unroll
+                     for (int c = 0; c < 3; ++c) blk[r * 3 + c] += w * fa[r] * fb[c];
+                 }
+               });
+    } else {
+      Tet t;
+      load_tet(ca, t);
+      Planes P;
+      double tolb;
+      load_planes(setup_b + (int64_t)b * kSetup3, P, tolb);
+      const double tol = fmin(tol_a[a], tolb);
+      TetStackLocal stk;
+      const double qa = 5.8541019662496852e-1, qb = 1.3819660112501050e-1;
+      clip_tet_dfs(t, P, tol, stk, [&](const Tet& o) {
+        const double meas = tet_volume_v1(o);
+        const double w = 0.25 * meas;
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+          double xq[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const double* comp = d == 0 ? o.x : (d == 1 ? o.y : o.z);
+            double s = 0.0;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) s = s + (v == qq ? qa : qb) * comp[v];
+            xq[d] = s;
+          }
+          double fa[4], fb[4];
+          p1_basis_3d(ca, xq[0], xq[1], xq[2], fa);
+          p1_basis_3d(cb, xq[0], xq[1], xq[2], fb);
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) blk[r * 4 + c] += w * fa[r] * fb[c];
+        }
+      });
+    }
+    if (blocks) {
+#pragma unroll
+      for (int j = 0; j < LOC * LOC; ++j) blocks[i * LOC * LOC + j] = blk[j];
+    }
+    if (u_a && v_b) {
+      double s = 0.0;
+#pragma unroll
+      for (int r = 0; r < LOC; ++r) {
+        const double ur = u_a[node_of<IDX>(en_a, a, LOC, r)];
+#pragma unroll
+        for (int c = 0; c < LOC; ++c) s += ur * blk[r * LOC + c] * v_b[node_of<IDX>(en_b, b, LOC, c)];
+      }
+      cs_add(sum, err, s);
+    }
+    ++ni;
+  }
+  block_reduce_partial<128>(sum, err, ni, 0ull, &partials[blockIdx.x]);
+}
+
+int p1_grid_blocks(int dim) { return sm_count() * (dim == 2 ? 4 : 2); }
+
+cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
+                           const double* coords_a, const double* tol_a, const double* coords_b,
+                           const double* setup_b, const void* enlist_a, const void* enlist_b,
+                           int idx_bytes, const double* u_a, const double* v_b, double* blocks,
+                           Partial* partials, cudaStream_t s) {
+  const int g = p1_grid_blocks(dim);
+  count_launch();
+  if (dim == 2 && idx_bytes == 4)
+    k_p1_mass<2, int32_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+  else if (dim == 2)
+    k_p1_mass<2, int64_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+  else if (idx_bytes == 4)
+    k_p1_mass<3, int32_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+  else
+    k_p1_mass<3, int64_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+  return cudaGetLastError();
+}
+
+}  // namespace lsm

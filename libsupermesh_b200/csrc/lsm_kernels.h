@@ -1,0 +1,117 @@
+// Host-side launchers for the supermesh kernels (all asynchronous on the
+// given stream).  Device buffers are owned by the caller (lsm_capi.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace lsm {
+
+// Per-element records written by the prep kernels.
+//   coords  [nel][loc*dim]  float64 vertex coordinates (gathered)
+//   box64   [nel][2*dim]    float64 AABB (lo..., hi...)
+//   box32   [nel][8]        float32 AABB rounded outwards (lo.xyz, pad, hi.xyz, pad)
+//   setup   [nel][kSetup]   clip setup of a B element: 2D lines (12) or 3D
+//                           planes (16), then tol = 10*spacing(measure)
+//   tolv    [nel]           10*spacing(measure) (A elements)
+constexpr int kSetup2 = 13;
+constexpr int kSetup3 = 17;
+
+// Per-block partial of a narrow-phase launch: compensated measure sum,
+// intersecting pairs and output simplices.
+struct Partial {
+  double sum;
+  double err;
+  unsigned long long n_int;
+  unsigned long long n_out;
+};
+
+// Process-wide count of kernel launches issued by this library.
+unsigned long long launches();
+
+struct BVH {
+  int n = 0;                 // leaves
+  float4* lo_left = nullptr;  // [2n-1]: lo.xyz, .w = left child / element (int bits)
+  float4* hi_esc = nullptr;   // [2n-1]: hi.xyz, .w = escape node (int bits), -1 = end
+};
+
+// Mesh prep: gather coordinates, boxes, measures/tolerances, B clip setup.
+// idx_bytes selects the enlist element type (4 = int32, 8 = int64).
+cudaError_t launch_prep(int dim, int loc, int64_t nel, const double* pos, const void* enlist, int idx_bytes,
+                        double* coords, double* box64, float* box32, double* tolv, double* setup,
+                        int* bad_index, int64_t nnodes, cudaStream_t s);
+
+// Root box (float64) of a set of element boxes: rootbox[2*dim].
+cudaError_t launch_root_box(int dim, int64_t nel, const double* box64, double* partial,
+                            int partial_cap, double* rootbox, cudaStream_t s);
+
+cudaError_t launch_morton(int dim, int64_t nel, const double* box64, const double* rootbox,
+                          uint32_t* keys, int32_t* vals, cudaStream_t s);
+
+// Stable LSD radix sort of (key, val) pairs, 8 bits per pass over the low
+// `bits` bits.  tmp buffers must hold n entries; hist must hold
+// radix_hist_entries(n).  Result ends in keys/vals.
+int64_t radix_hist_entries(int64_t n);
+cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals, uint32_t* keys_tmp,
+                             int32_t* vals_tmp, uint32_t* hist, cudaStream_t s);
+
+// LBVH over sorted Morton codes.  work_int needs 8*n ints.
+cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const int32_t* sorted_vals,
+                             const float* box32, BVH bvh, int* work_int, cudaStream_t s);
+
+// Candidate search.  Pass 1 (fill=false) writes counts[nel_a]; pass 2 writes
+// pair_a/pair_b at offsets[a].
+cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_a, BVH bvh,
+                         const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
+                         int32_t* pair_b, cudaStream_t s);
+
+// Exclusive scan of int32 counts into int64 offsets[n+1] (offsets[n] = total).
+int64_t scan_tmp_entries(int64_t n);
+cudaError_t launch_scan(int64_t n, const int* counts, int64_t* offsets, int64_t* tmp, cudaStream_t s);
+
+// Narrow phase over candidate pairs.  pair_measure/pair_nout are per pair;
+// partials receives (sum, err) per block for the compensated total.
+// overflow_list collects pairs whose polygon outgrew the fast-path buffers
+// (2D only); they are re-run by launch_clip_tris_wide.
+int clip_grid_blocks(int dim);
+cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
+                        const double* coords_a, const double* tol_a, const double* setup_b,
+                        double* pair_measure, int32_t* pair_nout, Partial* partials,
+                        int32_t* overflow_list, int* overflow_count, cudaStream_t s);
+// Opt-in shared-memory limits for the clip kernels on the current device.
+cudaError_t init_device_attributes();
+cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
+                                  const int32_t* pair_a, const int32_t* pair_b,
+                                  const double* coords_a, const double* tol_a,
+                                  const double* setup_b, double* pair_measure, int32_t* pair_nout,
+                                  Partial* partial, cudaStream_t s);
+
+// Totals: merge of the per-block partials into out[0] (in order).
+cudaError_t launch_finalize(const Partial* partials, int npartials, Partial* out, cudaStream_t s);
+
+// Per-A-element measure: sum of pair measures over each CSR row, in order.
+cudaError_t launch_row_sums(int64_t nel_a, const int64_t* offsets, const double* pair_measure,
+                            double* elem_measure, cudaStream_t s);
+
+// Convert int32 CSR to int64 (C API output).
+cudaError_t launch_i32_to_i64(int64_t n, const int32_t* in, int64_t* out, cudaStream_t s);
+
+// Single-pair style batched intersections over explicit element arrays
+// (tri: [n][3][2]; tet: [n][4][3]).  out_elems optional ([n][22][3][2] or
+// [n][81][4][3]).
+cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const double* b,
+                                  double* measure, int32_t* nout, double* out_elems,
+                                  cudaStream_t s);
+cudaError_t launch_measure_explicit(int dim, int64_t n, const double* elems, double* out,
+                                    cudaStream_t s);
+
+// P1-P1 mixed mass blocks per candidate pair and u^T M v partials.
+cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
+                           const double* coords_a, const double* tol_a, const double* coords_b,
+                           const double* setup_b, const void* enlist_a, const void* enlist_b,
+                           int idx_bytes, const double* u_a, const double* v_b, double* blocks,
+                           Partial* partials, cudaStream_t s);
+int p1_grid_blocks(int dim);
+
+}  // namespace lsm

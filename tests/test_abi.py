@@ -1,0 +1,86 @@
+"""The CUDA library loads and exports every function include/*.h declares
+(CPU-only: no device calls)."""
+import ctypes
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+DECL = re.compile(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(libsupermesh_\w+)\s*\(", re.M)
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in DECL.finditer(text):
+            line = text[m.start():text.index("(", m.start())]
+            if "static" in line or "#define" in line:
+                continue
+            names.add(m.group(1))
+    return names
+
+
+@pytest.fixture(scope="module")
+def lib():
+    sys.path.insert(0, str(ROOT))
+    from libsupermesh_b200 import build
+
+    build.build()
+    return ctypes.CDLL(str(build.OUT))
+
+
+def test_headers_declare_the_reference_api():
+    names = declared_symbols()
+    # the 14 entries of libsupermesh-c.h upstream
+    ref = {"libsupermesh_sort_intersection_finder_set_input", "libsupermesh_sort_intersection_finder_query_output",
+           "libsupermesh_sort_intersection_finder_get_output", "libsupermesh_tree_intersection_finder_set_input",
+           "libsupermesh_tree_intersection_finder_query_output", "libsupermesh_tree_intersection_finder_get_output",
+           "libsupermesh_intersect_tris_real", "libsupermesh_intersect_tets_real", "libsupermesh_triangle_area",
+           "libsupermesh_tetrahedron_volume", "libsupermesh_interval_size", "libsupermesh_intersect_intervals",
+           "libsupermesh_intersect_tet_hex", "libsupermesh_intersect_tri_quad"}
+    assert ref <= names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [n for n in sorted(declared_symbols()) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_library_is_sm100a_cuda(lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(ROOT / "libsupermesh_b200" / "lib" / "libsupermesh.so")],
+                         capture_output=True, text=True, check=True).stdout
+    assert "libsupermesh_gpu_supermesh" in out
+
+
+def test_context_create_without_gpu_fails_cleanly(lib):
+    """On a machine without a usable GPU the GPU API returns a status code;
+    it neither crashes nor silently computes on the CPU."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present; covered by the gpu tests")
+    h = ctypes.c_void_p()
+    lib.libsupermesh_gpu_context_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    st = lib.libsupermesh_gpu_context_create(0, ctypes.byref(h))
+    assert st == 5 and not h.value  # LSM_ERROR_CUDA
+
+
+def test_legacy_api_without_gpu_aborts_loudly():
+    """The drop-in entries have no status channel: like libsupermesh_abort
+    they print and exit(1) when no device is usable."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "import libsupermesh_b200 as L\n"
+        "print(L.triangle_area([[0,0],[1,0],[0,1]]))\n" % str(ROOT))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1
+    assert "libsupermesh (B200) error" in r.stderr

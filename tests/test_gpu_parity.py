@@ -1,0 +1,266 @@
+"""GPU parity: the CUDA library against the CPU oracle and the reference's
+known answers.  All calls go through the C-ABI (libsupermesh_b200 is a
+ctypes binding of lib/libsupermesh.so).
+
+Bars (from the path's correctness contract):
+  * candidate sets per A element: identical to the oracle's quadtree/octree
+    set (integer work: exact);
+  * number of output simplices per pair and the intersecting-pair set:
+    exact;
+  * per-pair measure: relative difference <= 1e-12 (the clipped vertices
+    are computed with the reference's FP64 operation order, so in practice
+    they agree bit for bit);
+  * totals: |total - oracle total| <= 1e-12 and, for meshes that tile the
+    same domain, |total - domain measure| <= 1e-12.
+"""
+import numpy as np
+import pytest
+
+import libsupermesh_b200 as lsm
+from libsupermesh_b200 import meshes as M
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-12
+
+
+def rows(ip, ind):
+    return [np.sort(ind[ip[a]:ip[a + 1]]) for a in range(len(ip) - 1)]
+
+
+def pair_table(ip, ind, *vals):
+    """Sort pairs by (row, b) so GPU and oracle orders line up."""
+    r = np.repeat(np.arange(len(ip) - 1), np.diff(ip))
+    order = np.lexsort((ind, r))
+    return (r[order], np.asarray(ind)[order]) + tuple(np.asarray(v)[order] for v in vals)
+
+
+def check_pipeline(ctx, oracle, dim, A, B, domain=None):
+    ip_o, ind_o = oracle.tree_finder(dim, A, B)
+    pm_o, pn_o, em_o, st_o = oracle.narrow(dim, A, B, ip_o, ind_o, nthreads=oracle.lib().orc_num_threads_available())
+    st, em = ctx.supermesh(A, B, elem_measure=True)
+    n = st.n_candidates
+    assert n == len(ind_o)
+    ip_g, ind_g = ctx.get_candidates(len(A[1]), n)
+    assert np.array_equal(ip_g, ip_o)
+    pm_g, pn_g = ctx.pair_results(n)
+    ro, bo, mo, no = pair_table(ip_o, ind_o, pm_o, pn_o)
+    rg, bg, mg, ng = pair_table(ip_g, ind_g, pm_g, pn_g)
+    assert np.array_equal(ro, rg) and np.array_equal(bo, bg), "candidate sets differ"
+    assert np.array_equal(no, ng), "output simplex counts differ"
+    scale = np.maximum(np.abs(mo), 1e-300)
+    rel = np.abs(mg - mo) / scale
+    assert rel.max(initial=0.0) <= REL_TOL
+    # intersecting-pair set, with and without the 1e-14 element-measure filter
+    assert np.array_equal(no > 0, ng > 0)
+    assert st.n_intersecting == int((no > 0).sum())
+    assert st.n_out_simplices == int(no.sum())
+    assert abs(st.total_measure - st_o.total) <= REL_TOL
+    if domain is not None:
+        assert abs(st.total_measure - domain) <= REL_TOL
+    assert np.abs(em - em_o).max(initial=0.0) <= REL_TOL * max(1.0, np.abs(em_o).max(initial=0.0))
+    return st
+
+
+@pytest.mark.parametrize("name", ["small2d_7x9", "small2d_40x31", "small3d_4x5", "small3d_9x7"])
+def test_small_configs(gpu_ctx, oracle_mod, name):
+    dim, A, B = M.config_meshes(name)
+    check_pipeline(gpu_ctx, oracle_mod, dim, A, B, domain=1.0)
+
+
+def test_config_tri2d_73x100_full(gpu_ctx, oracle_mod):
+    dim, A, B = M.config_meshes("tri2d_73x100")
+    st = check_pipeline(gpu_ctx, oracle_mod, dim, A, B, domain=1.0)
+    assert st.n_candidates > 100000
+
+
+def test_config_tet3d_27x32_full(gpu_ctx, oracle_mod):
+    dim, A, B = M.config_meshes("tet3d_27x32")
+    st = check_pipeline(gpu_ctx, oracle_mod, dim, A, B, domain=1.0)
+    assert st.n_candidates > 10_000_000
+
+
+def test_int64_and_int32_enlists_agree(gpu_ctx):
+    dim, A, B = M.config_meshes("small3d_5x6")
+    s32, _ = gpu_ctx.supermesh(A, B)
+    A64 = (A[0], A[1].astype(np.int64))
+    B64 = (B[0], B[1].astype(np.int64))
+    s64, _ = gpu_ctx.supermesh(A64, B64)
+    assert s32.as_dict() == s64.as_dict()
+
+
+def test_reference_known_answers(gpu_ctx, oracle_mod, ref_meshes):
+    # test_tri_intersector.F90:104 and test_tet_intersector.F90:104
+    st, _ = gpu_ctx.supermesh(ref_meshes("triangle_0_01"), ref_meshes("square_0_01"))
+    assert oracle_mod.fequals(st.total_measure, 0.5)
+    st, _ = gpu_ctx.supermesh(ref_meshes("pyramid_0_05"), ref_meshes("cube_0_05"))
+    assert oracle_mod.fequals(st.total_measure, 1.0 / 3.0)
+
+
+@pytest.mark.parametrize("dim,na,nb", [(2, "square.1", "square.2"), (3, "cube.1", "cube.2")])
+def test_reference_completeness(gpu_ctx, oracle_mod, ref_meshes, dim, na, nb):
+    # test_intersection_finder_completeness_{2d,3d}.F90: rows are B elements
+    MA, MB = ref_meshes(na), ref_meshes(nb)
+    st, em = gpu_ctx.supermesh(MB, MA, elem_measure=True)
+    for b in range(len(MB[1])):
+        v = MB[0][MB[1][b]]
+        own = oracle_mod.triangle_area(v) if dim == 2 else oracle_mod.tetrahedron_volume(v)
+        assert oracle_mod.fequals(own, em[b])
+    check_pipeline(gpu_ctx, oracle_mod, dim, MB, MA)
+
+
+def test_reference_tiny_candidate_sets(gpu_ctx, ref_meshes):
+    t1, t2, tet = ref_meshes("triangle.1"), ref_meshes("triangle.2"), ref_meshes("tet")
+    ip, ind = lsm.tree_intersection_finder(*t1, *t1)
+    assert list(ind) == [0] and list(ip) == [0, 1]
+    ip, ind = lsm.tree_intersection_finder(*t1, *t2)
+    assert sorted(ind) == [0, 1, 2]
+    ip, ind = lsm.tree_intersection_finder(*t2, *t2)
+    for i in range(3):
+        assert i in set(ind[ip[i]:ip[i + 1]])
+    ip, ind = lsm.tree_intersection_finder(*tet, *tet)
+    assert list(ind) == [0]
+
+
+def test_legacy_tree_finder_matches_oracle(oracle_mod):
+    for name in ("small2d_11x13", "small3d_5x4"):
+        dim, A, B = M.config_meshes(name)
+        ip, ind = lsm.tree_intersection_finder(A[0], A[1], B[0], B[1])
+        ip_o, ind_o = oracle_mod.tree_finder(dim, A, B)
+        assert np.array_equal(ip, ip_o)
+        for r_g, r_o in zip(rows(ip, ind), rows(ip_o, ind_o)):
+            assert np.array_equal(r_g, r_o)
+
+
+def test_legacy_tree_finder_quads(oracle_mod):
+    # the tree finder accepts any element type (here quads, loc 4)
+    n = 6
+    idx = np.arange(n + 1)
+    jj, ii = np.meshgrid(idx, idx, indexing="ij")
+    pos = np.stack([ii.ravel() / n, jj.ravel() / n], axis=1).astype(np.float64)
+    cj, ci = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    v00 = (cj * (n + 1) + ci).ravel()
+    quads = np.stack([v00, v00 + 1, v00 + n + 2, v00 + n + 1], axis=1).astype(np.int32)
+    _, B = M.grid2d(5, 0, 0.3), M.grid2d(5, 0, 0.3)
+    ip, ind = lsm.tree_intersection_finder(pos, quads, *B)
+    ip_o, ind_o = oracle_mod.brute_force_finder(2, (pos, quads), B)
+    assert np.array_equal(ip, ip_o)
+    for r_g, r_o in zip(rows(ip, ind), rows(ip_o, ind_o)):
+        assert np.array_equal(r_g, r_o)
+
+
+def _random_pairs(dim, n, seed):
+    rng = np.random.default_rng(seed)
+    per = (3, 2) if dim == 2 else (4, 3)
+    a = rng.random((n,) + per)
+    b = rng.random((n,) + per) * 0.8 + 0.1
+    # include identical and shared-vertex pairs
+    b[: n // 8] = a[: n // 8]
+    b[n // 8: n // 4, 0] = a[n // 8: n // 4, 0]
+    return a, b
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_intersect_pairs_bitexact(gpu_ctx, oracle_mod, dim):
+    a, b = _random_pairs(dim, 400, 7 + dim)
+    m, k, e = gpu_ctx.intersect_pairs(dim, a, b, want_elems=True)
+    for i in range(len(a)):
+        ref = oracle_mod.intersect_tris(a[i], b[i]) if dim == 2 else oracle_mod.intersect_tets(a[i], b[i])
+        assert k[i] == len(ref)
+        assert np.array_equal(e[i, : k[i]], ref), i
+        meas = 0.0
+        for o in ref:
+            meas += oracle_mod.triangle_area(o) if dim == 2 else oracle_mod.tetrahedron_volume(o)
+        assert m[i] == meas
+
+
+def test_legacy_single_pair_entries(oracle_mod):
+    a, b = _random_pairs(2, 16, 3)
+    for i in range(len(a)):
+        assert np.array_equal(lsm.intersect_tris_real(a[i], b[i]), oracle_mod.intersect_tris(a[i], b[i]))
+        assert lsm.triangle_area(a[i]) == oracle_mod.triangle_area(a[i])
+    a, b = _random_pairs(3, 16, 4)
+    for i in range(len(a)):
+        assert np.array_equal(lsm.intersect_tets_real(a[i], b[i]), oracle_mod.intersect_tets(a[i], b[i]))
+        assert lsm.tetrahedron_volume(a[i]) == oracle_mod.tetrahedron_volume(a[i])
+
+
+def test_p1_mass_reference_answers(gpu_ctx, oracle_mod, ref_meshes):
+    A, B = ref_meshes("triangle_0_01"), ref_meshes("square_0_01")
+    integral, _ = gpu_ctx.p1_mass(A, B, A[0][:, 0], B[0][:, 1])
+    assert oracle_mod.fequals(integral, 8.3333333333333398e-2)
+    A, B = ref_meshes("pyramid_0_05"), ref_meshes("cube_0_05")
+    integral, _ = gpu_ctx.p1_mass(A, B, A[0][:, 0] + A[0][:, 2], B[0][:, 1])
+    assert oracle_mod.fequals(integral, 1.2499999999999989e-1)
+
+
+@pytest.mark.parametrize("name", ["small2d_12x17", "small3d_4x5"])
+def test_p1_mass_blocks_match_oracle(gpu_ctx, oracle_mod, name):
+    dim, A, B = M.config_meshes(name)
+    u = np.cos(3 * A[0][:, 0]) + A[0][:, 1]
+    v = np.sin(2 * B[0][:, 1]) - B[0][:, 0]
+    integral, blocks = gpu_ctx.p1_mass(A, B, u, v, want_blocks=True)
+    ip_g, ind_g = gpu_ctx.get_candidates(len(A[1]), len(blocks))
+    ip_o, ind_o = oracle_mod.tree_finder(dim, A, B)
+    i_o, _, blocks_o = oracle_mod.p1_mass(dim, A, B, ip_o, ind_o, u, v, want_blocks=True)
+    assert abs(integral - i_o) <= 1e-12 * max(1.0, abs(i_o))
+    ro, bo, ko = pair_table(ip_o, ind_o, np.arange(len(ind_o)))
+    rg, bg, kg = pair_table(ip_g, ind_g, np.arange(len(ind_g)))
+    assert np.array_equal(bo, bg)
+    diff = np.abs(blocks[kg] - blocks_o[ko]).max(initial=0.0)
+    assert diff <= 1e-12 * max(1e-300, np.abs(blocks_o).max(initial=0.0))
+
+
+def test_empty_and_single_element_meshes(gpu_ctx):
+    dim, A, B = M.config_meshes("small2d_3x4")
+    empty = (A[0], np.zeros((0, 3), dtype=np.int32))
+    st, em = gpu_ctx.supermesh(empty, B, elem_measure=True)
+    assert st.n_candidates == 0 and st.total_measure == 0.0
+    st, em = gpu_ctx.supermesh(A, (B[0], np.zeros((0, 3), dtype=np.int32)), elem_measure=True)
+    assert st.n_candidates == 0 and (em == 0).all()
+    one = (np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]]), np.array([[0, 1, 2]], dtype=np.int32))
+    st, em = gpu_ctx.supermesh(one, one, elem_measure=True)
+    assert st.n_candidates == 1 and st.n_intersecting == 1 and abs(st.total_measure - 0.5) < 1e-15
+
+
+def test_touching_boxes_are_not_candidates(gpu_ctx):
+    A = (np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]]), np.array([[0, 1, 2]], dtype=np.int32))
+    B = (np.array([[1.0, 0.0], [2.0, 0.0], [1.0, 1.0]]), np.array([[0, 1, 2]], dtype=np.int32))
+    assert gpu_ctx.find_candidates(A, B) == 0
+
+
+def test_invalid_input_is_reported(gpu_ctx):
+    dim, A, B = M.config_meshes("small2d_3x4")
+    bad = (A[0], A[1].copy())
+    bad[1][0, 0] = len(A[0]) + 5
+    with pytest.raises(lsm.LsmError) as e:
+        gpu_ctx.supermesh(bad, B)
+    assert e.value.status == 1
+    with pytest.raises(lsm.LsmError):
+        gpu_ctx.supermesh(A, M.config_meshes("small3d_2x2")[1])
+    # the context stays usable after an error
+    st, _ = gpu_ctx.supermesh(A, B)
+    assert abs(st.total_measure - 1.0) < 1e-12
+
+
+def test_device_resident_inputs(gpu_ctx):
+    torch = pytest.importorskip("torch")
+    dim, A, B = M.config_meshes("small3d_6x7")
+    ref, em_ref = gpu_ctx.supermesh(A, B, elem_measure=True)
+    dev = torch.device("cuda:0")
+    tA = (torch.from_numpy(A[0]).to(dev), torch.from_numpy(A[1]).to(dev))
+    tB = (torch.from_numpy(B[0]).to(dev), torch.from_numpy(B[1]).to(dev))
+    out = torch.zeros(len(A[1]), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    st, _ = gpu_ctx.supermesh(tA, tB, elem_measure=True, on_device=True, out=out)
+    assert st.as_dict() == ref.as_dict()
+    assert np.array_equal(out.cpu().numpy(), em_ref)
+
+
+def test_batched_matches_single(gpu_ctx):
+    pairs = M.batched_pairs(6, seed=6, emin=2e2, emax=2e3)
+    totals, nc, ni = gpu_ctx.supermesh_batched([(A, B) for _, A, B in pairs])
+    for i, (dim, A, B) in enumerate(pairs):
+        st, _ = gpu_ctx.supermesh(A, B)
+        assert totals[i] == st.total_measure and nc[i] == st.n_candidates and ni[i] == st.n_intersecting
+        assert abs(totals[i] - 1.0) <= 1e-12
