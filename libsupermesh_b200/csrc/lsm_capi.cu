@@ -312,27 +312,25 @@ void narrow(Ctx* c, cudaStream_t s) {
   const int64_t nnz = c->ncand;
   double* pm = ensure<double>(c, c->pair_measure, nnz);
   int32_t* pn = ensure<int32_t>(c, c->pair_nout, nnz);
-  const int nblk = lsm::clip_grid_blocks(c->dim);
-  lsm::Partial* part = ensure<lsm::Partial>(c, c->partials, nblk + 1);
+  const int nred = lsm::reduce_pairs_blocks();
+  lsm::Partial* part = ensure<lsm::Partial>(c, c->partials, nred);
   lsm::Partial* tot = ensure<lsm::Partial>(c, c->totals, 1);
-  int32_t* ovf = nullptr;
+  // 2D: overflow list of the fast-path clipper; 3D: list of pairs that
+  // survive the exact early-out.
+  int32_t* ovf = ensure<int32_t>(c, c->ovf_list, nnz);
   int* ovf_count = bad_flag(c) + 2;
-  if (c->dim == 2) {
-    ovf = ensure<int32_t>(c, c->ovf_list, nnz);
-    CU(cudaMemsetAsync(ovf_count, 0, sizeof(int), s));
-  }
+  if (c->dim == 2) CU(cudaMemsetAsync(ovf_count, 0, sizeof(int), s));
+  unsigned long long* work = reinterpret_cast<unsigned long long*>(bad_flag(c) + 8);
   CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                       static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
-                      static_cast<double*>(c->b_setup.p), pm, pn, part, ovf, ovf_count, s));
-  int np = nblk;
-  if (c->dim == 2) {
+                      static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s));
+  if (c->dim == 2)
     CU(lsm::launch_clip_tris_wide(ovf, ovf_count, nnz, static_cast<int32_t*>(c->pair_a.p),
                                   static_cast<int32_t*>(c->pair_b.p), static_cast<double*>(c->a_coords.p),
                                   static_cast<double*>(c->a_tol.p), static_cast<double*>(c->b_setup.p), pm,
-                                  pn, part + nblk, s));
-    np = nblk + 1;
-  }
-  CU(lsm::launch_finalize(part, np, tot, s));
+                                  pn, s));
+  CU(lsm::launch_reduce_pairs(nnz, pm, pn, part, s));
+  CU(lsm::launch_finalize(part, nred, tot, s));
   c->have_pairs = true;
 }
 

@@ -279,138 +279,180 @@ __device__ __forceinline__ V3 interp(const V3& vp, const V3& vn, double dp, doub
   return V3{w0 * vp.x + w1 * vn.x, w0 * vp.y + w1 * vn.y, w0 * vp.z + w1 * vn.z};
 }
 
-// Result of clipping one tet by one plane: up to three children.
-// c0 is written in place of the input; c1, c2 are returned separately.
-struct Split {
-  int k;  // number of children (0..3)
+// Classification of a tet's vertices against one plane
+// (Tetrahedron_Intersection.F90:257-276): zero if |d| < eps, else by sign.
+// Index lists are packed 2 bits per entry in ascending vertex order.
+struct TetClass {
+  double d[4];
+  unsigned negl, posl, zerl;
+  int nn, np;
 };
 
-// Clip tet `t` by plane (nx,ny,nz,c).  On return t holds child 0 (if any)
-// and c1/c2 hold children 1/2, in the reference's output order.
-__device__ __forceinline__ int clip_tet_plane(Tet& t, double nx, double ny, double nz, double c,
-                                              Tet& c1, Tet& c2) {
-  double d[4];
+__device__ __forceinline__ void classify_tet(const Tet& t, double nx, double ny, double nz, double c,
+                                             TetClass& k) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i) d[i] = ((nx * t.x[i] + ny * t.y[i]) + nz * t.z[i]) - c;
-  // Classify: index lists packed 2 bits per entry, in ascending vertex order.
+  for (int i = 0; i < 4; ++i) k.d[i] = ((nx * t.x[i] + ny * t.y[i]) + nz * t.z[i]) - c;
   unsigned negl = 0, posl = 0, zerl = 0;
   int nn = 0, np = 0, nz0 = 0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    if (fabs(d[i]) < kEps) {
-      zerl |= (unsigned)i << (2 * nz0);
-      ++nz0;
-    } else if (d[i] < 0.0) {
-      negl |= (unsigned)i << (2 * nn);
-      ++nn;
-    } else if (d[i] > 0.0) {
-      posl |= (unsigned)i << (2 * np);
-      ++np;
+    const bool zero = fabs(k.d[i]) < kEps;
+    const bool neg = !zero && k.d[i] < 0.0;
+    const bool pos = !zero && k.d[i] > 0.0;
+    zerl |= zero ? (unsigned)i << (2 * nz0) : 0u;
+    negl |= neg ? (unsigned)i << (2 * nn) : 0u;
+    posl |= pos ? (unsigned)i << (2 * np) : 0u;
+    nz0 += zero;
+    nn += neg;
+    np += pos;
+  }
+  k.negl = negl;
+  k.posl = posl;
+  k.zerl = zerl;
+  k.nn = nn;
+  k.np = np;
+}
+
+// Split a tet that has both positive and negative vertices
+// (Tetrahedron_Intersection.F90:290-434).  Returns the number of children
+// (1..3); `t` becomes child 0 and c1, c2 children 1 and 2, in the
+// reference's output order.
+//
+// Every case (+++-, ++-0, +-00, ++--, +---, +--0) creates its new vertices
+// by the same interpolation between a positive and a negative vertex, so the
+// interpolations run in one predicated loop shared by all cases (warp lanes
+// in different cases stay converged for the FP64 work); the cases differ
+// only in which (positive, negative) pairs they interpolate and in how the
+// children are assembled from vertices, which is register moves.
+__device__ __forceinline__ int split_tet(Tet& t, const TetClass& k, Tet& c1, Tet& c2) {
+  const int nn = k.nn, np = k.np;
+  const int n0 = k.negl & 3, n1 = (k.negl >> 2) & 3, n2 = (k.negl >> 4) & 3;
+  const int p0 = k.posl & 3, p1 = (k.posl >> 2) & 3, p2 = (k.posl >> 4) & 3;
+  // interpolation list: entry i = (positive vertex, negative vertex)
+  int ni;
+  unsigned pairs;
+  if (nn == 1) {  // every positive vertex towards n0
+    ni = np;
+    pairs = (unsigned)(p0 | n0 << 2) | (unsigned)(p1 | n0 << 2) << 4 | (unsigned)(p2 | n0 << 2) << 8;
+  } else if (np == 2) {  // ++--: t0 = (p0,n0), t1 = (p1,n0), t2 = (p0,n1), t3 = (p1,n1)
+    ni = 4;
+    pairs = (unsigned)(p0 | n0 << 2) | (unsigned)(p1 | n0 << 2) << 4 | (unsigned)(p0 | n1 << 2) << 8 |
+            (unsigned)(p1 | n1 << 2) << 12;
+  } else {  // +--- / +--0: p0 towards each negative vertex
+    ni = nn;
+    pairs = (unsigned)(p0 | n0 << 2) | (unsigned)(p0 | n1 << 2) << 4 | (unsigned)(p0 | n2 << 2) << 8;
+  }
+  V3 T[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (i < ni) {
+      const int P = (pairs >> (4 * i)) & 3, N = (pairs >> (4 * i + 2)) & 3;
+      T[i] = interp(vget(t, P), vget(t, N), sel4(P, k.d[0], k.d[1], k.d[2], k.d[3]),
+                    sel4(N, k.d[0], k.d[1], k.d[2], k.d[3]));
+    } else {
+      T[i] = V3{0.0, 0.0, 0.0};
     }
   }
-  if (nn == 0) return 0;
-  if (np == 0) return 1;
-  const int n0 = negl & 3;
-  const V3 vn0 = vget(t, n0);
-  const double dn0 = sel4(n0, d[0], d[1], d[2], d[3]);
   if (nn == 1) {
-    // +++-, ++-0, +-00: every positive vertex slides towards the negative one
-    Tet o = t;
+    // +++-, ++-0, +-00: positive vertex of rank r becomes T[r]
+    unsigned pm = 0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (d[k] > 0.0 && !(fabs(d[k]) < kEps)) {
-        const V3 p = interp(V3{t.x[k], t.y[k], t.z[k]}, vn0, d[k], dn0);
-        o.x[k] = p.x;
-        o.y[k] = p.y;
-        o.z[k] = p.z;
+    for (int i = 0; i < 3; ++i)
+      if (i < np) pm |= 1u << ((k.posl >> (2 * i)) & 3);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      if (pm & (1u << v)) {
+        const int r = __popc(pm & ((1u << v) - 1u));
+        const V3 q = r == 0 ? T[0] : (r == 1 ? T[1] : T[2]);
+        t.x[v] = q.x;
+        t.y[v] = q.y;
+        t.z[v] = q.z;
       }
     }
-    t = o;
     return 1;
   }
-  const int p0 = posl & 3;
-  const V3 vp0 = vget(t, p0);
-  const double dp0 = sel4(p0, d[0], d[1], d[2], d[3]);
-  const int n1 = (negl >> 2) & 3;
-  const V3 vn1 = vget(t, n1);
-  const double dn1 = sel4(n1, d[0], d[1], d[2], d[3]);
+  const V3 vn0 = vget(t, n0), vn1 = vget(t, n1);
   if (np == 2) {
-    // ++--
-    const int p1 = (posl >> 2) & 3;
-    const V3 vp1 = vget(t, p1);
-    const double dp1 = sel4(p1, d[0], d[1], d[2], d[3]);
-    const V3 t0 = interp(vp0, vn0, dp0, dn0);
-    const V3 t1 = interp(vp1, vn0, dp1, dn0);
-    const V3 t2 = interp(vp0, vn1, dp0, dn1);
-    const V3 t3 = interp(vp1, vn1, dp1, dn1);
-    // child 1: (v[n1], t3, t2, t1); child 2: (v[n0], t0, t1, t2)
+    // ++--: child 0 = tet with v[p0] = t2, v[p1] = t1;
+    //       child 1 = (v[n1], t3, t2, t1); child 2 = (v[n0], t0, t1, t2)
     vset(c1, 0, vn1);
-    vset(c1, 1, t3);
-    vset(c1, 2, t2);
-    vset(c1, 3, t1);
+    vset(c1, 1, T[3]);
+    vset(c1, 2, T[2]);
+    vset(c1, 3, T[1]);
     vset(c2, 0, vn0);
-    vset(c2, 1, t0);
-    vset(c2, 2, t1);
-    vset(c2, 3, t2);
-    // child 0: tet with v[p0] = t2, v[p1] = t1
+    vset(c2, 1, T[0]);
+    vset(c2, 2, T[1]);
+    vset(c2, 3, T[2]);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (k == p0) {
-        t.x[k] = t2.x;
-        t.y[k] = t2.y;
-        t.z[k] = t2.z;
-      } else if (k == p1) {
-        t.x[k] = t1.x;
-        t.y[k] = t1.y;
-        t.z[k] = t1.z;
+    for (int v = 0; v < 4; ++v) {
+      if (v == p0) {
+        t.x[v] = T[2].x;
+        t.y[v] = T[2].y;
+        t.z[v] = T[2].z;
+      } else if (v == p1) {
+        t.x[v] = T[1].x;
+        t.y[v] = T[1].y;
+        t.z[v] = T[1].z;
       }
     }
     return 3;
   }
-  // np == 1
-  const V3 t0 = interp(vp0, vn0, dp0, dn0);
-  const V3 t1 = interp(vp0, vn1, dp0, dn1);
+  int kk;
   if (nn == 3) {
-    // +---
-    const int n2 = (negl >> 4) & 3;
+    // +---: child 1 = (t0, v[n1], v[n2], t1); child 2 = (v[n2], t1, t2, t0)
     const V3 vn2 = vget(t, n2);
-    const double dn2 = sel4(n2, d[0], d[1], d[2], d[3]);
-    const V3 t2 = interp(vp0, vn2, dp0, dn2);
-    // child 1: (t0, v[n1], v[n2], t1); child 2: (v[n2], t1, t2, t0)
-    vset(c1, 0, t0);
+    vset(c1, 0, T[0]);
     vset(c1, 1, vn1);
     vset(c1, 2, vn2);
-    vset(c1, 3, t1);
+    vset(c1, 3, T[1]);
     vset(c2, 0, vn2);
-    vset(c2, 1, t1);
-    vset(c2, 2, t2);
-    vset(c2, 3, t0);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (k == p0) {
-        t.x[k] = t0.x;
-        t.y[k] = t0.y;
-        t.z[k] = t0.z;
-      }
-    }
-    return 3;
+    vset(c2, 1, T[1]);
+    vset(c2, 2, T[2]);
+    vset(c2, 3, T[0]);
+    kk = 3;
+  } else {
+    // +--0: child 1 = (t1, v[z0], v[n1], t0)
+    const V3 vz0 = vget(t, k.zerl & 3);
+    vset(c1, 0, T[1]);
+    vset(c1, 1, vz0);
+    vset(c1, 2, vn1);
+    vset(c1, 3, T[0]);
+    kk = 2;
   }
-  // +--0: child 1: (t1, v[z0], v[n1], t0)
-  const int z0 = zerl & 3;
-  const V3 vz0 = vget(t, z0);
-  vset(c1, 0, t1);
-  vset(c1, 1, vz0);
-  vset(c1, 2, vn1);
-  vset(c1, 3, t0);
+  // child 0 = tet with v[p0] = t0
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k == p0) {
-      t.x[k] = t0.x;
-      t.y[k] = t0.y;
-      t.z[k] = t0.z;
+  for (int v = 0; v < 4; ++v) {
+    if (v == p0) {
+      t.x[v] = T[0].x;
+      t.y[v] = T[0].y;
+      t.z[v] = T[0].z;
     }
   }
-  return 2;
+  return kk;
+}
+
+// Clip tet `t` by plane (nx,ny,nz,c) (Tetrahedron_Intersection.F90:244-436).
+// Returns the number of children k (0..3); `t` holds child 0.  The children
+// are handed to the sink in the reference's output order: emit.begin(k),
+// emit.child(0, t), emit.child(1, c1), emit.child(2, c2).
+template <class Emit>
+__device__ __forceinline__ int clip_tet_plane(Tet& t, double nx, double ny, double nz, double c,
+                                              Emit& emit) {
+  TetClass k;
+  classify_tet(t, nx, ny, nz, c, k);
+  if (k.nn == 0) return 0;
+  if (k.np == 0) {
+    emit.begin(1);
+    emit.child(0, t);
+    return 1;
+  }
+  Tet c1, c2;
+  const int n = split_tet(t, k, c1, c2);
+  emit.begin(n);
+  emit.child(0, t);
+  if (n >= 2) emit.child(1, c1);
+  if (n >= 3) emit.child(2, c2);
+  return n;
 }
 
 }  // namespace lsm

@@ -22,6 +22,7 @@
 
 #include <cfloat>
 #include <cstdio>
+#include <cstdlib>
 
 namespace lsm {
 
@@ -30,6 +31,22 @@ unsigned long long g_launches = 0;
 }  // namespace
 
 unsigned long long launches() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+namespace {
+int g_tet_bps = 0;
+}  // namespace
+
+// Blocks per SM of the persistent tet clipper (3: up to 170 registers per
+// thread, 4: up to 128).  LSM_TET_BLOCKS_PER_SM overrides the default.
+int tet_blocks_per_sm() {
+  if (g_tet_bps == 0) {
+    const char* e = getenv("LSM_TET_BLOCKS_PER_SM");
+    g_tet_bps = (e && atoi(e) == 3) ? 3 : 4;
+  }
+  return g_tet_bps;
+}
+
+void set_tet_blocks_per_sm(int v) { g_tet_bps = (v == 3) ? 3 : 4; }
 
 namespace {
 
@@ -193,6 +210,7 @@ __global__ void k_prep(int64_t nel, const double* __restrict__ pos, const IDX* _
           o[4 * i + 3] = L.py[i];
         }
         o[12] = tol;
+        o[13] = 0.0;
       } else {
         Planes P;
         tet_planes(t, P);
@@ -205,6 +223,9 @@ __global__ void k_prep(int64_t nel, const double* __restrict__ pos, const IDX* _
           o[4 * i + 3] = P.c[i];
         }
         o[16] = tol;
+        o[17] = 0.0;
+        o[18] = 0.0;
+        o[19] = 0.0;
       }
     }
   }
@@ -826,7 +847,9 @@ constexpr int kTriBlock = 128;
 constexpr int kTriCap = 8;  // fast-path polygon slots (geometric max is 6)
 constexpr int kTriWideCap = 24;
 constexpr int kTetBlock = 128;
-constexpr int kTetStack = 6;  // max pending tets: 2 per level for planes 1-3
+constexpr int kTetStack = 6;      // max pending tets: 2 per level for planes 0-2
+constexpr int kTetSmemSlots = 3;  // stack slots kept in shared memory
+constexpr int kReduceBlocks = 1024;  // fixed: the totals' summation order
 }  // namespace
 
 // Polygon in shared memory: slot i, coord c at base[(2*i + c) * BLOCK].
@@ -873,12 +896,9 @@ __global__ void __launch_bounds__(kTriBlock) k_clip_tris(int64_t npairs, const i
                                                          const double* __restrict__ tol_a,
                                                          const double* __restrict__ setup_b,
                                                          double* pair_measure, int32_t* pair_nout,
-                                                         Partial* partials, int32_t* ovf_list,
-                                                         int* ovf_count) {
+                                                         int32_t* ovf_list, int* ovf_count) {
   __shared__ double poly[2 * 2 * kTriCap * kTriBlock];
   SmemPoly<kTriBlock> p{poly + threadIdx.x}, q{poly + 2 * kTriCap * kTriBlock + threadIdx.x};
-  double sum = 0.0, err = 0.0;
-  unsigned long long ni = 0, no = 0;
   for (int64_t i = (int64_t)blockIdx.x * kTriBlock + threadIdx.x; i < npairs;
        i += (int64_t)gridDim.x * kTriBlock) {
     const int a = pa[i], b = pb[i];
@@ -896,11 +916,7 @@ __global__ void __launch_bounds__(kTriBlock) k_clip_tris(int64_t npairs, const i
     }
     pair_measure[i] = m;
     pair_nout[i] = n;
-    cs_add(sum, err, m);
-    ni += n > 0;
-    no += n;
   }
-  block_reduce_partial<kTriBlock>(sum, err, ni, no, &partials[blockIdx.x]);
 }
 
 __global__ void __launch_bounds__(32) k_clip_tris_wide(const int32_t* __restrict__ list, const int* __restrict__ count,
@@ -909,10 +925,7 @@ __global__ void __launch_bounds__(32) k_clip_tris_wide(const int32_t* __restrict
                                                        const double* __restrict__ coords_a,
                                                        const double* __restrict__ tol_a,
                                                        const double* __restrict__ setup_b,
-                                                       double* pair_measure, int32_t* pair_nout,
-                                                       Partial* partial) {
-  double sum = 0.0, err = 0.0;
-  unsigned long long ni = 0, no = 0;
+                                                       double* pair_measure, int32_t* pair_nout) {
   int64_t nl = *count;
   if (nl > cap) nl = cap;
   for (int64_t j = threadIdx.x; j < nl; j += 32) {
@@ -932,33 +945,41 @@ __global__ void __launch_bounds__(32) k_clip_tris_wide(const int32_t* __restrict
     }
     pair_measure[i] = m;
     pair_nout[i] = n;
-    cs_add(sum, err, m);
-    ni += n > 0;
-    no += n;
   }
-  block_reduce_partial<32>(sum, err, ni, no, partial);
 }
 
 // ======================================================================
 // K6: tetrahedron clipping, depth-first
 // ======================================================================
+// Stack of pending tets.  Slots [0, kTetSmemSlots) live in shared memory
+// (slot s, component j at base[(s*12 + j) * BLOCK]); deeper slots, which
+// few pairs reach, live in per-thread local memory.
 template <int BLOCK>
 struct TetStack {
-  double* base;  // slot s, component j at base[(s*12 + j) * BLOCK]
+  double* base;
+  Tet deep[kTetStack - kTetSmemSlots];
   __device__ __forceinline__ void store(int s, const Tet& t) {
+    if (s < kTetSmemSlots) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      base[(s * 12 + 3 * k + 0) * BLOCK] = t.x[k];
-      base[(s * 12 + 3 * k + 1) * BLOCK] = t.y[k];
-      base[(s * 12 + 3 * k + 2) * BLOCK] = t.z[k];
+      for (int k = 0; k < 4; ++k) {
+        base[(s * 12 + 3 * k + 0) * BLOCK] = t.x[k];
+        base[(s * 12 + 3 * k + 1) * BLOCK] = t.y[k];
+        base[(s * 12 + 3 * k + 2) * BLOCK] = t.z[k];
+      }
+    } else {
+      deep[s - kTetSmemSlots] = t;
     }
   }
   __device__ __forceinline__ void load(int s, Tet& t) const {
+    if (s < kTetSmemSlots) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      t.x[k] = base[(s * 12 + 3 * k + 0) * BLOCK];
-      t.y[k] = base[(s * 12 + 3 * k + 1) * BLOCK];
-      t.z[k] = base[(s * 12 + 3 * k + 2) * BLOCK];
+      for (int k = 0; k < 4; ++k) {
+        t.x[k] = base[(s * 12 + 3 * k + 0) * BLOCK];
+        t.y[k] = base[(s * 12 + 3 * k + 1) * BLOCK];
+        t.z[k] = base[(s * 12 + 3 * k + 2) * BLOCK];
+      }
+    } else {
+      t = deep[s - kTetSmemSlots];
     }
   }
 };
@@ -969,46 +990,79 @@ struct TetStackLocal {
   __device__ __forceinline__ void load(int s, Tet& t) const { t = slot[s]; }
 };
 
-// Depth-first clip of tet `t` by planes P; visits kept output tets in the
-// reference's (breadth-first) order.  `leaf(t)` is called for each final
-// tet with vol_v4 >= tol.  Returns the number of kept tets.
+// Sink for clip_tet_plane inside the depth-first walk: at the last plane it
+// evaluates final tets (vol_v4 >= tol, then the vertex-1 volume) in order;
+// before that it parks children 1..k-1 on the stack so that child 1 is on
+// top (pre-order = the reference's breadth-first output order).
 template <class Stack, class Leaf>
-__device__ __forceinline__ int clip_tet_dfs(Tet t, const Planes& P, double tol, Stack& stk, Leaf leaf) {
+struct DfsSink {
+  Stack& stk;
+  Leaf& leaf;
+  int sp;
+  bool last;
+  double tol;
+  int k;
+  int kept;
+  __device__ __forceinline__ void begin(int kk) { k = kk; }
+  __device__ __forceinline__ void child(int j, const Tet& c) {
+    if (last) {
+      if (tet_volume_v4(c) >= tol) {
+        leaf(c);
+        ++kept;
+      }
+    } else if (j > 0) {
+      stk.store(sp + (k - 1) - j, c);
+    }
+  }
+};
+
+__device__ __forceinline__ void load_plane(const double* __restrict__ planes, int L, double& nx, double& ny,
+                                           double& nz, double& c) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(planes + 4 * L));
+  const double2 b = __ldg(reinterpret_cast<const double2*>(planes + 4 * L + 2));
+  nx = a.x;
+  ny = a.y;
+  nz = b.x;
+  c = b.y;
+}
+
+// Plane sources for the depth-first walk.
+struct GlobalPlanes {  // B's planes in global memory (setup row, stride 4)
+  const double* p;
+  __device__ __forceinline__ void get(int L, double& nx, double& ny, double& nz, double& c) const {
+    load_plane(p, L, nx, ny, nz, c);
+  }
+};
+
+struct RegPlanes {  // planes computed in registers
+  const Planes& P;
+  __device__ __forceinline__ void get(int L, double& nx, double& ny, double& nz, double& c) const {
+    nx = sel4(L, P.nx[0], P.nx[1], P.nx[2], P.nx[3]);
+    ny = sel4(L, P.ny[0], P.ny[1], P.ny[2], P.ny[3]);
+    nz = sel4(L, P.nz[0], P.nz[1], P.nz[2], P.nz[3]);
+    c = sel4(L, P.c[0], P.c[1], P.c[2], P.c[3]);
+  }
+};
+
+// Depth-first clip of tet `t` by 4 planes; calls leaf(tet) for each final
+// tet with vol_v4 >= tol, in the reference's output order.  Returns the
+// number of kept tets.
+template <class Src, class Stack, class Leaf>
+__device__ __forceinline__ int clip_tet_dfs(Tet t, const Src& planes, double tol, Stack& stk, Leaf leaf) {
   int sp = 0;
   unsigned levels = 0;  // 2 bits per stack slot
   int L = 0;
   int kept = 0;
-  for (int guard = 0; guard < 200; ++guard) {
-    const double nx = sel4(L, P.nx[0], P.nx[1], P.nx[2], P.nx[3]);
-    const double ny = sel4(L, P.ny[0], P.ny[1], P.ny[2], P.ny[3]);
-    const double nz = sel4(L, P.nz[0], P.nz[1], P.nz[2], P.nz[3]);
-    const double c = sel4(L, P.c[0], P.c[1], P.c[2], P.c[3]);
-    Tet c1, c2;
-    const int k = clip_tet_plane(t, nx, ny, nz, c, c1, c2);
-    if (L == 3) {
-      if (k >= 1 && tet_volume_v4(t) >= tol) {
-        leaf(t);
-        ++kept;
-      }
-      if (k >= 2 && tet_volume_v4(c1) >= tol) {
-        leaf(c1);
-        ++kept;
-      }
-      if (k >= 3 && tet_volume_v4(c2) >= tol) {
-        leaf(c2);
-        ++kept;
-      }
-    } else if (k > 0) {
-      if (k == 3) {
-        stk.store(sp, c2);
-        levels |= (unsigned)(L + 1) << (2 * sp);
-        ++sp;
-      }
-      if (k >= 2) {
-        stk.store(sp, c1);
-        levels |= (unsigned)(L + 1) << (2 * sp);
-        ++sp;
-      }
+  for (int guard = 0; guard < 64; ++guard) {  // at most 1+3+9+27 tets are clipped
+    double nx, ny, nz, c;
+    planes.get(L, nx, ny, nz, c);
+    DfsSink<Stack, Leaf> sink{stk, leaf, sp, L == 3, tol, 0, 0};
+    const int k = clip_tet_plane(t, nx, ny, nz, c, sink);
+    kept += sink.kept;
+    if (L < 3 && k > 0) {
+      if (k > 1) levels |= (unsigned)(L + 1) << (2 * sp);
+      if (k > 2) levels |= (unsigned)(L + 1) << (2 * (sp + 1));
+      sp += k - 1;
       ++L;
       continue;
     }
@@ -1021,92 +1075,229 @@ __device__ __forceinline__ int clip_tet_dfs(Tet t, const Planes& P, double tol, 
   return kept;
 }
 
-__device__ __forceinline__ void load_planes(const double* __restrict__ o, Planes& P, double& tol) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    P.nx[i] = o[4 * i + 0];
-    P.ny[i] = o[4 * i + 1];
-    P.nz[i] = o[4 * i + 2];
-    P.c[i] = o[4 * i + 3];
-  }
-  tol = o[16];
-}
-
 __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
+  const double2* q = reinterpret_cast<const double2*>(v);
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    t.x[k] = v[3 * k + 0];
-    t.y[k] = v[3 * k + 1];
-    t.z[k] = v[3 * k + 2];
+  for (int k = 0; k < 2; ++k) {
+    const double2 a = __ldg(q + 3 * k), b = __ldg(q + 3 * k + 1), c = __ldg(q + 3 * k + 2);
+    // vertices 2k and 2k+1: (a.x a.y b.x) (b.y c.x c.y)
+    t.x[2 * k] = a.x;
+    t.y[2 * k] = a.y;
+    t.z[2 * k] = b.x;
+    t.x[2 * k + 1] = b.y;
+    t.y[2 * k + 1] = c.x;
+    t.z[2 * k + 1] = c.y;
   }
 }
 
-__global__ void __launch_bounds__(kTetBlock) k_clip_tets(int64_t npairs, const int32_t* __restrict__ pa,
-                                                         const int32_t* __restrict__ pb,
-                                                         const double* __restrict__ coords_a,
-                                                         const double* __restrict__ tol_a,
-                                                         const double* __restrict__ setup_b,
-                                                         double* pair_measure, int32_t* pair_nout,
-                                                         Partial* partials) {
+// Exact early-out for the tet clipper.  If every vertex of A lies at
+// distance >= eps + margin on the outer side of one of B's face planes, then
+// so does every tet the reference's clipping derives from A: derived
+// vertices are convex combinations of A's vertices, and the rounding of at
+// most three nested interpolations plus the distance evaluation moves them by
+// far less than margin = 64*eps*(1 + 2M) (M bounds the coordinates and plane
+// offsets involved).  Such a tet is classified entirely positive at that
+// plane and discarded, so the reference returns no tets: the pair's result is
+// written here (0 tets, measure 0) and only the remaining pairs are listed
+// for the clipper.
+__global__ void __launch_bounds__(256) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ pa,
+                                                        const int32_t* __restrict__ pb,
+                                                        const double* __restrict__ coords_a,
+                                                        const double* __restrict__ setup_b,
+                                                        double* pair_measure, int32_t* pair_nout,
+                                                        int32_t* survivors, unsigned long long* nsurv) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < npairs; base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = base + threadIdx.x;
+    bool live = false;
+    if (i < npairs) {
+      const int a = pa[i], b = pb[i];
+      Tet t;
+      load_tet(coords_a + (int64_t)a * 12, t);
+      const double* pl = setup_b + (int64_t)b * kSetup3;
+      double M = 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) M = fmax(M, fmax(fabs(t.x[k]), fmax(fabs(t.y[k]), fabs(t.z[k]))));
+      bool reject = false;
+#pragma unroll
+      for (int L = 0; L < 4; ++L) {
+        double nx, ny, nz, c;
+        load_plane(pl, L, nx, ny, nz, c);
+        const double thr = kEps + 64.0 * kEps * (1.0 + 2.0 * fmax(M, fabs(c)));
+        double dmin = DBL_MAX;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dmin = fmin(dmin, ((nx * t.x[k] + ny * t.y[k]) + nz * t.z[k]) - c);
+        reject = reject || dmin >= thr;
+      }
+      if (reject) {
+        pair_measure[i] = 0.0;
+        pair_nout[i] = 0;
+      } else {
+        live = true;
+      }
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, live);
+    if (mask) {
+      const int leader = __ffs(mask) - 1;
+      unsigned long long off = 0;
+      if (lane == leader) off = atomicAdd(nsurv, (unsigned long long)__popc(mask));
+      off = __shfl_sync(0xffffffffu, off, leader);
+      if (live) survivors[off + __popc(mask & lt)] = (int32_t)i;
+    }
+  }
+}
+
+// Persistent clipper over the surviving pairs: one pair per lane, one
+// tet-vs-plane clip per loop iteration (depth-first, children 1..k-1 parked
+// on the lane's stack).  A lane whose pair is finished takes the next pair
+// from a global counter (one atomic per warp per refill), so lanes stay busy
+// even though pairs differ in work by more than 10x.
+template <int BPS>
+__global__ void __launch_bounds__(kTetBlock, BPS) k_clip_tets(
+    const int32_t* __restrict__ list, const unsigned long long* __restrict__ nlist,
+    const int32_t* __restrict__ pa, const int32_t* __restrict__ pb, const double* __restrict__ coords_a,
+    const double* __restrict__ tol_a, const double* __restrict__ setup_b, double* pair_measure,
+    int32_t* pair_nout, unsigned long long* work) {
   extern __shared__ double stack_mem[];
   TetStack<kTetBlock> stk{stack_mem + threadIdx.x};
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t npairs = (int64_t)*nlist;
+  int64_t p = -1;
+  bool exhausted = false;
+  Tet t;
+  const double* planes = nullptr;
+  double tol = 0.0, m = 0.0;
+  int L = 0, sp = 0, kept = 0;
+  unsigned levels = 0;
+  for (;;) {
+    const bool need = p < 0 && !exhausted;
+    const unsigned needmask = __ballot_sync(0xffffffffu, need);
+    if (needmask) {
+      const int leader = __ffs(needmask) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(work, (unsigned long long)__popc(needmask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const int64_t q = (int64_t)(base + __popc(needmask & lt));
+        if (q < npairs) {
+          p = list[q];
+          const int a = pa[p], b = pb[p];
+          load_tet(coords_a + (int64_t)a * 12, t);
+          planes = setup_b + (int64_t)b * kSetup3;
+          tol = fmin(tol_a[a], planes[16]);
+          m = 0.0;
+          L = 0;
+          sp = 0;
+          kept = 0;
+          levels = 0;
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, p < 0)) break;
+    if (p < 0) continue;
+    double nx, ny, nz, c;
+    load_plane(planes, L, nx, ny, nz, c);
+    auto leaf = [&](const Tet& o) { m = m + tet_volume_v1(o); };
+    DfsSink<TetStack<kTetBlock>, decltype(leaf)> sink{stk, leaf, sp, L == 3, tol, 0, 0};
+    const int k = clip_tet_plane(t, nx, ny, nz, c, sink);
+    kept += sink.kept;
+    if (L < 3 && k > 0) {
+      if (k > 1) levels |= (unsigned)(L + 1) << (2 * sp);
+      if (k > 2) levels |= (unsigned)(L + 1) << (2 * (sp + 1));
+      sp += k - 1;
+      ++L;
+      continue;
+    }
+    if (sp > 0) {
+      --sp;
+      stk.load(sp, t);
+      L = (int)((levels >> (2 * sp)) & 3u);
+      levels &= ~(3u << (2 * sp));
+      continue;
+    }
+    pair_measure[p] = m;
+    pair_nout[p] = kept;
+    p = -1;
+  }
+}
+
+// Deterministic per-block partials of the pair measures: block b reduces the
+// contiguous range [b*chunk, (b+1)*chunk) in a fixed thread order.
+__global__ void __launch_bounds__(256) k_reduce_pairs(int64_t npairs, const double* __restrict__ pm,
+                                                      const int32_t* __restrict__ pn, Partial* partials) {
+  const int64_t chunk = (npairs + gridDim.x - 1) / gridDim.x;
+  const int64_t beg = (int64_t)blockIdx.x * chunk;
+  const int64_t end = beg + chunk < npairs ? beg + chunk : npairs;
   double sum = 0.0, err = 0.0;
   unsigned long long ni = 0, no = 0;
-  for (int64_t i = (int64_t)blockIdx.x * kTetBlock + threadIdx.x; i < npairs;
-       i += (int64_t)gridDim.x * kTetBlock) {
-    const int a = pa[i], b = pb[i];
-    Tet t;
-    load_tet(coords_a + (int64_t)a * 12, t);
-    Planes P;
-    double tolb;
-    load_planes(setup_b + (int64_t)b * kSetup3, P, tolb);
-    const double tol = fmin(tol_a[a], tolb);
-    double m = 0.0;
-    const int n = clip_tet_dfs(t, P, tol, stk, [&](const Tet& o) { m = m + tet_volume_v1(o); });
-    pair_measure[i] = m;
-    pair_nout[i] = n;
-    cs_add(sum, err, m);
-    ni += n > 0;
-    no += n;
+  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    cs_add(sum, err, pm[i]);
+    const int k = pn[i];
+    ni += k > 0;
+    no += k;
   }
-  block_reduce_partial<kTetBlock>(sum, err, ni, no, &partials[blockIdx.x]);
+  block_reduce_partial<256>(sum, err, ni, no, &partials[blockIdx.x]);
 }
 
 int clip_grid_blocks(int dim) {
   if (dim == 2) return sm_count() * 8;
-  return sm_count() * 3;
+  return sm_count() * tet_blocks_per_sm();
 }
 
 cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                         const double* coords_a, const double* tol_a, const double* setup_b,
-                        double* pair_measure, int32_t* pair_nout, Partial* partials,
-                        int32_t* overflow_list, int* overflow_count, cudaStream_t s) {
+                        double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
+                        int* overflow_count, unsigned long long* work, cudaStream_t s) {
   const int g = clip_grid_blocks(dim);
   count_launch();
   if (dim == 2) {
     k_clip_tris<<<g, kTriBlock, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure,
-                                        pair_nout, partials, overflow_list, overflow_count);
+                                        pair_nout, overflow_list, overflow_count);
   } else {
-    const size_t smem = sizeof(double) * kTetStack * 12 * kTetBlock;
-    k_clip_tets<<<g, kTetBlock, smem, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure,
-                                           pair_nout, partials);
+    // work[0]: survivor count, work[1]: clipper pair counter
+    const size_t smem = sizeof(double) * kTetSmemSlots * 12 * kTetBlock;
+    cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
+    count_launch();
+    k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, pair_a, pair_b, coords_a, setup_b,
+                                                              pair_measure, pair_nout, overflow_list, work);
+    if (tet_blocks_per_sm() == 3)
+      k_clip_tets<3><<<sm_count() * 3, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,
+                                                              setup_b, pair_measure, pair_nout, work + 1);
+    else
+      k_clip_tets<4><<<sm_count() * 4, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,
+                                                              setup_b, pair_measure, pair_nout, work + 1);
   }
   return cudaGetLastError();
 }
 
+int reduce_pairs_blocks() { return kReduceBlocks; }
+
+cudaError_t launch_reduce_pairs(int64_t npairs, const double* pair_measure, const int32_t* pair_nout,
+                                Partial* partials, cudaStream_t s) {
+  count_launch();
+  k_reduce_pairs<<<kReduceBlocks, 256, 0, s>>>(npairs, pair_measure, pair_nout, partials);
+  return cudaGetLastError();
+}
+
 cudaError_t init_device_attributes() {
-  const int smem = (int)(sizeof(double) * kTetStack * 12 * kTetBlock);
-  return cudaFuncSetAttribute(k_clip_tets, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int smem = (int)(sizeof(double) * kTetSmemSlots * 12 * kTetBlock);
+  cudaError_t e = cudaFuncSetAttribute(k_clip_tets<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_clip_tets<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
                                   const int32_t* pair_a, const int32_t* pair_b,
                                   const double* coords_a, const double* tol_a,
                                   const double* setup_b, double* pair_measure, int32_t* pair_nout,
-                                  Partial* partial, cudaStream_t s) {
+                                  cudaStream_t s) {
   count_launch();
   k_clip_tris_wide<<<1, 32, 0, s>>>(overflow_list, overflow_count, cap, pair_a, pair_b, coords_a, tol_a,
-                                    setup_b, pair_measure, pair_nout, partial);
+                                    setup_b, pair_measure, pair_nout);
   return cudaGetLastError();
 }
 
@@ -1214,7 +1405,7 @@ __global__ void k_pairs_tets(int64_t n, const double* __restrict__ A, const doub
     double m = 0.0;
     int idx = 0;
     double* o = out_elems ? out_elems + (int64_t)81 * 12 * i : nullptr;
-    const int k = clip_tet_dfs(ta, P, tol, stk, [&](const Tet& t) {
+    const int k = clip_tet_dfs(ta, RegPlanes{P}, tol, stk, [&](const Tet& t) {
       m = m + tet_volume_v1(t);
       if (o && idx < 81) {
 #pragma unroll
@@ -1398,13 +1589,11 @@ __global__ void __launch_bounds__(128) k_p1_mass(int64_t npairs, const int32_t* 
     } else {
       Tet t;
       load_tet(ca, t);
-      Planes P;
-      double tolb;
-      load_planes(setup_b + (int64_t)b * kSetup3, P, tolb);
-      const double tol = fmin(tol_a[a], tolb);
+      const double* planes = setup_b + (int64_t)b * kSetup3;
+      const double tol = fmin(tol_a[a], planes[16]);
       TetStackLocal stk;
       const double qa = 5.8541019662496852e-1, qb = 1.3819660112501050e-1;
-      clip_tet_dfs(t, P, tol, stk, [&](const Tet& o) {
+      clip_tet_dfs(t, GlobalPlanes{planes}, tol, stk, [&](const Tet& o) {
         const double meas = tet_volume_v1(o);
         const double w = 0.25 * meas;
 #pragma unroll

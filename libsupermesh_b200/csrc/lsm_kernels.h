@@ -15,8 +15,8 @@ namespace lsm {
 //   setup   [nel][kSetup]   clip setup of a B element: 2D lines (12) or 3D
 //                           planes (16), then tol = 10*spacing(measure)
 //   tolv    [nel]           10*spacing(measure) (A elements)
-constexpr int kSetup2 = 13;
-constexpr int kSetup3 = 17;
+constexpr int kSetup2 = 14;  // 3 lines x (nx, ny, px, py), tol, pad
+constexpr int kSetup3 = 20;  // 4 planes x (nx, ny, nz, c), tol, pad (16-byte aligned rows)
 
 // Per-block partial of a narrow-phase launch: compensated measure sum,
 // intersecting pairs and output simplices.
@@ -29,6 +29,10 @@ struct Partial {
 
 // Process-wide count of kernel launches issued by this library.
 unsigned long long launches();
+
+// Launch shape of the persistent tet clipper (3 or 4 blocks per SM).
+int tet_blocks_per_sm();
+void set_tet_blocks_per_sm(int v);
 
 struct BVH {
   int n = 0;                 // leaves
@@ -70,22 +74,28 @@ cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_
 int64_t scan_tmp_entries(int64_t n);
 cudaError_t launch_scan(int64_t n, const int* counts, int64_t* offsets, int64_t* tmp, cudaStream_t s);
 
-// Narrow phase over candidate pairs.  pair_measure/pair_nout are per pair;
-// partials receives (sum, err) per block for the compensated total.
-// overflow_list collects pairs whose polygon outgrew the fast-path buffers
-// (2D only); they are re-run by launch_clip_tris_wide.
+// Narrow phase over candidate pairs: pair_measure/pair_nout per pair.
+// 2D: overflow_list collects pairs whose polygon outgrew the fast-path
+// buffers; launch_clip_tris_wide re-runs them.  3D: overflow_list (npairs
+// entries) receives the pairs that survive the exact early-out; `work`
+// holds two counters (survivors, clipper progress), reset by the launch.
 int clip_grid_blocks(int dim);
 cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                         const double* coords_a, const double* tol_a, const double* setup_b,
-                        double* pair_measure, int32_t* pair_nout, Partial* partials,
-                        int32_t* overflow_list, int* overflow_count, cudaStream_t s);
+                        double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
+                        int* overflow_count, unsigned long long* work, cudaStream_t s);
 // Opt-in shared-memory limits for the clip kernels on the current device.
 cudaError_t init_device_attributes();
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
                                   const int32_t* pair_a, const int32_t* pair_b,
                                   const double* coords_a, const double* tol_a,
                                   const double* setup_b, double* pair_measure, int32_t* pair_nout,
-                                  Partial* partial, cudaStream_t s);
+                                  cudaStream_t s);
+// Per-block partials of the pair measures/counts in a fixed order
+// (reduce_pairs_blocks() entries).
+int reduce_pairs_blocks();
+cudaError_t launch_reduce_pairs(int64_t npairs, const double* pair_measure, const int32_t* pair_nout,
+                                Partial* partials, cudaStream_t s);
 
 // Totals: merge of the per-block partials into out[0] (in order).
 cudaError_t launch_finalize(const Partial* partials, int npartials, Partial* out, cudaStream_t s);
