@@ -134,6 +134,25 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context *ctx, int npairs,
                                        int64_t *n_candidates, int64_t *n_intersecting,
                                        void *stream);
 
+/* Allocation-free clipping of explicit tetrahedron pairs (no counterpart in
+ * the reference).  For callers that cannot let a library allocate device
+ * memory: applications whose GPU memory is owned by another pool allocator,
+ * and stream-overlapped loops where cudaFree's implicit device-wide
+ * synchronisation would serialise other work.  Same results as
+ * libsupermesh_gpu_intersect_pairs (dim 3) for measure[n] and n_out[n]; total
+ * (host, optional) receives the compensated sum of measure.  tet_a, tet_b
+ * ([n][4][3]), measure and n_out are device memory; n <= LSM_NOALLOC_MAX_PAIRS
+ * (larger n returns LSM_ERROR_CAPACITY with a message on stderr).
+ * Scratch lives in one fixed device array of LSM_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until exit; the first call on a device
+ * looks up its address (make that first call before any stream capture).
+ * All calls share the array, so calls that overlap on the GPU race. */
+#define LSM_NOALLOC_MAX_PAIRS 32768
+#define LSM_NOALLOC_SCRATCH_BYTES 5800448
+int libsupermesh_gpu_intersect_tets_noalloc(int64_t n, const double *tet_a, const double *tet_b,
+                                            double *measure, int32_t *n_out, double *total,
+                                            void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,7 @@ ROOT = PKG.parent
 SRC = PKG / "csrc"
 OUT = PKG / "lib" / "libsupermesh.so"
 PROBE = PKG / "lib" / "liblsm_probe.so"
-SOURCES = ["lsm_kernels.cu", "lsm_capi.cu"]
+SOURCES = ["lsm_kernels.cu", "lsm_capi.cu", "lsm_noalloc.cu"]
 HEADERS = ["lsm_geom.cuh", "lsm_kernels.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
