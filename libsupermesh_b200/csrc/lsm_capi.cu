@@ -18,6 +18,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/libsupermesh-c.h"
 #include "../../include/libsupermesh-gpu.h"
@@ -49,6 +50,10 @@ struct Ctx {
   DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals;
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
+  DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand;
+  DevBuf bt_stage_pa, bt_stage_ea, bt_stage_pb, bt_stage_eb;
+  void* host_stage = nullptr;  // pinned, grow-only
+  size_t host_stage_cap = 0;
   // pinned host scalars
   void* host_scalars = nullptr;
 
@@ -167,10 +172,15 @@ void fini_ctx(Ctx* c) {
                    &c->bvh_hi, &c->bvh_work, &c->counts, &c->offsets, &c->scan_tmp, &c->pair_a,
                    &c->pair_b, &c->i64_tmp, &c->pair_measure, &c->pair_nout, &c->partials,
                    &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->x_a, &c->x_b, &c->x_measure,
-                   &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks};
+                   &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
+                   &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
+                   &c->bt_ncand, &c->bt_stage_pa, &c->bt_stage_ea, &c->bt_stage_pb, &c->bt_stage_eb};
   for (DevBuf* b : all) free_buf(*b);
   if (c->host_scalars) cudaFreeHost(c->host_scalars);
+  if (c->host_stage) cudaFreeHost(c->host_stage);
   if (c->stream) cudaStreamDestroy(c->stream);
+  c->host_stage = nullptr;
+  c->host_stage_cap = 0;
   c->host_scalars = nullptr;
   c->stream = nullptr;
 }
@@ -359,6 +369,197 @@ int guarded(Ctx* c, F&& f) {
   } catch (const std::bad_alloc&) {
     set_error(c, "host allocation failed");
     return LSM_ERROR_OUT_OF_MEMORY;
+  }
+}
+
+// ------------------------------------------------------------ batched path
+void* host_stage(Ctx* c, size_t bytes) {
+  if (c->host_stage_cap < bytes) {
+    if (c->host_stage) cudaFreeHost(c->host_stage);
+    c->host_stage = nullptr;
+    c->host_stage_cap = 0;
+    const size_t want = bytes + bytes / 2 + 4096;
+    if (cudaMallocHost(&c->host_stage, want) != cudaSuccess) {
+      (void)cudaGetLastError();
+      set_error(c, "pinned host allocation of %zu bytes failed", want);
+      throw Fail{LSM_ERROR_OUT_OF_MEMORY};
+    }
+    c->host_stage_cap = want;
+  }
+  return c->host_stage;
+}
+
+// All mesh pairs of one dimension through each phase in one launch:
+// batched prep (pointer tables), one sort by (mesh, Morton), one LBVH with a
+// subtree per mesh, one traversal, the usual clipper over all candidates,
+// and a per-mesh-pair reduction.  One host synchronisation (candidate count).
+void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu_mesh* ma,
+                     const lsm_gpu_mesh* mb, int on_device, double* totals, int64_t* ncand, int64_t* nint,
+                     cudaStream_t s) {
+  const int nm = (int)idx.size();
+  const int ib = ma[idx[0]].index_bytes;
+  const int loc = dim + 1;
+  // host tables: elem_off_a[nm+1] elem_off_b[nm+1] nnodes_a[nm] nnodes_b[nm]
+  //              pos_a[nm] en_a[nm] pos_b[nm] en_b[nm]
+  const size_t tab_words = 2 * (nm + 1) + 6 * (size_t)nm;
+  std::vector<int64_t> tab(tab_words);
+  int64_t* eoa = tab.data();
+  int64_t* eob = eoa + (nm + 1);
+  int64_t* nna = eob + (nm + 1);
+  int64_t* nnb = nna + nm;
+  uint64_t* pta = reinterpret_cast<uint64_t*>(nnb + nm);
+  uint64_t* eta = pta + nm;
+  uint64_t* ptb = eta + nm;
+  uint64_t* etb = ptb + nm;
+  int64_t na = 0, nb = 0, va = 0, vb = 0;
+  for (int i = 0; i < nm; ++i) {
+    const lsm_gpu_mesh& A = ma[idx[i]];
+    const lsm_gpu_mesh& B = mb[idx[i]];
+    eoa[i] = na;
+    eob[i] = nb;
+    nna[i] = A.nnodes;
+    nnb[i] = B.nnodes;
+    na += A.nelements;
+    nb += B.nelements;
+    va += A.nnodes;
+    vb += B.nnodes;
+  }
+  eoa[nm] = na;
+  eob[nm] = nb;
+  REQUIRE(na < (int64_t)0x7fffffff && nb < (int64_t)0x7fffffff, "batch has more than 2^31-1 elements");
+  if (on_device) {
+    for (int i = 0; i < nm; ++i) {
+      pta[i] = (uint64_t)ma[idx[i]].positions;
+      eta[i] = (uint64_t)ma[idx[i]].enlist;
+      ptb[i] = (uint64_t)mb[idx[i]].positions;
+      etb[i] = (uint64_t)mb[idx[i]].enlist;
+    }
+  } else {
+    // stage host meshes into device buffers (one copy per array and mesh)
+    double* spa = ensure<double>(c, c->bt_stage_pa, va * dim);
+    double* spb = ensure<double>(c, c->bt_stage_pb, vb * dim);
+    char* sea = ensure<char>(c, c->bt_stage_ea, na * loc * ib);
+    char* seb = ensure<char>(c, c->bt_stage_eb, nb * loc * ib);
+    int64_t oa = 0, ob = 0;
+    for (int i = 0; i < nm; ++i) {
+      const lsm_gpu_mesh& A = ma[idx[i]];
+      const lsm_gpu_mesh& B = mb[idx[i]];
+      pta[i] = (uint64_t)(spa + oa * dim);
+      ptb[i] = (uint64_t)(spb + ob * dim);
+      eta[i] = (uint64_t)(sea + eoa[i] * loc * ib);
+      etb[i] = (uint64_t)(seb + eob[i] * loc * ib);
+      if (A.nnodes) CU(cudaMemcpyAsync(spa + oa * dim, A.positions, sizeof(double) * A.nnodes * dim, cudaMemcpyHostToDevice, s));
+      if (B.nnodes) CU(cudaMemcpyAsync(spb + ob * dim, B.positions, sizeof(double) * B.nnodes * dim, cudaMemcpyHostToDevice, s));
+      if (A.nelements) CU(cudaMemcpyAsync(sea + eoa[i] * loc * ib, A.enlist, (size_t)A.nelements * loc * ib, cudaMemcpyHostToDevice, s));
+      if (B.nelements) CU(cudaMemcpyAsync(seb + eob[i] * loc * ib, B.enlist, (size_t)B.nelements * loc * ib, cudaMemcpyHostToDevice, s));
+      oa += A.nnodes;
+      ob += B.nnodes;
+    }
+  }
+  int64_t* dtab = ensure<int64_t>(c, c->bt_tabs, (int64_t)tab_words);
+  void* htab = host_stage(c, sizeof(int64_t) * tab_words);
+  CU(cudaStreamSynchronize(s));  // the pinned stage may still feed a previous copy
+  memcpy(htab, tab.data(), sizeof(int64_t) * tab_words);
+  CU(cudaMemcpyAsync(dtab, htab, sizeof(int64_t) * tab_words, cudaMemcpyHostToDevice, s));
+  const int64_t* d_eoa = dtab;
+  const int64_t* d_eob = d_eoa + (nm + 1);
+  const int64_t* d_nna = d_eob + (nm + 1);
+  const int64_t* d_nnb = d_nna + nm;
+  const unsigned long long* d_pta = reinterpret_cast<const unsigned long long*>(d_nnb + nm);
+  const unsigned long long* d_eta = d_pta + nm;
+  const unsigned long long* d_ptb = d_eta + nm;
+  const unsigned long long* d_etb = d_ptb + nm;
+
+  int* bad = bad_flag(c);
+  CU(cudaMemsetAsync(bad, 0, sizeof(int) * 64, s));
+  double* a_coords = ensure<double>(c, c->a_coords, na * loc * dim);
+  double* a_box = ensure<double>(c, c->a_box64, na * 2 * dim);
+  double* a_tol = ensure<double>(c, c->a_tol, na);
+  int32_t* pair_of_a = ensure<int32_t>(c, c->bt_pair_a, na);
+  double* b_box = ensure<double>(c, c->b_box64, nb * 2 * dim);
+  float* b_box32 = ensure<float>(c, c->b_box32, nb * 8);
+  double* b_setup = ensure<double>(c, c->b_setup, nb * (dim == 2 ? lsm::kSetup2 : lsm::kSetup3));
+  int32_t* pair_of_b = ensure<int32_t>(c, c->bt_pair_b, nb);
+  CU(lsm::launch_prep_batched(dim, na, nm, d_eoa, d_pta, d_eta, d_nna, ib, a_coords, a_box, nullptr, a_tol,
+                              nullptr, pair_of_a, bad, s));
+  CU(lsm::launch_prep_batched(dim, nb, nm, d_eob, d_ptb, d_etb, d_nnb, ib, nullptr, b_box, b_box32, nullptr,
+                              b_setup, pair_of_b, bad, s));
+  // tree over all B meshes
+  lsm::BVH bvh;
+  bvh.n = (int)nb;
+  int* roots = ensure<int>(c, c->bt_roots, nm);
+  int* stops = ensure<int>(c, c->bt_stops, nm);
+  if (nb > 0) {
+    uint32_t* keys = ensure<uint32_t>(c, c->keys, nb);
+    int32_t* vals = ensure<int32_t>(c, c->vals, nb);
+    uint32_t* kt = ensure<uint32_t>(c, c->keys_tmp, nb);
+    int32_t* vt = ensure<int32_t>(c, c->vals_tmp, nb);
+    uint32_t* hist = ensure<uint32_t>(c, c->hist, lsm::radix_hist_entries(nb));
+    uint32_t* mort = ensure<uint32_t>(c, c->bt_mort, nb);
+    const int pcap = 4096;
+    double* part = ensure<double>(c, c->root_partial, (int64_t)pcap * 2 * dim);
+    double* root = ensure<double>(c, c->rootbox, 2 * dim);
+    CU(lsm::launch_root_box(dim, nb, b_box, part, pcap, root, s));
+    CU(lsm::launch_morton(dim, nb, b_box, root, keys, vals, s));
+    CU(cudaMemcpyAsync(mort, keys, sizeof(uint32_t) * nb, cudaMemcpyDeviceToDevice, s));
+    CU(lsm::radix_sort_pairs(nb, dim == 2 ? 32 : 30, keys, vals, kt, vt, hist, s));
+    int mbits = 1;
+    while ((1 << mbits) < nm) ++mbits;
+    CU(lsm::launch_pair_keys(nb, vals, pair_of_b, keys, s));
+    CU(lsm::radix_sort_pairs(nb, mbits, keys, vals, kt, vt, hist, s));
+    bvh.lo_left = ensure<float4>(c, c->bvh_lo, 2 * nb - 1);
+    bvh.hi_esc = ensure<float4>(c, c->bvh_hi, 2 * nb - 1);
+    int* work = ensure<int>(c, c->bvh_work, 8 * nb);
+    unsigned long long* codes = ensure<unsigned long long>(c, c->bt_codes, nb);
+    CU(lsm::launch_batched_tree((int)nb, nm, vals, pair_of_b, mort, codes, b_box32, d_eob, bvh, work, roots,
+                                stops, s));
+  } else {
+    CU(cudaMemsetAsync(roots, 0xff, sizeof(int) * nm, s));
+    CU(cudaMemsetAsync(stops, 0xff, sizeof(int) * nm, s));
+  }
+  int64_t* offsets = ensure<int64_t>(c, c->offsets, na + 1);
+  int* counts = ensure<int>(c, c->counts, na);
+  int64_t* stmp = ensure<int64_t>(c, c->scan_tmp, lsm::scan_tmp_entries(na) + 1);
+  if (na > 0 && nb > 0)
+    CU(lsm::launch_query_batched(dim, false, na, a_box, pair_of_a, roots, stops, bvh, b_box, counts, nullptr,
+                                 nullptr, nullptr, s));
+  else if (na > 0)
+    CU(cudaMemsetAsync(counts, 0, sizeof(int) * na, s));
+  CU(lsm::launch_scan(na, counts, offsets, stmp, s));
+  int64_t* h = static_cast<int64_t*>(c->host_scalars) + 8;
+  int* hb = static_cast<int*>(c->host_scalars);
+  CU(cudaMemcpyAsync(h, offsets + na, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  REQUIRE(hb[0] == 0, "Invalid node index in an element list");
+  const int64_t nnz = *h;
+  int32_t* pa = ensure<int32_t>(c, c->pair_a, nnz);
+  int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);
+  if (nnz > 0)
+    CU(lsm::launch_query_batched(dim, true, na, a_box, pair_of_a, roots, stops, bvh, b_box, nullptr, offsets,
+                                 pa, pb, s));
+  c->dim = dim;
+  c->loc_a = c->loc_b = loc;
+  c->nel_a = na;
+  c->nel_b = nb;
+  c->ncand = nnz;
+  c->simplex_prep = true;
+  narrow(c, s);
+  lsm::Partial* tot = ensure<lsm::Partial>(c, c->bt_tot, nm);
+  int64_t* nc = ensure<int64_t>(c, c->bt_ncand, nm);
+  CU(lsm::launch_mesh_totals(nm, d_eoa, offsets, static_cast<double*>(c->pair_measure.p),
+                             static_cast<int32_t*>(c->pair_nout.p), tot, nc, s));
+  const size_t bytes = sizeof(lsm::Partial) * nm + sizeof(int64_t) * nm;
+  char* hs = static_cast<char*>(host_stage(c, bytes));
+  CU(cudaMemcpyAsync(hs, tot, sizeof(lsm::Partial) * nm, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(hs + sizeof(lsm::Partial) * nm, nc, sizeof(int64_t) * nm, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  const lsm::Partial* ht = reinterpret_cast<const lsm::Partial*>(hs);
+  const int64_t* hn = reinterpret_cast<const int64_t*>(hs + sizeof(lsm::Partial) * nm);
+  for (int i = 0; i < nm; ++i) {
+    if (totals) totals[idx[i]] = ht[i].sum;
+    if (ncand) ncand[idx[i]] = hn[i];
+    if (nint) nint[idx[i]] = (int64_t)ht[i].n_int;
   }
 }
 
@@ -728,15 +929,19 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context* ctx, int npairs, const l
   return guarded(c, [&] {
     REQUIRE(npairs >= 0 && (npairs == 0 || (a && b)), "invalid batch");
     cudaStream_t s = pick(c, stream);
+    std::vector<int> g2, g3;
     for (int i = 0; i < npairs; ++i) {
-      find_candidates(c, &a[i], &b[i], on_device, true, false, s);
-      narrow(c, s);
-      lsm_gpu_stats st{};
-      read_stats(c, &st, s);
-      if (totals) totals[i] = st.total_measure;
-      if (n_candidates) n_candidates[i] = st.n_candidates;
-      if (n_intersecting) n_intersecting[i] = st.n_intersecting;
+      check_mesh(c, &a[i], "A", true);
+      check_mesh(c, &b[i], "B", true);
+      REQUIRE(a[i].dim == b[i].dim, "Invalid dimension: pair %d mixes %dD and %dD", i, a[i].dim, b[i].dim);
+      REQUIRE(a[i].index_bytes == a[0].index_bytes && b[i].index_bytes == a[0].index_bytes,
+              "all meshes of a batch must use the same index width");
+      (a[i].dim == 2 ? g2 : g3).push_back(i);
     }
+    c->have_pairs = false;
+    c->ncand = -1;
+    if (!g2.empty()) run_batch_group(c, 2, g2, a, b, on_device, totals, n_candidates, n_intersecting, s);
+    if (!g3.empty()) run_batch_group(c, 3, g3, a, b, on_device, totals, n_candidates, n_intersecting, s);
   });
 }
 

@@ -37,11 +37,12 @@ int g_tet_bps = 0;
 }  // namespace
 
 // Blocks per SM of the persistent tet clipper (3: up to 170 registers per
-// thread, 4: up to 128).  LSM_TET_BLOCKS_PER_SM overrides the default.
+// thread, no spills; 4: up to 128, spills).  Default 3 (measured faster on
+// B200); LSM_TET_BLOCKS_PER_SM overrides it.
 int tet_blocks_per_sm() {
   if (g_tet_bps == 0) {
     const char* e = getenv("LSM_TET_BLOCKS_PER_SM");
-    g_tet_bps = (e && atoi(e) == 3) ? 3 : 4;
+    g_tet_bps = (e && atoi(e) == 4) ? 4 : 3;
   }
   return g_tet_bps;
 }
@@ -125,109 +126,150 @@ __device__ void block_reduce_partial(double sum, double err, unsigned long long 
 // ======================================================================
 // K1: element prep
 // ======================================================================
+// One element of the prep: gather, boxes, measure/tolerance, clip setup.
 // LOC = DIM + 1 for simplices; other LOC (quads, hexes) only get boxes,
 // which is all the candidate search needs.
+template <int DIM, int LOC, typename IDX>
+__device__ __forceinline__ void prep_element(int64_t e, const double* __restrict__ pos,
+                                             const IDX* __restrict__ row, int64_t nnodes, double* coords,
+                                             double* box64, float* box32, double* tolv, double* setup,
+                                             int* bad) {
+  constexpr bool SIMPLEX = LOC == DIM + 1;
+  double v[LOC * DIM];
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < LOC; ++k) {
+    int64_t node = (int64_t)row[k];
+    if (node < 0 || node >= nnodes) {
+      ok = false;
+      node = 0;
+    }
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) v[k * DIM + c] = pos[node * DIM + c];
+  }
+  if (!ok) atomicExch(bad, 1);
+  if (coords) {
+#pragma unroll
+    for (int j = 0; j < LOC * DIM; ++j) coords[e * LOC * DIM + j] = v[j];
+  }
+  double lo[DIM], hi[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) lo[c] = hi[c] = v[c];
+#pragma unroll
+  for (int k = 1; k < LOC; ++k)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      lo[c] = fmin(lo[c], v[k * DIM + c]);
+      hi[c] = fmax(hi[c], v[k * DIM + c]);
+    }
+  if (box64) {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      box64[e * 2 * DIM + c] = lo[c];
+      box64[e * 2 * DIM + DIM + c] = hi[c];
+    }
+  }
+  if (box32) {
+    float4 l = make_float4(0.f, 0.f, 0.f, 0.f), h = make_float4(0.f, 0.f, 0.f, 0.f);
+    l.x = __double2float_rd(lo[0]);
+    l.y = __double2float_rd(lo[1]);
+    h.x = __double2float_ru(hi[0]);
+    h.y = __double2float_ru(hi[1]);
+    if (DIM == 3) {
+      l.z = __double2float_rd(lo[DIM - 1]);
+      h.z = __double2float_ru(hi[DIM - 1]);
+    }
+    reinterpret_cast<float4*>(box32)[2 * e] = l;
+    reinterpret_cast<float4*>(box32)[2 * e + 1] = h;
+  }
+  if (!SIMPLEX) return;
+  double meas;
+  Tet t;
+  if (DIM == 2) {
+    meas = tri_area(v[0], v[1], v[2], v[3], v[4], v[5]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      t.x[k] = v[k * DIM + 0];
+      t.y[k] = v[k * DIM + 1];
+      t.z[k] = v[k * DIM + DIM - 1];
+    }
+    meas = tet_volume_v4(t);
+  }
+  const double tol = 10.0 * spacing(meas);
+  if (tolv) tolv[e] = tol;
+  if (setup) {
+    if (DIM == 2) {
+      Lines L;
+      tri_lines(v, L);
+      double* o = setup + e * kSetup2;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        o[4 * i + 0] = L.nx[i];
+        o[4 * i + 1] = L.ny[i];
+        o[4 * i + 2] = L.px[i];
+        o[4 * i + 3] = L.py[i];
+      }
+      o[12] = tol;
+      o[13] = 0.0;
+    } else {
+      Planes P;
+      tet_planes(t, P);
+      double* o = setup + e * kSetup3;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        o[4 * i + 0] = P.nx[i];
+        o[4 * i + 1] = P.ny[i];
+        o[4 * i + 2] = P.nz[i];
+        o[4 * i + 3] = P.c[i];
+      }
+      o[16] = tol;
+      o[17] = 0.0;
+      o[18] = 0.0;
+      o[19] = 0.0;
+    }
+  }
+}
+
 template <int DIM, int LOC, typename IDX>
 __global__ void k_prep(int64_t nel, const double* __restrict__ pos, const IDX* __restrict__ en,
                        double* coords, double* box64, float* box32, double* tolv, double* setup,
                        int* bad, int64_t nnodes) {
-  constexpr bool SIMPLEX = LOC == DIM + 1;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
+       e += (int64_t)gridDim.x * blockDim.x)
+    prep_element<DIM, LOC, IDX>(e, pos, en + e * LOC, nnodes, coords, box64, box32, tolv, setup, bad);
+}
+
+// Batched prep over the concatenation of many meshes.  Element e belongs to
+// mesh p = the last p with elem_off[p] <= e; its nodes are read through the
+// per-mesh pointer tables.  pair_of[e] receives p.
+__device__ __forceinline__ int find_mesh(const int64_t* __restrict__ off, int nm, int64_t e) {
+  int lo = 0, hi = nm;  // off[lo] <= e < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= e)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+template <int DIM, typename IDX>
+__global__ void k_prep_batched(int64_t nel, int nm, const int64_t* __restrict__ elem_off,
+                               const unsigned long long* __restrict__ pos_ptr,
+                               const unsigned long long* __restrict__ en_ptr,
+                               const int64_t* __restrict__ nnodes, double* coords, double* box64,
+                               float* box32, double* tolv, double* setup, int32_t* pair_of, int* bad) {
+  constexpr int LOC = DIM + 1;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
        e += (int64_t)gridDim.x * blockDim.x) {
-    double v[LOC * DIM];
-    bool ok = true;
-#pragma unroll
-    for (int k = 0; k < LOC; ++k) {
-      int64_t node = (int64_t)en[e * LOC + k];
-      if (node < 0 || node >= nnodes) {
-        ok = false;
-        node = 0;
-      }
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) v[k * DIM + c] = pos[node * DIM + c];
-    }
-    if (!ok) atomicExch(bad, 1);
-    if (coords) {
-#pragma unroll
-      for (int j = 0; j < LOC * DIM; ++j) coords[e * LOC * DIM + j] = v[j];
-    }
-    double lo[DIM], hi[DIM];
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) lo[c] = hi[c] = v[c];
-#pragma unroll
-    for (int k = 1; k < LOC; ++k)
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        lo[c] = fmin(lo[c], v[k * DIM + c]);
-        hi[c] = fmax(hi[c], v[k * DIM + c]);
-      }
-    if (box64) {
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        box64[e * 2 * DIM + c] = lo[c];
-        box64[e * 2 * DIM + DIM + c] = hi[c];
-      }
-    }
-    if (box32) {
-      float4 l = make_float4(0.f, 0.f, 0.f, 0.f), h = make_float4(0.f, 0.f, 0.f, 0.f);
-      l.x = __double2float_rd(lo[0]);
-      l.y = __double2float_rd(lo[1]);
-      h.x = __double2float_ru(hi[0]);
-      h.y = __double2float_ru(hi[1]);
-      if (DIM == 3) {
-        l.z = __double2float_rd(lo[DIM - 1]);
-        h.z = __double2float_ru(hi[DIM - 1]);
-      }
-      reinterpret_cast<float4*>(box32)[2 * e] = l;
-      reinterpret_cast<float4*>(box32)[2 * e + 1] = h;
-    }
-    if (!SIMPLEX) continue;
-    double meas;
-    Tet t;
-    if (DIM == 2) {
-      meas = tri_area(v[0], v[1], v[2], v[3], v[4], v[5]);
-    } else {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        t.x[k] = v[k * DIM + 0];
-        t.y[k] = v[k * DIM + 1];
-        t.z[k] = v[k * DIM + DIM - 1];
-      }
-      meas = tet_volume_v4(t);
-    }
-    const double tol = 10.0 * spacing(meas);
-    if (tolv) tolv[e] = tol;
-    if (setup) {
-      if (DIM == 2) {
-        Lines L;
-        tri_lines(v, L);
-        double* o = setup + e * kSetup2;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          o[4 * i + 0] = L.nx[i];
-          o[4 * i + 1] = L.ny[i];
-          o[4 * i + 2] = L.px[i];
-          o[4 * i + 3] = L.py[i];
-        }
-        o[12] = tol;
-        o[13] = 0.0;
-      } else {
-        Planes P;
-        tet_planes(t, P);
-        double* o = setup + e * kSetup3;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          o[4 * i + 0] = P.nx[i];
-          o[4 * i + 1] = P.ny[i];
-          o[4 * i + 2] = P.nz[i];
-          o[4 * i + 3] = P.c[i];
-        }
-        o[16] = tol;
-        o[17] = 0.0;
-        o[18] = 0.0;
-        o[19] = 0.0;
-      }
-    }
+    const int p = find_mesh(elem_off, nm, e);
+    const int64_t local = e - elem_off[p];
+    const double* pos = reinterpret_cast<const double*>(pos_ptr[p]);
+    const IDX* en = reinterpret_cast<const IDX*>(en_ptr[p]);
+    prep_element<DIM, LOC, IDX>(e, pos, en + local * LOC, nnodes[p], coords, box64, box32, tolv, setup, bad);
+    pair_of[e] = p;
   }
 }
 
@@ -258,6 +300,26 @@ cudaError_t launch_prep(int dim, int loc, int64_t nel, const double* pos, const 
     prep_dispatch_idx<3, 8>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes);
   else
     return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prep_batched(int dim, int64_t nel, int nm, const int64_t* elem_off,
+                                const unsigned long long* pos_ptr, const unsigned long long* en_ptr,
+                                const int64_t* nnodes, int idx_bytes, double* coords, double* box64,
+                                float* box32, double* tolv, double* setup, int32_t* pair_of, int* bad,
+                                cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  const int B = 256;
+  const int g = grid_for(nel, B, 8);
+  count_launch();
+  if (dim == 2 && idx_bytes == 4)
+    k_prep_batched<2, int32_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32, tolv, setup, pair_of, bad);
+  else if (dim == 2)
+    k_prep_batched<2, int64_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32, tolv, setup, pair_of, bad);
+  else if (idx_bytes == 4)
+    k_prep_batched<3, int32_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32, tolv, setup, pair_of, bad);
+  else
+    k_prep_batched<3, int64_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32, tolv, setup, pair_of, bad);
   return cudaGetLastError();
 }
 
@@ -312,24 +374,47 @@ __global__ void k_root_partial(int64_t nel, const double* __restrict__ box64, do
 }
 
 template <int DIM>
-__global__ void k_root_final(int np, const double* partial, double* root) {
-  if (threadIdx.x != 0) return;
+__global__ void __launch_bounds__(256) k_root_final(int np, const double* partial, double* root) {
   double lo[DIM], hi[DIM];
 #pragma unroll
   for (int c = 0; c < DIM; ++c) {
     lo[c] = DBL_MAX;
     hi[c] = -DBL_MAX;
   }
-  for (int b = 0; b < np; ++b)
+  for (int b = threadIdx.x; b < np; b += blockDim.x)
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
       lo[c] = fmin(lo[c], partial[b * 2 * DIM + c]);
       hi[c] = fmax(hi[c], partial[b * 2 * DIM + DIM + c]);
     }
 #pragma unroll
-  for (int c = 0; c < DIM; ++c) {
-    root[c] = lo[c];
-    root[DIM + c] = hi[c];
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      lo[c] = fmin(lo[c], __shfl_down_sync(0xffffffffu, lo[c], o));
+      hi[c] = fmax(hi[c], __shfl_down_sync(0xffffffffu, hi[c], o));
+    }
+  __shared__ double sl[8][DIM], sh[8][DIM];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      sl[wid][c] = lo[c];
+      sh[wid][c] = hi[c];
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < 8; ++w)
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        lo[c] = fmin(lo[c], sl[w][c]);
+        hi[c] = fmax(hi[c], sh[w][c]);
+      }
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      root[c] = lo[c];
+      root[DIM + c] = hi[c];
+    }
   }
 }
 
@@ -341,10 +426,10 @@ cudaError_t launch_root_box(int dim, int64_t nel, const double* box64, double* p
   count_launch(2);
   if (dim == 2) {
     k_root_partial<2><<<g, B, 0, s>>>(nel, box64, partial);
-    k_root_final<2><<<1, 32, 0, s>>>(g, partial, rootbox);
+    k_root_final<2><<<1, 256, 0, s>>>(g, partial, rootbox);
   } else {
     k_root_partial<3><<<g, B, 0, s>>>(nel, box64, partial);
-    k_root_final<3><<<1, 32, 0, s>>>(g, partial, rootbox);
+    k_root_final<3><<<1, 256, 0, s>>>(g, partial, rootbox);
   }
   return cudaGetLastError();
 }
@@ -1161,13 +1246,14 @@ __global__ void __launch_bounds__(kTetBlock, BPS) k_clip_tets(
     int32_t* pair_nout, unsigned long long* work) {
   extern __shared__ double stack_mem[];
   TetStack<kTetBlock> stk{stack_mem + threadIdx.x};
+  // the current pair's four planes, plane L component j at my_planes[(4L+j)*kTetBlock]
+  double* my_planes = stack_mem + kTetSmemSlots * 12 * kTetBlock + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const int64_t npairs = (int64_t)*nlist;
   int64_t p = -1;
   bool exhausted = false;
   Tet t;
-  const double* planes = nullptr;
   double tol = 0.0, m = 0.0;
   int L = 0, sp = 0, kept = 0;
   unsigned levels = 0;
@@ -1185,8 +1271,14 @@ __global__ void __launch_bounds__(kTetBlock, BPS) k_clip_tets(
           p = list[q];
           const int a = pa[p], b = pb[p];
           load_tet(coords_a + (int64_t)a * 12, t);
-          planes = setup_b + (int64_t)b * kSetup3;
-          tol = fmin(tol_a[a], planes[16]);
+          const double2* pl = reinterpret_cast<const double2*>(setup_b + (int64_t)b * kSetup3);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const double2 v = __ldg(pl + j);
+            my_planes[(2 * j) * kTetBlock] = v.x;
+            my_planes[(2 * j + 1) * kTetBlock] = v.y;
+          }
+          tol = fmin(tol_a[a], setup_b[(int64_t)b * kSetup3 + 16]);
           m = 0.0;
           L = 0;
           sp = 0;
@@ -1199,8 +1291,8 @@ __global__ void __launch_bounds__(kTetBlock, BPS) k_clip_tets(
     }
     if (__all_sync(0xffffffffu, p < 0)) break;
     if (p < 0) continue;
-    double nx, ny, nz, c;
-    load_plane(planes, L, nx, ny, nz, c);
+    const double nx = my_planes[(4 * L + 0) * kTetBlock], ny = my_planes[(4 * L + 1) * kTetBlock];
+    const double nz = my_planes[(4 * L + 2) * kTetBlock], c = my_planes[(4 * L + 3) * kTetBlock];
     auto leaf = [&](const Tet& o) { m = m + tet_volume_v1(o); };
     DfsSink<TetStack<kTetBlock>, decltype(leaf)> sink{stk, leaf, sp, L == 3, tol, 0, 0};
     const int k = clip_tet_plane(t, nx, ny, nz, c, sink);
@@ -1259,7 +1351,7 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                                         pair_nout, overflow_list, overflow_count);
   } else {
     // work[0]: survivor count, work[1]: clipper pair counter
-    const size_t smem = sizeof(double) * kTetSmemSlots * 12 * kTetBlock;
+    const size_t smem = sizeof(double) * (kTetSmemSlots * 12 + 16) * kTetBlock;
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
     count_launch();
     k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, pair_a, pair_b, coords_a, setup_b,
@@ -1284,7 +1376,7 @@ cudaError_t launch_reduce_pairs(int64_t npairs, const double* pair_measure, cons
 }
 
 cudaError_t init_device_attributes() {
-  const int smem = (int)(sizeof(double) * kTetSmemSlots * 12 * kTetBlock);
+  const int smem = (int)(sizeof(double) * (kTetSmemSlots * 12 + 16) * kTetBlock);
   cudaError_t e = cudaFuncSetAttribute(k_clip_tets<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_clip_tets<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1304,21 +1396,28 @@ cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overf
 // ======================================================================
 // K7: finalize totals and per-row sums
 // ======================================================================
-__global__ void k_finalize(const Partial* __restrict__ partials, int np, Partial* out) {
-  if (threadIdx.x != 0) return;
-  Partial p{0.0, 0.0, 0ull, 0ull};
-  for (int b = 0; b < np; ++b) {
-    two_sum_merge(p.sum, p.err, partials[b].sum, partials[b].err);
-    p.n_int += partials[b].n_int;
-    p.n_out += partials[b].n_out;
+// Merges the per-block partials in a fixed tree order (deterministic).
+__global__ void __launch_bounds__(1024) k_finalize(const Partial* __restrict__ partials, int np, Partial* out) {
+  double sum = 0.0, err = 0.0;
+  unsigned long long ni = 0, no = 0;
+  for (int b = threadIdx.x; b < np; b += blockDim.x) {
+    two_sum_merge(sum, err, partials[b].sum, partials[b].err);
+    ni += partials[b].n_int;
+    no += partials[b].n_out;
   }
-  p.sum = p.sum + p.err;
-  *out = p;
+  __shared__ Partial r;
+  block_reduce_partial<1024>(sum, err, ni, no, &r);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Partial p = r;
+    p.sum = p.sum + p.err;
+    *out = p;
+  }
 }
 
 cudaError_t launch_finalize(const Partial* partials, int npartials, Partial* out, cudaStream_t s) {
   count_launch();
-  k_finalize<<<1, 32, 0, s>>>(partials, npartials, out);
+  k_finalize<<<1, 1024, 0, s>>>(partials, npartials, out);
   return cudaGetLastError();
 }
 
@@ -1349,6 +1448,235 @@ cudaError_t launch_i32_to_i64(int64_t n, const int32_t* in, int64_t* out, cudaSt
   if (n <= 0) return cudaSuccess;
   count_launch();
   k_i32_to_i64<<<grid_for(n, 256, 8), 256, 0, s>>>(n, in, out);
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// Batched search: one LBVH over many meshes, one subtree per mesh
+// ======================================================================
+// After sorting the B elements of all meshes by (mesh, Morton) the combined
+// 64-bit keys (mesh << 32 | Morton) give a Karras hierarchy in which every
+// mesh's elements form one subtree (they share the mesh-id prefix, no other
+// key does).  A query of mesh p starts at p's subtree root and stops at the
+// root's escape node.
+__global__ void k_pair_keys(int64_t n, const int32_t* __restrict__ vals, const int32_t* __restrict__ pair_of,
+                            uint32_t* keys) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    keys[i] = (uint32_t)pair_of[vals[i]];
+}
+
+__global__ void k_combined_codes(int64_t n, const int32_t* __restrict__ vals, const int32_t* __restrict__ pair_of,
+                                 const uint32_t* __restrict__ mort, unsigned long long* codes) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = vals[i];
+    codes[i] = ((unsigned long long)(uint32_t)pair_of[v] << 32) | (unsigned long long)mort[v];
+  }
+}
+
+__device__ __forceinline__ int bvh_delta64(const unsigned long long* __restrict__ codes, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  const unsigned long long a = codes[i], b = codes[j];
+  if (a != b) return __clzll((long long)(a ^ b));
+  return 64 + __clz((uint32_t)i ^ (uint32_t)j);
+}
+
+__global__ void k_bvh_internal64(int n, const unsigned long long* __restrict__ codes, int* parent, int* rope,
+                                 int* last, int* left, int* right, const int64_t* __restrict__ mesh_off,
+                                 int* roots) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int d = (bvh_delta64(codes, n, i, i + 1) - bvh_delta64(codes, n, i, i - 1)) >= 0 ? 1 : -1;
+  const int dmin = bvh_delta64(codes, n, i, i - d);
+  int lmax = 2;
+  while (bvh_delta64(codes, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (bvh_delta64(codes, n, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int dnode = bvh_delta64(codes, n, i, j);
+  int s = 0;
+  int t = l;
+  do {
+    t = (t + 1) >> 1;
+    if (bvh_delta64(codes, n, i, i + (s + t) * d) > dnode) s += t;
+  } while (t > 1);
+  const int gamma = i + s * d + (d < 0 ? -1 : 0);
+  const int first = i < j ? i : j;
+  const int lst = i < j ? j : i;
+  const int lc = (first == gamma) ? (n - 1) + gamma : gamma;
+  const int rc = (lst == gamma + 1) ? (n - 1) + gamma + 1 : gamma + 1;
+  left[i] = lc;
+  right[i] = rc;
+  parent[lc] = i;
+  parent[rc] = i;
+  rope[gamma + 1] = rc;
+  last[i] = lst;
+  const int mesh = (int)(codes[first] >> 32);
+  if (mesh_off[mesh] == first && mesh_off[mesh + 1] - 1 == lst) roots[mesh] = i;
+}
+
+// Roots of single-element meshes, and the stop node (the root's escape) of
+// every mesh.  Meshes without elements get root -1.
+__global__ void k_mesh_roots(int nm, int n, const int64_t* __restrict__ mesh_off, const int* __restrict__ rope,
+                             const int* __restrict__ last, int* roots, int* stops) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nm) return;
+  const int64_t cnt = mesh_off[p + 1] - mesh_off[p];
+  int r = -1;
+  if (cnt == 1)
+    r = (n - 1) + (int)mesh_off[p];
+  else if (cnt > 1)
+    r = roots[p];
+  roots[p] = r;
+  stops[p] = r >= 0 ? bvh_escape(n, r, rope, last) : -1;
+}
+
+cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const int32_t* pair_of_b,
+                                const uint32_t* mort, unsigned long long* codes, const float* box32,
+                                const int64_t* mesh_off_b, BVH bvh, int* work, int* roots, int* stops,
+                                cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  int* parent = work;
+  int* rope = parent + (2 * n - 1);
+  int* visit = rope + n;
+  int* last = visit + n;
+  int* left = last + n;
+  int* right = left + n;
+  count_launch(4);
+  k_combined_codes<<<grid_for(n, 256, 8), 256, 0, s>>>(n, sorted_vals, pair_of_b, mort, codes);
+  cudaMemsetAsync(visit, 0, sizeof(int) * n, s);
+  cudaMemsetAsync(rope, 0xff, sizeof(int) * n, s);
+  cudaMemsetAsync(roots, 0xff, sizeof(int) * nm, s);
+  if (n > 1) k_bvh_internal64<<<(n - 1 + 255) / 256, 256, 0, s>>>(n, codes, parent, rope, last, left, right, mesh_off_b, roots);
+  cudaMemsetAsync(parent, 0xff, sizeof(int), s);
+  k_mesh_roots<<<(nm + 255) / 256, 256, 0, s>>>(nm, n, mesh_off_b, rope, last, roots, stops);
+  k_bvh_refit<<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
+                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_keys(int64_t n, const int32_t* vals, const int32_t* pair_of, uint32_t* keys,
+                             cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launch();
+  k_pair_keys<<<grid_for(n, 256, 8), 256, 0, s>>>(n, vals, pair_of, keys);
+  return cudaGetLastError();
+}
+
+template <int DIM, bool FILL>
+__global__ void __launch_bounds__(128) k_query_batched(int64_t nel_a, const double* __restrict__ box64_a,
+                                                       const int32_t* __restrict__ pair_of_a,
+                                                       const int* __restrict__ roots, const int* __restrict__ stops,
+                                                       const float4* __restrict__ lo_left,
+                                                       const float4* __restrict__ hi_esc, int n,
+                                                       const double* __restrict__ box64_b, int* counts,
+                                                       const int64_t* __restrict__ offsets, int32_t* pair_a,
+                                                       int32_t* pair_b) {
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < nel_a;
+       a += (int64_t)gridDim.x * blockDim.x) {
+    double lo[DIM], hi[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      lo[c] = box64_a[a * 2 * DIM + c];
+      hi[c] = box64_a[a * 2 * DIM + DIM + c];
+    }
+    float ql[3], qh[3];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      ql[c] = __double2float_rd(lo[c]);
+      qh[c] = __double2float_ru(hi[c]);
+    }
+    const int mesh = pair_of_a[a];
+    int node = roots[mesh];
+    const int stop = stops[mesh];
+    int cnt = 0;
+    int64_t out = FILL ? offsets[a] : 0;
+    const int nodes = 2 * n - 1;
+    for (int guard = 0; node >= 0 && node != stop && guard < 2 * n + 1; ++guard) {
+      if (node >= nodes) break;  // never taken for a well-formed hierarchy
+      const float4 L = __ldg(&lo_left[node]);
+      const float4 H = __ldg(&hi_esc[node]);
+      bool ov = H.x > ql[0] && L.x < qh[0] && H.y > ql[1] && L.y < qh[1];
+      if (DIM == 3) ov = ov && H.z > ql[2] && L.z < qh[2];
+      if (ov) {
+        const int w = __float_as_int(L.w);
+        if (node < n - 1) {
+          node = w;
+          continue;
+        }
+        const double* bb = box64_b + (int64_t)w * 2 * DIM;
+        bool ex = true;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) ex = ex && (hi[c] > bb[c]) && (lo[c] < bb[DIM + c]);
+        if (ex) {
+          if (FILL) {
+            pair_a[out + cnt] = (int32_t)a;
+            pair_b[out + cnt] = w;
+          }
+          ++cnt;
+        }
+      }
+      node = __float_as_int(H.w);
+    }
+    if (!FILL) counts[a] = cnt;
+  }
+}
+
+cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double* box64_a,
+                                 const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
+                                 const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
+                                 int32_t* pair_b, cudaStream_t s) {
+  if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
+  const int B = 128;
+  const int g = grid_for(nel_a, B, 16);
+  count_launch();
+  if (dim == 2) {
+    if (fill)
+      k_query_batched<2, true><<<g, B, 0, s>>>(nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+    else
+      k_query_batched<2, false><<<g, B, 0, s>>>(nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+  } else {
+    if (fill)
+      k_query_batched<3, true><<<g, B, 0, s>>>(nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+    else
+      k_query_batched<3, false><<<g, B, 0, s>>>(nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+  }
+  return cudaGetLastError();
+}
+
+// Per-mesh-pair totals: block p reduces the candidates of mesh pair p (CSR
+// rows elem_off_a[p] .. elem_off_a[p+1]-1) in a fixed order.
+__global__ void __launch_bounds__(256) k_mesh_totals(int nm, const int64_t* __restrict__ elem_off_a,
+                                                     const int64_t* __restrict__ offsets,
+                                                     const double* __restrict__ pm, const int32_t* __restrict__ pn,
+                                                     Partial* out, int64_t* ncand) {
+  const int p = blockIdx.x;
+  if (p >= nm) return;
+  const int64_t beg = offsets[elem_off_a[p]], end = offsets[elem_off_a[p + 1]];
+  double sum = 0.0, err = 0.0;
+  unsigned long long ni = 0, no = 0;
+  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    cs_add(sum, err, pm[i]);
+    const int k = pn[i];
+    ni += k > 0;
+    no += k;
+  }
+  __shared__ Partial r;
+  block_reduce_partial<256>(sum, err, ni, no, &r);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Partial q = r;
+    q.sum = q.sum + q.err;
+    out[p] = q;
+    ncand[p] = end - beg;
+  }
+}
+
+cudaError_t launch_mesh_totals(int nm, const int64_t* elem_off_a, const int64_t* offsets, const double* pm,
+                               const int32_t* pn, Partial* out, int64_t* ncand, cudaStream_t s) {
+  if (nm <= 0) return cudaSuccess;
+  count_launch();
+  k_mesh_totals<<<nm, 256, 0, s>>>(nm, elem_off_a, offsets, pm, pn, out, ncand);
   return cudaGetLastError();
 }
 

@@ -124,4 +124,26 @@ cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const
                            Partial* partials, cudaStream_t s);
 int p1_grid_blocks(int dim);
 
+// ---- batched (many mesh pairs per launch) --------------------------------
+cudaError_t launch_prep_batched(int dim, int64_t nel, int nm, const int64_t* elem_off,
+                                const unsigned long long* pos_ptr, const unsigned long long* en_ptr,
+                                const int64_t* nnodes, int idx_bytes, double* coords, double* box64,
+                                float* box32, double* tolv, double* setup, int32_t* pair_of, int* bad,
+                                cudaStream_t s);
+// keys[i] = pair_of[vals[i]] (second sort pass: by mesh)
+cudaError_t launch_pair_keys(int64_t n, const int32_t* vals, const int32_t* pair_of, uint32_t* keys,
+                             cudaStream_t s);
+// One LBVH over all B meshes (sorted by mesh, then Morton); roots/stops per
+// mesh.  codes: n u64; work: 8n ints.
+cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const int32_t* pair_of_b,
+                                const uint32_t* mort, unsigned long long* codes, const float* box32,
+                                const int64_t* mesh_off_b, BVH bvh, int* work, int* roots, int* stops,
+                                cudaStream_t s);
+cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double* box64_a,
+                                 const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
+                                 const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
+                                 int32_t* pair_b, cudaStream_t s);
+cudaError_t launch_mesh_totals(int nm, const int64_t* elem_off_a, const int64_t* offsets, const double* pm,
+                               const int32_t* pn, Partial* out, int64_t* ncand, cudaStream_t s);
+
 }  // namespace lsm

@@ -80,6 +80,23 @@ def test_config_tet3d_27x32_full(gpu_ctx, oracle_mod):
     assert st.n_candidates > 10_000_000
 
 
+def test_config_tri2d_777x1024_rot7_full(gpu_ctx, oracle_mod):
+    # 1.2M x 2.1M triangles, target rotated 7 degrees and clamped (it has
+    # degenerate and folded elements, so the total is the oracle's, not 1)
+    dim, A, B = M.config_meshes("tri2d_777x1024_rot7")
+    st = check_pipeline(gpu_ctx, oracle_mod, dim, A, B)
+    assert st.n_candidates > 10_000_000
+
+
+def test_config_tri2d_777x1024_rot7_p1_mass(gpu_ctx, oracle_mod):
+    dim, A, B = M.config_meshes("tri2d_777x1024_rot7")
+    u, v = A[0][:, 0], B[0][:, 1]
+    integral, _ = gpu_ctx.p1_mass(A, B, u, v)
+    ip, ind = oracle_mod.tree_finder(dim, A, B)
+    i_o, meas_o, _ = oracle_mod.p1_mass(dim, A, B, ip, ind, u, v)
+    assert abs(integral - i_o) <= 1e-12 * abs(i_o)
+
+
 def test_int64_and_int32_enlists_agree(gpu_ctx):
     dim, A, B = M.config_meshes("small3d_5x6")
     s32, _ = gpu_ctx.supermesh(A, B)
@@ -141,7 +158,7 @@ def test_legacy_tree_finder_quads(oracle_mod):
     cj, ci = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
     v00 = (cj * (n + 1) + ci).ravel()
     quads = np.stack([v00, v00 + 1, v00 + n + 2, v00 + n + 1], axis=1).astype(np.int32)
-    _, B = M.grid2d(5, 0, 0.3), M.grid2d(5, 0, 0.3)
+    B = M.grid2d(5, 0, 0.3)
     ip, ind = lsm.tree_intersection_finder(pos, quads, *B)
     ip_o, ind_o = oracle_mod.brute_force_finder(2, (pos, quads), B)
     assert np.array_equal(ip, ip_o)
@@ -262,5 +279,33 @@ def test_batched_matches_single(gpu_ctx):
     totals, nc, ni = gpu_ctx.supermesh_batched([(A, B) for _, A, B in pairs])
     for i, (dim, A, B) in enumerate(pairs):
         st, _ = gpu_ctx.supermesh(A, B)
-        assert totals[i] == st.total_measure and nc[i] == st.n_candidates and ni[i] == st.n_intersecting
+        assert nc[i] == st.n_candidates and ni[i] == st.n_intersecting
+        assert abs(totals[i] - st.total_measure) <= 1e-14
         assert abs(totals[i] - 1.0) <= 1e-12
+
+
+def test_batched_vs_oracle(gpu_ctx, oracle_mod):
+    pairs = M.batched_pairs(24, seed=16, emin=1e2, emax=3e3)
+    totals, nc, ni = gpu_ctx.supermesh_batched([(A, B) for _, A, B in pairs])
+    for i, (dim, A, B) in enumerate(pairs):
+        ip, ind = oracle_mod.tree_finder(dim, A, B)
+        _, _, _, st = oracle_mod.narrow(dim, A, B, ip, ind)
+        assert nc[i] == st.n_candidates and ni[i] == st.n_intersecting
+        assert abs(totals[i] - st.total) <= REL_TOL
+
+
+def test_batched_device_inputs_and_empty_mesh(gpu_ctx):
+    torch = pytest.importorskip("torch")
+    pairs = M.batched_pairs(8, seed=26, emin=1e2, emax=1e3)
+    host = [(A, B) for _, A, B in pairs]
+    # one pair with an empty target mesh
+    A0, B0 = host[1]
+    host[1] = ((A0[0], A0[1][:0]), B0)
+    t_ref, nc_ref, ni_ref = gpu_ctx.supermesh_batched(host)
+    assert nc_ref[1] == 0 and t_ref[1] == 0.0
+    dev = torch.device("cuda:0")
+    tdev = [tuple((torch.from_numpy(np.ascontiguousarray(x[0])).to(dev), torch.from_numpy(np.ascontiguousarray(x[1])).to(dev))
+                  for x in pr) for pr in host]
+    torch.cuda.synchronize()
+    t, nc, ni = gpu_ctx.supermesh_batched(tdev, on_device=True)
+    assert np.array_equal(nc, nc_ref) and np.array_equal(ni, ni_ref) and np.array_equal(t, t_ref)
