@@ -237,12 +237,101 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, world, rank, local):
+    """256 independent mesh pairs (half 2D, half 3D, element counts
+    log-uniform in [1e3, 1e5]) per step through libsupermesh_gpu_supermesh_batched."""
+    import torch
+
+    import libsupermesh_b200 as lsm
+    from libsupermesh_b200 import meshes as M
+
+    pairs = M.batched_pairs(256, seed=6)
+    dev = torch.device("cuda", local)
+    ctx = lsm.Context(local)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    probe = load_probe()
+    flush_buf = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    tdev = [tuple((torch.from_numpy(m[0]).to(dev), torch.from_numpy(m[1]).to(dev)) for m in (A, B))
+            for _, A, B in pairs]
+    host = []
+    h2d = 0
+    for _, A, B in pairs:
+        pin = []
+        for m in (A, B):
+            pin.append((torch.from_numpy(m[0]).pin_memory().numpy(), torch.from_numpy(m[1]).pin_memory().numpy()))
+            h2d += m[0].nbytes + m[1].nbytes
+        host.append(tuple(pin))
+    torch.cuda.synchronize()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier(world)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        out = None
+        for e0, e1 in evs:
+            probe.lsm_probe_flush_l2(flush_buf.data_ptr(), L2_FLUSH_BYTES, sp)
+            e0.record(stream)
+            out = fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return sum(e0.elapsed_time(e1) for e0, e1 in evs), out
+
+    launches0 = lsm.kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, (tot, nc, ni) = timed(lambda: ctx.supermesh_batched(tdev, on_device=True, stream=sp), args.steps, args.warmup)
+    clock_rec = clocks.stop()
+    launches = (lsm.kernel_launches() - launches0) // (args.steps + args.warmup)
+    ms = all_max(ms, world)
+    ncand = int(nc.sum())
+    value = ncand * args.steps * world / (ms * 1e-3)
+    ms_e2e, (tot2, nc2, _) = timed(lambda: ctx.supermesh_batched(host, on_device=False, stream=sp), args.steps,
+                                   max(3, args.warmup // 2))
+    ms_e2e = all_max(ms_e2e, world)
+    assert np.array_equal(nc2, nc) and np.array_equal(tot2, tot)
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "mesh_pairs": len(pairs), "candidates": ncand,
+                   "intersecting": int(ni.sum()), "max_total_err": float(np.abs(tot - 1.0).max()),
+                   "l2": "flushed before every timed step (256 MiB write, outside the events)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": ncand * args.steps * world / (ms_e2e * 1e-3), "unit": "pairs/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": len(pairs) * 24,
+                "ms_per_step": ms_e2e / args.steps},
+        "gpu_launches": launches * args.steps,
+        "clocks": clock_rec,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        sample = pairs[::16]
+        t0 = time.perf_counter()
+        cand = 0
+        for dim, A, B in sample:
+            cand += oracle.supermesh(dim, A, B, nthreads=1).n_candidates
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": cand / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
+                                "sample": f"every 16th mesh pair ({len(sample)} pairs, {cand} candidates), "
+                                          f"oracle finder + clipping, 1 thread, {dt:.2f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def run_ours(args, world, rank, local):
     import torch
 
     import libsupermesh_b200 as lsm
     from libsupermesh_b200 import meshes as M
 
+    if args.workload == "batched256":
+        return run_batched(args, world, rank, local)
     dim, A, B = M.config_meshes(args.workload)
     dev = torch.device("cuda", local)
     ctx = lsm.Context(local)

@@ -100,6 +100,13 @@ int libsupermesh_gpu_supermesh(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
  * search. */
 int libsupermesh_gpu_clip_candidates(lsm_gpu_context *ctx, lsm_gpu_stats *stats, void *stream);
 
+/* As libsupermesh_gpu_clip_candidates, taking the candidates in the order
+ * given by `order` (a permutation of 0 .. n_candidates-1, e.g. a schedule that
+ * groups pairs of similar cost into the same warps).  The results, stored
+ * per candidate, do not depend on the order. */
+int libsupermesh_gpu_clip_candidates_ordered(lsm_gpu_context *ctx, const int32_t *order, int on_device,
+                                             lsm_gpu_stats *stats, void *stream);
+
 /* Per-pair results of the last libsupermesh_gpu_supermesh call, in CSR
  * order: measure[n_candidates] and n_out[n_candidates]. */
 int libsupermesh_gpu_get_pair_results(lsm_gpu_context *ctx, double *measure,

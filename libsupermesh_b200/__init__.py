@@ -104,6 +104,8 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_supermesh.argtypes = [vp, mp, mp, ctypes.c_int, vp, ctypes.POINTER(Stats), vp]
     L.libsupermesh_gpu_get_pair_results.argtypes = [vp, vp, vp, ctypes.c_int, vp]
     L.libsupermesh_gpu_clip_candidates.argtypes = [vp, ctypes.POINTER(Stats), vp]
+    L.libsupermesh_gpu_clip_candidates_ordered.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(Stats), vp]
+    L.libsupermesh_gpu_clip_candidates_ordered.restype = ctypes.c_int
     L.libsupermesh_gpu_intersect_pairs.argtypes = [vp, ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp, vp,
                                                    ctypes.c_int, vp]
     L.libsupermesh_gpu_p1_mass.argtypes = [vp, mp, mp, vp, vp, vp, _dp, ctypes.c_int, vp]
@@ -214,6 +216,15 @@ class Context:
         self._check(self.lib.libsupermesh_gpu_clip_candidates(self._h, ctypes.byref(st), stream))
         return st
 
+    def clip_candidates_ordered(self, order, on_device: bool = False, stream: int | None = None) -> Stats:
+        """Narrow phase over the last candidates, taken in the given order."""
+        st = Stats()
+        if not on_device:
+            order = np.ascontiguousarray(order, dtype=np.int32)
+        self._check(self.lib.libsupermesh_gpu_clip_candidates_ordered(self._h, _ptr(order), int(on_device),
+                                                                      ctypes.byref(st), stream))
+        return st
+
     def pair_results(self, n: int):
         m = np.zeros(max(n, 1), dtype=np.float64)
         k = np.zeros(max(n, 1), dtype=np.int32)
@@ -251,7 +262,7 @@ class Context:
                                                       _ptr(v), _ptr(blocks), ctypes.byref(integral), 0, None))
         return (integral.value if u is not None else None), (blocks[:n] if blocks is not None else None)
 
-    def supermesh_batched(self, pairs, on_device: bool = False):
+    def supermesh_batched(self, pairs, on_device: bool = False, stream: int | None = None):
         """pairs: list of (mesh_a, mesh_b).  Returns (totals, n_candidates,
         n_intersecting) as numpy arrays."""
         n = len(pairs)
@@ -266,7 +277,7 @@ class Context:
         nc = np.zeros(max(n, 1), dtype=np.int64)
         ni = np.zeros(max(n, 1), dtype=np.int64)
         self._check(self.lib.libsupermesh_gpu_supermesh_batched(self._h, n, A, B, int(on_device), totals.ctypes.data,
-                                                                nc.ctypes.data, ni.ctypes.data, None))
+                                                                nc.ctypes.data, ni.ctypes.data, stream))
         return totals[:n], nc[:n], ni[:n]
 
 

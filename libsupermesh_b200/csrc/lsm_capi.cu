@@ -318,7 +318,7 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
 
 // Narrow phase over the current candidates.  Leaves the merged totals in
 // c->totals (one lsm::Partial).
-void narrow(Ctx* c, cudaStream_t s) {
+void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
   const int64_t nnz = c->ncand;
   double* pm = ensure<double>(c, c->pair_measure, nnz);
   int32_t* pn = ensure<int32_t>(c, c->pair_nout, nnz);
@@ -333,7 +333,7 @@ void narrow(Ctx* c, cudaStream_t s) {
   unsigned long long* work = reinterpret_cast<unsigned long long*>(bad_flag(c) + 8);
   CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                       static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
-                      static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s));
+                      static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order));
   if (c->dim == 2)
     CU(lsm::launch_clip_tris_wide(ovf, ovf_count, nnz, static_cast<int32_t*>(c->pair_a.p),
                                   static_cast<int32_t*>(c->pair_b.p), static_cast<double*>(c->a_coords.p),
@@ -826,6 +826,26 @@ int libsupermesh_gpu_clip_candidates(lsm_gpu_context* ctx, lsm_gpu_stats* stats,
     }
     cudaStream_t s = pick(c, stream);
     narrow(c, s);
+    read_stats(c, stats, s);
+  });
+}
+
+int libsupermesh_gpu_clip_candidates_ordered(lsm_gpu_context* ctx, const int32_t* order, int on_device,
+                                              lsm_gpu_stats* stats, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    if (c->ncand < 0 || !c->simplex_prep) {
+      set_error(c, "no simplex candidate search has run on this context");
+      throw Fail{LSM_ERROR_STATE};
+    }
+    cudaStream_t s = pick(c, stream);
+    const int32_t* d = order;
+    if (order && !on_device) {
+      int32_t* t = ensure<int32_t>(c, c->x_nout, c->ncand);
+      CU(cudaMemcpyAsync(t, order, sizeof(int32_t) * c->ncand, cudaMemcpyHostToDevice, s));
+      d = t;
+    }
+    narrow(c, s, d);
     read_stats(c, stats, s);
   });
 }

@@ -981,11 +981,13 @@ __global__ void __launch_bounds__(kTriBlock) k_clip_tris(int64_t npairs, const i
                                                          const double* __restrict__ tol_a,
                                                          const double* __restrict__ setup_b,
                                                          double* pair_measure, int32_t* pair_nout,
-                                                         int32_t* ovf_list, int* ovf_count) {
+                                                         int32_t* ovf_list, int* ovf_count,
+                                                         const int32_t* __restrict__ order) {
   __shared__ double poly[2 * 2 * kTriCap * kTriBlock];
   SmemPoly<kTriBlock> p{poly + threadIdx.x}, q{poly + 2 * kTriCap * kTriBlock + threadIdx.x};
-  for (int64_t i = (int64_t)blockIdx.x * kTriBlock + threadIdx.x; i < npairs;
-       i += (int64_t)gridDim.x * kTriBlock) {
+  for (int64_t j = (int64_t)blockIdx.x * kTriBlock + threadIdx.x; j < npairs;
+       j += (int64_t)gridDim.x * kTriBlock) {
+    const int64_t i = order ? (int64_t)order[j] : j;
     const int a = pa[i], b = pb[i];
     const double* va = coords_a + (int64_t)a * 6;
     Lines L;
@@ -1185,7 +1187,10 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 // plane and discarded, so the reference returns no tets: the pair's result is
 // written here (0 tets, measure 0) and only the remaining pairs are listed
 // for the clipper.
-__global__ void __launch_bounds__(256) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ pa,
+// `order` (optional) lists the pairs in the order the clipper should take
+// them (a schedule); survivors are appended in that order, warp by warp.
+__global__ void __launch_bounds__(256) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ order,
+                                                        const int32_t* __restrict__ pa,
                                                         const int32_t* __restrict__ pb,
                                                         const double* __restrict__ coords_a,
                                                         const double* __restrict__ setup_b,
@@ -1194,9 +1199,11 @@ __global__ void __launch_bounds__(256) k_prefilter_tets(int64_t npairs, const in
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < npairs; base += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = base + threadIdx.x;
+    const int64_t j = base + threadIdx.x;
     bool live = false;
-    if (i < npairs) {
+    int64_t i = j;
+    if (j < npairs) {
+      if (order) i = order[j];
       const int a = pa[i], b = pb[i];
       Tet t;
       load_tet(coords_a + (int64_t)a * 12, t);
@@ -1343,18 +1350,19 @@ int clip_grid_blocks(int dim) {
 cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                         const double* coords_a, const double* tol_a, const double* setup_b,
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
-                        int* overflow_count, unsigned long long* work, cudaStream_t s) {
+                        int* overflow_count, unsigned long long* work, cudaStream_t s,
+                        const int32_t* order) {
   const int g = clip_grid_blocks(dim);
   count_launch();
   if (dim == 2) {
     k_clip_tris<<<g, kTriBlock, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure,
-                                        pair_nout, overflow_list, overflow_count);
+                                        pair_nout, overflow_list, overflow_count, order);
   } else {
     // work[0]: survivor count, work[1]: clipper pair counter
     const size_t smem = sizeof(double) * (kTetSmemSlots * 12 + 16) * kTetBlock;
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
     count_launch();
-    k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, pair_a, pair_b, coords_a, setup_b,
+    k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, setup_b,
                                                               pair_measure, pair_nout, overflow_list, work);
     if (tet_blocks_per_sm() == 3)
       k_clip_tets<3><<<sm_count() * 3, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,

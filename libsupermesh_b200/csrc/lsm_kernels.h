@@ -79,11 +79,14 @@ cudaError_t launch_scan(int64_t n, const int* counts, int64_t* offsets, int64_t*
 // buffers; launch_clip_tris_wide re-runs them.  3D: overflow_list (npairs
 // entries) receives the pairs that survive the exact early-out; `work`
 // holds two counters (survivors, clipper progress), reset by the launch.
+// `order` (optional, npairs entries) is the schedule: the pairs in the order
+// in which the clipper takes them.  Results do not depend on it.
 int clip_grid_blocks(int dim);
 cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                         const double* coords_a, const double* tol_a, const double* setup_b,
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
-                        int* overflow_count, unsigned long long* work, cudaStream_t s);
+                        int* overflow_count, unsigned long long* work, cudaStream_t s,
+                        const int32_t* order = nullptr);
 // Opt-in shared-memory limits for the clip kernels on the current device.
 cudaError_t init_device_attributes();
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,

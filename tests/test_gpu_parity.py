@@ -274,6 +274,19 @@ def test_device_resident_inputs(gpu_ctx):
     assert np.array_equal(out.cpu().numpy(), em_ref)
 
 
+@pytest.mark.parametrize("name", ["small2d_30x41", "small3d_8x9"])
+def test_ordered_clip_matches_unordered(gpu_ctx, name):
+    # a schedule changes only the order in which pairs are clipped
+    dim, A, B = M.config_meshes(name)
+    st, _ = gpu_ctx.supermesh(A, B)
+    pm, pn = gpu_ctx.pair_results(st.n_candidates)
+    order = np.random.default_rng(3).permutation(st.n_candidates).astype(np.int32)
+    st2 = gpu_ctx.clip_candidates_ordered(order)
+    pm2, pn2 = gpu_ctx.pair_results(st.n_candidates)
+    assert np.array_equal(pm, pm2) and np.array_equal(pn, pn2)
+    assert st2.as_dict() == st.as_dict()
+
+
 def test_batched_matches_single(gpu_ctx):
     pairs = M.batched_pairs(6, seed=6, emin=2e2, emax=2e3)
     totals, nc, ni = gpu_ctx.supermesh_batched([(A, B) for _, A, B in pairs])
