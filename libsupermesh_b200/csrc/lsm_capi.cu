@@ -47,7 +47,7 @@ struct Ctx {
   // candidates
   DevBuf counts, offsets, scan_tmp, pair_a, pair_b, i64_tmp;
   // narrow phase
-  DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals;
+  DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals, wq_scratch;
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
   DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand;
@@ -171,7 +171,7 @@ void fini_ctx(Ctx* c) {
                    &c->keys_tmp, &c->vals_tmp, &c->hist, &c->root_partial, &c->rootbox, &c->bvh_lo,
                    &c->bvh_hi, &c->bvh_work, &c->counts, &c->offsets, &c->scan_tmp, &c->pair_a,
                    &c->pair_b, &c->i64_tmp, &c->pair_measure, &c->pair_nout, &c->partials,
-                   &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->x_a, &c->x_b, &c->x_measure,
+                   &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->wq_scratch, &c->x_a, &c->x_b, &c->x_measure,
                    &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
                    &c->bt_ncand, &c->bt_stage_pa, &c->bt_stage_ea, &c->bt_stage_pb, &c->bt_stage_eb};
@@ -331,9 +331,26 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
   int* ovf_count = bad_flag(c) + 2;
   if (c->dim == 2) CU(cudaMemsetAsync(ovf_count, 0, sizeof(int), s));
   unsigned long long* work = reinterpret_cast<unsigned long long*>(bad_flag(c) + 8);
-  CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
-                      static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
-                      static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order));
+  bool queued = false;
+  if (c->dim == 3 && lsm::tet_clipper_variant() == 1) {
+    unsigned char* scr = ensure<unsigned char>(c, c->wq_scratch, (int64_t)lsm::wq_scratch_bytes());
+    int* err = bad_flag(c) + 16;
+    CU(lsm::launch_clip_tets_wq(nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+                                static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
+                                static_cast<double*>(c->b_setup.p), pm, pn, ovf, work, scr, err, s, order));
+    int* h = static_cast<int*>(c->host_scalars) + 4;
+    CU(cudaMemcpyAsync(h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(h + 2, work, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    queued = h[0] == 0;  // on overflow the per-lane clipper redoes the pairs
+    if (getenv("LSM_DEBUG"))
+      fprintf(stderr, "task-queue clipper: err=%d survivors=%llu deepest clip stack=%llu\n", h[0],
+              reinterpret_cast<unsigned long long*>(h + 2)[0], reinterpret_cast<unsigned long long*>(h + 2)[2]);
+  }
+  if (!queued)
+    CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+                        static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
+                        static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order));
   if (c->dim == 2)
     CU(lsm::launch_clip_tris_wide(ovf, ovf_count, nnz, static_cast<int32_t*>(c->pair_a.p),
                                   static_cast<int32_t*>(c->pair_b.p), static_cast<double*>(c->a_coords.p),

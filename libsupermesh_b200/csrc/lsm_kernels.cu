@@ -50,6 +50,24 @@ int tet_blocks_per_sm() {
 void set_tet_blocks_per_sm(int v) { g_tet_bps = (v == 3) ? 3 : 4; }
 
 namespace {
+int g_tet_variant = -1;
+}  // namespace
+
+// 3D clipper variant: 0 = per-lane depth-first walk (k_clip_tets, default),
+// 1 = per-warp task queues (k_clip_tets_wq).  LSM_TET_CLIPPER=lane|queue.
+// On B200 the task queues keep ~20 of 32 lanes busy (vs ~9) but wait on
+// their L2-resident queues at 8 warps per SM, which makes them slower.
+int tet_clipper_variant() {
+  if (g_tet_variant < 0) {
+    const char* e = getenv("LSM_TET_CLIPPER");
+    g_tet_variant = (e && e[0] == 'q') ? 1 : 0;
+  }
+  return g_tet_variant;
+}
+
+void set_tet_clipper_variant(int v) { g_tet_variant = v ? 1 : 0; }
+
+namespace {
 
 inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 
@@ -1324,6 +1342,323 @@ __global__ void __launch_bounds__(kTetBlock, BPS) k_clip_tets(
   }
 }
 
+// ----------------------------------------------------------------------
+// K6b: tet clipper with per-warp task queues
+// ----------------------------------------------------------------------
+// Each warp works on up to kWqSlots pairs at a time and keeps three stacks of
+// tasks in global scratch (L2-resident): tets to classify against their next
+// plane (clip), tets to split (split), and final tets whose volume decides
+// whether they are kept (leaf).  Every phase takes up to 32 tasks of ONE kind,
+// one per lane, so the FP64-heavy split and leaf work runs with full warps
+// instead of the few lanes that happen to need it in a per-pair walk.
+//
+// Tasks are processed out of the reference's order, so each final tet
+// carries its rank in the reference's output order (its base-3 path of child
+// indices over the four planes, 0..80).  Kept volumes land in a per-pair
+// buffer indexed by rank and the pair's measure is summed in rank order when
+// its last task completes: the per-pair sums are the reference's, bit for
+// bit.
+namespace {
+constexpr int kWqWarps = 4;    // warps per block
+#ifndef LSM_WQ_BPS
+#define LSM_WQ_BPS 2
+#endif
+constexpr int kWqBlocksPerSm = LSM_WQ_BPS;
+constexpr int kWqSlots = 32;   // pairs in flight per warp
+constexpr int kWqCapC = 1024;  // clip stack entries
+constexpr int kWqCapS = 64;    // split stack entries (<= 31 + 32)
+constexpr int kWqCapL = 128;   // leaf stack entries (<= 31 + 96)
+constexpr size_t kWqClipD = 12 * (size_t)kWqCapC;
+constexpr size_t kWqSplitD = 16 * (size_t)kWqCapS;
+constexpr size_t kWqLeafD = 12 * (size_t)kWqCapL;
+constexpr size_t kWqVolD = (size_t)kWqSlots * 81;
+constexpr size_t kWqDoubles = kWqClipD + kWqSplitD + kWqLeafD + kWqVolD;
+constexpr size_t kWqInts = kWqCapC + 2 * kWqCapS + kWqCapL;
+constexpr size_t kWqWarpBytes = ((kWqDoubles * 8 + kWqInts * 4) + 255) / 256 * 256;
+}  // namespace
+
+size_t wq_scratch_bytes() { return (size_t)sm_count() * kWqBlocksPerSm * kWqWarps * kWqWarpBytes; }
+
+__device__ __forceinline__ void wq_store_tet(double* base, int cap, int i, const Tet& t) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    base[(3 * k + 0) * cap + i] = t.x[k];
+    base[(3 * k + 1) * cap + i] = t.y[k];
+    base[(3 * k + 2) * cap + i] = t.z[k];
+  }
+}
+
+__device__ __forceinline__ void wq_load_tet(const double* base, int cap, int i, Tet& t) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    t.x[k] = base[(3 * k + 0) * cap + i];
+    t.y[k] = base[(3 * k + 1) * cap + i];
+    t.z[k] = base[(3 * k + 2) * cap + i];
+  }
+}
+
+// warp prefix of per-lane counts 0..3
+__device__ __forceinline__ int wq_prefix(int cnt, unsigned lt, int& total) {
+  const unsigned b0 = __ballot_sync(0xffffffffu, cnt & 1), b1 = __ballot_sync(0xffffffffu, cnt & 2);
+  total = __popc(b0) + 2 * __popc(b1);
+  return __popc(b0 & lt) + 2 * __popc(b1 & lt);
+}
+
+__global__ void __launch_bounds__(kWqWarps * 32, kWqBlocksPerSm) k_clip_tets_wq(
+    const int32_t* __restrict__ list, const unsigned long long* __restrict__ nlist,
+    const int32_t* __restrict__ pa, const int32_t* __restrict__ pb, const double* __restrict__ coords_a,
+    const double* __restrict__ tol_a, const double* __restrict__ setup_b, double* pair_measure,
+    int32_t* pair_nout, unsigned long long* work, unsigned char* scratch, int* err) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const size_t gw = (size_t)blockIdx.x * kWqWarps + wid;
+  double* clipD = reinterpret_cast<double*>(scratch + gw * kWqWarpBytes);
+  double* splitD = clipD + kWqClipD;
+  double* leafD = splitD + kWqSplitD;
+  double* vol = leafD + kWqLeafD;
+  int* clipM = reinterpret_cast<int*>(vol + kWqVolD);
+  int* splitM = clipM + kWqCapC;
+  int* splitC = splitM + kWqCapS;
+  int* leafM = splitC + kWqCapS;
+
+  __shared__ int s_pair[kWqWarps][kWqSlots], s_b[kWqWarps][kWqSlots], s_cnt[kWqWarps][kWqSlots];
+  __shared__ unsigned s_mask[kWqWarps][kWqSlots][3];
+  __shared__ double s_tol[kWqWarps][kWqSlots];
+  __shared__ int s_free[kWqWarps][kWqSlots];
+  __shared__ int s_nfree[kWqWarps];
+  s_free[wid][lane] = lane;
+  if (lane == 0) s_nfree[wid] = kWqSlots;
+  __syncwarp();
+
+  const int64_t npairs = (int64_t)*nlist;
+  int topC = 0, topS = 0, topL = 0;  // warp-uniform
+  bool exhausted = false;
+
+  // finish a pair: sum its kept volumes in rank order, free its slot
+  auto finalize = [&](int slot) {
+    const int p = s_pair[wid][slot];
+    double m = 0.0;
+    int nout = 0;
+    for (int w = 0; w < 3; ++w) {
+      unsigned bits = s_mask[wid][slot][w];
+      while (bits) {
+        const int r = __ffs(bits) - 1;
+        bits &= bits - 1u;
+        m = m + vol[slot * 81 + w * 32 + r];
+        ++nout;
+      }
+    }
+    pair_measure[p] = m;
+    pair_nout[p] = nout;
+    const int f = atomicAdd(&s_nfree[wid], 1);
+    s_free[wid][f] = slot;
+  };
+
+  int maxC = 0;
+  // every phase retires or creates at least one task; a pair creates at most
+  // 40 clip, 40 split and 81 leaf tasks
+  const long long guard_max = (long long)(npairs + kWqSlots) * 256 + 1024;
+  for (long long guard = 0;; ++guard) {
+    int phase;  // 0 leaf, 1 split, 2 clip, -1 done
+    if (topL >= 32) {
+      phase = 0;
+    } else if (topS >= 32) {
+      phase = 1;
+    } else {
+      const int nfree = s_nfree[wid];
+      if (topC < 32 && !exhausted && nfree > 0) {
+        // ---- admit new pairs
+        const int want = min(nfree, 32 - topC);
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&work[1], (unsigned long long)want);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const bool take = lane < want && (int64_t)(base + lane) < npairs;
+        const unsigned tk = __ballot_sync(0xffffffffu, take);
+        const int ntake = __popc(tk);
+        if ((int64_t)(base + want) >= npairs) exhausted = true;
+        if (take) {
+          const int p = list[base + lane];
+          const int slot = s_free[wid][nfree - 1 - lane];
+          const int a = pa[p], b = pb[p];
+          Tet t;
+          load_tet(coords_a + (int64_t)a * 12, t);
+          s_pair[wid][slot] = p;
+          s_b[wid][slot] = b;
+          s_tol[wid][slot] = fmin(tol_a[a], setup_b[(int64_t)b * kSetup3 + 16]);
+          s_cnt[wid][slot] = 1;
+          s_mask[wid][slot][0] = s_mask[wid][slot][1] = s_mask[wid][slot][2] = 0u;
+          wq_store_tet(clipD, kWqCapC, topC + lane, t);
+          clipM[topC + lane] = slot;  // level 0, rank 0
+        }
+        __syncwarp();
+        if (lane == 0) s_nfree[wid] = nfree - ntake;
+        topC += ntake;
+        __syncwarp();
+      }
+      if (topC > 0)
+        phase = 2;
+      else if (topS > 0)
+        phase = 1;
+      else if (topL > 0)
+        phase = 0;
+      else
+        phase = -1;
+    }
+    if (phase < 0) {
+      // all stacks empty: either every pair is done, or slots are held by
+      // pairs without tasks (cannot happen; reported, never waited on)
+      if ((!exhausted || s_nfree[wid] != kWqSlots) && lane == 0) atomicExch(err, 2);
+      break;
+    }
+    if (guard > guard_max) {
+      if (lane == 0) atomicExch(err, 3);
+      break;
+    }
+
+    if (phase == 2) {
+      // ---- clip: classify tets against their next plane
+      const int n = min(32, topC);
+      const bool act = lane < n;
+      Tet t;
+      TetClass cls;
+      int meta = 0, slot = 0, L = 0, rank = 0, type = -1;  // 0 drop, 1 keep, 2 split
+      if (act) {
+        const int idx = topC - n + lane;
+        wq_load_tet(clipD, kWqCapC, idx, t);
+        meta = clipM[idx];
+        slot = meta & 31;
+        L = (meta >> 5) & 3;
+        rank = meta >> 7;
+        const double* pl = setup_b + (int64_t)s_b[wid][slot] * kSetup3;
+        double nx, ny, nz, c;
+        load_plane(pl, L, nx, ny, nz, c);
+        classify_tet(t, nx, ny, nz, c, cls);
+        type = cls.nn == 0 ? 0 : (cls.np == 0 ? 1 : 2);
+      }
+      __syncwarp();
+      topC -= n;
+      const int pc = (type == 1 && L < 3) ? 1 : 0;
+      const int pl_ = (type == 1 && L == 3) ? 1 : 0;
+      const int ps = type == 2 ? 1 : 0;
+      int tc, tl, ts;
+      const int oc = wq_prefix(pc, lt, tc), ol = wq_prefix(pl_, lt, tl), os = wq_prefix(ps, lt, ts);
+      if (topC + tc > kWqCapC || topL + tl > kWqCapL || topS + ts > kWqCapS) {
+        if (lane == 0) atomicExch(err, 1);
+        break;
+      }
+      if (pc) {
+        wq_store_tet(clipD, kWqCapC, topC + oc, t);
+        clipM[topC + oc] = slot | ((L + 1) << 5) | ((rank * 3) << 7);
+      }
+      if (pl_) {
+        wq_store_tet(leafD, kWqCapL, topL + ol, t);
+        leafM[topL + ol] = slot | ((rank * 3) << 5);
+      }
+      if (ps) {
+        const int i = topS + os;
+        wq_store_tet(splitD, kWqCapS, i, t);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) splitD[(12 + q) * kWqCapS + i] = cls.d[q];
+        splitM[i] = meta;
+        splitC[i] = (int)(cls.negl | cls.posl << 6 | cls.zerl << 12 | (unsigned)cls.nn << 18 | (unsigned)cls.np << 21);
+      }
+      topC += tc;
+      topL += tl;
+      topS += ts;
+      __syncwarp();
+      if (type == 0 && atomicSub(&s_cnt[wid][slot], 1) == 1) finalize(slot);
+      __syncwarp();
+    } else if (phase == 1) {
+      // ---- split: interpolate and assemble children
+      const int n = min(32, topS);
+      const bool act = lane < n;
+      Tet t, c1, c2;
+      TetClass cls;
+      int meta = 0, k = 0;
+      if (act) {
+        const int idx = topS - n + lane;
+        wq_load_tet(splitD, kWqCapS, idx, t);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cls.d[q] = splitD[(12 + q) * kWqCapS + idx];
+        meta = splitM[idx];
+        const unsigned cw = (unsigned)splitC[idx];
+        cls.negl = cw & 63u;
+        cls.posl = (cw >> 6) & 63u;
+        cls.zerl = (cw >> 12) & 63u;
+        cls.nn = (int)((cw >> 18) & 7u);
+        cls.np = (int)((cw >> 21) & 7u);
+      }
+      __syncwarp();
+      topS -= n;
+      if (act) k = split_tet(t, cls, c1, c2);
+      const int slot = meta & 31, L = (meta >> 5) & 3, rank = meta >> 7;
+      const int kc = (act && L < 3) ? k : 0;
+      const int kl = (act && L == 3) ? k : 0;
+      int tc, tl;
+      const int oc = wq_prefix(kc, lt, tc), ol = wq_prefix(kl, lt, tl);
+      if (topC + tc > kWqCapC || topL + tl > kWqCapL) {
+        if (lane == 0) atomicExch(err, 1);
+        break;
+      }
+      if (kc) {
+        const int m0 = slot | ((L + 1) << 5);
+        wq_store_tet(clipD, kWqCapC, topC + oc, t);
+        clipM[topC + oc] = m0 | ((rank * 3) << 7);
+        if (kc > 1) {
+          wq_store_tet(clipD, kWqCapC, topC + oc + 1, c1);
+          clipM[topC + oc + 1] = m0 | ((rank * 3 + 1) << 7);
+        }
+        if (kc > 2) {
+          wq_store_tet(clipD, kWqCapC, topC + oc + 2, c2);
+          clipM[topC + oc + 2] = m0 | ((rank * 3 + 2) << 7);
+        }
+      }
+      if (kl) {
+        wq_store_tet(leafD, kWqCapL, topL + ol, t);
+        leafM[topL + ol] = slot | ((rank * 3) << 5);
+        if (kl > 1) {
+          wq_store_tet(leafD, kWqCapL, topL + ol + 1, c1);
+          leafM[topL + ol + 1] = slot | ((rank * 3 + 1) << 5);
+        }
+        if (kl > 2) {
+          wq_store_tet(leafD, kWqCapL, topL + ol + 2, c2);
+          leafM[topL + ol + 2] = slot | ((rank * 3 + 2) << 5);
+        }
+      }
+      topC += tc;
+      topL += tl;
+      if (act && k != 1) atomicAdd(&s_cnt[wid][slot], k - 1);
+      __syncwarp();
+    } else {
+      // ---- leaf: tolerance test and volume of final tets
+      const int n = min(32, topL);
+      const bool act = lane < n;
+      Tet t;
+      int slot = 0, rank = 0;
+      if (act) {
+        const int idx = topL - n + lane;
+        wq_load_tet(leafD, kWqCapL, idx, t);
+        const int meta = leafM[idx];
+        slot = meta & 31;
+        rank = meta >> 5;
+      }
+      __syncwarp();
+      topL -= n;
+      if (act && tet_volume_v4(t) >= s_tol[wid][slot]) {
+        vol[slot * 81 + rank] = tet_volume_v1(t);
+        atomicOr(&s_mask[wid][slot][rank >> 5], 1u << (rank & 31));
+      }
+      __syncwarp();
+      if (act && atomicSub(&s_cnt[wid][slot], 1) == 1) finalize(slot);
+      __syncwarp();
+    }
+    maxC = max(maxC, topC);
+  }
+  if (lane == 0) atomicMax(&work[2], (unsigned long long)maxC);
+}
+
+int wq_grid_blocks() { return sm_count() * kWqBlocksPerSm; }
+
 // Deterministic per-block partials of the pair measures: block b reduces the
 // contiguous range [b*chunk, (b+1)*chunk) in a fixed thread order.
 __global__ void __launch_bounds__(256) k_reduce_pairs(int64_t npairs, const double* __restrict__ pm,
@@ -1371,6 +1706,22 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
       k_clip_tets<4><<<sm_count() * 4, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,
                                                               setup_b, pair_measure, pair_nout, work + 1);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
+                                const double* coords_a, const double* tol_a, const double* setup_b,
+                                double* pair_measure, int32_t* pair_nout, int32_t* survivors,
+                                unsigned long long* work, unsigned char* scratch, int* err, cudaStream_t s,
+                                const int32_t* order) {
+  // work[0]: survivors, work[1]: admitted pairs, work[2]: deepest clip stack
+  cudaMemsetAsync(work, 0, 3 * sizeof(unsigned long long), s);
+  cudaMemsetAsync(err, 0, sizeof(int), s);
+  count_launch(2);
+  k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, setup_b,
+                                                            pair_measure, pair_nout, survivors, work);
+  k_clip_tets_wq<<<wq_grid_blocks(), kWqWarps * 32, 0, s>>>(survivors, work, pair_a, pair_b, coords_a, tol_a,
+                                                            setup_b, pair_measure, pair_nout, work, scratch, err);
   return cudaGetLastError();
 }
 

@@ -33,6 +33,9 @@ unsigned long long launches();
 // Launch shape of the persistent tet clipper (3 or 4 blocks per SM).
 int tet_blocks_per_sm();
 void set_tet_blocks_per_sm(int v);
+// 3D clipper variant: 0 per-lane depth-first, 1 per-warp task queues.
+int tet_clipper_variant();
+void set_tet_clipper_variant(int v);
 
 struct BVH {
   int n = 0;                 // leaves
@@ -94,6 +97,16 @@ cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overf
                                   const double* coords_a, const double* tol_a,
                                   const double* setup_b, double* pair_measure, int32_t* pair_nout,
                                   cudaStream_t s);
+// Task-queue tet clipper (prefilter + k_clip_tets_wq).  scratch:
+// wq_scratch_bytes(); work: 3 counters; err != 0 after the launch means the
+// queues overflowed (results invalid: re-run with launch_clip).
+size_t wq_scratch_bytes();
+cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
+                                const double* coords_a, const double* tol_a, const double* setup_b,
+                                double* pair_measure, int32_t* pair_nout, int32_t* survivors,
+                                unsigned long long* work, unsigned char* scratch, int* err, cudaStream_t s,
+                                const int32_t* order = nullptr);
+
 // Per-block partials of the pair measures/counts in a fixed order
 // (reduce_pairs_blocks() entries).
 int reduce_pairs_blocks();

@@ -13,6 +13,8 @@ Bars (from the path's correctness contract):
   * totals: |total - oracle total| <= 1e-12 and, for meshes that tile the
     same domain, |total - domain measure| <= 1e-12.
 """
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -20,6 +22,7 @@ import libsupermesh_b200 as lsm
 from libsupermesh_b200 import meshes as M
 
 pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
 
 REL_TOL = 1e-12
 
@@ -95,6 +98,32 @@ def test_config_tri2d_777x1024_rot7_p1_mass(gpu_ctx, oracle_mod):
     ip, ind = oracle_mod.tree_finder(dim, A, B)
     i_o, meas_o, _ = oracle_mod.p1_mass(dim, A, B, ip, ind, u, v)
     assert abs(integral - i_o) <= 1e-12 * abs(i_o)
+
+
+def test_task_queue_clipper_matches(oracle_mod, tmp_path):
+    """The alternative task-queue tet clipper gives the same per-pair results."""
+    import subprocess
+    import sys
+
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r)\n"
+        "import libsupermesh_b200 as L; from libsupermesh_b200 import meshes as M\n"
+        "dim, A, B = M.config_meshes('small3d_12x14')\n"
+        "c = L.Context(0); st, _ = c.supermesh(A, B); pm, pn = c.pair_results(st.n_candidates)\n"
+        "ip, ind = c.get_candidates(len(A[1]), st.n_candidates)\n"
+        "np.savez(%r, pm=pm, pn=pn, ip=ip, ind=ind, tot=st.total_measure)\n" % (str(ROOT), str(tmp_path / "q.npz")))
+    import os
+    env = dict(os.environ, LSM_TET_CLIPPER="queue")
+    subprocess.run([sys.executable, "-c", code], check=True, env=env, timeout=600)
+    q = np.load(tmp_path / "q.npz")
+    dim, A, B = M.config_meshes("small3d_12x14")
+    ip_o, ind_o = oracle_mod.tree_finder(dim, A, B)
+    pm_o, pn_o, _, st_o = oracle_mod.narrow(dim, A, B, ip_o, ind_o)
+    ro, bo, mo, no = pair_table(ip_o, ind_o, pm_o, pn_o)
+    rg, bg, mg, ng = pair_table(q["ip"], q["ind"], q["pm"], q["pn"])
+    assert np.array_equal(bo, bg) and np.array_equal(no, ng)
+    assert np.array_equal(mo, mg)  # rank-ordered sums: bit-identical
+    assert abs(float(q["tot"]) - st_o.total) <= REL_TOL
 
 
 def test_int64_and_int32_enlists_agree(gpu_ctx):
