@@ -69,6 +69,17 @@ int64_t libsupermesh_gpu_context_bytes(const lsm_gpu_context *ctx);
 /* Kernel launches issued by this library in this process so far. */
 int64_t libsupermesh_gpu_kernel_launches(void);
 
+/* Process-wide tuning options.  They change launch shapes and the 3D clipper
+ * variant, never results (the autotuner in libsupermesh_b200/autotune.py
+ * picks them per GPU and workload):
+ *   "tet_clipper"        0 per-lane depth-first walk (default), 1 per-warp task queues
+ *   "tet_blocks_per_sm"  3 (default) or 4 blocks of 128 threads per SM (3D clipper)
+ *   "tri_blocks_per_sm"  4, 8 (default) or 16 blocks of 128 threads per SM (2D clipper)
+ *   "query_block"        64, 128 (default) or 256 threads per block (candidate search)
+ * Unknown names or values return LSM_ERROR_INVALID_ARGUMENT. */
+int libsupermesh_gpu_set_option(const char *name, int64_t value);
+int libsupermesh_gpu_get_option(const char *name, int64_t *value);
+
 /* Candidate search only (tree finder): the work of
  * tree_intersection_finder_set_input_c (C_bindings.F90:346-366) on the GPU.
  * Results stay in the context; read them with

@@ -98,6 +98,10 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_context_bytes.argtypes = [vp]
     L.libsupermesh_gpu_kernel_launches.restype = ctypes.c_int64
     L.libsupermesh_gpu_kernel_launches.argtypes = []
+    L.libsupermesh_gpu_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
+    L.libsupermesh_gpu_set_option.restype = ctypes.c_int
+    L.libsupermesh_gpu_get_option.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
+    L.libsupermesh_gpu_get_option.restype = ctypes.c_int
     mp = ctypes.POINTER(Mesh)
     L.libsupermesh_gpu_find_candidates.argtypes = [vp, mp, mp, ctypes.c_int, _i64p, vp]
     L.libsupermesh_gpu_get_candidates.argtypes = [vp, vp, vp, ctypes.c_int, vp]
@@ -279,6 +283,21 @@ class Context:
         self._check(self.lib.libsupermesh_gpu_supermesh_batched(self._h, n, A, B, int(on_device), totals.ctypes.data,
                                                                 nc.ctypes.data, ni.ctypes.data, stream))
         return totals[:n], nc[:n], ni[:n]
+
+
+def set_option(name: str, value: int) -> None:
+    """Set a process-wide tuning option (see libsupermesh-gpu.h)."""
+    st = load().libsupermesh_gpu_set_option(name.encode(), int(value))
+    if st != 0:
+        raise LsmError(st, f"invalid option {name}={value}")
+
+
+def get_option(name: str) -> int:
+    v = ctypes.c_int64(0)
+    st = load().libsupermesh_gpu_get_option(name.encode(), ctypes.byref(v))
+    if st != 0:
+        raise LsmError(st, f"unknown option {name}")
+    return v.value
 
 
 def kernel_launches() -> int:

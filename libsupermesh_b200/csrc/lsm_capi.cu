@@ -783,6 +783,39 @@ int64_t libsupermesh_gpu_context_bytes(const lsm_gpu_context* ctx) {
 
 int64_t libsupermesh_gpu_kernel_launches(void) { return (int64_t)lsm::launches(); }
 
+int libsupermesh_gpu_set_option(const char* name, int64_t value) {
+  if (!name) return LSM_ERROR_INVALID_ARGUMENT;
+  const std::string n(name);
+  if (n == "tet_clipper" && (value == 0 || value == 1)) {
+    lsm::set_tet_clipper_variant((int)value);
+  } else if (n == "tet_blocks_per_sm" && (value == 3 || value == 4)) {
+    lsm::set_tet_blocks_per_sm((int)value);
+  } else if (n == "tri_blocks_per_sm" && (value == 4 || value == 8 || value == 16)) {
+    lsm::set_tri_blocks_per_sm((int)value);
+  } else if (n == "query_block" && (value == 64 || value == 128 || value == 256)) {
+    lsm::set_query_block((int)value);
+  } else {
+    return LSM_ERROR_INVALID_ARGUMENT;
+  }
+  return LSM_SUCCESS;
+}
+
+int libsupermesh_gpu_get_option(const char* name, int64_t* value) {
+  if (!name || !value) return LSM_ERROR_INVALID_ARGUMENT;
+  const std::string n(name);
+  if (n == "tet_clipper")
+    *value = lsm::tet_clipper_variant();
+  else if (n == "tet_blocks_per_sm")
+    *value = lsm::tet_blocks_per_sm();
+  else if (n == "tri_blocks_per_sm")
+    *value = lsm::tri_blocks_per_sm();
+  else if (n == "query_block")
+    *value = lsm::query_block();
+  else
+    return LSM_ERROR_INVALID_ARGUMENT;
+  return LSM_SUCCESS;
+}
+
 int libsupermesh_gpu_find_candidates(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b,
                                      int on_device, int64_t* n_candidates, void* stream) {
   Ctx* c = C(ctx);

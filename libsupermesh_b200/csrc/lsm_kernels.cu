@@ -68,6 +68,16 @@ int tet_clipper_variant() {
 void set_tet_clipper_variant(int v) { g_tet_variant = v ? 1 : 0; }
 
 namespace {
+int g_tri_bps = 8;
+int g_query_block = 128;
+}  // namespace
+
+int tri_blocks_per_sm() { return g_tri_bps; }
+void set_tri_blocks_per_sm(int v) { g_tri_bps = v; }
+int query_block() { return g_query_block; }
+void set_query_block(int v) { g_query_block = v; }
+
+namespace {
 
 inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 
@@ -765,7 +775,7 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
 // K4: candidate search
 // ======================================================================
 template <int DIM, bool FILL>
-__global__ void __launch_bounds__(128) k_query(int64_t nel_a, const double* __restrict__ box64_a,
+__global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __restrict__ box64_a,
                                                const float4* __restrict__ lo_left,
                                                const float4* __restrict__ hi_esc, int n,
                                                const double* __restrict__ box64_b, int* counts,
@@ -824,8 +834,8 @@ cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_
                          const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
                          int32_t* pair_b, cudaStream_t s) {
   if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
-  const int B = 128;
-  const int g = grid_for(nel_a, B, 16);
+  const int B = query_block();
+  const int g = grid_for(nel_a, B, 2048 / B);
   count_launch();
   if (dim == 2) {
     if (fill)
@@ -1678,7 +1688,7 @@ __global__ void __launch_bounds__(256) k_reduce_pairs(int64_t npairs, const doub
 }
 
 int clip_grid_blocks(int dim) {
-  if (dim == 2) return sm_count() * 8;
+  if (dim == 2) return sm_count() * tri_blocks_per_sm();
   return sm_count() * tet_blocks_per_sm();
 }
 
@@ -1923,7 +1933,7 @@ cudaError_t launch_pair_keys(int64_t n, const int32_t* vals, const int32_t* pair
 }
 
 template <int DIM, bool FILL>
-__global__ void __launch_bounds__(128) k_query_batched(int64_t nel_a, const double* __restrict__ box64_a,
+__global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const double* __restrict__ box64_a,
                                                        const int32_t* __restrict__ pair_of_a,
                                                        const int* __restrict__ roots, const int* __restrict__ stops,
                                                        const float4* __restrict__ lo_left,
@@ -1986,8 +1996,8 @@ cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
                                  int32_t* pair_b, cudaStream_t s) {
   if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
-  const int B = 128;
-  const int g = grid_for(nel_a, B, 16);
+  const int B = query_block();
+  const int g = grid_for(nel_a, B, 2048 / B);
   count_launch();
   if (dim == 2) {
     if (fill)

@@ -36,6 +36,11 @@ void set_tet_blocks_per_sm(int v);
 // 3D clipper variant: 0 per-lane depth-first, 1 per-warp task queues.
 int tet_clipper_variant();
 void set_tet_clipper_variant(int v);
+// Grid of the 2D clipper (blocks per SM) and block size of the search.
+int tri_blocks_per_sm();
+void set_tri_blocks_per_sm(int v);
+int query_block();
+void set_query_block(int v);
 
 struct BVH {
   int n = 0;                 // leaves

@@ -126,6 +126,22 @@ def test_task_queue_clipper_matches(oracle_mod, tmp_path):
     assert abs(float(q["tot"]) - st_o.total) <= REL_TOL
 
 
+def test_autotuner_keeps_results(gpu_ctx, tmp_path, monkeypatch):
+    from libsupermesh_b200 import autotune
+
+    monkeypatch.setenv("LIBSUPERMESH_TUNING_CACHE", str(tmp_path / "tuning.json"))
+    for name in ("small2d_60x70", "small3d_10x12"):
+        dim, A, B = M.config_meshes(name)
+        ref, em_ref = gpu_ctx.supermesh(A, B, elem_measure=True)
+        res = autotune.tune(gpu_ctx, A, B, reps=1)
+        assert res["tried"] == (9 if dim == 2 else 12)
+        st, em = gpu_ctx.supermesh(A, B, elem_measure=True)
+        assert st.as_dict() == ref.as_dict() and np.array_equal(em, em_ref)
+        assert autotune.apply_cached(dim, len(A[1]), len(B[1])) == res["setting"]
+    for n, v in {"tet_clipper": 0, "tet_blocks_per_sm": 3, "tri_blocks_per_sm": 8, "query_block": 128}.items():
+        lsm.set_option(n, v)
+
+
 def test_int64_and_int32_enlists_agree(gpu_ctx):
     dim, A, B = M.config_meshes("small3d_5x6")
     s32, _ = gpu_ctx.supermesh(A, B)
