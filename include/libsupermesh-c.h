@@ -40,8 +40,15 @@ extern "C" {
 #include <math.h>
 #endif
 
-/* 1D sort finder (C_bindings.F90:66-111): not provided by the GPU build;
- * calls abort with a message. */
+/* 1D sort finder (C_bindings.F90:66-111; Intersection_Finder.F90:811-921):
+ * 2-node elements, first coordinate of each node, sort by left end then one
+ * sweep, on the GPU.  Shares the tree finder's result state, as the
+ * reference's module arrays do.  Rows list B elements in sweep order
+ * (ascending left end, ties by element number).  The sort is the stable sort
+ * by left end; the reference's merge sort gives the same order whenever each
+ * block of at most 4 elements it sorts directly is already in order (true
+ * for meshes numbered along the line); otherwise its output can repeat and
+ * lose elements, which this build does not reproduce. */
 void libsupermesh_sort_intersection_finder_set_input(long *nnodes_a, int *dim_a, long *nelements_a, int *loc_a,
                                                      long *nnodes_b, int *dim_b, long *nelements_b, int *loc_b,
                                                      c_kind *positions_a, long *enlist_a, c_kind *positions_b,
@@ -64,8 +71,10 @@ void libsupermesh_intersect_tets_real(c_kind *tet_a, c_kind *tet_b, c_kind *tets
 void libsupermesh_triangle_area(c_kind *tri, c_kind *area);
 void libsupermesh_tetrahedron_volume(c_kind *tet, c_kind *volume);
 
-/* 1D and mixed-element entries (C_bindings.F90:42-64, 113-132): not
- * provided by the GPU build; calls abort with a message. */
+/* 1D and mixed-element entries (C_bindings.F90:42-64, 113-132), on the GPU:
+ * intervals (Interval_Intersection.F90), triangle vs quadrilateral
+ * (Supermesh.F90:211-228, <= 46 output triangles) and tetrahedron vs
+ * Gmsh-ordered hexahedron (Supermesh.F90:248-295, <= 729 output tets). */
 void libsupermesh_interval_size(c_kind *interval, c_kind *size);
 void libsupermesh_intersect_intervals(c_kind *interval_a, c_kind *interval_b, c_kind *intervals_c, int *n_intervals_c);
 void libsupermesh_intersect_tet_hex(c_kind *tet_a, c_kind *hex_b, c_kind *tets_c, int *n_tets_c);

@@ -41,8 +41,8 @@ typedef enum {
 typedef struct lsm_gpu_context lsm_gpu_context;
 
 typedef struct {
-  int dim;               /* 2 or 3 */
-  int loc;               /* dim + 1 (simplices) */
+  int dim;               /* 1, 2 or 3 */
+  int loc;               /* dim + 1 (simplices); 2 for 1D interval meshes */
   int64_t nnodes;
   int64_t nelements;
   const double *positions; /* [nnodes][dim] */
@@ -82,6 +82,8 @@ int libsupermesh_gpu_get_option(const char *name, int64_t *value);
 
 /* Candidate search only (tree finder): the work of
  * tree_intersection_finder_set_input_c (C_bindings.F90:346-366) on the GPU.
+ * 1D meshes (dim 1, loc 2) take the sort finder instead
+ * (sort_intersection_finder_set_input_c, C_bindings.F90:66-86).
  * Results stay in the context; read them with
  * libsupermesh_gpu_get_candidates. */
 int libsupermesh_gpu_find_candidates(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
@@ -131,6 +133,20 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context *ctx, int dim, int64_t n,
                                      const double *a, const double *b,
                                      double *measure, int32_t *n_out,
                                      double *elems, int on_device, void *stream);
+
+/* Mixed element pairs, batched: the per-pair entries libsupermesh_intersect_
+ * intervals, _tri_quad and _tet_hex (C_bindings.F90:42-64, :113-125).
+ *   LSM_PAIR_INTERVALS  a, b [n][2]         elems [n][1][2]
+ *   LSM_PAIR_TRI_QUAD   a [n][3][2], b [n][4][2]   elems [n][46][3][2]
+ *   LSM_PAIR_TET_HEX    a [n][4][3], b [n][8][3] (Gmsh hexahedron node
+ *                       order)          elems [n][729][4][3]
+ * measure[n] = sum of output measures, n_out[n] = number of outputs, elems
+ * optional, in the reference's output order. */
+enum { LSM_PAIR_INTERVALS = 0, LSM_PAIR_TRI_QUAD = 1, LSM_PAIR_TET_HEX = 2 };
+int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context *ctx, int kind, int64_t n,
+                                           const double *a, const double *b,
+                                           double *measure, int32_t *n_out,
+                                           double *elems, int on_device, void *stream);
 
 /* P1-P1 mixed mass matrix over the supermesh of A and B: per candidate pair
  * the local block M[i][j] = sum_c |c| sum_q w_q phi_i^A(x_q) phi_j^B(x_q)

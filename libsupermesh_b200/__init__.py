@@ -112,17 +112,24 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_clip_candidates_ordered.restype = ctypes.c_int
     L.libsupermesh_gpu_intersect_pairs.argtypes = [vp, ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp, vp,
                                                    ctypes.c_int, vp]
+    L.libsupermesh_gpu_intersect_pairs_mixed.argtypes = [vp, ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp, vp,
+                                                         ctypes.c_int, vp]
     L.libsupermesh_gpu_p1_mass.argtypes = [vp, mp, mp, vp, vp, vp, _dp, ctypes.c_int, vp]
     L.libsupermesh_gpu_supermesh_batched.argtypes = [vp, ctypes.c_int, mp, mp, ctypes.c_int, vp, vp, vp, vp]
     for name in ("libsupermesh_gpu_context_create", "libsupermesh_gpu_context_destroy",
                  "libsupermesh_gpu_find_candidates", "libsupermesh_gpu_get_candidates",
                  "libsupermesh_gpu_supermesh", "libsupermesh_gpu_get_pair_results",
                  "libsupermesh_gpu_clip_candidates",
-                 "libsupermesh_gpu_intersect_pairs", "libsupermesh_gpu_p1_mass",
+                 "libsupermesh_gpu_intersect_pairs", "libsupermesh_gpu_intersect_pairs_mixed",
+                 "libsupermesh_gpu_p1_mass",
                  "libsupermesh_gpu_supermesh_batched"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
+
+
+PAIR_INTERVALS, PAIR_TRI_QUAD, PAIR_TET_HEX = 0, 1, 2
+_MIXED = {PAIR_INTERVALS: (2, 2, (1, 2)), PAIR_TRI_QUAD: (6, 8, (46, 3, 2)), PAIR_TET_HEX: (12, 24, (729, 4, 3))}
 
 
 def _ptr(a) -> int | None:
@@ -249,6 +256,20 @@ class Context:
                                                               m.ctypes.data, k.ctypes.data, _ptr(e), 0, None))
         return m[:n], k[:n], (e[:n] if e is not None else None)
 
+    def intersect_pairs_mixed(self, kind: int, a, b, want_elems: bool = False):
+        """kind: PAIR_INTERVALS, PAIR_TRI_QUAD or PAIR_TET_HEX."""
+        per_a, per_b, out_shape = _MIXED[kind]
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, per_a)
+        b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, per_b)
+        n = a.shape[0]
+        m = np.zeros(max(n, 1))
+        k = np.zeros(max(n, 1), dtype=np.int32)
+        e = np.zeros((max(n, 1),) + out_shape) if want_elems else None
+        self._check(self.lib.libsupermesh_gpu_intersect_pairs_mixed(self._h, kind, n, a.ctypes.data, b.ctypes.data,
+                                                                    m.ctypes.data, k.ctypes.data, _ptr(e), 0,
+                                                                    None))
+        return m[:n], k[:n], (e[:n] if e is not None else None)
+
     def p1_mass(self, mesh_a, mesh_b, u_a=None, v_b=None, want_blocks: bool = False):
         """Returns (u^T M v or None, blocks or None) for host meshes."""
         ma, mb = _mesh(*mesh_a, False), _mesh(*mesh_b, False)
@@ -313,23 +334,36 @@ def _long(a):
 
 def tree_intersection_finder(pos_a, en_a, pos_b, en_b):
     """set_input -> query_output -> get_output through the C API."""
+    return _finder("tree", pos_a, en_a, pos_b, en_b)
+
+
+def sort_intersection_finder(pos_a, en_a, pos_b, en_b):
+    """1D sort finder through the C API (2-node elements, first coordinate)."""
+    return _finder("sort", pos_a, en_a, pos_b, en_b)
+
+
+def _finder(kind, pos_a, en_a, pos_b, en_b):
     L = load()
     pa = np.ascontiguousarray(pos_a, dtype=np.float64)
     pb = np.ascontiguousarray(pos_b, dtype=np.float64)
+    if pa.ndim == 1:
+        pa = pa.reshape(-1, 1)
+    if pb.ndim == 1:
+        pb = pb.reshape(-1, 1)
     ea, eb = _long(en_a), _long(en_b)
     c_long, c_int = ctypes.c_long, ctypes.c_int
     args = [c_long(pa.shape[0]), c_int(pa.shape[1]), c_long(ea.shape[0]), c_int(ea.shape[1]),
             c_long(pb.shape[0]), c_int(pb.shape[1]), c_long(eb.shape[0]), c_int(eb.shape[1])]
-    L.libsupermesh_tree_intersection_finder_set_input(
+    getattr(L, f"libsupermesh_{kind}_intersection_finder_set_input")(
         *[ctypes.byref(x) for x in args], pa.ctypes.data_as(_dp), ea.ctypes.data_as(_lp),
         pb.ctypes.data_as(_dp), eb.ctypes.data_as(_lp))
     n = c_long(0)
-    L.libsupermesh_tree_intersection_finder_query_output(ctypes.byref(n))
+    getattr(L, f"libsupermesh_{kind}_intersection_finder_query_output")(ctypes.byref(n))
     indices = np.zeros(max(n.value, 1), dtype=np.int64)
     indptr = np.zeros(ea.shape[0] + 1, dtype=np.int64)
     nel = c_long(ea.shape[0])
-    L.libsupermesh_tree_intersection_finder_get_output(ctypes.byref(nel), ctypes.byref(n),
-                                                       indices.ctypes.data_as(_lp), indptr.ctypes.data_as(_lp))
+    getattr(L, f"libsupermesh_{kind}_intersection_finder_get_output")(
+        ctypes.byref(nel), ctypes.byref(n), indices.ctypes.data_as(_lp), indptr.ctypes.data_as(_lp))
     return indptr, indices[: n.value]
 
 
@@ -368,4 +402,35 @@ def tetrahedron_volume(tet) -> float:
     t = np.ascontiguousarray(tet, dtype=np.float64).reshape(12)
     r = ctypes.c_double(0.0)
     L.libsupermesh_tetrahedron_volume(t.ctypes.data_as(_dp), ctypes.byref(r))
+    return r.value
+
+
+def _pair_call(fn, a, b, shape_a, shape_b, out_shape):
+    L = load()
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(shape_a)
+    b = np.ascontiguousarray(b, dtype=np.float64).reshape(shape_b)
+    out = np.zeros(out_shape)
+    n = ctypes.c_int(0)
+    getattr(L, fn)(a.ctypes.data_as(_dp), b.ctypes.data_as(_dp), out.ctypes.data_as(_dp), ctypes.byref(n))
+    return out[: n.value].copy()
+
+
+def intersect_tri_quad(tri_a, quad_b):
+    return _pair_call("libsupermesh_intersect_tri_quad", tri_a, quad_b, (3, 2), (4, 2), (46, 3, 2))
+
+
+def intersect_tet_hex(tet_a, hex_b):
+    return _pair_call("libsupermesh_intersect_tet_hex", tet_a, hex_b, (4, 3), (8, 3), (729, 4, 3))
+
+
+def intersect_intervals(interval_a, interval_b):
+    """Returns an array of shape (n, 2), n in {0, 1}."""
+    return _pair_call("libsupermesh_intersect_intervals", interval_a, interval_b, (2,), (2,), (1, 2))
+
+
+def interval_size(interval) -> float:
+    L = load()
+    t = np.ascontiguousarray(interval, dtype=np.float64).reshape(2)
+    r = ctypes.c_double(0.0)
+    L.libsupermesh_interval_size(t.ctypes.data_as(_dp), ctypes.byref(r))
     return r.value

@@ -52,6 +52,8 @@ struct Ctx {
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
   DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand;
   DevBuf bt_stage_pa, bt_stage_ea, bt_stage_pb, bt_stage_eb;
+  // 1D sort finder
+  DevBuf d1_keyhi, d1_perm_a, d1_perm_b, d1_lo_a, d1_hi_a, d1_lo_b, d1_hi_b, d1_tree, d1_e, d1_l, d1_js;
   void* host_stage = nullptr;  // pinned, grow-only
   size_t host_stage_cap = 0;
   // pinned host scalars
@@ -195,10 +197,16 @@ struct MeshDev {
   const void* en;
 };
 
-void check_mesh(Ctx* c, const lsm_gpu_mesh* m, const char* name, bool simplex) {
+// intervals = true: 2-node elements whose nodes' first coordinates are read
+// (the sort finder's input), any dimension.
+void check_mesh(Ctx* c, const lsm_gpu_mesh* m, const char* name, bool simplex, bool intervals = false) {
   REQUIRE(m != nullptr, "mesh %s is NULL", name);
-  REQUIRE(m->dim == 2 || m->dim == 3, "Invalid dimension %d for mesh %s", m->dim, name);
-  if (simplex)
+  if (intervals)
+    REQUIRE(m->dim >= 1 && m->loc == 2, "mesh %s: the sort finder takes 2-node elements (loc %d)", name, m->loc);
+  else
+    REQUIRE(m->dim >= 1 && m->dim <= 3, "Invalid dimension %d for mesh %s", m->dim, name);
+  if (intervals) {
+  } else if (simplex)
     REQUIRE(m->loc == m->dim + 1, "mesh %s: loc %d is not a simplex of dimension %d", name, m->loc, m->dim);
   else
     REQUIRE(m->loc == m->dim + 1 || m->loc == (1 << m->dim), "mesh %s: unsupported loc %d", name, m->loc);
@@ -267,11 +275,84 @@ lsm::BVH build_tree(Ctx* c, const MeshDev& b, cudaStream_t s) {
   return bvh;
 }
 
-// Broad phase: candidates as CSR (offsets) + pair arrays.
+// Gather, sort by left end (stable) and take sorted left/right ends of one
+// interval mesh; coords[2*nel] keeps the element's two node coordinates.
+void sort_intervals(Ctx* c, const MeshDev& m, DevBuf& coords_buf, DevBuf& perm_buf, DevBuf& lo_buf, DevBuf& hi_buf,
+                    cudaStream_t s) {
+  const int64_t n = m.nel;
+  double* coords = ensure<double>(c, coords_buf, 2 * n);
+  uint32_t* klo = ensure<uint32_t>(c, c->keys, n);
+  uint32_t* khi = ensure<uint32_t>(c, c->d1_keyhi, n);
+  int32_t* perm = ensure<int32_t>(c, perm_buf, n);
+  uint32_t* kt = ensure<uint32_t>(c, c->keys_tmp, n);
+  int32_t* vt = ensure<int32_t>(c, c->vals_tmp, n);
+  uint32_t* hist = ensure<uint32_t>(c, c->hist, lsm::radix_hist_entries(n));
+  CU(lsm::launch_prep_1d(n, m.pos, m.dim, m.en, m.idx_bytes, m.nnodes, coords, klo, khi, perm, bad_flag(c), s));
+  CU(lsm::sort_by_key64(n, klo, khi, perm, kt, vt, hist, s));
+  CU(lsm::launch_sorted_ends_1d(n, perm, coords, ensure<double>(c, lo_buf, n), ensure<double>(c, hi_buf, n), s));
+}
+
+// 1D sort finder (Intersection_Finder.F90:811-921) on the GPU; the first
+// coordinate of each node is used, positions have stride dim.
+void find_candidates_1d(Ctx* c, const MeshDev& a, const MeshDev& b, cudaStream_t s) {
+  const int64_t na = a.nel, nb = b.nel;
+  CU(cudaMemsetAsync(bad_flag(c), 0, sizeof(int) * 64, s));
+  sort_intervals(c, a, c->a_coords, c->d1_perm_a, c->d1_lo_a, c->d1_hi_a, s);
+  sort_intervals(c, b, c->b_coords, c->d1_perm_b, c->d1_lo_b, c->d1_hi_b, s);
+  const double* lo_a = static_cast<double*>(c->d1_lo_a.p);
+  const double* hi_a = static_cast<double*>(c->d1_hi_a.p);
+  const double* lo_b = static_cast<double*>(c->d1_lo_b.p);
+  const double* hi_b = static_cast<double*>(c->d1_hi_b.p);
+  double* tree = nb > 0 ? ensure<double>(c, c->d1_tree, 2 * lsm::tree_leaves_1d(nb)) : nullptr;
+  CU(lsm::launch_max_tree(nb, hi_b, tree, s));
+  int32_t* E = ensure<int32_t>(c, c->d1_e, na);
+  int32_t* L = ensure<int32_t>(c, c->d1_l, na);
+  int32_t* JS = ensure<int32_t>(c, c->d1_js, na);
+  CU(lsm::launch_rows_1d(na, lo_a, hi_a, nb, lo_b, tree, E, L, s));
+  CU(lsm::launch_sweep_1d(na, nb, E, L, lo_a, hi_a, hi_b, JS, s));
+  int64_t* offsets = ensure<int64_t>(c, c->offsets, na + 1);
+  int* counts = ensure<int>(c, c->counts, na);
+  int64_t* stmp = ensure<int64_t>(c, c->scan_tmp, lsm::scan_tmp_entries(na) + 1);
+  const int32_t* perm_a = static_cast<int32_t*>(c->d1_perm_a.p);
+  const int32_t* perm_b = static_cast<int32_t*>(c->d1_perm_b.p);
+  CU(lsm::launch_emit_1d(false, na, JS, E, lo_a, hi_b, perm_a, perm_b, counts, nullptr, nullptr, nullptr, s));
+  CU(lsm::launch_scan(na, counts, offsets, stmp, s));
+  int64_t* h = static_cast<int64_t*>(c->host_scalars) + 8;
+  CU(cudaMemcpyAsync(h, offsets + na, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  int* hb = static_cast<int*>(c->host_scalars);
+  CU(cudaMemcpyAsync(hb, c->misc.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  REQUIRE(hb[0] == 0, "Invalid node index in an element list");
+  const int64_t nnz = *h;
+  int32_t* pa = ensure<int32_t>(c, c->pair_a, nnz);
+  int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);
+  if (nnz > 0) CU(lsm::launch_emit_1d(true, na, JS, E, lo_a, hi_b, perm_a, perm_b, nullptr, offsets, pa, pb, s));
+  c->dim = 1;
+  c->loc_a = 2;
+  c->loc_b = 2;
+  c->nel_a = na;
+  c->nel_b = nb;
+  c->ncand = nnz;
+  c->simplex_prep = true;  // coords of both meshes are current
+}
+
+// Broad phase: candidates as CSR (offsets) + pair arrays.  1D meshes (and
+// intervals = true, the sort finder's entry) take the sort-and-sweep
+// search, 2D/3D the LBVH search.
 void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int on_device, bool simplex,
-                     bool want_b_coords, cudaStream_t s) {
-  check_mesh(c, ma, "A", simplex);
-  check_mesh(c, mb, "B", simplex);
+                     bool want_b_coords, cudaStream_t s, bool intervals = false) {
+  intervals = intervals || (ma && ma->dim == 1);
+  check_mesh(c, ma, "A", simplex, intervals);
+  check_mesh(c, mb, "B", simplex, intervals);
+  c->have_pairs = false;
+  c->ncand = -1;
+  c->simplex_prep = false;
+  if (intervals) {
+    MeshDev a = upload(c, ma, on_device, c->a_pos, c->a_en, s);
+    MeshDev b = upload(c, mb, on_device, c->b_pos, c->b_en, s);
+    find_candidates_1d(c, a, b, s);
+    return;
+  }
   REQUIRE(ma->dim == mb->dim, "Invalid dimension: A is %dD, B is %dD", ma->dim, mb->dim);
   c->have_pairs = false;
   c->ncand = -1;
@@ -331,6 +412,15 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
   int* ovf_count = bad_flag(c) + 2;
   if (c->dim == 2) CU(cudaMemsetAsync(ovf_count, 0, sizeof(int), s));
   unsigned long long* work = reinterpret_cast<unsigned long long*>(bad_flag(c) + 8);
+  if (c->dim == 1) {
+    CU(lsm::launch_clip_intervals(nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+                                  static_cast<double*>(c->a_coords.p), static_cast<double*>(c->b_coords.p), pm, pn,
+                                  s));
+    CU(lsm::launch_reduce_pairs(nnz, pm, pn, part, s));
+    CU(lsm::launch_finalize(part, nred, tot, s));
+    c->have_pairs = true;
+    return;
+  }
   bool queued = false;
   if (c->dim == 3 && lsm::tet_clipper_variant() == 1) {
     unsigned char* scr = ensure<unsigned char>(c, c->wq_scratch, (int64_t)lsm::wq_scratch_bytes());
@@ -632,10 +722,45 @@ void single_pair(int dim, const double* a, const double* b, double* out_elems, i
   }));
 }
 
+// Element shapes of the mixed pair kinds: doubles per A and B element, output
+// capacity and doubles per output element.
+struct MixedShape {
+  int per_a, per_b, cap, per_out;
+};
+MixedShape mixed_shape(int kind) {
+  if (kind == LSM_PAIR_INTERVALS) return {2, 2, 1, 2};
+  if (kind == LSM_PAIR_TRI_QUAD) return {6, 8, 46, 6};
+  return {12, 24, 729, 12};
+}
+
+void single_mixed(int kind, const double* a, const double* b, double* out_elems, int* n_out) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  Ctx* c = legacy_ctx();
+  const MixedShape m = mixed_shape(kind);
+  legacy_check(c, guarded(c, [&] {
+    cudaStream_t s = c->stream;
+    double* da = ensure<double>(c, c->x_a, m.per_a);
+    double* db = ensure<double>(c, c->x_b, m.per_b);
+    int32_t* dn = ensure<int32_t>(c, c->x_nout, 1);
+    double* de = ensure<double>(c, c->x_elems, (int64_t)m.cap * m.per_out);
+    CU(cudaMemcpyAsync(da, a, sizeof(double) * m.per_a, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(db, b, sizeof(double) * m.per_b, cudaMemcpyHostToDevice, s));
+    CU(lsm::launch_pairs_mixed(kind, 1, da, db, nullptr, dn, de, s));
+    int32_t* hn = static_cast<int32_t*>(c->host_scalars);
+    CU(cudaMemcpyAsync(hn, dn, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    *n_out = hn[0];
+    if (hn[0] > 0) {
+      CU(cudaMemcpyAsync(out_elems, de, sizeof(double) * m.per_out * hn[0], cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+    }
+  }));
+}
+
 double single_measure(int dim, const double* e) {
   std::lock_guard<std::mutex> lk(g_mutex);
   Ctx* c = legacy_ctx();
-  const int per = dim == 2 ? 6 : 12;
+  const int per = dim == 1 ? 2 : dim == 2 ? 6 : 12;
   double r = 0.0;
   legacy_check(c, guarded(c, [&] {
     cudaStream_t s = c->stream;
@@ -679,16 +804,16 @@ void libsupermesh_tree_intersection_finder_set_input(long* nnodes_a, int* dim_a,
 
 void libsupermesh_tree_intersection_finder_query_output(long* nindices) {
   std::lock_guard<std::mutex> lk(g_mutex);
-  if (!g_tree_state) legacy_abort("tree intersection finder: query_output without set_input");
+  if (!g_tree_state) legacy_abort("intersection finder: query_output without set_input");
   *nindices = (long)g_ctx->ncand;
 }
 
 void libsupermesh_tree_intersection_finder_get_output(long* nelements, long* nindices, long* indices, long* ind_ptr) {
   std::lock_guard<std::mutex> lk(g_mutex);
-  if (!g_tree_state) legacy_abort("tree intersection finder: get_output without set_input");
+  if (!g_tree_state) legacy_abort("intersection finder: get_output without set_input");
   Ctx* c = g_ctx;
   if (*nelements != (long)c->nel_a || *nindices != (long)c->ncand)
-    legacy_abort("tree intersection finder: get_output sizes do not match set_input");
+    legacy_abort("intersection finder: get_output sizes do not match set_input");
   legacy_check(c, guarded(c, [&] {
     cudaStream_t s = c->stream;
     const int64_t nnz = c->ncand;
@@ -715,27 +840,45 @@ void libsupermesh_triangle_area(double* tri, double* area) { *area = single_meas
 
 void libsupermesh_tetrahedron_volume(double* tet, double* volume) { *volume = single_measure(3, tet); }
 
-void libsupermesh_sort_intersection_finder_set_input(long*, int*, long*, int*, long*, int*, long*, int*, double*,
-                                                     long*, double*, long*) {
-  legacy_abort("libsupermesh_sort_intersection_finder_set_input is not provided by the GPU build");
+void libsupermesh_sort_intersection_finder_set_input(long* nnodes_a, int* dim_a, long* nelements_a, int* loc_a,
+                                                     long* nnodes_b, int* dim_b, long* nelements_b, int* loc_b,
+                                                     double* positions_a, long* enlist_a, double* positions_b,
+                                                     long* enlist_b) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  if (g_tree_state) legacy_abort("sort intersection finder: set_input called again before get_output");
+  if (*dim_a < 1 || *dim_b < 1) legacy_abort("Invalid dimension");
+  if (*loc_a != 2 || *loc_b != 2) legacy_abort("sort intersection finder: elements must have 2 nodes");
+  Ctx* c = legacy_ctx();
+  lsm_gpu_mesh a{*dim_a, 2, (int64_t)*nnodes_a, (int64_t)*nelements_a, positions_a, enlist_a, (int)sizeof(long)};
+  lsm_gpu_mesh b{*dim_b, 2, (int64_t)*nnodes_b, (int64_t)*nelements_b, positions_b, enlist_b, (int)sizeof(long)};
+  legacy_check(c, guarded(c, [&] { find_candidates(c, &a, &b, 0, false, false, c->stream, true); }));
+  g_tree_state = true;
 }
-void libsupermesh_sort_intersection_finder_query_output(long*) {
-  legacy_abort("libsupermesh_sort_intersection_finder_query_output is not provided by the GPU build");
+
+// The reference's tree and sort finders keep their output in the same module
+// arrays (C_bindings.F90:30-32), so either query/get_output pair reads the
+// result of the last set_input.
+void libsupermesh_sort_intersection_finder_query_output(long* nindices) {
+  libsupermesh_tree_intersection_finder_query_output(nindices);
 }
-void libsupermesh_sort_intersection_finder_get_output(long*, long*, long*, long*) {
-  legacy_abort("libsupermesh_sort_intersection_finder_get_output is not provided by the GPU build");
+
+void libsupermesh_sort_intersection_finder_get_output(long* nelements, long* nindices, long* indices, long* ind_ptr) {
+  libsupermesh_tree_intersection_finder_get_output(nelements, nindices, indices, ind_ptr);
 }
-void libsupermesh_interval_size(double*, double*) {
-  legacy_abort("libsupermesh_interval_size is not provided by the GPU build");
+
+void libsupermesh_interval_size(double* interval, double* size) { *size = single_measure(1, interval); }
+
+void libsupermesh_intersect_intervals(double* interval_a, double* interval_b, double* intervals_c,
+                                      int* n_intervals_c) {
+  single_mixed(LSM_PAIR_INTERVALS, interval_a, interval_b, intervals_c, n_intervals_c);
 }
-void libsupermesh_intersect_intervals(double*, double*, double*, int*) {
-  legacy_abort("libsupermesh_intersect_intervals is not provided by the GPU build");
+
+void libsupermesh_intersect_tet_hex(double* tet_a, double* hex_b, double* tets_c, int* n_tets_c) {
+  single_mixed(LSM_PAIR_TET_HEX, tet_a, hex_b, tets_c, n_tets_c);
 }
-void libsupermesh_intersect_tet_hex(double*, double*, double*, int*) {
-  legacy_abort("libsupermesh_intersect_tet_hex is not provided by the GPU build");
-}
-void libsupermesh_intersect_tri_quad(double*, double*, double*, int*) {
-  legacy_abort("libsupermesh_intersect_tri_quad is not provided by the GPU build");
+
+void libsupermesh_intersect_tri_quad(double* tri_a, double* quad_b, double* tris_c, int* n_tris_c) {
+  single_mixed(LSM_PAIR_TRI_QUAD, tri_a, quad_b, tris_c, n_tris_c);
 }
 
 // ------------------------------------------------------------- GPU API
@@ -953,12 +1096,51 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context* ctx, int dim, int64_t n, c
   });
 }
 
+int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context* ctx, int kind, int64_t n, const double* a,
+                                           const double* b, double* measure, int32_t* n_out, double* elems,
+                                           int on_device, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(kind == LSM_PAIR_INTERVALS || kind == LSM_PAIR_TRI_QUAD || kind == LSM_PAIR_TET_HEX,
+            "unknown pair kind %d", kind);
+    REQUIRE(n >= 0, "negative pair count");
+    if (n == 0) return;
+    REQUIRE(a && b, "NULL element arrays");
+    cudaStream_t s = pick(c, stream);
+    const MixedShape m = mixed_shape(kind);
+    const double *da = a, *db = b;
+    double* dm = measure;
+    int32_t* dn = n_out;
+    double* de = elems;
+    if (!on_device) {
+      double* ta = ensure<double>(c, c->x_a, n * m.per_a);
+      double* tb = ensure<double>(c, c->x_b, n * m.per_b);
+      CU(cudaMemcpyAsync(ta, a, sizeof(double) * n * m.per_a, cudaMemcpyHostToDevice, s));
+      CU(cudaMemcpyAsync(tb, b, sizeof(double) * n * m.per_b, cudaMemcpyHostToDevice, s));
+      da = ta;
+      db = tb;
+      dm = measure ? ensure<double>(c, c->x_measure, n) : nullptr;
+      dn = n_out ? ensure<int32_t>(c, c->x_nout, n) : nullptr;
+      de = elems ? ensure<double>(c, c->x_elems, n * m.cap * m.per_out) : nullptr;
+    }
+    CU(lsm::launch_pairs_mixed(kind, n, da, db, dm, dn, de, s));
+    if (!on_device) {
+      if (measure) CU(cudaMemcpyAsync(measure, dm, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      if (n_out) CU(cudaMemcpyAsync(n_out, dn, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+      if (elems)
+        CU(cudaMemcpyAsync(elems, de, sizeof(double) * n * m.cap * m.per_out, cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaStreamSynchronize(s));
+  });
+}
+
 int libsupermesh_gpu_p1_mass(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b, const double* u_a,
                              const double* v_b, double* blocks, double* integral, int on_device, void* stream) {
   Ctx* c = C(ctx);
   return guarded(c, [&] {
     cudaStream_t s = pick(c, stream);
     REQUIRE(a && b && a->index_bytes == b->index_bytes, "A and B must use the same index width");
+    REQUIRE(a->dim == 2 || a->dim == 3, "P1 mass matrix: Invalid dimension %d", a->dim);
     find_candidates(c, a, b, on_device, true, true, s);
     const int64_t nnz = c->ncand;
     const int loc = c->dim + 1;
@@ -1003,6 +1185,7 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context* ctx, int npairs, const l
     for (int i = 0; i < npairs; ++i) {
       check_mesh(c, &a[i], "A", true);
       check_mesh(c, &b[i], "B", true);
+      REQUIRE(a[i].dim >= 2, "batched supermesh: pair %d is 1D (use libsupermesh_gpu_supermesh)", i);
       REQUIRE(a[i].dim == b[i].dim, "Invalid dimension: pair %d mixes %dD and %dD", i, a[i].dim, b[i].dim);
       REQUIRE(a[i].index_bytes == a[0].index_bytes && b[i].index_bytes == a[0].index_bytes,
               "all meshes of a batch must use the same index width");

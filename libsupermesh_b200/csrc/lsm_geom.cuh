@@ -119,6 +119,29 @@ __device__ __forceinline__ void tri_lines(const double* v, Lines& L) {
   }
 }
 
+// Edge lines of a convex polygon B with `loc` vertices
+// (Triangle_Intersection.F90:422-451): normal (y_{i+1}-y_i, -(x_{i+1}-x_i)),
+// point v_i, all flipped when (v_1 - p_2) . n_2 > 0.
+template <int LOC>
+__device__ __forceinline__ void poly_lines(const double* v, double* nx, double* ny, double* px, double* py) {
+#pragma unroll
+  for (int i = 0; i < LOC; ++i) {
+    const int j = (i + 1) % LOC;
+    nx[i] = (v[2 * j + 1] - v[2 * i + 1]);
+    ny[i] = -(v[2 * j] - v[2 * i]);
+    px[i] = v[2 * i];
+    py[i] = v[2 * i + 1];
+  }
+  const double dot = (v[0] - px[1]) * nx[1] + (v[1] - py[1]) * ny[1];
+  if (dot > 0.0) {
+#pragma unroll
+    for (int i = 0; i < LOC; ++i) {
+      nx[i] = -nx[i];
+      ny[i] = -ny[i];
+    }
+  }
+}
+
 // ------------------------------------------------------------- tet setup
 struct Planes {
   double nx[4], ny[4], nz[4], c[4];
@@ -157,6 +180,37 @@ __device__ __forceinline__ void tet_planes(const Tet& t, Planes& P) {
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) P.c[i] = (t.x[i] * P.nx[i] + t.y[i] * P.ny[i]) + t.z[i] * P.nz[i];
+}
+
+// Face planes of a hexahedron in Gmsh node order (Supermesh.F90:262-280):
+// plane f = unit_cross(h[a] - h[b], h[c] - h[d]) with offset h[b] . n; no
+// orientation fix-up.
+__device__ __forceinline__ void hex_planes(const double* h, double* nx, double* ny, double* nz, double* c) {
+  const int F[6][4] = {{1, 0, 5, 0}, {5, 4, 6, 4}, {1, 5, 2, 5}, {0, 1, 3, 1}, {4, 0, 7, 0}, {6, 7, 2, 7}};
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const double* a = h + 3 * F[f][0];
+    const double* b = h + 3 * F[f][1];
+    const double* cc = h + 3 * F[f][2];
+    const double* d = h + 3 * F[f][3];
+    unit_cross(a[0] - b[0], a[1] - b[1], a[2] - b[2], cc[0] - d[0], cc[1] - d[1], cc[2] - d[2], nx[f], ny[f],
+               nz[f]);
+    c[f] = (b[0] * nx[f] + b[1] * ny[f]) + b[2] * nz[f];
+  }
+}
+
+// Interval length and intersection (Interval_Intersection.F90:45-110).
+__device__ __forceinline__ double interval_size(double a0, double a1) { return fabs(a1 - a0); }
+
+__device__ __forceinline__ int intersect_intervals(double a0, double a1, double b0, double b1, double& c0,
+                                                   double& c1) {
+  const double min_a = fmin(a0, a1), max_a = fmax(a0, a1);
+  const double min_b = fmin(b0, b1), max_b = fmax(b0, b1);
+  if (max_b <= min_a || min_b >= max_a) return 0;
+  c0 = fmax(min_a, min_b);
+  c1 = fmin(max_a, max_b);
+  const double tol = 10.0 * fmin(spacing(interval_size(a0, a1)), spacing(interval_size(b0, b1)));
+  return interval_size(c0, c1) < tol ? 0 : 1;
 }
 
 // ------------------------------------------------------------ tri clipping

@@ -1159,24 +1159,24 @@ struct RegPlanes {  // planes computed in registers
   }
 };
 
-// Depth-first clip of tet `t` by 4 planes; calls leaf(tet) for each final
+// Depth-first clip of tet `t` by NP planes; calls leaf(tet) for each final
 // tet with vol_v4 >= tol, in the reference's output order.  Returns the
-// number of kept tets.
-template <class Src, class Stack, class Leaf>
+// number of kept tets.  The stack needs 2*(NP-1) slots.
+template <int NP = 4, class Src, class Stack, class Leaf>
 __device__ __forceinline__ int clip_tet_dfs(Tet t, const Src& planes, double tol, Stack& stk, Leaf leaf) {
   int sp = 0;
-  unsigned levels = 0;  // 2 bits per stack slot
+  unsigned long long levels = 0;  // 3 bits per stack slot
   int L = 0;
   int kept = 0;
-  for (int guard = 0; guard < 64; ++guard) {  // at most 1+3+9+27 tets are clipped
+  for (int guard = 0; guard < 1200; ++guard) {  // at most (3^NP - 1)/2 tets are clipped
     double nx, ny, nz, c;
     planes.get(L, nx, ny, nz, c);
-    DfsSink<Stack, Leaf> sink{stk, leaf, sp, L == 3, tol, 0, 0};
+    DfsSink<Stack, Leaf> sink{stk, leaf, sp, L == NP - 1, tol, 0, 0};
     const int k = clip_tet_plane(t, nx, ny, nz, c, sink);
     kept += sink.kept;
-    if (L < 3 && k > 0) {
-      if (k > 1) levels |= (unsigned)(L + 1) << (2 * sp);
-      if (k > 2) levels |= (unsigned)(L + 1) << (2 * (sp + 1));
+    if (L < NP - 1 && k > 0) {
+      if (k > 1) levels |= (unsigned long long)(L + 1) << (3 * sp);
+      if (k > 2) levels |= (unsigned long long)(L + 1) << (3 * (sp + 1));
       sp += k - 1;
       ++L;
       continue;
@@ -1184,11 +1184,30 @@ __device__ __forceinline__ int clip_tet_dfs(Tet t, const Src& planes, double tol
     if (sp == 0) break;
     --sp;
     stk.load(sp, t);
-    L = (int)((levels >> (2 * sp)) & 3u);
-    levels &= ~(3u << (2 * sp));
+    L = (int)((levels >> (3 * sp)) & 7ull);
+    levels &= ~(7ull << (3 * sp));
   }
   return kept;
 }
+
+// Planes in a per-thread array (explicit pairs: hex faces).
+template <int NP>
+struct ArrPlanes {
+  double nx[NP], ny[NP], nz[NP], c[NP];
+  __device__ __forceinline__ void get(int L, double& a, double& b, double& d, double& e) const {
+    a = nx[L];
+    b = ny[L];
+    d = nz[L];
+    e = c[L];
+  }
+};
+
+template <int N>
+struct TetStackN {
+  Tet slot[N];
+  __device__ __forceinline__ void store(int s, const Tet& t) { slot[s] = t; }
+  __device__ __forceinline__ void load(int s, Tet& t) const { t = slot[s]; }
+};
 
 __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
   const double2* q = reinterpret_cast<const double2*>(v);
@@ -2119,6 +2138,380 @@ __global__ void k_pairs_tets(int64_t n, const double* __restrict__ A, const doub
   }
 }
 
+// Triangle vs quadrilateral (Supermesh.F90:211-228): clip by the quad's 4
+// edge lines, tolerance from the triangle's area only.
+struct TriQuadEmit {
+  double* out;  // [46][3][2] for this pair, or nullptr
+  __device__ __forceinline__ void operator()(int k, double x0, double y0, double x1, double y1, double x2,
+                                             double y2) const {
+    if (!out || k >= 46) return;
+    double* o = out + 6 * k;
+    o[0] = x0;
+    o[1] = y0;
+    o[2] = x1;
+    o[3] = y1;
+    o[4] = x2;
+    o[5] = y2;
+  }
+};
+
+__global__ void k_pairs_tri_quad(int64_t n, const double* __restrict__ A, const double* __restrict__ B,
+                                 double* measure, int32_t* nout, double* out_elems) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* va = A + 6 * i;
+    double nx[4], ny[4], px[4], py[4];
+    poly_lines<4>(B + 8 * i, nx, ny, px, py);
+    const double tol = 10.0 * spacing(tri_area(va[0], va[1], va[2], va[3], va[4], va[5]));
+    LocalPoly<48> p, q;
+    p.set(0, va[0], va[1]);
+    p.set(1, va[2], va[3]);
+    p.set(2, va[4], va[5]);
+    int m = 3;
+    bool empty = false;
+    for (int l = 0; l < 4 && !empty; ++l) {
+      m = (l & 1) ? clip_stage(q, p, m, 48, nx[l], ny[l], px[l], py[l])
+                  : clip_stage(p, q, m, 48, nx[l], ny[l], px[l], py[l]);
+      empty = m < 3;
+    }
+    double meas = 0.0;
+    int kept = 0;
+    if (!empty) {  // after 4 stages the polygon is back in p
+      TriQuadEmit emit{out_elems ? out_elems + 46 * 6 * i : nullptr};
+      const double x0 = p.x(0), y0 = p.y(0);
+      for (int j = 1; j < m - 1; ++j) {
+        const double xi = p.x(j), yi = p.y(j), xj = p.x(j + 1), yj = p.y(j + 1);
+        const double ar = tri_area(x0, y0, xi, yi, xj, yj);
+        if (!(ar < tol)) {
+          meas = meas + ar;
+          emit(kept, x0, y0, xi, yi, xj, yj);
+          ++kept;
+        }
+      }
+    }
+    if (measure) measure[i] = meas;
+    if (nout) nout[i] = kept;
+  }
+}
+
+// Tetrahedron vs hexahedron (Supermesh.F90:248-295): clip by the hex's 6
+// face planes, tolerance from the tet's volume only.
+__global__ void __launch_bounds__(64) k_pairs_tet_hex(int64_t n, const double* __restrict__ A,
+                                                      const double* __restrict__ B, double* measure,
+                                                      int32_t* nout, double* out_elems) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    Tet ta;
+    load_tet(A + 12 * i, ta);
+    ArrPlanes<6> P;
+    hex_planes(B + 24 * i, P.nx, P.ny, P.nz, P.c);
+    const double tol = 10.0 * spacing(tet_volume_v4(ta));
+    TetStackN<10> stk;
+    double m = 0.0;
+    int idx = 0;
+    double* o = out_elems ? out_elems + (int64_t)729 * 12 * i : nullptr;
+    const int k = clip_tet_dfs<6>(ta, P, tol, stk, [&](const Tet& t) {
+      m = m + tet_volume_v1(t);
+      if (o && idx < 729) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          o[12 * idx + 3 * v + 0] = t.x[v];
+          o[12 * idx + 3 * v + 1] = t.y[v];
+          o[12 * idx + 3 * v + 2] = t.z[v];
+        }
+      }
+      ++idx;
+    });
+    if (measure) measure[i] = m;
+    if (nout) nout[i] = k;
+  }
+}
+
+__global__ void k_pairs_intervals(int64_t n, const double* __restrict__ A, const double* __restrict__ B,
+                                  double* measure, int32_t* nout, double* out_elems) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double c0 = 0.0, c1 = 0.0;
+    const int k = intersect_intervals(A[2 * i], A[2 * i + 1], B[2 * i], B[2 * i + 1], c0, c1);
+    if (out_elems && k) {
+      out_elems[2 * i] = c0;
+      out_elems[2 * i + 1] = c1;
+    }
+    if (measure) measure[i] = k ? interval_size(c0, c1) : 0.0;
+    if (nout) nout[i] = k;
+  }
+}
+
+cudaError_t launch_pairs_mixed(int kind, int64_t n, const double* a, const double* b, double* measure,
+                               int32_t* nout, double* out_elems, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launch();
+  if (kind == 0)
+    k_pairs_intervals<<<grid_for(n, 256, 8), 256, 0, s>>>(n, a, b, measure, nout, out_elems);
+  else if (kind == 1)
+    k_pairs_tri_quad<<<grid_for(n, 128, 8), 128, 0, s>>>(n, a, b, measure, nout, out_elems);
+  else
+    k_pairs_tet_hex<<<grid_for(n, 64, 8), 64, 0, s>>>(n, a, b, measure, nout, out_elems);
+  return cudaGetLastError();
+}
+
+// ======================================================================
+// 1D sort finder (Intersection_Finder.F90:811-921): elements sorted by left
+// end, then one sweep pointer over the sorted B elements.  Restated as
+//   E_i  = first sorted B element whose left end >= right end of sorted A_i
+//   L_i  = last sorted B element before E_i whose right end > left end of A_i
+//   row_i records {j in [js_i, E_i) : right_B(j) > left_A(i)}
+//   js_{i+1} = y_i - [js_i <= L_i],  y_i = max(js_i, E_i) advanced past B
+//              points equal to a point A_i
+// E_i and L_i (binary search, max segment tree) and the rows are computed in
+// parallel; only the integer recurrence for js runs on one warp.
+// ======================================================================
+__device__ __forceinline__ uint64_t ordered_key(double x) {
+  if (x == 0.0) x = 0.0;  // -0 and +0 compare equal: give them one key
+  const uint64_t u = (uint64_t)__double_as_longlong(x);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+__global__ void k_prep_1d(int64_t nel, const double* __restrict__ pos, int stride, const void* __restrict__ en,
+                          int idx_bytes, int64_t nnodes, double* coords, uint32_t* key_lo, uint32_t* key_hi,
+                          int32_t* vals, int* bad) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t n0, n1;
+    if (idx_bytes == 8) {
+      n0 = static_cast<const int64_t*>(en)[2 * e];
+      n1 = static_cast<const int64_t*>(en)[2 * e + 1];
+    } else {
+      n0 = static_cast<const int32_t*>(en)[2 * e];
+      n1 = static_cast<const int32_t*>(en)[2 * e + 1];
+    }
+    if (n0 < 0 || n0 >= nnodes || n1 < 0 || n1 >= nnodes) {
+      atomicExch(bad, 1);
+      n0 = n1 = 0;
+    }
+    const double x0 = pos[n0 * stride], x1 = pos[n1 * stride];
+    coords[2 * e] = x0;
+    coords[2 * e + 1] = x1;
+    const uint64_t k = ordered_key(x1 < x0 ? x1 : x0);
+    key_lo[e] = (uint32_t)k;
+    key_hi[e] = (uint32_t)(k >> 32);
+    vals[e] = (int32_t)e;
+  }
+}
+
+__global__ void k_permute_u32(int64_t n, const int32_t* __restrict__ perm, const uint32_t* __restrict__ in,
+                              uint32_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[perm[i]];
+}
+
+__global__ void k_sorted_ends_1d(int64_t n, const int32_t* __restrict__ perm, const double* __restrict__ coords,
+                                 double* lo, double* hi) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t e = perm[i];
+    const double x0 = coords[2 * e], x1 = coords[2 * e + 1];
+    lo[i] = x1 < x0 ? x1 : x0;
+    hi[i] = x1 > x0 ? x1 : x0;
+  }
+}
+
+__global__ void k_tree_leaves(int64_t n, int64_t P, const double* __restrict__ v, double* tree) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += (int64_t)gridDim.x * blockDim.x)
+    tree[P + i] = i < n ? v[i] : -INFINITY;
+}
+
+__global__ void k_tree_level(int64_t w, double* tree) {
+  for (int64_t k = w + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 2 * w; k += (int64_t)gridDim.x * blockDim.x)
+    tree[k] = fmax(tree[2 * k], tree[2 * k + 1]);
+}
+
+// Last leaf index < E whose value is > t, or -1 (tree over P leaves).
+__device__ __forceinline__ int rightmost_greater(const double* __restrict__ tree, int64_t P, int64_t E, double t) {
+  if (E <= 0) return -1;
+  int64_t node = P + E - 1;
+  for (int guard = 0; guard < 256; ++guard) {
+    if (tree[node] > t) {
+      while (node < P) node = tree[2 * node + 1] > t ? 2 * node + 1 : 2 * node;
+      return (int)(node - P);
+    }
+    // move to the subtree just left of `node`
+    while ((node & (node - 1)) != 0 && (node & 1) == 0) node >>= 1;
+    if ((node & (node - 1)) == 0) return -1;  // leftmost at its level
+    node -= 1;
+  }
+  return -1;
+}
+
+__global__ void k_rows_1d(int64_t na, const double* __restrict__ lo_a, const double* __restrict__ hi_a, int64_t nb,
+                          const double* __restrict__ lo_b, const double* __restrict__ tree, int64_t P, int32_t* E,
+                          int32_t* L) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (int64_t)gridDim.x * blockDim.x) {
+    const double h = hi_a[i];
+    int64_t lo = 0, hi = nb;  // first j with lo_b[j] >= h
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (lo_b[mid] < h)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    E[i] = (int32_t)lo;
+    L[i] = nb > 0 ? rightmost_greater(tree, P, lo, lo_a[i]) : -1;
+  }
+}
+
+__global__ void __launch_bounds__(32) k_sweep_1d(int64_t na, int64_t nb, const int32_t* __restrict__ E,
+                                                 const int32_t* __restrict__ L, const double* __restrict__ lo_a,
+                                                 const double* __restrict__ hi_a, const double* __restrict__ hi_b,
+                                                 int32_t* JS) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x;
+  int64_t js = 0;
+  for (int64_t base = 0; base < na; base += 32) {
+    const int64_t i = base + lane;
+    int e = 0, l = -1;
+    double lo = 0.0, hi = 1.0;
+    if (i < na) {
+      e = E[i];
+      l = L[i];
+      lo = lo_a[i];
+      hi = hi_a[i];
+    }
+    const unsigned point = __ballot_sync(full, i < na && !(lo < hi));
+    const int cnt = (int)(na - base < 32 ? na - base : 32);
+    int64_t mine = 0;
+    for (int k = 0; k < cnt; ++k) {
+      const int ek = __shfl_sync(full, e, k);
+      const int lk = __shfl_sync(full, l, k);
+      if (lane == k) mine = js;
+      int64_t y = js > ek ? js : ek;
+      if ((point >> k) & 1u) {
+        const double t = __shfl_sync(full, lo, k);
+        while (y < nb && hi_b[y] <= t) ++y;
+      }
+      js = js <= lk ? y - 1 : y;
+    }
+    if (i < na) JS[i] = (int32_t)mine;
+  }
+}
+
+template <bool FILL>
+__global__ void k_emit_1d(int64_t na, const int32_t* __restrict__ JS, const int32_t* __restrict__ E,
+                          const double* __restrict__ lo_a, const double* __restrict__ hi_b,
+                          const int32_t* __restrict__ perm_a, const int32_t* __restrict__ perm_b, int* counts,
+                          const int64_t* __restrict__ offsets, int32_t* pair_a, int32_t* pair_b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t a = perm_a[i];
+    const double t = lo_a[i];
+    const int32_t end = E[i];
+    int64_t out = FILL ? offsets[a] : 0;
+    int cnt = 0;
+    for (int32_t j = JS[i]; j < end; ++j) {
+      if (hi_b[j] > t) {
+        if (FILL) {
+          pair_a[out + cnt] = a;
+          pair_b[out + cnt] = perm_b[j];
+        }
+        ++cnt;
+      }
+    }
+    if (!FILL) counts[a] = cnt;
+  }
+}
+
+cudaError_t launch_prep_1d(int64_t nel, const double* pos, int stride, const void* en, int idx_bytes,
+                           int64_t nnodes, double* coords, uint32_t* key_lo, uint32_t* key_hi, int32_t* vals,
+                           int* bad, cudaStream_t s) {
+  if (nel <= 0) return cudaSuccess;
+  count_launch();
+  k_prep_1d<<<grid_for(nel, 256, 8), 256, 0, s>>>(nel, pos, stride, en, idx_bytes, nnodes, coords, key_lo, key_hi,
+                                                  vals, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t sort_by_key64(int64_t n, uint32_t* key_lo, const uint32_t* key_hi, int32_t* vals, uint32_t* keys_tmp,
+                          int32_t* vals_tmp, uint32_t* hist, cudaStream_t s) {
+  if (n <= 1) return cudaSuccess;
+  cudaError_t e = radix_sort_pairs(n, 32, key_lo, vals, keys_tmp, vals_tmp, hist, s);
+  if (e != cudaSuccess) return e;
+  count_launch();
+  k_permute_u32<<<grid_for(n, 256, 8), 256, 0, s>>>(n, vals, key_hi, key_lo);
+  return radix_sort_pairs(n, 32, key_lo, vals, keys_tmp, vals_tmp, hist, s);
+}
+
+cudaError_t launch_sorted_ends_1d(int64_t n, const int32_t* perm, const double* coords, double* lo, double* hi,
+                                  cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launch();
+  k_sorted_ends_1d<<<grid_for(n, 256, 8), 256, 0, s>>>(n, perm, coords, lo, hi);
+  return cudaGetLastError();
+}
+
+int64_t tree_leaves_1d(int64_t n) {
+  int64_t P = 1;
+  while (P < n) P <<= 1;
+  return P;
+}
+
+cudaError_t launch_max_tree(int64_t n, const double* v, double* tree, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t P = tree_leaves_1d(n);
+  count_launch();
+  k_tree_leaves<<<grid_for(P, 256, 8), 256, 0, s>>>(n, P, v, tree);
+  for (int64_t w = P / 2; w >= 1; w /= 2) {
+    count_launch();
+    k_tree_level<<<grid_for(w, 256, 8), 256, 0, s>>>(w, tree);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows_1d(int64_t na, const double* lo_a, const double* hi_a, int64_t nb, const double* lo_b,
+                           const double* tree, int32_t* E, int32_t* L, cudaStream_t s) {
+  if (na <= 0) return cudaSuccess;
+  count_launch();
+  k_rows_1d<<<grid_for(na, 256, 8), 256, 0, s>>>(na, lo_a, hi_a, nb, lo_b, tree, tree_leaves_1d(nb), E, L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_1d(int64_t na, int64_t nb, const int32_t* E, const int32_t* L, const double* lo_a,
+                            const double* hi_a, const double* hi_b, int32_t* JS, cudaStream_t s) {
+  if (na <= 0) return cudaSuccess;
+  count_launch();
+  k_sweep_1d<<<1, 32, 0, s>>>(na, nb, E, L, lo_a, hi_a, hi_b, JS);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_emit_1d(bool fill, int64_t na, const int32_t* JS, const int32_t* E, const double* lo_a,
+                           const double* hi_b, const int32_t* perm_a, const int32_t* perm_b, int* counts,
+                           const int64_t* offsets, int32_t* pair_a, int32_t* pair_b, cudaStream_t s) {
+  if (na <= 0) return cudaSuccess;
+  count_launch();
+  if (fill)
+    k_emit_1d<true><<<grid_for(na, 256, 8), 256, 0, s>>>(na, JS, E, lo_a, hi_b, perm_a, perm_b, counts, offsets,
+                                                         pair_a, pair_b);
+  else
+    k_emit_1d<false><<<grid_for(na, 256, 8), 256, 0, s>>>(na, JS, E, lo_a, hi_b, perm_a, perm_b, counts, offsets,
+                                                          pair_a, pair_b);
+  return cudaGetLastError();
+}
+
+// Narrow phase of 1D candidates: intersect_intervals per pair.
+__global__ void k_clip_intervals(int64_t n, const int32_t* __restrict__ pa, const int32_t* __restrict__ pb,
+                                 const double* __restrict__ ca, const double* __restrict__ cb, double* measure,
+                                 int32_t* nout) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t a = pa[i], b = pb[i];
+    double c0 = 0.0, c1 = 0.0;
+    const int k = intersect_intervals(ca[2 * a], ca[2 * a + 1], cb[2 * b], cb[2 * b + 1], c0, c1);
+    measure[i] = k ? interval_size(c0, c1) : 0.0;
+    nout[i] = k;
+  }
+}
+
+cudaError_t launch_clip_intervals(int64_t n, const int32_t* pa, const int32_t* pb, const double* ca,
+                                  const double* cb, double* measure, int32_t* nout, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launch();
+  k_clip_intervals<<<grid_for(n, 256, 8), 256, 0, s>>>(n, pa, pb, ca, cb, measure, nout);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const double* b,
                                   double* measure, int32_t* nout, double* out_elems,
                                   cudaStream_t s) {
@@ -2135,7 +2528,9 @@ cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const dou
 
 __global__ void k_measure_explicit(int dim, int64_t n, const double* __restrict__ e, double* out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    if (dim == 2) {
+    if (dim == 1) {
+      out[i] = interval_size(e[2 * i], e[2 * i + 1]);
+    } else if (dim == 2) {
       const double* v = e + 6 * i;
       out[i] = tri_area(v[0], v[1], v[2], v[3], v[4], v[5]);
     } else {

@@ -136,6 +136,33 @@ cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const dou
                                   cudaStream_t s);
 cudaError_t launch_measure_explicit(int dim, int64_t n, const double* elems, double* out,
                                     cudaStream_t s);
+// Mixed pairs: kind 0 intervals ([n][2] x [n][2] -> [n][2]), 1 tri vs quad
+// ([n][3][2] x [n][4][2] -> [n][46][3][2]), 2 tet vs hex ([n][4][3] x
+// [n][8][3] -> [n][729][4][3]).
+cudaError_t launch_pairs_mixed(int kind, int64_t n, const double* a, const double* b, double* measure,
+                               int32_t* nout, double* out_elems, cudaStream_t s);
+// 1D sort finder.  prep gathers the first coordinate of both nodes of each
+// element (coords[2*nel]) and the 64-bit order key of its left end;
+// sort_by_key64 is a stable sort of (key, val) pairs; the max tree over the
+// sorted right ends of B holds 2*tree_leaves_1d(nb) doubles.
+cudaError_t launch_prep_1d(int64_t nel, const double* pos, int stride, const void* en, int idx_bytes,
+                           int64_t nnodes, double* coords, uint32_t* key_lo, uint32_t* key_hi, int32_t* vals,
+                           int* bad, cudaStream_t s);
+cudaError_t sort_by_key64(int64_t n, uint32_t* key_lo, const uint32_t* key_hi, int32_t* vals, uint32_t* keys_tmp,
+                          int32_t* vals_tmp, uint32_t* hist, cudaStream_t s);
+cudaError_t launch_sorted_ends_1d(int64_t n, const int32_t* perm, const double* coords, double* lo, double* hi,
+                                  cudaStream_t s);
+int64_t tree_leaves_1d(int64_t n);
+cudaError_t launch_max_tree(int64_t n, const double* v, double* tree, cudaStream_t s);
+cudaError_t launch_rows_1d(int64_t na, const double* lo_a, const double* hi_a, int64_t nb, const double* lo_b,
+                           const double* tree, int32_t* E, int32_t* L, cudaStream_t s);
+cudaError_t launch_sweep_1d(int64_t na, int64_t nb, const int32_t* E, const int32_t* L, const double* lo_a,
+                            const double* hi_a, const double* hi_b, int32_t* JS, cudaStream_t s);
+cudaError_t launch_emit_1d(bool fill, int64_t na, const int32_t* JS, const int32_t* E, const double* lo_a,
+                           const double* hi_b, const int32_t* perm_a, const int32_t* perm_b, int* counts,
+                           const int64_t* offsets, int32_t* pair_a, int32_t* pair_b, cudaStream_t s);
+cudaError_t launch_clip_intervals(int64_t n, const int32_t* pa, const int32_t* pb, const double* ca,
+                                  const double* cb, double* measure, int32_t* nout, cudaStream_t s);
 
 // P1-P1 mixed mass blocks per candidate pair and u^T M v partials.
 cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,

@@ -55,6 +55,7 @@ def lib():
         L.orc_kahan_sum.restype = ctypes.c_double
         L.orc_kahan_sum.argtypes = [_dp, ctypes.c_long]
         L.orc_num_threads_available.restype = ctypes.c_int
+        L.orc_interval_size.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -101,6 +102,63 @@ def intersect_tets(tet_a, tet_b):
     n = ctypes.c_int(0)
     lib().orc_intersect_tets(_d(a), _d(b), _d(out), ctypes.byref(n))
     return out[: n.value].copy()
+
+
+def intersect_tri_quad(tri_a, quad_b):
+    a = np.ascontiguousarray(tri_a, dtype=np.float64).reshape(6)
+    b = np.ascontiguousarray(quad_b, dtype=np.float64).reshape(8)
+    out = np.zeros((46, 3, 2))
+    n = ctypes.c_int(0)
+    lib().orc_intersect_tri_quad(_d(a), _d(b), _d(out), ctypes.byref(n))
+    return out[: n.value].copy()
+
+
+def intersect_tet_hex(tet_a, hex_b):
+    a = np.ascontiguousarray(tet_a, dtype=np.float64).reshape(12)
+    b = np.ascontiguousarray(hex_b, dtype=np.float64).reshape(24)
+    out = np.zeros((729, 4, 3))
+    n = ctypes.c_int(0)
+    lib().orc_intersect_tet_hex(_d(a), _d(b), _d(out), ctypes.byref(n))
+    return out[: n.value].copy()
+
+
+def intersect_intervals(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(2)
+    b = np.ascontiguousarray(b, dtype=np.float64).reshape(2)
+    out = np.zeros(2)
+    n = ctypes.c_int(0)
+    lib().orc_intersect_intervals(_d(a), _d(b), _d(out), ctypes.byref(n))
+    return out.copy() if n.value else np.zeros(0)
+
+
+def interval_size(iv) -> float:
+    iv = np.ascontiguousarray(iv, dtype=np.float64).reshape(2)
+    return lib().orc_interval_size(_d(iv))
+
+
+def sort_finder_1d(mesh_a, mesh_b, stable: bool = True):
+    """Sort-and-sweep finder for 2-node meshes (first coordinate of each
+    node).  stable=False keeps the reference's merge sort leaf step as
+    written; stable=True uses the stable sort by left end."""
+    pa = np.ascontiguousarray(mesh_a[0], dtype=np.float64)
+    pb = np.ascontiguousarray(mesh_b[0], dtype=np.float64)
+    sa = 1 if pa.ndim == 1 else pa.shape[1]
+    sb = 1 if pb.ndim == 1 else pb.shape[1]
+    ea = np.ascontiguousarray(mesh_a[1], dtype=np.int32)
+    eb = np.ascontiguousarray(mesh_b[1], dtype=np.int32)
+    indptr = np.zeros(ea.shape[0] + 1, dtype=np.int64)
+    ind = _i32p()
+    nnz = ctypes.c_int64(0)
+    rc = lib().orc_sort_finder_1d(ctypes.c_long(pa.shape[0]), _d(pa), ctypes.c_int(sa), ctypes.c_long(ea.shape[0]),
+                                  _i32(ea), ctypes.c_long(pb.shape[0]), _d(pb), ctypes.c_int(sb),
+                                  ctypes.c_long(eb.shape[0]), _i32(eb), ctypes.c_int(int(stable)),
+                                  _i64(indptr), ctypes.byref(ind), ctypes.byref(nnz))
+    if rc != 0:
+        raise RuntimeError("oracle 1D finder failed")
+    n = nnz.value
+    indices = np.ctypeslib.as_array(ind, shape=(max(n, 1),))[:n].copy()
+    lib().orc_free(ind)
+    return indptr, indices
 
 
 def _mesh_args(pos, en):

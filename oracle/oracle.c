@@ -159,7 +159,7 @@ static void get_lines_tri(const double v[6], orc_line L[3]) {
 /* One Sutherland-Hodgman pass; returns the output vertex count. */
 static int clip_buf_tri(const orc_line *L, const double *pts, int n,
                         double *out) {
-  double d[ORC_PBUF];
+  double d[64]; /* polygons of up to 48 vertices (tri vs quad) */
   for (int i = 0; i < n; ++i) {
     d[i] = L->n[0] * (pts[2 * i] - L->p[0]) + L->n[1] * (pts[2 * i + 1] - L->p[1]);
   }
@@ -448,6 +448,128 @@ void orc_intersect_tets(const double tet_a[12], const double tet_b[12],
 }
 
 /* ------------------------------------------------------------------ */
+/* Mixed element pairs and intervals (Supermesh.F90:211-301,            */
+/* Triangle_Intersection.F90:216-276, 422-451,                          */
+/* Tetrahedron_Intersection.F90:190-242, Interval_Intersection.F90)     */
+/* ------------------------------------------------------------------ */
+static void get_lines_poly(const double *v, int loc, orc_line *L) {
+  /* get_lines_poly: normal (y_{i+1}-y_i, -(x_{i+1}-x_i)), point v_i;
+   * flipped when (v_1 - p_2) . n_2 > 0 */
+  for (int i = 0; i < loc; ++i) {
+    int j = (i + 1) % loc;
+    L[i].n[0] = (v[2 * j + 1] - v[2 * i + 1]);
+    L[i].n[1] = -(v[2 * j] - v[2 * i]);
+    L[i].p[0] = v[2 * i];
+    L[i].p[1] = v[2 * i + 1];
+  }
+  FL(4 * loc);
+  double dot = (v[0] - L[1].p[0]) * L[1].n[0] + (v[1] - L[1].p[1]) * L[1].n[1];
+  FL(5);
+  if (dot > 0.0)
+    for (int i = 0; i < loc; ++i) {
+      L[i].n[0] = -L[i].n[0];
+      L[i].n[1] = -L[i].n[1];
+    }
+}
+
+#define ORC_QBUF 48 /* 3 * 2**4 */
+
+void orc_intersect_tri_quad(const double tri_a[6], const double quad_b[8], double *tris_c, int *n_tris_c) {
+  /* intersect_polys_lines with area_a only: tol = 10*spacing(area(tri_a)) */
+  orc_line L[4];
+  get_lines_poly(quad_b, 4, L);
+  double pa[2 * ORC_QBUF], pb[2 * ORC_QBUF];
+  memcpy(pa, tri_a, 6 * sizeof(double));
+  int n = 3;
+  double *cur = pa, *nxt = pb;
+  *n_tris_c = 0;
+  for (int i = 0; i < 4; ++i) {
+    n = clip_buf_tri(&L[i], cur, n, nxt);
+    if (n < 3) return;
+    double *t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  double tol = 10.0 * orc_spacing(orc_triangle_area(tri_a));
+  int nt = 0;
+  for (int i = 0; i < n - 2; ++i) {
+    double *t = tris_c + 6 * nt;
+    t[0] = cur[0];
+    t[1] = cur[1];
+    t[2] = cur[2 * (i + 1)];
+    t[3] = cur[2 * (i + 1) + 1];
+    t[4] = cur[2 * (i + 2)];
+    t[5] = cur[2 * (i + 2) + 1];
+    if (!(orc_triangle_area(t) < tol)) ++nt;
+  }
+  *n_tris_c = nt;
+}
+
+static void hex_planes(const double *h, orc_plane P[6]) {
+  /* Supermesh.F90 intersect_tet_hex: Gmsh node order, no orientation flip */
+  static const int F[6][4] = {{1, 0, 5, 0}, {5, 4, 6, 4}, {1, 5, 2, 5}, {0, 1, 3, 1}, {4, 0, 7, 0}, {6, 7, 2, 7}};
+  for (int f = 0; f < 6; ++f) {
+    /* unit_cross(h[a] - h[b], h[c] - h[d]); c = h[b] . n (point on the face) */
+    double u[3], w[3];
+    for (int k = 0; k < 3; ++k) {
+      u[k] = h[3 * F[f][0] + k] - h[3 * F[f][1] + k];
+      w[k] = h[3 * F[f][2] + k] - h[3 * F[f][3] + k];
+    }
+    FL(6);
+    unit_cross(u, w, P[f].n);
+    const double *q = h + 3 * F[f][1];
+    P[f].c = (q[0] * P[f].n[0] + q[1] * P[f].n[1]) + q[2] * P[f].n[2];
+    FL(5);
+  }
+}
+
+#define ORC_HBUF 729 /* 3**6 */
+
+void orc_intersect_tet_hex(const double tet_a[12], const double hex_b[24], double *tets_c, int *n_tets_c) {
+  /* intersect_tet_planes over 6 planes, tol = 10*spacing(vol_v4(tet_a)) */
+  orc_plane P[6];
+  hex_planes(hex_b, P);
+  double tol = 10.0 * orc_spacing(orc_tetrahedron_volume_v4(tet_a));
+  double *cur = tets_c;
+  double *buf = (double *)malloc(sizeof(double) * 12 * ORC_HBUF);
+  int n = 1;
+  memcpy(cur, tet_a, 12 * sizeof(double));
+  for (int i = 0; i < 6; ++i) {
+    int m = 0;
+    for (int j = 0; j < n; ++j) m += clip_buf_tet(&P[i], cur + 12 * j, buf + 12 * m);
+    if (i != 5) {
+      n = m;
+      memcpy(cur, buf, (size_t)n * 12 * sizeof(double));
+    } else {
+      n = 0;
+      for (int j = 0; j < m; ++j) {
+        if (orc_tetrahedron_volume_v4(buf + 12 * j) >= tol) {
+          memcpy(cur + 12 * n, buf + 12 * j, 12 * sizeof(double));
+          ++n;
+        }
+      }
+    }
+  }
+  free(buf);
+  *n_tets_c = n;
+}
+
+double orc_interval_size(const double iv[2]) { return fabs(iv[1] - iv[0]); }
+
+void orc_intersect_intervals(const double a[2], const double b[2], double *c, int *n) {
+  double min_a = fmin(a[0], a[1]), max_a = fmax(a[0], a[1]);
+  double min_b = fmin(b[0], b[1]), max_b = fmax(b[0], b[1]);
+  if (max_b <= min_a || min_b >= max_a) {
+    *n = 0;
+    return;
+  }
+  c[0] = fmax(min_a, min_b);
+  c[1] = fmin(max_a, max_b);
+  double tol = 10.0 * fmin(orc_spacing(orc_interval_size(a)), orc_spacing(orc_interval_size(b)));
+  *n = orc_interval_size(c) < tol ? 0 : 1;
+}
+
+/* ------------------------------------------------------------------ */
 /* Quadtree / octree intersection finder                               */
 /* ------------------------------------------------------------------ */
 typedef struct orc_node {
@@ -696,6 +818,122 @@ int orc_brute_force_finder(int dim, long nnodes_a, const double *pos_a,
     memcpy(rows[a].v, buf, sizeof(int32_t) * (size_t)n);
   }
   free(bb);
+  free(buf);
+  int rc = rows_to_csr(rows, nel_a, indptr, indices, nnz);
+  free(rows);
+  return rc;
+}
+
+/* 1D sort finder (Intersection_Finder.F90:811-921).  Elements are ordered
+ * by their left end with the reference's merge sort, then one sweep pointer j
+ * walks the sorted B elements for each sorted A element: B elements ending at
+ * or before the A element's left end are passed for good, the sweep stops at
+ * the first B element starting at or after the A element's right end, and
+ * every other one is recorded; after a row with records j steps back by one.
+ *
+ * The reference's merge sort (Intersection_Finder.F90:871-910) handles blocks
+ * of at most 4 elements with a selection loop that writes, for each i, the
+ * position of the first strict minimum of v(i:n); that is a permutation only
+ * when the block is already non-decreasing.  stable_leaf = 0 restates it as
+ * written; stable_leaf = 1 replaces that step by a stable insertion sort, so
+ * the whole sort is the stable sort by left end. */
+static void ref_merge_sort(const double *v, int n, int *idx, int *work, int stable_leaf) {
+  if (n <= 4) {
+    if (stable_leaf) {
+      for (int i = 0; i < n; ++i) idx[i] = i;
+      for (int i = 1; i < n; ++i) {
+        int t = idx[i], k = i;
+        while (k > 0 && v[t] < v[idx[k - 1]]) {
+          idx[k] = idx[k - 1];
+          --k;
+        }
+        idx[k] = t;
+      }
+    } else {
+      for (int i = 0; i < n; ++i) {
+        idx[i] = i;
+        for (int j = i + 1; j < n; ++j)
+          if (v[j] < v[idx[i]]) idx[i] = j;
+      }
+    }
+    return;
+  }
+  const int h = n / 2;
+  ref_merge_sort(v, h, idx, work, stable_leaf);
+  ref_merge_sort(v + h, n - h, idx + h, work + h, stable_leaf);
+  for (int i = 0; i < h; ++i) work[i] = idx[i];
+  for (int i = h; i < n; ++i) work[i] = idx[i] + h;
+  int i1 = 0, i2 = h;
+  for (int i = 0; i < n; ++i) {
+    if (i1 >= h) {
+      for (int k = i; k < n; ++k) idx[k] = work[i2++];
+      break;
+    } else if (i2 >= n) {
+      for (int k = i; k < n; ++k) idx[k] = work[i1++];
+      break;
+    } else if (v[work[i1]] <= v[work[i2]]) {
+      idx[i] = work[i1++];
+    } else {
+      idx[i] = work[i2++];
+    }
+  }
+}
+
+/* minval / maxval of a 2-node element's coordinates (first coordinate of
+ * each node, positions stored with stride `stride`). */
+static void interval_ends(const double *pos, int stride, const int32_t *en, long e, double *lo, double *hi) {
+  const double x0 = pos[(size_t)en[2 * e] * stride], x1 = pos[(size_t)en[2 * e + 1] * stride];
+  *lo = x1 < x0 ? x1 : x0;
+  *hi = x1 > x0 ? x1 : x0;
+}
+
+int orc_sort_finder_1d(long nnodes_a, const double *pos_a, int stride_a, long nel_a, const int32_t *en_a,
+                       long nnodes_b, const double *pos_b, int stride_b, long nel_b, const int32_t *en_b,
+                       int stable_leaf, int64_t *indptr, int32_t **indices, int64_t *nnz) {
+  (void)nnodes_a;
+  (void)nnodes_b;
+  const size_t na = (size_t)(nel_a > 0 ? nel_a : 1), nb = (size_t)(nel_b > 0 ? nel_b : 1);
+  double *la = (double *)calloc(na, sizeof(double)), *ha = (double *)calloc(na, sizeof(double));
+  double *lb = (double *)calloc(nb, sizeof(double)), *hb = (double *)calloc(nb, sizeof(double));
+  int *ia = (int *)malloc(sizeof(int) * na), *ib = (int *)malloc(sizeof(int) * nb);
+  int *work = (int *)malloc(sizeof(int) * (na > nb ? na : nb));
+  int32_t *buf = (int32_t *)malloc(sizeof(int32_t) * nb);
+  orc_row *rows = (orc_row *)calloc(na, sizeof(orc_row));
+  if (!la || !ha || !lb || !hb || !ia || !ib || !work || !buf || !rows) return -1;
+  for (long e = 0; e < nel_a; ++e) interval_ends(pos_a, stride_a, en_a, e, la + e, ha + e);
+  for (long e = 0; e < nel_b; ++e) interval_ends(pos_b, stride_b, en_b, e, lb + e, hb + e);
+  ref_merge_sort(la, (int)nel_a, ia, work, stable_leaf);
+  ref_merge_sort(lb, (int)nel_b, ib, work, stable_leaf);
+  long j = 0;
+  for (long i = 0; i < nel_a; ++i) {
+    const int a = ia[i];
+    int n = 0;
+    while (j < nel_b) {
+      const int b = ib[j];
+      if (hb[b] <= la[a]) {
+        ++j;
+      } else if (lb[b] >= ha[a]) {
+        break;
+      } else {
+        buf[n++] = (int32_t)b;
+        ++j;
+      }
+    }
+    if (n > 0) --j;
+    /* with a non-permutation sort an element can come twice: the reference
+     * then reallocates that row; the last write wins */
+    free(rows[a].v);
+    rows[a].n = n;
+    rows[a].v = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    memcpy(rows[a].v, buf, sizeof(int32_t) * (size_t)n);
+  }
+  free(la);
+  free(ha);
+  free(lb);
+  free(hb);
+  free(ia);
+  free(ib);
+  free(work);
   free(buf);
   int rc = rows_to_csr(rows, nel_a, indptr, indices, nnz);
   free(rows);

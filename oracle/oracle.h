@@ -18,7 +18,12 @@
  *                                     max_nelist_degree, allocate_node,
  *                                     add_element, query_node_internal, bbox,
  *                                     bboxes_intersect
- *   src/Intersection_Finder.F90       brute_force finder (:989-1077)
+ *   src/Intersection_Finder.F90       brute_force finder (:989-1077), sort
+ *                                     finder (:811-921)
+ *   src/Triangle_Intersection.F90     intersect_polys / get_lines_poly
+ *                                     (:187-239, :422-451) for tri vs quad
+ *   src/Supermesh.F90                 intersect_tet_hex (:248-295)
+ *   src/Interval_Intersection.F90     intersect_intervals, interval_size
  *   src/Intersections.F90:48-71       ragged -> CSR
  *   src/Precision.F90:72-113          Kahan compensated sum
  *   src/tests/test_parallel_p1_inner_product_{2d,3d}.F90  P1 quadrature
@@ -55,6 +60,13 @@ void orc_intersect_tris(const double tri_a[6], const double tri_b[6],
 void orc_intersect_tets(const double tet_a[12], const double tet_b[12],
                         double *tets_c, int *n_tets_c);
 
+/* Mixed pairs: tri vs quad ([3][2] x [4][2] -> <= 46 tris [46][3][2]); tet
+ * vs hex in Gmsh order ([4][3] x [8][3] -> <= 729 tets); intervals. */
+void orc_intersect_tri_quad(const double tri_a[6], const double quad_b[8], double *tris_c, int *n_tris_c);
+void orc_intersect_tet_hex(const double tet_a[12], const double hex_b[24], double *tets_c, int *n_tets_c);
+double orc_interval_size(const double iv[2]);
+void orc_intersect_intervals(const double a[2], const double b[2], double *c, int *n);
+
 /* Tree (quadtree/octree) intersection finder.  A = query mesh (CSR rows),
  * B = tree mesh.  enlist is 0-based int32.  On success *indices is malloc'd
  * (free with orc_free) and indptr[nel_a+1] is filled.  Returns 0 on success. */
@@ -68,6 +80,12 @@ int orc_brute_force_finder(int dim, long nnodes_a, const double *pos_a,
                            long nnodes_b, const double *pos_b, long nel_b,
                            int loc_b, const int32_t *en_b, int64_t *indptr,
                            int32_t **indices, int64_t *nnz);
+/* 1D sort finder over 2-node elements; the first coordinate of each node is
+ * read with stride `stride_*`.  stable_leaf selects the stable sort instead
+ * of the reference's merge sort leaf step (see oracle.c). */
+int orc_sort_finder_1d(long nnodes_a, const double *pos_a, int stride_a, long nel_a, const int32_t *en_a,
+                       long nnodes_b, const double *pos_b, int stride_b, long nel_b, const int32_t *en_b,
+                       int stable_leaf, int64_t *indptr, int32_t **indices, int64_t *nnz);
 void orc_free(void *p);
 
 /* Narrow phase over a candidate CSR.  Per candidate pair p it writes the

@@ -19,7 +19,8 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 from libsupermesh_b200.meshes import read_mesh  # noqa: E402
 
-SMALL = ["triangle.1", "triangle.2", "tet", "square.1", "square.2", "cube.1", "cube.2"]
+SMALL = ["triangle.1", "triangle.2", "tet", "square.1", "square.2", "square.3", "square.4", "cube.1",
+         "cube.2", "cube.3", "cube.4", "line.1", "line.2"]
 ARCHIVES = {"2D_0_01.tar.bz2": ["triangle_0_01", "square_0_01"],
             "3D_0_05.tar.bz2": ["pyramid_0_05", "cube_0_05"]}
 

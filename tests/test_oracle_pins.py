@@ -119,3 +119,110 @@ def test_single_pair_cases(oracle_mod):
     T = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=float)
     out = oracle_mod.intersect_tets(T, T)
     assert abs(sum(oracle_mod.tetrahedron_volume(o) for o in out) - 1.0 / 6.0) < 1e-15
+
+
+# -- mixed element pairs and 1D entries --------------------------------------
+
+def _mixed_total(oracle, dim, A, B, swap=False):
+    """Sum of output measures over the strict-AABB candidates, clipping each
+    simplex of one mesh by the quad/hex of the other (Supermesh.F90:176-194
+    passes (simplex, box element) whichever side the simplex is on)."""
+    ip, ind = oracle.brute_force_finder(dim, A, B)
+    total = 0.0
+    for a in range(len(ip) - 1):
+        ea = A[0][A[1][a]]
+        for b in ind[ip[a]:ip[a + 1]]:
+            eb = B[0][B[1][b]]
+            s, q = (eb, ea) if swap else (ea, eb)
+            if dim == 2:
+                for t in oracle.intersect_tri_quad(s, q):
+                    total += oracle.triangle_area(t)
+            else:
+                for t in oracle.intersect_tet_hex(s, q):
+                    total += oracle.tetrahedron_volume(t)
+    return total
+
+
+def test_tri_quad_area_one(oracle_mod, ref_meshes):
+    # src/tests/test_element_intersector.F90:134-158: tri-quad, total 1
+    assert oracle_mod.fequals(_mixed_total(oracle_mod, 2, ref_meshes("square.1"), ref_meshes("square.4")), 1.0)
+
+
+def test_quad_tri_area_one(oracle_mod, ref_meshes):
+    # src/tests/test_element_intersector.F90:163-187: quad-tri, total 1
+    assert oracle_mod.fequals(
+        _mixed_total(oracle_mod, 2, ref_meshes("square.3"), ref_meshes("square.2"), swap=True), 1.0)
+
+
+def test_tet_hex_volume_half(oracle_mod, ref_meshes):
+    # src/tests/test_element_intersector.F90:250-274: tet-hex, total 0.5
+    assert oracle_mod.fequals(_mixed_total(oracle_mod, 3, ref_meshes("cube.1"), ref_meshes("cube.3")), 0.5)
+
+
+def test_hex_tet_volume_half(oracle_mod, ref_meshes):
+    # src/tests/test_element_intersector.F90:279-303: hex-tet, total 0.5
+    assert oracle_mod.fequals(
+        _mixed_total(oracle_mod, 3, ref_meshes("cube.3"), ref_meshes("cube.2"), swap=True), 0.5)
+
+
+def _interval_total(oracle, A, B, ip, ind):
+    total = 0.0
+    for a in range(len(ip) - 1):
+        for b in ind[ip[a]:ip[a + 1]]:
+            c = oracle.intersect_intervals(A[0][A[1][a], 0], B[0][B[1][b], 0])
+            if c.size:
+                total += oracle.interval_size(c)
+    return total
+
+
+@pytest.mark.parametrize("stable", [False, True])
+def test_intervals_size_one(oracle_mod, ref_meshes, stable):
+    # src/tests/test_interval_intersector.F90:84-99: total size 1 over the
+    # 1D finder's candidates (line.1 vs line.2)
+    A, B = ref_meshes("line.1"), ref_meshes("line.2")
+    ip, ind = oracle_mod.sort_finder_1d(A, B, stable=stable)
+    assert oracle_mod.fequals(_interval_total(oracle_mod, A, B, ip, ind), 1.0)
+
+
+@pytest.mark.parametrize("stable", [False, True])
+def test_sort_finder_completeness_1d(oracle_mod, ref_meshes, stable):
+    # src/tests/test_intersection_finder_completeness_1d.F90:94-121: map_ba
+    # from the sort finder; every B interval is covered by its candidates.
+    A, B = ref_meshes("line.1"), ref_meshes("line.2")
+    ip, ind = oracle_mod.sort_finder_1d(B, A, stable=stable)
+    for b in range(len(ip) - 1):
+        own = oracle_mod.interval_size(B[0][B[1][b], 0])
+        got = 0.0
+        for a in ind[ip[b]:ip[b + 1]]:
+            c = oracle_mod.intersect_intervals(A[0][A[1][a], 0], B[0][B[1][b], 0])
+            if c.size:
+                got += oracle_mod.interval_size(c)
+        assert oracle_mod.fequals(own, got), b
+
+
+def test_sort_finder_leaf_sort_on_shuffled_mesh(oracle_mod, ref_meshes):
+    # The reference's merge sort orders blocks of <= 4 elements with a
+    # selection loop (Intersection_Finder.F90:871-879) that is a permutation
+    # only for blocks already in order.  On a shuffled numbering the faithful
+    # restatement repeats and drops elements, so rows go missing; the stable
+    # sort used by the GPU library keeps the finder complete.
+    A, B = ref_meshes("line.1"), ref_meshes("line.2")
+    perm = np.random.default_rng(0).permutation(B[1].shape[0])
+    Bs = (B[0], B[1][perm])
+    faithful = oracle_mod.sort_finder_1d(Bs, A, stable=False)
+    stable = oracle_mod.sort_finder_1d(Bs, A, stable=True)
+    brute = [sorted(a for a in range(A[1].shape[0])
+                    if max(A[0][A[1][a], 0]) > min(Bs[0][Bs[1][b], 0])
+                    and min(A[0][A[1][a], 0]) < max(Bs[0][Bs[1][b], 0])) for b in range(Bs[1].shape[0])]
+    rows = lambda r: [sorted(r[1][r[0][b]:r[0][b + 1]]) for b in range(len(r[0]) - 1)]
+    assert rows(stable) == brute
+    assert rows(faithful) != brute
+
+
+def test_interval_basics(oracle_mod):
+    # Interval_Intersection.F90: |b - a|, open-overlap test, tolerance
+    # 10*min(spacing(|a|), spacing(|b|))
+    assert oracle_mod.interval_size([0.75, 0.25]) == 0.5
+    assert np.array_equal(oracle_mod.intersect_intervals([0.0, 1.0], [1.0, 0.5]), [0.5, 1.0])
+    assert oracle_mod.intersect_intervals([0.0, 1.0], [1.0, 2.0]).size == 0
+    assert oracle_mod.intersect_intervals([0.0, 1.0], [1.0 - 2.0 ** -50, 2.0]).size == 0
