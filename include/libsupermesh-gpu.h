@@ -72,8 +72,9 @@ int64_t libsupermesh_gpu_kernel_launches(void);
 /* Process-wide tuning options.  They change launch shapes and the 3D clipper
  * variant, never results (the autotuner in libsupermesh_b200/autotune.py
  * picks them per GPU and workload):
- *   "tet_clipper"        0 per-lane depth-first walk (default), 1 per-warp task queues
- *   "tet_blocks_per_sm"  3 (default) or 4 blocks of 128 threads per SM (3D clipper)
+ *   "tet_clipper"        0 per-lane depth-first walk over point indices (default),
+ *                        1 per-warp task queues, 2 per-lane walk over tets in registers
+ *   "tet_blocks_per_sm"  3 (default) or 4 blocks of 128 threads per SM (clipper 2)
  *   "tri_blocks_per_sm"  4, 8 (default) or 16 blocks of 128 threads per SM (2D clipper)
  *   "query_block"        64, 128 (default) or 256 threads per block (candidate search)
  * Unknown names or values return LSM_ERROR_INVALID_ARGUMENT. */

@@ -423,8 +423,8 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
   }
   bool queued = false;
   if (c->dim == 3 && lsm::tet_clipper_variant() == 1) {
-    unsigned char* scr = ensure<unsigned char>(c, c->wq_scratch, (int64_t)lsm::wq_scratch_bytes());
     int* err = bad_flag(c) + 16;
+    unsigned char* scr = ensure<unsigned char>(c, c->wq_scratch, (int64_t)lsm::wq_scratch_bytes());
     CU(lsm::launch_clip_tets_wq(nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                                 static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                                 static_cast<double*>(c->b_setup.p), pm, pn, ovf, work, scr, err, s, order));
@@ -929,7 +929,7 @@ int64_t libsupermesh_gpu_kernel_launches(void) { return (int64_t)lsm::launches()
 int libsupermesh_gpu_set_option(const char* name, int64_t value) {
   if (!name) return LSM_ERROR_INVALID_ARGUMENT;
   const std::string n(name);
-  if (n == "tet_clipper" && (value == 0 || value == 1)) {
+  if (n == "tet_clipper" && value >= 0 && value <= 2) {
     lsm::set_tet_clipper_variant((int)value);
   } else if (n == "tet_blocks_per_sm" && (value == 3 || value == 4)) {
     lsm::set_tet_blocks_per_sm((int)value);

@@ -53,19 +53,20 @@ namespace {
 int g_tet_variant = -1;
 }  // namespace
 
-// 3D clipper variant: 0 = per-lane depth-first walk (k_clip_tets, default),
-// 1 = per-warp task queues (k_clip_tets_wq).  LSM_TET_CLIPPER=lane|queue.
-// On B200 the task queues keep ~20 of 32 lanes busy (vs ~9) but wait on
-// their L2-resident queues at 8 warps per SM, which makes them slower.
+// 3D clipper variant: 0 = per-lane depth-first walk over point indices
+// (k_clip_tets_ix, default), 1 = per-warp task queues in L2
+// (k_clip_tets_wq), 2 = per-lane depth-first walk over tets held in
+// registers (k_clip_tets).  LSM_TET_CLIPPER=index|queue|register.
+// Measured on B200 (tet3d_27x32): 3.0 ms, 6.3 ms and 4.6 ms.
 int tet_clipper_variant() {
   if (g_tet_variant < 0) {
     const char* e = getenv("LSM_TET_CLIPPER");
-    g_tet_variant = (e && e[0] == 'q') ? 1 : 0;
+    g_tet_variant = (e && e[0] == 'q') ? 1 : (e && e[0] == 'r') ? 2 : 0;
   }
   return g_tet_variant;
 }
 
-void set_tet_clipper_variant(int v) { g_tet_variant = v ? 1 : 0; }
+void set_tet_clipper_variant(int v) { g_tet_variant = (v == 1 || v == 2) ? v : 0; }
 
 namespace {
 int g_tri_bps = 8;
@@ -1686,7 +1687,254 @@ __global__ void __launch_bounds__(kWqWarps * 32, kWqBlocksPerSm) k_clip_tets_wq(
   if (lane == 0) atomicMax(&work[2], (unsigned long long)maxC);
 }
 
+// ----------------------------------------------------------------------
+// K6d: depth-first tet clipper over point indices
+// ----------------------------------------------------------------------
+// As K6 (one pair per lane, depth-first, lane refill), but a tet is four
+// 5-bit indices into the lane's point pool in shared memory instead of twelve
+// doubles in registers.  Pool slots 0-3 hold A's vertices; the split at
+// plane L writes its (at most four) new points to slots 4+4L .. 7+4L.  In
+// depth-first order that is safe: a tet at plane L references only points of
+// planes < L, and when a sibling is taken from the stack every point written
+// by the previous sibling's subtree belongs to planes >= its own.  Child
+// assembly becomes integer work on index tuples, a pending tet is one word,
+// and vertices are fetched by index with shared-memory loads instead of
+// chains of selects.
+constexpr int kIxPoints = 20;  // 4 + 4 per plane
+constexpr int kIxStack = 6;    // pending tets: 2 per plane for planes 0-2
+
+__device__ __forceinline__ unsigned ix_pack(unsigned a, unsigned b, unsigned c, unsigned d) {
+  return a | b << 5 | c << 10 | d << 15;
+}
+
+__device__ __forceinline__ unsigned ix_vert(unsigned tet, int v) { return (tet >> (5 * v)) & 31u; }
+
+__device__ __forceinline__ unsigned ix_set(unsigned tet, int v, unsigned j) {
+  return (tet & ~(31u << (5 * v))) | j << (5 * v);
+}
+
+// A lane's point pool: point j, coordinate c at pool[(3j + c) * BLOCK]
+// (consecutive lanes hit consecutive banks).
+template <int BLOCK>
+struct IxPool {
+  double* pool;
+  __device__ __forceinline__ V3 get(unsigned j) const {
+    const double* q = pool + 3 * j * BLOCK;
+    return V3{q[0], q[BLOCK], q[2 * BLOCK]};
+  }
+  __device__ __forceinline__ void put(unsigned j, const V3& v) const {
+    double* q = pool + 3 * j * BLOCK;
+    q[0] = v.x;
+    q[BLOCK] = v.y;
+    q[2 * BLOCK] = v.z;
+  }
+};
+
+template <class Pool>
+__device__ __forceinline__ void ix_gather(const Pool& pool, unsigned tet, Tet& t) {
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const V3 q = pool.get(ix_vert(tet, v));
+    t.x[v] = q.x;
+    t.y[v] = q.y;
+    t.z[v] = q.z;
+  }
+}
+
+// Split of tet `cur` (coordinates t, classification k) at the plane whose new
+// points go to pool slots base .. base+3 (Tetrahedron_Intersection.F90:290-434,
+// same cases, interpolations and child order as split_tet).  Returns the
+// number of children; c0..c2 receive their index tuples.
+template <class Pool>
+__device__ __forceinline__ int ix_split(unsigned cur, const TetClass& k, const Pool& pool, unsigned base,
+                                        unsigned& c0, unsigned& c1, unsigned& c2) {
+  const int nn = k.nn, np = k.np;
+  const int n0 = k.negl & 3, n1 = (k.negl >> 2) & 3, n2 = (k.negl >> 4) & 3;
+  const int p0 = k.posl & 3, p1 = (k.posl >> 2) & 3, p2 = (k.posl >> 4) & 3;
+  int ni;
+  unsigned pairs;
+  if (nn == 1) {
+    ni = np;
+    pairs = (unsigned)(p0 | n0 << 2) | (unsigned)(p1 | n0 << 2) << 4 | (unsigned)(p2 | n0 << 2) << 8;
+  } else if (np == 2) {
+    ni = 4;
+    pairs = (unsigned)(p0 | n0 << 2) | (unsigned)(p1 | n0 << 2) << 4 | (unsigned)(p0 | n1 << 2) << 8 |
+            (unsigned)(p1 | n1 << 2) << 12;
+  } else {
+    ni = nn;
+    pairs = (unsigned)(p0 | n0 << 2) | (unsigned)(p0 | n1 << 2) << 4 | (unsigned)(p0 | n2 << 2) << 8;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (i < ni) {
+      const int P = (pairs >> (4 * i)) & 3, N = (pairs >> (4 * i + 2)) & 3;
+      const V3 T = interp(pool.get(ix_vert(cur, P)), pool.get(ix_vert(cur, N)),
+                          sel4(P, k.d[0], k.d[1], k.d[2], k.d[3]), sel4(N, k.d[0], k.d[1], k.d[2], k.d[3]));
+      pool.put(base + i, T);
+    }
+  }
+  if (nn == 1) {  // +++-, ++-0, +-00: the r-th positive vertex becomes new point r
+    unsigned c = cur;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      if (r < np) c = ix_set(c, (k.posl >> (2 * r)) & 3, base + r);
+    c0 = c;
+    return 1;
+  }
+  if (np == 2) {  // ++--
+    c0 = ix_set(ix_set(cur, p0, base + 2), p1, base + 1);
+    c1 = ix_pack(ix_vert(cur, n1), base + 3, base + 2, base + 1);
+    c2 = ix_pack(ix_vert(cur, n0), base + 0, base + 1, base + 2);
+    return 3;
+  }
+  c0 = ix_set(cur, p0, base);
+  if (nn == 3) {  // +---
+    c1 = ix_pack(base + 0, ix_vert(cur, n1), ix_vert(cur, n2), base + 1);
+    c2 = ix_pack(ix_vert(cur, n2), base + 1, base + 2, base + 0);
+    return 3;
+  }
+  // +--0
+  c1 = ix_pack(base + 1, ix_vert(cur, k.zerl & 3), ix_vert(cur, n1), base + 0);
+  return 2;
+}
+
+// Pairs reach the lanes through a two-step software pipeline so that the
+// dependent loads of a new pair (list entry -> element indices -> A
+// coordinates) never stall the warp: every lane prefetches its next pair one
+// stage per loop iteration while it clips the current one.  Pair numbers are
+// taken from a warp-private cursor over chunks of kIxChunk list entries
+// (one atomic per chunk).
+constexpr int kIxChunk = 64;
+
+__global__ void __launch_bounds__(kTetBlock, 3) k_clip_tets_ix(
+    const int32_t* __restrict__ list, const unsigned long long* __restrict__ nlist,
+    const int32_t* __restrict__ pa, const int32_t* __restrict__ pb, const double* __restrict__ coords_a,
+    const double* __restrict__ tol_a, const double* __restrict__ setup_b, double* pair_measure,
+    int32_t* pair_nout, unsigned long long* work) {
+  extern __shared__ double ix_mem[];
+  IxPool<kTetBlock> pool{ix_mem + threadIdx.x};
+  unsigned* stk = reinterpret_cast<unsigned*>(ix_mem + 3 * kIxPoints * kTetBlock) + threadIdx.x;
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t npairs = (int64_t)*nlist;
+  // warp cursor over the list (warp-uniform)
+  int64_t cbeg = 0, cend = 0;
+  bool exhausted = false;
+  // prefetch pipeline of the next pair: stage 0 idle, 1 list entry loading,
+  // 2 element data loading, 3 ready
+  int nstage = 0;
+  int np_ = 0, na = 0, nb = 0;
+  Tet nt;
+  double ntol = 0.0;
+  // current pair
+  int64_t p = -1;
+  const double* planes = setup_b;
+  unsigned cur = 0;
+  double tol = 0.0, m = 0.0;
+  int L = 0, sp = 0, kept = 0;
+  for (;;) {
+    // ---- prefetch pipeline
+    if (nstage == 2) {
+      load_tet(coords_a + (int64_t)na * 12, nt);
+      ntol = fmin(tol_a[na], setup_b[(int64_t)nb * kSetup3 + 16]);
+      nstage = 3;
+    } else if (nstage == 1) {
+      na = pa[np_];
+      nb = pb[np_];
+      nstage = 2;
+    }
+    if (p < 0 && nstage == 3) {
+      p = np_;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) pool.put(v, V3{nt.x[v], nt.y[v], nt.z[v]});
+      planes = setup_b + (int64_t)nb * kSetup3;
+      tol = ntol;
+      cur = ix_pack(0, 1, 2, 3);
+      m = 0.0;
+      L = 0;
+      sp = 0;
+      kept = 0;
+      nstage = 0;
+    }
+    {
+      const bool want = nstage == 0 && !exhausted;
+      unsigned wm = __ballot_sync(full, want);
+      while (wm) {
+        if (cbeg >= cend) {
+          unsigned long long base = 0;
+          if (lane == 0) base = atomicAdd(work, (unsigned long long)kIxChunk);
+          base = __shfl_sync(full, base, 0);
+          cbeg = (int64_t)base;
+          cend = cbeg + kIxChunk < npairs ? cbeg + kIxChunk : npairs;
+          if (cbeg >= npairs) {
+            exhausted = true;
+            break;
+          }
+        }
+        const int navail = (int)(cend - cbeg);
+        const int rank = __popc(wm & lt);
+        const bool take = want && ((wm >> lane) & 1u) && rank < navail;
+        if (take) {
+          np_ = list[cbeg + rank];
+          nstage = 1;
+        }
+        const unsigned tm = __ballot_sync(full, take);
+        cbeg += __popc(tm);
+        wm &= ~tm;
+      }
+    }
+    if (__all_sync(full, p < 0 && nstage == 0 && exhausted)) break;
+    if (p < 0) continue;
+    Tet t;
+    ix_gather(pool, cur, t);
+    double nx, ny, nz, c;
+    load_plane(planes, L, nx, ny, nz, c);
+    TetClass cls;
+    classify_tet(t, nx, ny, nz, c, cls);
+    int k = 0;
+    unsigned c0 = cur, c1 = 0, c2 = 0;
+    if (cls.nn > 0) k = cls.np == 0 ? 1 : ix_split(cur, cls, pool, 4 + 4 * L, c0, c1, c2);
+    if (L == 3) {
+      // final tets, in the reference's order
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        if (j < k) {
+          Tet o;
+          ix_gather(pool, j == 0 ? c0 : (j == 1 ? c1 : c2), o);
+          if (tet_volume_v4(o) >= tol) {
+            m = m + tet_volume_v1(o);
+            ++kept;
+          }
+        }
+      }
+      k = 0;
+    }
+    if (k > 0) {
+      const unsigned lv = (unsigned)(L + 1) << 20;
+      if (k == 3) stk[(sp++) * kTetBlock] = c2 | lv;
+      if (k >= 2) stk[(sp++) * kTetBlock] = c1 | lv;
+      cur = c0;
+      ++L;
+      continue;
+    }
+    if (sp > 0) {
+      const unsigned e = stk[(--sp) * kTetBlock];
+      cur = e & 0xfffffu;
+      L = (int)(e >> 20);
+      continue;
+    }
+    pair_measure[p] = m;
+    pair_nout[p] = kept;
+    p = -1;
+  }
+}
+
+size_t ix_smem_bytes() { return (size_t)kTetBlock * (3 * kIxPoints * sizeof(double) + kIxStack * sizeof(unsigned)); }
+
 int wq_grid_blocks() { return sm_count() * kWqBlocksPerSm; }
+
+
 
 // Deterministic per-block partials of the pair measures: block b reduces the
 // contiguous range [b*chunk, (b+1)*chunk) in a fixed thread order.
@@ -1728,7 +1976,10 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     count_launch();
     k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, setup_b,
                                                               pair_measure, pair_nout, overflow_list, work);
-    if (tet_blocks_per_sm() == 3)
+    if (tet_clipper_variant() == 0)
+      k_clip_tets_ix<<<sm_count() * 3, kTetBlock, ix_smem_bytes(), s>>>(
+          overflow_list, work, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure, pair_nout, work + 1);
+    else if (tet_blocks_per_sm() == 3)
       k_clip_tets<3><<<sm_count() * 3, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,
                                                               setup_b, pair_measure, pair_nout, work + 1);
     else
@@ -1767,8 +2018,12 @@ cudaError_t init_device_attributes() {
   const int smem = (int)(sizeof(double) * (kTetSmemSlots * 12 + 16) * kTetBlock);
   cudaError_t e = cudaFuncSetAttribute(k_clip_tets<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_clip_tets<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  e = cudaFuncSetAttribute(k_clip_tets<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_clip_tets_ix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
 }
+
+
 
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
                                   const int32_t* pair_a, const int32_t* pair_b,

@@ -33,7 +33,8 @@ unsigned long long launches();
 // Launch shape of the persistent tet clipper (3 or 4 blocks per SM).
 int tet_blocks_per_sm();
 void set_tet_blocks_per_sm(int v);
-// 3D clipper variant: 0 per-lane depth-first, 1 per-warp task queues.
+// 3D clipper variant: 0 per-lane depth-first over point indices (default),
+// 1 per-warp task queues in L2, 2 per-lane depth-first over tets in registers.
 int tet_clipper_variant();
 void set_tet_clipper_variant(int v);
 // Grid of the 2D clipper (blocks per SM) and block size of the search.
@@ -106,6 +107,7 @@ cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overf
 // wq_scratch_bytes(); work: 3 counters; err != 0 after the launch means the
 // queues overflowed (results invalid: re-run with launch_clip).
 size_t wq_scratch_bytes();
+
 cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                                 const double* coords_a, const double* tol_a, const double* setup_b,
                                 double* pair_measure, int32_t* pair_nout, int32_t* survivors,

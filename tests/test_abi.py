@@ -91,11 +91,11 @@ def test_tuning_options_host_side(lib):
     invalid names/values are rejected (no GPU needed)."""
     import libsupermesh_b200 as L
 
-    for name, vals in {"tet_clipper": (1, 0), "tet_blocks_per_sm": (4, 3), "tri_blocks_per_sm": (16, 8),
+    for name, vals in {"tet_clipper": (1, 2, 0), "tet_blocks_per_sm": (4, 3), "tri_blocks_per_sm": (16, 8),
                        "query_block": (256, 128)}.items():
         for v in vals:
             L.set_option(name, v)
             assert L.get_option(name) == v
-    for bad in (("tet_clipper", 2), ("query_block", 100), ("nonsense", 1)):
+    for bad in (("tet_clipper", 3), ("query_block", 100), ("nonsense", 1)):
         with pytest.raises(L.LsmError):
             L.set_option(*bad)

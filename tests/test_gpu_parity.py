@@ -100,8 +100,10 @@ def test_config_tri2d_777x1024_rot7_p1_mass(gpu_ctx, oracle_mod):
     assert abs(integral - i_o) <= 1e-12 * abs(i_o)
 
 
-def test_task_queue_clipper_matches(oracle_mod, tmp_path):
-    """The alternative task-queue tet clipper gives the same per-pair results."""
+@pytest.mark.parametrize("variant", ["queue", "register"])
+def test_alternative_tet_clippers_match(oracle_mod, tmp_path, variant):
+    """The alternative tet clippers (task queues; tets held in registers)
+    give the same per-pair results, bit for bit."""
     import subprocess
     import sys
 
@@ -113,7 +115,7 @@ def test_task_queue_clipper_matches(oracle_mod, tmp_path):
         "ip, ind = c.get_candidates(len(A[1]), st.n_candidates)\n"
         "np.savez(%r, pm=pm, pn=pn, ip=ip, ind=ind, tot=st.total_measure)\n" % (str(ROOT), str(tmp_path / "q.npz")))
     import os
-    env = dict(os.environ, LSM_TET_CLIPPER="queue")
+    env = dict(os.environ, LSM_TET_CLIPPER=variant)
     subprocess.run([sys.executable, "-c", code], check=True, env=env, timeout=600)
     q = np.load(tmp_path / "q.npz")
     dim, A, B = M.config_meshes("small3d_12x14")
@@ -122,7 +124,7 @@ def test_task_queue_clipper_matches(oracle_mod, tmp_path):
     ro, bo, mo, no = pair_table(ip_o, ind_o, pm_o, pn_o)
     rg, bg, mg, ng = pair_table(q["ip"], q["ind"], q["pm"], q["pn"])
     assert np.array_equal(bo, bg) and np.array_equal(no, ng)
-    assert np.array_equal(mo, mg)  # rank-ordered sums: bit-identical
+    assert np.array_equal(mo, mg)  # sums in the reference's order: bit-identical
     assert abs(float(q["tot"]) - st_o.total) <= REL_TOL
 
 
@@ -134,7 +136,7 @@ def test_autotuner_keeps_results(gpu_ctx, tmp_path, monkeypatch):
         dim, A, B = M.config_meshes(name)
         ref, em_ref = gpu_ctx.supermesh(A, B, elem_measure=True)
         res = autotune.tune(gpu_ctx, A, B, reps=1)
-        assert res["tried"] == (9 if dim == 2 else 12)
+        assert res["tried"] == 9
         st, em = gpu_ctx.supermesh(A, B, elem_measure=True)
         assert st.as_dict() == ref.as_dict() and np.array_equal(em, em_ref)
         assert autotune.apply_cached(dim, len(A[1]), len(B[1])) == res["setting"]
