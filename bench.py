@@ -418,10 +418,21 @@ def run_ours(args, world, rank, local):
     e2e = whole_job_rate(n_cand, args.steps, world, ms_e2e)
     assert st_e2e.n_candidates == n_cand and st_e2e.total_measure == st.total_measure
 
-    # dominant kernel alone: the clipping launch over the same candidates
+    # dominant kernel alone: the clip kernel over the same candidates, timed
+    # by the library with CUDA events on its stream around that launch
     step_device()
-    ms_clip, _ = timed(lambda: ctx.clip_candidates(stream=sp), args.steps, 3)
-    clip_ms = ms_clip / args.steps
+    lsm.set_option("time_kernels", 1)
+    for _ in range(3):
+        ctx.clip_candidates(stream=sp)
+    kernel_ms = []
+    for _ in range(args.steps):
+        flush()
+        ctx.clip_candidates(stream=sp)
+        kernel_ms.append(ctx.clip_kernel_ms())
+    lsm.set_option("time_kernels", 0)
+    clip_ms = all_max(sum(kernel_ms), world) / args.steps
+    clip_kernel = ({0: "k_clip_tets_ix", 1: "k_clip_tets_wq", 2: "k_clip_tets"}[lsm.get_option("tet_clipper")]
+                   if dim == 3 else "k_clip_tris")
 
     line = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
@@ -456,10 +467,10 @@ def run_ours(args, world, rank, local):
         achieved = flops / (clip_ms * 1e-3) / 1e12 if flops else None
         peak = peak_rate / 1e12 if peak_rate > 0 else None
         line["roofline"] = {
-            "kernel": "k_clip_tets" if dim == 3 else "k_clip_tris",
+            "kernel": clip_kernel,
             "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": (achieved / peak) if (achieved and peak) else None,
-            "traffic": profile_traffic("k_clip_tets" if dim == 3 else "k_clip_tris", args.workload),
+            "traffic": profile_traffic(clip_kernel, args.workload),
             "launch_ms": clip_ms,
             "flops_per_launch": flops,
             "peak_source": "measured in-run: DADD+DMUL issue rate, 1 op each (the clipper is FMA-free); "

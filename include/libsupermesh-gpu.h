@@ -77,9 +77,16 @@ int64_t libsupermesh_gpu_kernel_launches(void);
  *   "tet_blocks_per_sm"  3 (default) or 4 blocks of 128 threads per SM (clipper 2)
  *   "tri_blocks_per_sm"  4, 8 (default) or 16 blocks of 128 threads per SM (2D clipper)
  *   "query_block"        64, 128 (default) or 256 threads per block (candidate search)
+ *   "time_kernels"       1: record CUDA events around the clip kernel of every
+ *                        narrow phase (read with libsupermesh_gpu_clip_kernel_ms); 0 (default)
  * Unknown names or values return LSM_ERROR_INVALID_ARGUMENT. */
 int libsupermesh_gpu_set_option(const char *name, int64_t value);
 int libsupermesh_gpu_get_option(const char *name, int64_t *value);
+
+/* Device time (ms) of the clip kernel of the last narrow phase on ctx, from
+ * CUDA events recorded on its stream (needs option time_kernels = 1 during
+ * that phase; waits for the kernel to finish). */
+int libsupermesh_gpu_clip_kernel_ms(lsm_gpu_context *ctx, double *ms);
 
 /* Candidate search only (tree finder): the work of
  * tree_intersection_finder_set_input_c (C_bindings.F90:346-366) on the GPU.

@@ -98,6 +98,8 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_context_bytes.argtypes = [vp]
     L.libsupermesh_gpu_kernel_launches.restype = ctypes.c_int64
     L.libsupermesh_gpu_kernel_launches.argtypes = []
+    L.libsupermesh_gpu_clip_kernel_ms.argtypes = [vp, _dp]
+    L.libsupermesh_gpu_clip_kernel_ms.restype = ctypes.c_int
     L.libsupermesh_gpu_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
     L.libsupermesh_gpu_set_option.restype = ctypes.c_int
     L.libsupermesh_gpu_get_option.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
@@ -235,6 +237,13 @@ class Context:
         self._check(self.lib.libsupermesh_gpu_clip_candidates_ordered(self._h, _ptr(order), int(on_device),
                                                                       ctypes.byref(st), stream))
         return st
+
+    def clip_kernel_ms(self) -> float:
+        """Device time of the last narrow phase's clip kernel (option
+        time_kernels must have been on)."""
+        r = ctypes.c_double(0.0)
+        self._check(self.lib.libsupermesh_gpu_clip_kernel_ms(self._h, ctypes.byref(r)))
+        return r.value
 
     def pair_results(self, n: int):
         m = np.zeros(max(n, 1), dtype=np.float64)

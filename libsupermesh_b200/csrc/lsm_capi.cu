@@ -26,6 +26,10 @@
 
 namespace {
 
+// Option time_kernels: record events around the clip kernel of every narrow
+// phase (libsupermesh_gpu_clip_kernel_ms reads them).
+bool g_time_kernels = false;
+
 // ------------------------------------------------------------------ buffers
 struct DevBuf {
   void* p = nullptr;
@@ -58,6 +62,9 @@ struct Ctx {
   size_t host_stage_cap = 0;
   // pinned host scalars
   void* host_scalars = nullptr;
+  // events around the clip kernel of the last narrow phase (option time_kernels)
+  cudaEvent_t clip_ev[2] = {nullptr, nullptr};
+  bool clip_timed = false;
 
   // state of the last candidate search
   int dim = 0;
@@ -158,7 +165,8 @@ int init_ctx(int device, Ctx* c) {
   DeviceGuard g(device);
   c->device = device;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMallocHost(&c->host_scalars, 4096) != cudaSuccess || lsm::init_device_attributes() != cudaSuccess) {
+      cudaMallocHost(&c->host_scalars, 4096) != cudaSuccess || lsm::init_device_attributes() != cudaSuccess ||
+      cudaEventCreate(&c->clip_ev[0]) != cudaSuccess || cudaEventCreate(&c->clip_ev[1]) != cudaSuccess) {
     (void)cudaGetLastError();
     return LSM_ERROR_CUDA;
   }
@@ -176,8 +184,15 @@ void fini_ctx(Ctx* c) {
                    &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->wq_scratch, &c->x_a, &c->x_b, &c->x_measure,
                    &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
-                   &c->bt_ncand, &c->bt_stage_pa, &c->bt_stage_ea, &c->bt_stage_pb, &c->bt_stage_eb};
+                   &c->bt_ncand, &c->bt_stage_pa, &c->bt_stage_ea, &c->bt_stage_pb, &c->bt_stage_eb,
+                   &c->d1_keyhi, &c->d1_perm_a, &c->d1_perm_b, &c->d1_lo_a, &c->d1_hi_a, &c->d1_lo_b,
+                   &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js};
   for (DevBuf* b : all) free_buf(*b);
+  for (cudaEvent_t& e : c->clip_ev)
+    if (e) {
+      cudaEventDestroy(e);
+      e = nullptr;
+    }
   if (c->host_scalars) cudaFreeHost(c->host_scalars);
   if (c->host_stage) cudaFreeHost(c->host_stage);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -440,7 +455,9 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
   if (!queued)
     CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                         static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
-                        static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order));
+                        static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order,
+                        g_time_kernels ? c->clip_ev[0] : nullptr, g_time_kernels ? c->clip_ev[1] : nullptr));
+  c->clip_timed = !queued && g_time_kernels;
   if (c->dim == 2)
     CU(lsm::launch_clip_tris_wide(ovf, ovf_count, nnz, static_cast<int32_t*>(c->pair_a.p),
                                   static_cast<int32_t*>(c->pair_b.p), static_cast<double*>(c->a_coords.p),
@@ -937,6 +954,8 @@ int libsupermesh_gpu_set_option(const char* name, int64_t value) {
     lsm::set_tri_blocks_per_sm((int)value);
   } else if (n == "query_block" && (value == 64 || value == 128 || value == 256)) {
     lsm::set_query_block((int)value);
+  } else if (n == "time_kernels" && (value == 0 || value == 1)) {
+    g_time_kernels = value == 1;
   } else {
     return LSM_ERROR_INVALID_ARGUMENT;
   }
@@ -954,9 +973,26 @@ int libsupermesh_gpu_get_option(const char* name, int64_t* value) {
     *value = lsm::tri_blocks_per_sm();
   else if (n == "query_block")
     *value = lsm::query_block();
+  else if (n == "time_kernels")
+    *value = g_time_kernels ? 1 : 0;
   else
     return LSM_ERROR_INVALID_ARGUMENT;
   return LSM_SUCCESS;
+}
+
+int libsupermesh_gpu_clip_kernel_ms(lsm_gpu_context* ctx, double* ms) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(ms != nullptr, "NULL output");
+    if (!c->clip_timed) {
+      set_error(c, "the last narrow phase ran without the time_kernels option");
+      throw Fail{LSM_ERROR_STATE};
+    }
+    CU(cudaEventSynchronize(c->clip_ev[1]));
+    float f = 0.0f;
+    CU(cudaEventElapsedTime(&f, c->clip_ev[0], c->clip_ev[1]));
+    *ms = (double)f;
+  });
 }
 
 int libsupermesh_gpu_find_candidates(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b,

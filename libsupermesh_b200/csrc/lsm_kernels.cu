@@ -1963,10 +1963,11 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         const double* coords_a, const double* tol_a, const double* setup_b,
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
-                        const int32_t* order) {
+                        const int32_t* order, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
   const int g = clip_grid_blocks(dim);
   count_launch();
   if (dim == 2) {
+    if (ev_begin) cudaEventRecord(ev_begin, s);
     k_clip_tris<<<g, kTriBlock, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure,
                                         pair_nout, overflow_list, overflow_count, order);
   } else {
@@ -1976,6 +1977,7 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     count_launch();
     k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, setup_b,
                                                               pair_measure, pair_nout, overflow_list, work);
+    if (ev_begin) cudaEventRecord(ev_begin, s);
     if (tet_clipper_variant() == 0)
       k_clip_tets_ix<<<sm_count() * 3, kTetBlock, ix_smem_bytes(), s>>>(
           overflow_list, work, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure, pair_nout, work + 1);
@@ -1986,6 +1988,7 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
       k_clip_tets<4><<<sm_count() * 4, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,
                                                               setup_b, pair_measure, pair_nout, work + 1);
   }
+  if (ev_end) cudaEventRecord(ev_end, s);
   return cudaGetLastError();
 }
 

@@ -95,7 +95,8 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         const double* coords_a, const double* tol_a, const double* setup_b,
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
-                        const int32_t* order = nullptr);
+                        const int32_t* order = nullptr, cudaEvent_t ev_begin = nullptr,
+                        cudaEvent_t ev_end = nullptr);
 // Opt-in shared-memory limits for the clip kernels on the current device.
 cudaError_t init_device_attributes();
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
