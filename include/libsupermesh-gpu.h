@@ -190,7 +190,7 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context *ctx, int npairs,
  * looks up its address (make that first call before any stream capture).
  * All calls share the array, so calls that overlap on the GPU race. */
 #define LSM_NOALLOC_MAX_PAIRS 32768
-#define LSM_NOALLOC_SCRATCH_BYTES 5800448
+#define LSM_NOALLOC_SCRATCH_BYTES 6193664
 int libsupermesh_gpu_intersect_tets_noalloc(int64_t n, const double *tet_a, const double *tet_b,
                                             double *measure, int32_t *n_out, double *total,
                                             void *stream);

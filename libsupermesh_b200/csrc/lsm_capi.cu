@@ -423,7 +423,8 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
   lsm::Partial* tot = ensure<lsm::Partial>(c, c->totals, 1);
   // 2D: overflow list of the fast-path clipper; 3D: list of pairs that
   // survive the exact early-out.
-  int32_t* ovf = ensure<int32_t>(c, c->ovf_list, nnz);
+  // (the default 3D clipper takes {pair, a, b, 0} records: 4 ints per pair)
+  int32_t* ovf = ensure<int32_t>(c, c->ovf_list, c->dim == 3 ? 4 * nnz : nnz);
   int* ovf_count = bad_flag(c) + 2;
   if (c->dim == 2) CU(cudaMemsetAsync(ovf_count, 0, sizeof(int), s));
   unsigned long long* work = reinterpret_cast<unsigned long long*>(bad_flag(c) + 8);

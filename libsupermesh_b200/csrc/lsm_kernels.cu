@@ -1237,6 +1237,9 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 // for the clipper.
 // `order` (optional) lists the pairs in the order the clipper should take
 // them (a schedule); survivors are appended in that order, warp by warp.
+// RECORDS: survivors are written as {pair, a, b, 0} so that the clipper gets
+// the element numbers with the pair number in one load.
+template <bool RECORDS>
 __global__ void __launch_bounds__(256) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ order,
                                                         const int32_t* __restrict__ pa,
                                                         const int32_t* __restrict__ pb,
@@ -1250,9 +1253,11 @@ __global__ void __launch_bounds__(256) k_prefilter_tets(int64_t npairs, const in
     const int64_t j = base + threadIdx.x;
     bool live = false;
     int64_t i = j;
+    int a = 0, b = 0;
     if (j < npairs) {
       if (order) i = order[j];
-      const int a = pa[i], b = pb[i];
+      a = pa[i];
+      b = pb[i];
       Tet t;
       load_tet(coords_a + (int64_t)a * 12, t);
       const double* pl = setup_b + (int64_t)b * kSetup3;
@@ -1283,7 +1288,13 @@ __global__ void __launch_bounds__(256) k_prefilter_tets(int64_t npairs, const in
       unsigned long long off = 0;
       if (lane == leader) off = atomicAdd(nsurv, (unsigned long long)__popc(mask));
       off = __shfl_sync(0xffffffffu, off, leader);
-      if (live) survivors[off + __popc(mask & lt)] = (int32_t)i;
+      if (live) {
+        const int64_t o = (int64_t)off + __popc(mask & lt);
+        if (RECORDS)
+          reinterpret_cast<int4*>(survivors)[o] = make_int4((int)i, a, b, 0);
+        else
+          survivors[o] = (int32_t)i;
+      }
     }
   }
 }
@@ -1702,6 +1713,16 @@ __global__ void __launch_bounds__(kWqWarps * 32, kWqBlocksPerSm) k_clip_tets_wq(
 // chains of selects.
 constexpr int kIxPoints = 20;  // 4 + 4 per plane
 constexpr int kIxStack = 6;    // pending tets: 2 per plane for planes 0-2
+#ifndef LSM_IX_BLOCK
+#define LSM_IX_BLOCK 224
+#endif
+#ifndef LSM_IX_BPS
+#define LSM_IX_BPS 2
+#endif
+// 504 B of shared memory per lane: 2 blocks of 224 threads (14 warps) fill
+// the 228 KB of an SM.
+constexpr int kIxBlock = LSM_IX_BLOCK;
+constexpr int kIxBlocksPerSm = LSM_IX_BPS;
 
 __device__ __forceinline__ unsigned ix_pack(unsigned a, unsigned b, unsigned c, unsigned d) {
   return a | b << 5 | c << 10 | d << 15;
@@ -1798,22 +1819,21 @@ __device__ __forceinline__ int ix_split(unsigned cur, const TetClass& k, const P
   return 2;
 }
 
-// Pairs reach the lanes through a two-step software pipeline so that the
-// dependent loads of a new pair (list entry -> element indices -> A
-// coordinates) never stall the warp: every lane prefetches its next pair one
-// stage per loop iteration while it clips the current one.  Pair numbers are
-// taken from a warp-private cursor over chunks of kIxChunk list entries
-// (one atomic per chunk).
+// Pairs reach the lanes through a software pipeline so that the dependent
+// loads of a new pair (survivor record {pair, a, b} -> A coordinates and
+// tolerances) never stall the warp: every lane prefetches its next pair one
+// stage per loop iteration while it clips the current one.  Records are
+// taken from a warp-private cursor over chunks of kIxChunk list entries (one
+// atomic per chunk).
 constexpr int kIxChunk = 64;
 
-__global__ void __launch_bounds__(kTetBlock, 3) k_clip_tets_ix(
-    const int32_t* __restrict__ list, const unsigned long long* __restrict__ nlist,
-    const int32_t* __restrict__ pa, const int32_t* __restrict__ pb, const double* __restrict__ coords_a,
+__global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
+    const int4* __restrict__ list, const unsigned long long* __restrict__ nlist, const double* __restrict__ coords_a,
     const double* __restrict__ tol_a, const double* __restrict__ setup_b, double* pair_measure,
     int32_t* pair_nout, unsigned long long* work) {
   extern __shared__ double ix_mem[];
-  IxPool<kTetBlock> pool{ix_mem + threadIdx.x};
-  unsigned* stk = reinterpret_cast<unsigned*>(ix_mem + 3 * kIxPoints * kTetBlock) + threadIdx.x;
+  IxPool<kIxBlock> pool{ix_mem + threadIdx.x};
+  unsigned* stk = reinterpret_cast<unsigned*>(ix_mem + 3 * kIxPoints * kIxBlock) + threadIdx.x;
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -1821,10 +1841,10 @@ __global__ void __launch_bounds__(kTetBlock, 3) k_clip_tets_ix(
   // warp cursor over the list (warp-uniform)
   int64_t cbeg = 0, cend = 0;
   bool exhausted = false;
-  // prefetch pipeline of the next pair: stage 0 idle, 1 list entry loading,
-  // 2 element data loading, 3 ready
+  // prefetch pipeline of the next pair: stage 0 idle, 1 record loading,
+  // 2 element data loading (ready for the next refill)
   int nstage = 0;
-  int np_ = 0, na = 0, nb = 0;
+  int4 nrec = make_int4(0, 0, 0, 0);
   Tet nt;
   double ntol = 0.0;
   // current pair
@@ -1835,20 +1855,16 @@ __global__ void __launch_bounds__(kTetBlock, 3) k_clip_tets_ix(
   int L = 0, sp = 0, kept = 0;
   for (;;) {
     // ---- prefetch pipeline
-    if (nstage == 2) {
-      load_tet(coords_a + (int64_t)na * 12, nt);
-      ntol = fmin(tol_a[na], setup_b[(int64_t)nb * kSetup3 + 16]);
-      nstage = 3;
-    } else if (nstage == 1) {
-      na = pa[np_];
-      nb = pb[np_];
+    if (nstage == 1) {
+      load_tet(coords_a + (int64_t)nrec.y * 12, nt);
+      ntol = fmin(tol_a[nrec.y], setup_b[(int64_t)nrec.z * kSetup3 + 16]);
       nstage = 2;
     }
-    if (p < 0 && nstage == 3) {
-      p = np_;
+    if (p < 0 && nstage == 2) {
+      p = nrec.x;
 #pragma unroll
       for (int v = 0; v < 4; ++v) pool.put(v, V3{nt.x[v], nt.y[v], nt.z[v]});
-      planes = setup_b + (int64_t)nb * kSetup3;
+      planes = setup_b + (int64_t)nrec.z * kSetup3;
       tol = ntol;
       cur = ix_pack(0, 1, 2, 3);
       m = 0.0;
@@ -1876,7 +1892,7 @@ __global__ void __launch_bounds__(kTetBlock, 3) k_clip_tets_ix(
         const int rank = __popc(wm & lt);
         const bool take = want && ((wm >> lane) & 1u) && rank < navail;
         if (take) {
-          np_ = list[cbeg + rank];
+          nrec = list[cbeg + rank];
           nstage = 1;
         }
         const unsigned tm = __ballot_sync(full, take);
@@ -1912,14 +1928,14 @@ __global__ void __launch_bounds__(kTetBlock, 3) k_clip_tets_ix(
     }
     if (k > 0) {
       const unsigned lv = (unsigned)(L + 1) << 20;
-      if (k == 3) stk[(sp++) * kTetBlock] = c2 | lv;
-      if (k >= 2) stk[(sp++) * kTetBlock] = c1 | lv;
+      if (k == 3) stk[(sp++) * kIxBlock] = c2 | lv;
+      if (k >= 2) stk[(sp++) * kIxBlock] = c1 | lv;
       cur = c0;
       ++L;
       continue;
     }
     if (sp > 0) {
-      const unsigned e = stk[(--sp) * kTetBlock];
+      const unsigned e = stk[(--sp) * kIxBlock];
       cur = e & 0xfffffu;
       L = (int)(e >> 20);
       continue;
@@ -1930,7 +1946,7 @@ __global__ void __launch_bounds__(kTetBlock, 3) k_clip_tets_ix(
   }
 }
 
-size_t ix_smem_bytes() { return (size_t)kTetBlock * (3 * kIxPoints * sizeof(double) + kIxStack * sizeof(unsigned)); }
+size_t ix_smem_bytes() { return (size_t)kIxBlock * (3 * kIxPoints * sizeof(double) + kIxStack * sizeof(unsigned)); }
 
 int wq_grid_blocks() { return sm_count() * kWqBlocksPerSm; }
 
@@ -1975,12 +1991,17 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     const size_t smem = sizeof(double) * (kTetSmemSlots * 12 + 16) * kTetBlock;
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
     count_launch();
-    k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, setup_b,
-                                                              pair_measure, pair_nout, overflow_list, work);
+    if (tet_clipper_variant() == 0)
+      k_prefilter_tets<true><<<grid_for(npairs, 256, 8), 256, 0, s>>>(
+          npairs, order, pair_a, pair_b, coords_a, setup_b, pair_measure, pair_nout, overflow_list, work);
+    else
+      k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(
+          npairs, order, pair_a, pair_b, coords_a, setup_b, pair_measure, pair_nout, overflow_list, work);
     if (ev_begin) cudaEventRecord(ev_begin, s);
     if (tet_clipper_variant() == 0)
-      k_clip_tets_ix<<<sm_count() * 3, kTetBlock, ix_smem_bytes(), s>>>(
-          overflow_list, work, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure, pair_nout, work + 1);
+      k_clip_tets_ix<<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
+          reinterpret_cast<const int4*>(overflow_list), work, coords_a, tol_a, setup_b, pair_measure, pair_nout,
+          work + 1);
     else if (tet_blocks_per_sm() == 3)
       k_clip_tets<3><<<sm_count() * 3, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,
                                                               setup_b, pair_measure, pair_nout, work + 1);
@@ -2001,8 +2022,9 @@ cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int
   cudaMemsetAsync(work, 0, 3 * sizeof(unsigned long long), s);
   cudaMemsetAsync(err, 0, sizeof(int), s);
   count_launch(2);
-  k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, setup_b,
-                                                            pair_measure, pair_nout, survivors, work);
+  k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
+                                                                   setup_b, pair_measure, pair_nout, survivors,
+                                                                   work);
   k_clip_tets_wq<<<wq_grid_blocks(), kWqWarps * 32, 0, s>>>(survivors, work, pair_a, pair_b, coords_a, tol_a,
                                                             setup_b, pair_measure, pair_nout, work, scratch, err);
   return cudaGetLastError();

@@ -32,8 +32,8 @@ constexpr size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign;
 constexpr size_t kOffSetup = 0;                                                      // [n][kSetup3] f64
 constexpr size_t kOffTol = align_up(kOffSetup + sizeof(double) * lsm::kSetup3 * kMaxPairs);  // [n] f64
 constexpr size_t kOffIota = align_up(kOffTol + sizeof(double) * kMaxPairs);              // [n] i32
-constexpr size_t kOffList = align_up(kOffIota + sizeof(int32_t) * kMaxPairs);            // [n] i32
-constexpr size_t kOffWork = align_up(kOffList + sizeof(int32_t) * kMaxPairs);            // misc counters
+constexpr size_t kOffList = align_up(kOffIota + sizeof(int32_t) * kMaxPairs);            // [n] survivor records
+constexpr size_t kOffWork = align_up(kOffList + 4 * sizeof(int32_t) * kMaxPairs);        // misc counters
 constexpr size_t kWorkBytes = 256;
 constexpr size_t kOffPartials = align_up(kOffWork + kWorkBytes);                         // reduction partials
 constexpr size_t kOffTotal = align_up(kOffPartials + sizeof(lsm::Partial) * 1024);
