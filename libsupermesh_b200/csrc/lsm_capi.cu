@@ -11,6 +11,7 @@
 // candidate count, needed to size the pair arrays.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
@@ -49,7 +50,7 @@ struct Ctx {
   // tree
   DevBuf keys, vals, keys_tmp, vals_tmp, hist, root_partial, rootbox, bvh_lo, bvh_hi, bvh_work;
   // candidates
-  DevBuf counts, offsets, scan_tmp, pair_a, pair_b, i64_tmp;
+  DevBuf counts, offsets, scan_tmp, pair_a, pair_b, i64_tmp, q_cache, q_over;
   // narrow phase
   DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals, wq_scratch;
   // explicit pairs / p1 / batched
@@ -186,7 +187,7 @@ void fini_ctx(Ctx* c) {
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
                    &c->bt_ncand, &c->bt_stage_pa, &c->bt_stage_ea, &c->bt_stage_pb, &c->bt_stage_eb,
                    &c->d1_keyhi, &c->d1_perm_a, &c->d1_perm_b, &c->d1_lo_a, &c->d1_hi_a, &c->d1_lo_b,
-                   &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js};
+                   &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over};
   for (DevBuf* b : all) free_buf(*b);
   for (cudaEvent_t& e : c->clip_ev)
     if (e) {
@@ -383,10 +384,17 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   int* counts = ensure<int>(c, c->counts, nel_a);
   int64_t* stmp = ensure<int64_t>(c, c->scan_tmp, lsm::scan_tmp_entries(nel_a) + 1);
   lsm::BVH bvh{};
+  // candidate cache of the count pass: up to kCacheBytes, at most 256 per row
+  constexpr int64_t kCacheBytes = 256ll << 20;
+  const int cap = nel_a > 0 ? (int)std::min<int64_t>(256, kCacheBytes / (4 * nel_a)) : 0;
+  int32_t* cache = cap >= 8 ? ensure<int32_t>(c, c->q_cache, nel_a * cap) : nullptr;
+  int* over = cache ? ensure<int>(c, c->q_over, nel_a + 1) : nullptr;
   if (b.nel > 0 && nel_a > 0) {
     bvh = build_tree(c, b, s);
+    if (over) CU(cudaMemsetAsync(over, 0, sizeof(int), s));
     CU(lsm::launch_query(a.dim, false, nel_a, static_cast<double*>(c->a_box64.p), bvh,
-                         static_cast<double*>(c->b_box64.p), counts, nullptr, nullptr, nullptr, s));
+                         static_cast<double*>(c->b_box64.p), counts, nullptr, nullptr, nullptr, s, cache, cap,
+                         over));
   } else if (nel_a > 0) {
     CU(cudaMemsetAsync(counts, 0, sizeof(int) * nel_a, s));
   }
@@ -402,7 +410,7 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);
   if (nnz > 0)
     CU(lsm::launch_query(a.dim, true, nel_a, static_cast<double*>(c->a_box64.p), bvh,
-                         static_cast<double*>(c->b_box64.p), nullptr, offsets, pa, pb, s));
+                         static_cast<double*>(c->b_box64.p), counts, offsets, pa, pb, s, cache, cap, over));
   c->dim = a.dim;
   c->loc_a = a.loc;
   c->loc_b = b.loc;

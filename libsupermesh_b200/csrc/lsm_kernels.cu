@@ -775,15 +775,23 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
 // ======================================================================
 // K4: candidate search
 // ======================================================================
+// The count pass (FILL = false) also keeps the first `cap` candidates of
+// every row in cache[a * cap ..] (when cache is given) and lists rows with
+// more than cap candidates in over_rows; the fill then copies cached rows
+// (k_fill_from_cache) and traverses again only for the listed rows
+// (FILL = true with `rows`).
 template <int DIM, bool FILL>
 __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __restrict__ box64_a,
                                                const float4* __restrict__ lo_left,
                                                const float4* __restrict__ hi_esc, int n,
                                                const double* __restrict__ box64_b, int* counts,
                                                const int64_t* __restrict__ offsets, int32_t* pair_a,
-                                               int32_t* pair_b) {
-  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < nel_a;
-       a += (int64_t)gridDim.x * blockDim.x) {
+                                               int32_t* pair_b, int32_t* cache, int cap,
+                                               const int32_t* __restrict__ rows, int* over_rows) {
+  const int64_t nrows = rows ? (int64_t)*over_rows : nel_a;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = rows ? rows[r] : r;
     double lo[DIM], hi[DIM];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
@@ -821,34 +829,81 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
           if (FILL) {
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = w;
+          } else if (cache && cnt < cap) {
+            cache[a * cap + cnt] = w;
           }
           ++cnt;
         }
       }
       node = __float_as_int(H.w);
     }
-    if (!FILL) counts[a] = cnt;
+    if (!FILL) {
+      counts[a] = cnt;
+      if (cache && cnt > cap) over_rows[1 + atomicAdd(over_rows, 1)] = (int32_t)a;
+    }
+  }
+}
+
+// Fill of the rows whose candidates the count pass cached: each warp copies
+// its 32 rows one after the other, lanes striding over the row (coalesced
+// reads of the cache and writes of the pair arrays).
+__global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const int* __restrict__ counts,
+                                                         const int64_t* __restrict__ offsets,
+                                                         const int32_t* __restrict__ cache, int cap,
+                                                         int32_t* pair_a, int32_t* pair_b) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < nel_a;
+       base += warps * 32) {
+    const int64_t a = base + lane;
+    int cnt = 0;
+    int64_t off = 0;
+    if (a < nel_a) {
+      cnt = counts[a];
+      off = offsets[a];
+    }
+    for (int r = 0; r < 32; ++r) {
+      const int c = __shfl_sync(0xffffffffu, cnt, r);
+      const int64_t o = __shfl_sync(0xffffffffu, off, r);
+      if (c > cap) continue;  // filled by the traversal over the listed rows
+      const int64_t row = base + r;
+      for (int k = lane; k < c; k += 32) {
+        pair_a[o + k] = (int32_t)row;
+        pair_b[o + k] = cache[row * cap + k];
+      }
+    }
   }
 }
 
 cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_a, BVH bvh,
                          const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
-                         int32_t* pair_b, cudaStream_t s) {
+                         int32_t* pair_b, cudaStream_t s, int32_t* cache, int cap, int* over_rows) {
   if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
   const int B = query_block();
   const int g = grid_for(nel_a, B, 2048 / B);
-  count_launch();
+  if (fill && cache) {
+    count_launch(2);
+    k_fill_from_cache<<<grid_for(nel_a, 256, 8), 256, 0, s>>>(nel_a, counts, offsets, cache, cap, pair_a, pair_b);
+  } else {
+    count_launch();
+  }
+  const int32_t* rows = (fill && cache) ? over_rows + 1 : nullptr;
+  int32_t* cc = fill ? nullptr : cache;
+#define LSM_QUERY_ARGS                                                                                    \
+  nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b, cc, cap, rows, \
+      over_rows
   if (dim == 2) {
     if (fill)
-      k_query<2, true><<<g, B, 0, s>>>(nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+      k_query<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
     else
-      k_query<2, false><<<g, B, 0, s>>>(nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+      k_query<2, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
   } else {
     if (fill)
-      k_query<3, true><<<g, B, 0, s>>>(nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+      k_query<3, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
     else
-      k_query<3, false><<<g, B, 0, s>>>(nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+      k_query<3, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
   }
+#undef LSM_QUERY_ARGS
   return cudaGetLastError();
 }
 
@@ -2289,6 +2344,7 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
     if (!FILL) counts[a] = cnt;
   }
 }
+
 
 cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double* box64_a,
                                  const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,

@@ -74,10 +74,14 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
                              const float* box32, BVH bvh, int* work_int, cudaStream_t s);
 
 // Candidate search.  Pass 1 (fill=false) writes counts[nel_a]; pass 2 writes
-// pair_a/pair_b at offsets[a].
+// pair_a/pair_b at offsets[a].  With a cache ([nel_a][cap] int32) pass 1 also
+// keeps each row's first cap candidates and lists the longer rows in
+// over_rows ({count, rows...}, count zeroed by the caller, nel_a + 1 ints);
+// pass 2 then copies the cached rows and traverses only the listed ones.
 cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_a, BVH bvh,
                          const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
-                         int32_t* pair_b, cudaStream_t s);
+                         int32_t* pair_b, cudaStream_t s, int32_t* cache = nullptr, int cap = 0,
+                         int* over_rows = nullptr);
 
 // Exclusive scan of int32 counts into int64 offsets[n+1] (offsets[n] = total).
 int64_t scan_tmp_entries(int64_t n);
