@@ -148,9 +148,19 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context *ctx, int dim, int64_t n,
  *   LSM_PAIR_TRI_QUAD   a [n][3][2], b [n][4][2]   elems [n][46][3][2]
  *   LSM_PAIR_TET_HEX    a [n][4][3], b [n][8][3] (Gmsh hexahedron node
  *                       order)          elems [n][729][4][3]
+ *   LSM_PAIR_QUAD_QUAD  a, b [n][4][2]  elems [n][62][3][2]   (intersect_quads,
+ *                       Supermesh.F90:230-246)
+ *   LSM_PAIR_HEX_HEX    a, b [n][8][3]  elems [n][3645][4][3] (intersect_hexes,
+ *                       Supermesh.F90:303-334: A sliced into five tets)
  * measure[n] = sum of output measures, n_out[n] = number of outputs, elems
  * optional, in the reference's output order. */
-enum { LSM_PAIR_INTERVALS = 0, LSM_PAIR_TRI_QUAD = 1, LSM_PAIR_TET_HEX = 2 };
+enum {
+  LSM_PAIR_INTERVALS = 0,
+  LSM_PAIR_TRI_QUAD = 1,
+  LSM_PAIR_TET_HEX = 2,
+  LSM_PAIR_QUAD_QUAD = 3,
+  LSM_PAIR_HEX_HEX = 4
+};
 int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context *ctx, int kind, int64_t n,
                                            const double *a, const double *b,
                                            double *measure, int32_t *n_out,

@@ -130,8 +130,9 @@ def load() -> ctypes.CDLL:
     return L
 
 
-PAIR_INTERVALS, PAIR_TRI_QUAD, PAIR_TET_HEX = 0, 1, 2
-_MIXED = {PAIR_INTERVALS: (2, 2, (1, 2)), PAIR_TRI_QUAD: (6, 8, (46, 3, 2)), PAIR_TET_HEX: (12, 24, (729, 4, 3))}
+PAIR_INTERVALS, PAIR_TRI_QUAD, PAIR_TET_HEX, PAIR_QUAD_QUAD, PAIR_HEX_HEX = 0, 1, 2, 3, 4
+_MIXED = {PAIR_INTERVALS: (2, 2, (1, 2)), PAIR_TRI_QUAD: (6, 8, (46, 3, 2)), PAIR_TET_HEX: (12, 24, (729, 4, 3)),
+          PAIR_QUAD_QUAD: (8, 8, (62, 3, 2)), PAIR_HEX_HEX: (24, 24, (5 * 729, 4, 3))}
 
 
 def _ptr(a) -> int | None:
@@ -266,7 +267,8 @@ class Context:
         return m[:n], k[:n], (e[:n] if e is not None else None)
 
     def intersect_pairs_mixed(self, kind: int, a, b, want_elems: bool = False):
-        """kind: PAIR_INTERVALS, PAIR_TRI_QUAD or PAIR_TET_HEX."""
+        """kind: PAIR_INTERVALS, PAIR_TRI_QUAD, PAIR_TET_HEX, PAIR_QUAD_QUAD or
+        PAIR_HEX_HEX."""
         per_a, per_b, out_shape = _MIXED[kind]
         a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, per_a)
         b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, per_b)

@@ -756,6 +756,8 @@ struct MixedShape {
 MixedShape mixed_shape(int kind) {
   if (kind == LSM_PAIR_INTERVALS) return {2, 2, 1, 2};
   if (kind == LSM_PAIR_TRI_QUAD) return {6, 8, 46, 6};
+  if (kind == LSM_PAIR_QUAD_QUAD) return {8, 8, 62, 6};
+  if (kind == LSM_PAIR_HEX_HEX) return {24, 24, 5 * 729, 12};
   return {12, 24, 729, 12};
 }
 
@@ -1146,8 +1148,7 @@ int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context* ctx, int kind, int64
                                            int on_device, void* stream) {
   Ctx* c = C(ctx);
   return guarded(c, [&] {
-    REQUIRE(kind == LSM_PAIR_INTERVALS || kind == LSM_PAIR_TRI_QUAD || kind == LSM_PAIR_TET_HEX,
-            "unknown pair kind %d", kind);
+    REQUIRE(kind >= LSM_PAIR_INTERVALS && kind <= LSM_PAIR_HEX_HEX, "unknown pair kind %d", kind);
     REQUIRE(n >= 0, "negative pair count");
     if (n == 0) return;
     REQUIRE(a && b, "NULL element arrays");

@@ -2561,6 +2561,97 @@ __global__ void __launch_bounds__(64) k_pairs_tet_hex(int64_t n, const double* _
   }
 }
 
+// Quadrilateral vs quadrilateral (Supermesh.F90:230-246): clip quad A by
+// quad B's 4 edge lines; no element area is given, so the fan keeps
+// triangles with area >= 10*tiny (Triangle_Intersection.F90:255-264).
+__global__ void k_pairs_quad_quad(int64_t n, const double* __restrict__ A, const double* __restrict__ B,
+                                  double* measure, int32_t* nout, double* out_elems) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* va = A + 8 * i;
+    double nx[4], ny[4], px[4], py[4];
+    poly_lines<4>(B + 8 * i, nx, ny, px, py);
+    LocalPoly<16> p, q;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) p.set(v, va[2 * v], va[2 * v + 1]);
+    int m = 4;
+    bool empty = false;
+    for (int l = 0; l < 4 && !empty; ++l) {
+      m = (l & 1) ? clip_stage(q, p, m, 16, nx[l], ny[l], px[l], py[l])
+                  : clip_stage(p, q, m, 16, nx[l], ny[l], px[l], py[l]);
+      empty = m < 3;
+    }
+    double meas = 0.0;
+    int kept = 0;
+    if (!empty) {
+      const double tol = 10.0 * DBL_MIN;
+      double* o = out_elems ? out_elems + 62 * 6 * i : nullptr;
+      const double x0 = p.x(0), y0 = p.y(0);
+      for (int j = 1; j < m - 1; ++j) {
+        const double xi = p.x(j), yi = p.y(j), xj = p.x(j + 1), yj = p.y(j + 1);
+        const double ar = tri_area(x0, y0, xi, yi, xj, yj);
+        if (!(ar < tol)) {
+          meas = meas + ar;
+          if (o && kept < 62) {
+            double* t = o + 6 * kept;
+            t[0] = x0;
+            t[1] = y0;
+            t[2] = xi;
+            t[3] = yi;
+            t[4] = xj;
+            t[5] = yj;
+          }
+          ++kept;
+        }
+      }
+    }
+    if (measure) measure[i] = meas;
+    if (nout) nout[i] = kept;
+  }
+}
+
+// Hexahedron vs hexahedron (Supermesh.F90:303-334): hex A sliced into five
+// tets (Gmsh corners 3,6,7,8 / 1,3,4,8 / 1,5,6,8 / 1,2,3,6 / 1,3,6,8), each
+// clipped by hex B as in intersect_tet_hex; outputs concatenated.
+__global__ void __launch_bounds__(64) k_pairs_hex_hex(int64_t n, const double* __restrict__ A,
+                                                      const double* __restrict__ B, double* measure,
+                                                      int32_t* nout, double* out_elems) {
+  const int T[5][4] = {{2, 5, 6, 7}, {0, 2, 3, 7}, {0, 4, 5, 7}, {0, 1, 2, 5}, {0, 2, 5, 7}};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* h = A + 24 * i;
+    ArrPlanes<6> P;
+    hex_planes(B + 24 * i, P.nx, P.ny, P.nz, P.c);
+    double m = 0.0;
+    int total = 0;
+    double* o = out_elems ? out_elems + (int64_t)5 * 729 * 12 * i : nullptr;
+    for (int s = 0; s < 5; ++s) {
+      Tet ta;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        ta.x[v] = h[3 * T[s][v]];
+        ta.y[v] = h[3 * T[s][v] + 1];
+        ta.z[v] = h[3 * T[s][v] + 2];
+      }
+      const double tol = 10.0 * spacing(tet_volume_v4(ta));
+      TetStackN<10> stk;
+      const int k = clip_tet_dfs<6>(ta, P, tol, stk, [&](const Tet& t) {
+        m = m + tet_volume_v1(t);
+        if (o && total < 5 * 729) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            o[12 * total + 3 * v + 0] = t.x[v];
+            o[12 * total + 3 * v + 1] = t.y[v];
+            o[12 * total + 3 * v + 2] = t.z[v];
+          }
+        }
+        ++total;
+      });
+      (void)k;
+    }
+    if (measure) measure[i] = m;
+    if (nout) nout[i] = total;
+  }
+}
+
 __global__ void k_pairs_intervals(int64_t n, const double* __restrict__ A, const double* __restrict__ B,
                                   double* measure, int32_t* nout, double* out_elems) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -2583,8 +2674,12 @@ cudaError_t launch_pairs_mixed(int kind, int64_t n, const double* a, const doubl
     k_pairs_intervals<<<grid_for(n, 256, 8), 256, 0, s>>>(n, a, b, measure, nout, out_elems);
   else if (kind == 1)
     k_pairs_tri_quad<<<grid_for(n, 128, 8), 128, 0, s>>>(n, a, b, measure, nout, out_elems);
-  else
+  else if (kind == 2)
     k_pairs_tet_hex<<<grid_for(n, 64, 8), 64, 0, s>>>(n, a, b, measure, nout, out_elems);
+  else if (kind == 3)
+    k_pairs_quad_quad<<<grid_for(n, 128, 8), 128, 0, s>>>(n, a, b, measure, nout, out_elems);
+  else
+    k_pairs_hex_hex<<<grid_for(n, 64, 8), 64, 0, s>>>(n, a, b, measure, nout, out_elems);
   return cudaGetLastError();
 }
 

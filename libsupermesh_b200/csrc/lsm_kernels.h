@@ -145,7 +145,8 @@ cudaError_t launch_measure_explicit(int dim, int64_t n, const double* elems, dou
                                     cudaStream_t s);
 // Mixed pairs: kind 0 intervals ([n][2] x [n][2] -> [n][2]), 1 tri vs quad
 // ([n][3][2] x [n][4][2] -> [n][46][3][2]), 2 tet vs hex ([n][4][3] x
-// [n][8][3] -> [n][729][4][3]).
+// [n][8][3] -> [n][729][4][3]), 3 quad vs quad (-> [n][62][3][2]), 4 hex vs
+// hex (-> [n][5*729][4][3]).
 cudaError_t launch_pairs_mixed(int kind, int64_t n, const double* a, const double* b, double* measure,
                                int32_t* nout, double* out_elems, cudaStream_t s);
 // 1D sort finder.  prep gathers the first coordinate of both nodes of each

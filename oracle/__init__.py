@@ -122,6 +122,24 @@ def intersect_tet_hex(tet_a, hex_b):
     return out[: n.value].copy()
 
 
+def intersect_quads(quad_a, quad_b):
+    a = np.ascontiguousarray(quad_a, dtype=np.float64).reshape(8)
+    b = np.ascontiguousarray(quad_b, dtype=np.float64).reshape(8)
+    out = np.zeros((62, 3, 2))
+    n = ctypes.c_int(0)
+    lib().orc_intersect_quads(_d(a), _d(b), _d(out), ctypes.byref(n))
+    return out[: n.value].copy()
+
+
+def intersect_hexes(hex_a, hex_b):
+    a = np.ascontiguousarray(hex_a, dtype=np.float64).reshape(24)
+    b = np.ascontiguousarray(hex_b, dtype=np.float64).reshape(24)
+    out = np.zeros((5 * 729, 4, 3))
+    n = ctypes.c_int(0)
+    lib().orc_intersect_hexes(_d(a), _d(b), _d(out), ctypes.byref(n))
+    return out[: n.value].copy()
+
+
 def intersect_intervals(a, b):
     a = np.ascontiguousarray(a, dtype=np.float64).reshape(2)
     b = np.ascontiguousarray(b, dtype=np.float64).reshape(2)

@@ -554,6 +554,59 @@ void orc_intersect_tet_hex(const double tet_a[12], const double hex_b[24], doubl
   *n_tets_c = n;
 }
 
+/* intersect_quads (Supermesh.F90:230-246): quad A clipped by quad B's four
+ * edge lines (get_lines_poly), no element areas given, so the fan keeps
+ * triangles with area >= 10*tiny (Triangle_Intersection.F90:255-264);
+ * buffers 4 * 2**4 points. */
+#define ORC_QQBUF 64
+void orc_intersect_quads(const double quad_a[8], const double quad_b[8], double *tris_c, int *n_tris_c) {
+  orc_line L[4];
+  get_lines_poly(quad_b, 4, L);
+  double pa[2 * ORC_QQBUF], pb[2 * ORC_QQBUF];
+  memcpy(pa, quad_a, 8 * sizeof(double));
+  int n = 4;
+  double *cur = pa, *nxt = pb;
+  *n_tris_c = 0;
+  for (int i = 0; i < 4; ++i) {
+    n = clip_buf_tri(&L[i], cur, n, nxt);
+    if (n < 3) return;
+    double *t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  const double tol = 10.0 * DBL_MIN;
+  int nt = 0;
+  for (int i = 0; i < n - 2; ++i) {
+    double *t = tris_c + 6 * nt;
+    t[0] = cur[0];
+    t[1] = cur[1];
+    t[2] = cur[2 * (i + 1)];
+    t[3] = cur[2 * (i + 1) + 1];
+    t[4] = cur[2 * (i + 2)];
+    t[5] = cur[2 * (i + 2) + 1];
+    if (!(orc_triangle_area(t) < tol)) ++nt;
+  }
+  *n_tris_c = nt;
+}
+
+/* intersect_hexes (Supermesh.F90:303-334): hex A sliced into five tets
+ * (Gmsh corners (3,6,7,8), (1,3,4,8), (1,5,6,8), (1,2,3,6), (1,3,6,8)), each
+ * clipped by hex B with intersect_tet_hex; outputs concatenated. */
+static const int ORC_HEX_TETS[5][4] = {{2, 5, 6, 7}, {0, 2, 3, 7}, {0, 4, 5, 7}, {0, 1, 2, 5}, {0, 2, 5, 7}};
+
+void orc_intersect_hexes(const double hex_a[24], const double hex_b[24], double *tets_c, int *n_tets_c) {
+  int n = 0;
+  for (int t = 0; t < 5; ++t) {
+    double tet[12];
+    for (int v = 0; v < 4; ++v)
+      for (int c = 0; c < 3; ++c) tet[3 * v + c] = hex_a[3 * ORC_HEX_TETS[t][v] + c];
+    int m = 0;
+    orc_intersect_tet_hex(tet, hex_b, tets_c + 12 * n, &m);
+    n += m;
+  }
+  *n_tets_c = n;
+}
+
 double orc_interval_size(const double iv[2]) { return fabs(iv[1] - iv[0]); }
 
 void orc_intersect_intervals(const double a[2], const double b[2], double *c, int *n) {

@@ -22,7 +22,9 @@
  *                                     finder (:811-921)
  *   src/Triangle_Intersection.F90     intersect_polys / get_lines_poly
  *                                     (:187-239, :422-451) for tri vs quad
- *   src/Supermesh.F90                 intersect_tet_hex (:248-295)
+ *   src/Supermesh.F90                 intersect_tet_hex (:248-295),
+ *                                     intersect_quads (:230-246),
+ *                                     intersect_hexes (:303-334)
  *   src/Interval_Intersection.F90     intersect_intervals, interval_size
  *   src/Intersections.F90:48-71       ragged -> CSR
  *   src/Precision.F90:72-113          Kahan compensated sum
@@ -61,9 +63,12 @@ void orc_intersect_tets(const double tet_a[12], const double tet_b[12],
                         double *tets_c, int *n_tets_c);
 
 /* Mixed pairs: tri vs quad ([3][2] x [4][2] -> <= 46 tris [46][3][2]); tet
- * vs hex in Gmsh order ([4][3] x [8][3] -> <= 729 tets); intervals. */
+ * vs hex in Gmsh order ([4][3] x [8][3] -> <= 729 tets); quad vs quad (<= 62
+ * tris); hex vs hex (<= 5 * 729 tets); intervals. */
 void orc_intersect_tri_quad(const double tri_a[6], const double quad_b[8], double *tris_c, int *n_tris_c);
 void orc_intersect_tet_hex(const double tet_a[12], const double hex_b[24], double *tets_c, int *n_tets_c);
+void orc_intersect_quads(const double quad_a[8], const double quad_b[8], double *tris_c, int *n_tris_c);
+void orc_intersect_hexes(const double hex_a[24], const double hex_b[24], double *tets_c, int *n_tets_c);
 double orc_interval_size(const double iv[2]);
 void orc_intersect_intervals(const double a[2], const double b[2], double *c, int *n);
 

@@ -1,5 +1,6 @@
 """GPU parity of the 1D and mixed-element entries of the C API: the sort
-finder, intervals, triangle vs quadrilateral and tetrahedron vs hexahedron.
+finder, intervals, triangle vs quadrilateral and tetrahedron vs hexahedron,
+and the quad-quad / hex-hex pairs of intersect_elements.
 
 All integer results (candidate CSR, row order, output counts) and all FP64
 outputs must equal the oracle's bit for bit: the kernels evaluate the
@@ -232,29 +233,70 @@ def test_tet_hex_bitexact(gpu_ctx, oracle_mod):
         assert np.array_equal(lsm.intersect_tet_hex(t[i], h[i]), oracle_mod.intersect_tet_hex(t[i], h[i]))
 
 
-def _gpu_mixed_total(ctx, dim, A, B, swap=False):
-    """Candidates from the GPU search, each (simplex, box element) pair
-    clipped on the GPU; compensated sum of the per-pair measures."""
+_ORACLE_FN = {lsm.PAIR_TRI_QUAD: "intersect_tri_quad", lsm.PAIR_TET_HEX: "intersect_tet_hex",
+              lsm.PAIR_QUAD_QUAD: "intersect_quads", lsm.PAIR_HEX_HEX: "intersect_hexes"}
+
+
+def test_quad_quad_bitexact(gpu_ctx, oracle_mod):
+    rng = np.random.default_rng(13)
+    n = 2000
+    a = _random_quads(rng, n)
+    b = _random_quads(rng, n)
+    unit = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], dtype=np.float64)
+    a[:64] = unit + rng.integers(-1, 2, (64, 1, 2))
+    b[:64] = unit
+    m, k, e = gpu_ctx.intersect_pairs_mixed(lsm.PAIR_QUAD_QUAD, a, b, want_elems=True)
+    for i in range(n):
+        ref = oracle_mod.intersect_quads(a[i], b[i])
+        assert k[i] == len(ref), i
+        assert np.array_equal(e[i, : k[i]], ref), i
+        meas = 0.0
+        for o in ref:
+            meas += oracle_mod.triangle_area(o)
+        assert m[i] == meas, i
+
+
+def test_hex_hex_bitexact(gpu_ctx, oracle_mod):
+    rng = np.random.default_rng(14)
+    n = 300
+    a = _random_hexes(rng, n)
+    b = _random_hexes(rng, n)
+    m, k, e = gpu_ctx.intersect_pairs_mixed(lsm.PAIR_HEX_HEX, a, b, want_elems=True)
+    for i in range(n):
+        ref = oracle_mod.intersect_hexes(a[i], b[i])
+        assert k[i] == len(ref), i
+        assert np.array_equal(e[i, : k[i]], ref), i
+        meas = 0.0
+        for o in ref:
+            meas += oracle_mod.tetrahedron_volume(o)
+        assert m[i] == meas, i
+
+
+def _gpu_mixed_total(ctx, kind, A, B, swap=False):
+    """Candidates from the GPU search, each element pair clipped on the GPU
+    (simplex first when one side is a box element); sum of the per-pair
+    measures."""
     n = ctx.find_candidates(A, B)
     ip, ind = ctx.get_candidates(len(A[1]), n)
     rows = np.repeat(np.arange(len(A[1])), np.diff(ip))
     ea, eb = A[0][A[1][rows]], B[0][B[1][ind]]
     s, q = (eb, ea) if swap else (ea, eb)
-    kind = lsm.PAIR_TRI_QUAD if dim == 2 else lsm.PAIR_TET_HEX
     m, k, _ = ctx.intersect_pairs_mixed(kind, s, q)
     return float(np.sum(m)), m, k, s, q
 
 
-@pytest.mark.parametrize("dim,na,nb,swap,expect", [
-    (2, "square.1", "square.4", False, 1.0),   # test_element_intersector.F90:134-158
-    (2, "square.3", "square.2", True, 1.0),    # :163-187
-    (3, "cube.1", "cube.3", False, 0.5),       # :250-274
-    (3, "cube.3", "cube.2", True, 0.5),        # :279-303
+@pytest.mark.parametrize("kind,na,nb,swap,expect", [
+    (lsm.PAIR_TRI_QUAD, "square.1", "square.4", False, 1.0),   # test_element_intersector.F90:134-158
+    (lsm.PAIR_TRI_QUAD, "square.3", "square.2", True, 1.0),    # :163-187
+    (lsm.PAIR_QUAD_QUAD, "square.3", "square.4", False, 1.0),  # :192-216
+    (lsm.PAIR_TET_HEX, "cube.1", "cube.3", False, 0.5),        # :250-274
+    (lsm.PAIR_TET_HEX, "cube.3", "cube.2", True, 0.5),         # :279-303
+    (lsm.PAIR_HEX_HEX, "cube.3", "cube.4", False, 0.5),        # :308-332
 ])
-def test_mixed_reference_known_answers(gpu_ctx, oracle_mod, ref_meshes, dim, na, nb, swap, expect):
+def test_mixed_reference_known_answers(gpu_ctx, oracle_mod, ref_meshes, kind, na, nb, swap, expect):
     A, B = ref_meshes(na), ref_meshes(nb)
-    total, m, k, s, q = _gpu_mixed_total(gpu_ctx, dim, A, B, swap)
+    total, m, k, s, q = _gpu_mixed_total(gpu_ctx, kind, A, B, swap)
     assert oracle_mod.fequals(total, expect)
+    fn = getattr(oracle_mod, _ORACLE_FN[kind])
     for i in range(len(m)):
-        ref = oracle_mod.intersect_tri_quad(s[i], q[i]) if dim == 2 else oracle_mod.intersect_tet_hex(s[i], q[i])
-        assert k[i] == len(ref)
+        assert k[i] == len(fn(s[i], q[i]))

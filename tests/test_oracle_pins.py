@@ -165,6 +165,28 @@ def test_hex_tet_volume_half(oracle_mod, ref_meshes):
         _mixed_total(oracle_mod, 3, ref_meshes("cube.3"), ref_meshes("cube.2"), swap=True), 0.5)
 
 
+def _same_type_total(oracle, dim, A, B):
+    ip, ind = oracle.brute_force_finder(dim, A, B)
+    fn = oracle.intersect_quads if dim == 2 else oracle.intersect_hexes
+    meas = oracle.triangle_area if dim == 2 else oracle.tetrahedron_volume
+    total = 0.0
+    for a in range(len(ip) - 1):
+        for b in ind[ip[a]:ip[a + 1]]:
+            for o in fn(A[0][A[1][a]], B[0][B[1][b]]):
+                total += meas(o)
+    return total
+
+
+def test_quad_quad_area_one(oracle_mod, ref_meshes):
+    # src/tests/test_element_intersector.F90:192-216: quad-quad, total 1
+    assert oracle_mod.fequals(_same_type_total(oracle_mod, 2, ref_meshes("square.3"), ref_meshes("square.4")), 1.0)
+
+
+def test_hex_hex_volume_half(oracle_mod, ref_meshes):
+    # src/tests/test_element_intersector.F90:308-332: hex-hex, total 0.5
+    assert oracle_mod.fequals(_same_type_total(oracle_mod, 3, ref_meshes("cube.3"), ref_meshes("cube.4")), 0.5)
+
+
 def _interval_total(oracle, A, B, ip, ind):
     total = 0.0
     for a in range(len(ip) - 1):
