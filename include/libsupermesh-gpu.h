@@ -176,6 +176,22 @@ int libsupermesh_gpu_p1_mass(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
                              const double *v_b, double *blocks, double *integral,
                              int on_device, void *stream);
 
+/* P2 inner product over the supermesh of two 2D triangle meshes, as
+ * test_parallel_p2_inner_product_2d.F90:398-522: P2 fields f_a, f_b given by
+ * element-node lists [nelements][6] (vertices 1-3, then the midpoints of edges
+ * 1-2, 2-3, 1-3; same index width as the meshes) and node values; for every
+ * supermesh triangle c both fields are interpolated at c's vertices and edge
+ * midpoints with the P2 basis of their own element and 2 |c| f_b . (M f_a) is
+ * added, M the P2 mass matrix of the unit triangle.  integral / area receive
+ * the compensated totals; pair_values (optional, [n_candidates], CSR order)
+ * each candidate pair's contribution. */
+int libsupermesh_gpu_p2_inner_product(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
+                                      const lsm_gpu_mesh *b, const void *enlist_p2_a,
+                                      const double *field_a, int64_t nnodes_p2_a,
+                                      const void *enlist_p2_b, const double *field_b,
+                                      int64_t nnodes_p2_b, double *pair_values, double *integral,
+                                      double *area, int on_device, void *stream);
+
 /* Many independent mesh pairs in one call.  totals[npairs] receives each
  * pair's supermesh measure
  * and n_candidates[npairs] / n_intersecting[npairs] (optional) its counts.

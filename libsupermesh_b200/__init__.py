@@ -117,13 +117,15 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_intersect_pairs_mixed.argtypes = [vp, ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp, vp,
                                                          ctypes.c_int, vp]
     L.libsupermesh_gpu_p1_mass.argtypes = [vp, mp, mp, vp, vp, vp, _dp, ctypes.c_int, vp]
+    L.libsupermesh_gpu_p2_inner_product.argtypes = [vp, mp, mp, vp, vp, ctypes.c_int64, vp, vp, ctypes.c_int64, vp,
+                                                    _dp, _dp, ctypes.c_int, vp]
     L.libsupermesh_gpu_supermesh_batched.argtypes = [vp, ctypes.c_int, mp, mp, ctypes.c_int, vp, vp, vp, vp]
     for name in ("libsupermesh_gpu_context_create", "libsupermesh_gpu_context_destroy",
                  "libsupermesh_gpu_find_candidates", "libsupermesh_gpu_get_candidates",
                  "libsupermesh_gpu_supermesh", "libsupermesh_gpu_get_pair_results",
                  "libsupermesh_gpu_clip_candidates",
                  "libsupermesh_gpu_intersect_pairs", "libsupermesh_gpu_intersect_pairs_mixed",
-                 "libsupermesh_gpu_p1_mass",
+                 "libsupermesh_gpu_p1_mass", "libsupermesh_gpu_p2_inner_product",
                  "libsupermesh_gpu_supermesh_batched"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -297,6 +299,29 @@ class Context:
         self._check(self.lib.libsupermesh_gpu_p1_mass(self._h, ctypes.byref(ma), ctypes.byref(mb), _ptr(u),
                                                       _ptr(v), _ptr(blocks), ctypes.byref(integral), 0, None))
         return (integral.value if u is not None else None), (blocks[:n] if blocks is not None else None)
+
+    def p2_inner_product(self, mesh_a, mesh_b, enlist_p2_a, field_a, enlist_p2_b, field_b,
+                         want_pairs: bool = False):
+        """2D P2 inner product over the supermesh.  Returns (integral, area,
+        per-pair contributions or None); host arrays."""
+        ma, mb = _mesh(*mesh_a, False), _mesh(*mesh_b, False)
+        if ma.index_bytes != mb.index_bytes:
+            raise ValueError("A and B must use the same index width")
+        dt = np.int32 if ma.index_bytes == 4 else np.int64
+        e2a = np.ascontiguousarray(enlist_p2_a, dtype=dt)
+        e2b = np.ascontiguousarray(enlist_p2_b, dtype=dt)
+        fa = np.ascontiguousarray(field_a, dtype=np.float64)
+        fb = np.ascontiguousarray(field_b, dtype=np.float64)
+        pv, n = None, 0
+        if want_pairs:
+            n = self.find_candidates(mesh_a, mesh_b)
+            pv = np.zeros(max(n, 1))
+        integral, area = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self._check(self.lib.libsupermesh_gpu_p2_inner_product(
+            self._h, ctypes.byref(ma), ctypes.byref(mb), e2a.ctypes.data, fa.ctypes.data, fa.size,
+            e2b.ctypes.data, fb.ctypes.data, fb.size, _ptr(pv), ctypes.byref(integral), ctypes.byref(area), 0,
+            None))
+        return integral.value, area.value, (pv[:n] if pv is not None else None)
 
     def supermesh_batched(self, pairs, on_device: bool = False, stream: int | None = None):
         """pairs: list of (mesh_a, mesh_b).  Returns (totals, n_candidates,

@@ -1220,6 +1220,70 @@ int libsupermesh_gpu_p1_mass(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const 
   });
 }
 
+int libsupermesh_gpu_p2_inner_product(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b,
+                                      const void* enlist_p2_a, const double* field_a, int64_t nnodes_p2_a,
+                                      const void* enlist_p2_b, const double* field_b, int64_t nnodes_p2_b,
+                                      double* pair_values, double* integral, double* area, int on_device,
+                                      void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    cudaStream_t s = pick(c, stream);
+    REQUIRE(a && b && a->index_bytes == b->index_bytes, "A and B must use the same index width");
+    REQUIRE(a->dim == 2 && b->dim == 2, "P2 inner product: meshes must be 2D triangles");
+    REQUIRE(enlist_p2_a && enlist_p2_b && field_a && field_b, "NULL P2 arrays");
+    REQUIRE(nnodes_p2_a > 0 && nnodes_p2_b > 0, "empty P2 spaces");
+    find_candidates(c, a, b, on_device, true, true, s);
+    const int64_t nnz = c->ncand;
+    const int ib = a->index_bytes;
+    const void *e2a = enlist_p2_a, *e2b = enlist_p2_b;
+    const double *fa = field_a, *fb = field_b;
+    if (!on_device) {
+      char* ta = ensure<char>(c, c->x_a, (a->nelements * 6 * ib + 7) / 8 * 8);
+      char* tb = ensure<char>(c, c->x_b, (b->nelements * 6 * ib + 7) / 8 * 8);
+      double* tfa = ensure<double>(c, c->u_a, nnodes_p2_a);
+      double* tfb = ensure<double>(c, c->v_b, nnodes_p2_b);
+      CU(cudaMemcpyAsync(ta, enlist_p2_a, (size_t)a->nelements * 6 * ib, cudaMemcpyHostToDevice, s));
+      CU(cudaMemcpyAsync(tb, enlist_p2_b, (size_t)b->nelements * 6 * ib, cudaMemcpyHostToDevice, s));
+      CU(cudaMemcpyAsync(tfa, field_a, sizeof(double) * nnodes_p2_a, cudaMemcpyHostToDevice, s));
+      CU(cudaMemcpyAsync(tfb, field_b, sizeof(double) * nnodes_p2_b, cudaMemcpyHostToDevice, s));
+      e2a = ta;
+      e2b = tb;
+      fa = tfa;
+      fb = tfb;
+    }
+    int* bad = bad_flag(c);
+    CU(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    CU(lsm::launch_check_index(a->nelements * 6, e2a, ib, nnodes_p2_a, bad, s));
+    CU(lsm::launch_check_index(b->nelements * 6, e2b, ib, nnodes_p2_b, bad, s));
+    double* pv = (pair_values && on_device) ? pair_values : ensure<double>(c, c->pair_measure, nnz);
+    double* pa_ = ensure<double>(c, c->elem_measure, std::max<int64_t>(nnz, c->nel_a));
+    int32_t* pn = ensure<int32_t>(c, c->pair_nout, nnz);
+    int* hb = static_cast<int*>(c->host_scalars);
+    CU(cudaMemcpyAsync(hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    REQUIRE(hb[0] == 0, "Invalid node index in a P2 element list");
+    CU(lsm::launch_p2_inner(nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+                            static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
+                            static_cast<double*>(c->b_coords.p), static_cast<double*>(c->b_setup.p), e2a, fa, e2b,
+                            fb, ib, pv, pa_, pn, s));
+    const int nred = lsm::reduce_pairs_blocks();
+    lsm::Partial* part = ensure<lsm::Partial>(c, c->partials, 2 * nred);
+    lsm::Partial* tot = ensure<lsm::Partial>(c, c->totals, 2);
+    CU(lsm::launch_reduce_pairs(nnz, pv, pn, part, s));
+    CU(lsm::launch_finalize(part, nred, tot, s));
+    CU(lsm::launch_reduce_pairs(nnz, pa_, pn, part + nred, s));
+    CU(lsm::launch_finalize(part + nred, nred, tot + 1, s));
+    lsm::Partial* h = reinterpret_cast<lsm::Partial*>(static_cast<char*>(c->host_scalars) + 512);
+    CU(cudaMemcpyAsync(h, tot, 2 * sizeof(lsm::Partial), cudaMemcpyDeviceToHost, s));
+    if (pair_values && !on_device && nnz > 0)
+      CU(cudaMemcpyAsync(pair_values, pv, sizeof(double) * nnz, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (integral) *integral = h[0].sum;
+    if (area) *area = h[1].sum;
+    c->have_pairs = false;  // pair_measure now holds P2 contributions
+  });
+}
+
 int libsupermesh_gpu_supermesh_batched(lsm_gpu_context* ctx, int npairs, const lsm_gpu_mesh* a,
                                        const lsm_gpu_mesh* b, int on_device, double* totals,
                                        int64_t* n_candidates, int64_t* n_intersecting, void* stream) {

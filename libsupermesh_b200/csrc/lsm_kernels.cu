@@ -3159,6 +3159,139 @@ __global__ void __launch_bounds__(128) k_p1_mass(int64_t npairs, const int32_t* 
   block_reduce_partial<128>(sum, err, ni, 0ull, &partials[blockIdx.x]);
 }
 
+// ----------------------------------------------------------------------
+// P2 inner product (test_parallel_p2_inner_product_2d.F90:398-522)
+// ----------------------------------------------------------------------
+// P2 basis of triangle cc ([3][2]) at point (x, y), basis_functions_p2
+// (:399-433): local coordinates through the inverse Jacobian, then the six
+// quadratic Lagrange functions (vertices 1-3, edge midpoints 1-2, 2-3, 1-3).
+__device__ __forceinline__ void p2_basis_2d(const double* cc, double x, double y, double f[6]) {
+  const double e10 = cc[2] - cc[0], e11 = cc[3] - cc[1];
+  const double e20 = cc[4] - cc[0], e21 = cc[5] - cc[1];
+  double j11 = e21, j12 = -e20, j21 = -e11, j22 = e10;
+  const double det = j11 * j22 - j12 * j21;
+  j11 = j11 / det;
+  j12 = j12 / det;
+  j21 = j21 / det;
+  j22 = j22 / det;
+  const double d1 = x - cc[0], d2 = y - cc[1];
+  const double lx = j11 * d1 + j12 * d2, ly = j21 * d1 + j22 * d2;
+  f[0] = ((1.0 - lx) - ly) * ((1.0 - 2.0 * lx) - 2.0 * ly);
+  f[1] = lx * (2.0 * lx - 1.0);
+  f[2] = ly * (2.0 * ly - 1.0);
+  f[3] = (4.0 * lx) * ((1.0 - lx) - ly);
+  f[4] = (4.0 * lx) * ly;
+  f[5] = (4.0 * ly) * ((1.0 - lx) - ly);
+}
+
+__device__ __forceinline__ double p2_interp_2d(const double* cc, const double v[6], double x, double y) {
+  double f[6];
+  p2_basis_2d(cc, x, y, f);
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) s = s + f[k] * v[k];
+  return s;
+}
+
+// Per candidate pair: clip, then for every supermesh triangle c the P2
+// fields of A and B at c's vertices and edge midpoints and the contribution
+// 2 |c| f_b . (M f_a), summed over c in output order.
+template <class IDX>
+__global__ void __launch_bounds__(128) k_p2_inner(int64_t npairs, const int32_t* __restrict__ pa,
+                                                  const int32_t* __restrict__ pb,
+                                                  const double* __restrict__ coords_a,
+                                                  const double* __restrict__ tol_a,
+                                                  const double* __restrict__ coords_b,
+                                                  const double* __restrict__ setup_b, const void* en_p2_a,
+                                                  const double* __restrict__ field_a, const void* en_p2_b,
+                                                  const double* __restrict__ field_b, double* pair_value,
+                                                  double* pair_area, int32_t* pair_n) {
+  constexpr double M[6][6] = {
+      {6.0 / 360.0, -1.0 / 360.0, -1.0 / 360.0, 0.0 / 360.0, -4.0 / 360.0, 0.0 / 360.0},
+      {-1.0 / 360.0, 6.0 / 360.0, -1.0 / 360.0, 0.0 / 360.0, 0.0 / 360.0, -4.0 / 360.0},
+      {-1.0 / 360.0, -1.0 / 360.0, 6.0 / 360.0, -4.0 / 360.0, 0.0 / 360.0, 0.0 / 360.0},
+      {0.0 / 360.0, 0.0 / 360.0, -4.0 / 360.0, 32.0 / 360.0, 16.0 / 360.0, 16.0 / 360.0},
+      {-4.0 / 360.0, 0.0 / 360.0, 0.0 / 360.0, 16.0 / 360.0, 32.0 / 360.0, 16.0 / 360.0},
+      {0.0 / 360.0, -4.0 / 360.0, 0.0 / 360.0, 16.0 / 360.0, 16.0 / 360.0, 32.0 / 360.0}};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npairs;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int a = pa[i], b = pb[i];
+    const double* ca = coords_a + (int64_t)a * 6;
+    const double* cb = coords_b + (int64_t)b * 6;
+    double va[6], vb[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      va[k] = field_a[node_of<IDX>(en_p2_a, a, 6, k)];
+      vb[k] = field_b[node_of<IDX>(en_p2_b, b, 6, k)];
+    }
+    Lines L;
+    double tolb;
+    load_lines(setup_b + (int64_t)b * kSetup2, L, tolb);
+    const double tol = fmin(tol_a[a], tolb);
+    LocalPoly<kTriWideCap> p, q;
+    double m;
+    double sp = 0.0, sa = 0.0;
+    int nt = 0;
+    clip_tri(ca[0], ca[1], ca[2], ca[3], ca[4], ca[5], L, tol, p, q, kTriWideCap, m,
+             [&](int, double x0, double y0, double x1, double y1, double x2, double y2) {
+               const double ar = tri_area(x0, y0, x1, y1, x2, y2);
+               sa = sa + ar;
+               ++nt;
+               const double px[6] = {x0, x1, x2, 0.5 * (x0 + x1), 0.5 * (x1 + x2), 0.5 * (x0 + x2)};
+               const double py[6] = {y0, y1, y2, 0.5 * (y0 + y1), 0.5 * (y1 + y2), 0.5 * (y0 + y2)};
+               double fa[6], fb[6];
+#pragma unroll
+               for (int l = 0; l < 6; ++l) {
+                 fb[l] = p2_interp_2d(cb, vb, px[l], py[l]);
+                 fa[l] = p2_interp_2d(ca, va, px[l], py[l]);
+               }
+               double dot = 0.0;
+#pragma unroll
+               for (int r = 0; r < 6; ++r) {
+                 double mi = 0.0;
+#pragma unroll
+                 for (int k = 0; k < 6; ++k) mi = mi + M[r][k] * fa[k];
+                 dot = dot + fb[r] * mi;
+               }
+               sp = sp + (2.0 * ar) * dot;
+             });
+    pair_value[i] = sp;
+    pair_area[i] = sa;
+    pair_n[i] = nt;
+  }
+}
+
+__global__ void k_check_index(int64_t n, const void* en, int idx_bytes, int64_t limit, int* bad) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = idx_bytes == 8 ? static_cast<const int64_t*>(en)[i] : static_cast<const int32_t*>(en)[i];
+    if (v < 0 || v >= limit) atomicExch(bad, 1);
+  }
+}
+
+cudaError_t launch_check_index(int64_t n, const void* en, int idx_bytes, int64_t limit, int* bad, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launch();
+  k_check_index<<<grid_for(n, 256, 8), 256, 0, s>>>(n, en, idx_bytes, limit, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p2_inner(int64_t npairs, const int32_t* pair_a, const int32_t* pair_b, const double* coords_a,
+                            const double* tol_a, const double* coords_b, const double* setup_b,
+                            const void* en_p2_a, const double* field_a, const void* en_p2_b,
+                            const double* field_b, int idx_bytes, double* pair_value, double* pair_area,
+                            int32_t* pair_n, cudaStream_t s) {
+  if (npairs <= 0) return cudaSuccess;
+  count_launch();
+  const int g = sm_count() * 4;
+  if (idx_bytes == 4)
+    k_p2_inner<int32_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, en_p2_a,
+                                          field_a, en_p2_b, field_b, pair_value, pair_area, pair_n);
+  else
+    k_p2_inner<int64_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, en_p2_a,
+                                          field_a, en_p2_b, field_b, pair_value, pair_area, pair_n);
+  return cudaGetLastError();
+}
+
 int p1_grid_blocks(int dim) { return sm_count() * (dim == 2 ? 4 : 2); }
 
 cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,

@@ -173,6 +173,15 @@ cudaError_t launch_clip_intervals(int64_t n, const int32_t* pa, const int32_t* p
                                   const double* cb, double* measure, int32_t* nout, cudaStream_t s);
 
 // P1-P1 mixed mass blocks per candidate pair and u^T M v partials.
+// P2 inner product over a 2D candidate list (per pair: contribution, area,
+// supermesh triangles); P2 element-node lists [nel][6] with idx_bytes.
+cudaError_t launch_p2_inner(int64_t npairs, const int32_t* pair_a, const int32_t* pair_b, const double* coords_a,
+                            const double* tol_a, const double* coords_b, const double* setup_b,
+                            const void* en_p2_a, const double* field_a, const void* en_p2_b,
+                            const double* field_b, int idx_bytes, double* pair_value, double* pair_area,
+                            int32_t* pair_n, cudaStream_t s);
+// bad = 1 if any of en[0..n) lies outside [0, limit).
+cudaError_t launch_check_index(int64_t n, const void* en, int idx_bytes, int64_t limit, int* bad, cudaStream_t s);
 cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                            const double* coords_a, const double* tol_a, const double* coords_b,
                            const double* setup_b, const void* enlist_a, const void* enlist_b,

@@ -225,3 +225,35 @@ def batched_pairs(count: int = 256, seed: int = 6, emin: float = 1e3, emax: floa
                 meshes.append(grid3d(n, mseed, 0.25))
         pairs.append((dim, meshes[0], meshes[1]))
     return pairs
+
+
+def p2_space(enlist):
+    """P2 element-node list of a triangle mesh: [nel][6] with the P1 vertices
+    first (same numbers), then new nodes for the edge midpoints 1-2, 2-3,
+    1-3, numbered in first-visit order.  Returns (enlist_p2, nnodes_p2,
+    edges) with edges mapping (min, max) vertex pairs to midpoint nodes."""
+    en = np.asarray(enlist, dtype=np.int64)
+    nv = int(en.max()) + 1 if en.size else 0
+    e2 = np.zeros((len(en), 6), dtype=np.int64)
+    e2[:, :3] = en
+    edges = {}
+    nxt = nv
+    for e in range(len(en)):
+        for l, (i, j) in enumerate(((0, 1), (1, 2), (0, 2))):
+            k = (min(en[e, i], en[e, j]), max(en[e, i], en[e, j]))
+            if k not in edges:
+                edges[k] = nxt
+                nxt += 1
+            e2[e, 3 + l] = edges[k]
+    return e2, nxt, edges
+
+
+def p1_to_p2(values_p1, nnodes_p2, edges):
+    """Interpolate a P1 nodal field onto the P2 space of p2_space: vertex
+    values copied, midpoint values 0.5 * (sum of the edge's end values)."""
+    v = np.asarray(values_p1, dtype=np.float64)
+    out = np.zeros(nnodes_p2)
+    out[: len(v)] = v
+    for (i, j), k in edges.items():
+        out[k] = 0.5 * (v[i] + v[j])
+    return out

@@ -271,6 +271,28 @@ def p1_mass(dim, mesh_a, mesh_b, indptr, indices, u_a, v_b, want_blocks: bool = 
     return integral.value, measure.value, (blocks[:nnz] if blocks is not None else None)
 
 
+def p2_inner_product(mesh_a, mesh_b, indptr, indices, en_p2_a, field_a, en_p2_b, field_b):
+    """Returns (integral, area, per-pair contributions[nnz])."""
+    pa, ea = _mesh_args(*mesh_a)
+    pb, eb = _mesh_args(*mesh_b)
+    indptr = np.ascontiguousarray(indptr, dtype=np.int64)
+    indices = np.ascontiguousarray(indices, dtype=np.int32)
+    e2a = np.ascontiguousarray(en_p2_a, dtype=np.int32)
+    e2b = np.ascontiguousarray(en_p2_b, dtype=np.int32)
+    fa = np.ascontiguousarray(field_a, dtype=np.float64)
+    fb = np.ascontiguousarray(field_b, dtype=np.float64)
+    nnz = int(indptr[-1])
+    pv = np.zeros(max(nnz, 1))
+    integral = ctypes.c_double(0.0)
+    area = ctypes.c_double(0.0)
+    rc = lib().orc_p2_inner_product(_d(pa), _i32(ea), ctypes.c_long(ea.shape[0]), _d(pb), _i32(eb), _i64(indptr),
+                                    _i32(indices), _i32(e2a), _d(fa), _i32(e2b), _d(fb), _d(pv),
+                                    ctypes.byref(integral), ctypes.byref(area))
+    if rc != 0:
+        raise RuntimeError("oracle p2 inner product failed")
+    return integral.value, area.value, pv[:nnz]
+
+
 def kahan_sum(x) -> float:
     x = np.ascontiguousarray(x, dtype=np.float64)
     return lib().orc_kahan_sum(_d(x), ctypes.c_long(x.size))

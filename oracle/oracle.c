@@ -995,6 +995,7 @@ int orc_sort_finder_1d(long nnodes_a, const double *pos_a, int stride_a, long ne
 
 void orc_free(void *p) { free(p); }
 
+
 /* ------------------------------------------------------------------ */
 /* Kahan compensated sum (Precision.F90:72-113)                         */
 /* ------------------------------------------------------------------ */
@@ -1302,5 +1303,98 @@ int orc_p1_mass(int dim, const double *pos_a, const int32_t *en_a, long nel_a,
   free(buf);
   if (integral) *integral = I.sum + I.err;
   if (measure) *measure = V.sum + V.err;
+  return 0;
+}
+
+/* P2 inner product (test_parallel_p2_inner_product_2d.F90:398-522): per
+ * supermesh triangle c of A x B, the P2 fields of A and B are interpolated
+ * at c's 3 vertices and 3 edge midpoints with the P2 basis of their own
+ * element (basis_functions_p2 :399-433, interpolate_p2 :436-451), and
+ * 2 * |c| * f_b . (M_p2 f_a) is added (:515-519), M_p2 the reference P2 mass
+ * matrix (:64-72) on the unit triangle. */
+static void p2_basis(const double *cc, const double *x, double fns[6]) {
+  const double e10 = cc[2] - cc[0], e11 = cc[3] - cc[1];
+  const double e20 = cc[4] - cc[0], e21 = cc[5] - cc[1];
+  double j11 = e21, j12 = -e20, j21 = -e11, j22 = e10;
+  const double det = j11 * j22 - j12 * j21;
+  j11 = j11 / det;
+  j12 = j12 / det;
+  j21 = j21 / det;
+  j22 = j22 / det;
+  const double d1 = x[0] - cc[0], d2 = x[1] - cc[1];
+  const double lx = j11 * d1 + j12 * d2, ly = j21 * d1 + j22 * d2;
+  fns[0] = ((1.0 - lx) - ly) * ((1.0 - 2.0 * lx) - 2.0 * ly);
+  fns[1] = lx * (2.0 * lx - 1.0);
+  fns[2] = ly * (2.0 * ly - 1.0);
+  fns[3] = (4.0 * lx) * ((1.0 - lx) - ly);
+  fns[4] = (4.0 * lx) * ly;
+  fns[5] = (4.0 * ly) * ((1.0 - lx) - ly);
+}
+
+static double p2_interp(const double *cc, const double vals[6], const double *x) {
+  double f[6];
+  p2_basis(cc, x, f);
+  double s = 0.0;
+  for (int k = 0; k < 6; ++k) s = s + f[k] * vals[k];
+  return s;
+}
+
+static const double ORC_MASS_P2[6][6] = {
+    {6.0 / 360.0, -1.0 / 360.0, -1.0 / 360.0, 0.0 / 360.0, -4.0 / 360.0, 0.0 / 360.0},
+    {-1.0 / 360.0, 6.0 / 360.0, -1.0 / 360.0, 0.0 / 360.0, 0.0 / 360.0, -4.0 / 360.0},
+    {-1.0 / 360.0, -1.0 / 360.0, 6.0 / 360.0, -4.0 / 360.0, 0.0 / 360.0, 0.0 / 360.0},
+    {0.0 / 360.0, 0.0 / 360.0, -4.0 / 360.0, 32.0 / 360.0, 16.0 / 360.0, 16.0 / 360.0},
+    {-4.0 / 360.0, 0.0 / 360.0, 0.0 / 360.0, 16.0 / 360.0, 32.0 / 360.0, 16.0 / 360.0},
+    {0.0 / 360.0, -4.0 / 360.0, 0.0 / 360.0, 16.0 / 360.0, 16.0 / 360.0, 32.0 / 360.0}};
+
+int orc_p2_inner_product(const double *pos_a, const int32_t *en_a, long nel_a, const double *pos_b,
+                         const int32_t *en_b, const int64_t *indptr, const int32_t *indices,
+                         const int32_t *en_p2_a, const double *field_a, const int32_t *en_p2_b,
+                         const double *field_b, double *pair_values, double *integral, double *area) {
+  orc_cs I = {0.0, 0.0}, V = {0.0, 0.0};
+  double buf[6 * ORC_TRI_BUF];
+  double va[6], vb[6], fa_n[6], fb_n[6];
+  for (long a = 0; a < nel_a; ++a) {
+    gather(2, 3, pos_a, en_a, a, va);
+    for (int k = 0; k < 6; ++k) fa_n[k] = field_a[en_p2_a[6 * a + k]];
+    for (int64_t p = indptr[a]; p < indptr[a + 1]; ++p) {
+      const long b = indices[p];
+      gather(2, 3, pos_b, en_b, b, vb);
+      for (int k = 0; k < 6; ++k) fb_n[k] = field_b[en_p2_b[6 * b + k]];
+      int n;
+      orc_intersect_tris(va, vb, buf, &n);
+      double sp = 0.0;
+      for (int t = 0; t < n; ++t) {
+        const double *c = buf + 6 * t;
+        const double ar = orc_triangle_area(c);
+        cs_add(&V, ar);
+        double pts[6][2];
+        for (int d = 0; d < 2; ++d) {
+          pts[0][d] = c[d];
+          pts[1][d] = c[2 + d];
+          pts[2][d] = c[4 + d];
+          pts[3][d] = 0.5 * (c[d] + c[2 + d]);
+          pts[4][d] = 0.5 * (c[2 + d] + c[4 + d]);
+          pts[5][d] = 0.5 * (c[d] + c[4 + d]);
+        }
+        double fac[6], fbc[6];
+        for (int l = 0; l < 6; ++l) {
+          fbc[l] = p2_interp(vb, fb_n, pts[l]);
+          fac[l] = p2_interp(va, fa_n, pts[l]);
+        }
+        double dot = 0.0;
+        for (int i = 0; i < 6; ++i) {
+          double mi = 0.0;
+          for (int k = 0; k < 6; ++k) mi = mi + ORC_MASS_P2[i][k] * fac[k];
+          dot = dot + fbc[i] * mi;
+        }
+        sp = sp + (2.0 * ar) * dot;
+      }
+      if (pair_values) pair_values[p] = sp;
+      cs_add(&I, sp);
+    }
+  }
+  if (integral) *integral = I.sum + I.err;
+  if (area) *area = V.sum + V.err;
   return 0;
 }

@@ -29,6 +29,7 @@
  *   src/Intersections.F90:48-71       ragged -> CSR
  *   src/Precision.F90:72-113          Kahan compensated sum
  *   src/tests/test_parallel_p1_inner_product_{2d,3d}.F90  P1 quadrature
+ *   src/tests/test_parallel_p2_inner_product_2d.F90      P2 interpolation
  *
  * Parity is pinned against the reference's own known answers and fixtures
  * (tests/test_oracle_pins.py).  The reference itself is Fortran 2008 + MPI and
@@ -131,6 +132,16 @@ int orc_p1_mass(int dim, const double *pos_a, const int32_t *en_a, long nel_a,
                 const int64_t *indptr, const int32_t *indices,
                 const double *u_a, const double *v_b, double *blocks,
                 double *integral, double *measure);
+
+/* P2 inner product over the 2D supermesh (test_parallel_p2_inner_product_2d
+ * .F90:398-522): P2 fields given by [nel][6] element-node lists (vertices
+ * 1-3, then edge midpoints 1-2, 2-3, 1-3) and node values.  pair_values
+ * [nnz] (optional) receives each candidate pair's contribution (summed over
+ * its supermesh triangles in output order); totals are compensated sums. */
+int orc_p2_inner_product(const double *pos_a, const int32_t *en_a, long nel_a, const double *pos_b,
+                         const int32_t *en_b, const int64_t *indptr, const int32_t *indices,
+                         const int32_t *en_p2_a, const double *field_a, const int32_t *en_p2_b,
+                         const double *field_b, double *pair_values, double *integral, double *area);
 
 /* Kahan compensated sum of an array (Precision.F90:72-113). */
 double orc_kahan_sum(const double *x, long n);

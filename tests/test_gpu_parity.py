@@ -275,6 +275,52 @@ def test_p1_mass_blocks_match_oracle(gpu_ctx, oracle_mod, name):
     assert diff <= 1e-12 * max(1e-300, np.abs(blocks_o).max(initial=0.0))
 
 
+def _p2_fields(A, B):
+    e2a, na, eda = M.p2_space(A[1])
+    e2b, nb, edb = M.p2_space(B[1])
+    fa = M.p1_to_p2(A[0][:, 0], na, eda) * M.p1_to_p2(A[0][:, 1], na, eda)
+    fb = M.p1_to_p2(B[0][:, 0], nb, edb) ** 2
+    return e2a, fa, e2b, fb
+
+
+def test_p2_inner_product_reference_answer(gpu_ctx, oracle_mod, ref_meshes):
+    # test_parallel_p2_inner_product_2d.F90:45-46: area 0.5, integral
+    # 2.7083333333333272e-2; per-pair contributions bit-identical to the oracle
+    A, B = ref_meshes("triangle_0_01"), ref_meshes("square_0_01")
+    e2a, fa, e2b, fb = _p2_fields(A, B)
+    integral, area, pv = gpu_ctx.p2_inner_product(A, B, e2a, fa, e2b, fb, want_pairs=True)
+    assert oracle_mod.fequals(area, 0.5) and oracle_mod.fequals(integral, 2.7083333333333272e-2)
+    n = len(pv)
+    ip_g, ind_g = gpu_ctx.get_candidates(len(A[1]), n)
+    ip_o, ind_o = oracle_mod.tree_finder(2, A, B)
+    i_o, a_o, pv_o = oracle_mod.p2_inner_product(A, B, ip_g, ind_g, e2a, fa, e2b, fb)
+    assert np.array_equal(pv, pv_o)
+    assert abs(integral - i_o) <= 1e-15 * abs(i_o) and abs(area - a_o) <= 1e-15
+
+
+@pytest.mark.parametrize("name", ["small2d_30x41", "tri2d_73x100"])
+def test_p2_inner_product_matches_oracle(gpu_ctx, oracle_mod, name):
+    dim, A, B = M.config_meshes(name)
+    e2a, fa, e2b, fb = _p2_fields(A, B)
+    integral, area, pv = gpu_ctx.p2_inner_product(A, B, e2a, fa, e2b, fb, want_pairs=True)
+    ip_g, ind_g = gpu_ctx.get_candidates(len(A[1]), len(pv))
+    i_o, a_o, pv_o = oracle_mod.p2_inner_product(A, B, ip_g, ind_g, e2a, fa, e2b, fb)
+    assert np.array_equal(pv, pv_o)
+    assert abs(integral - i_o) <= 1e-13 * abs(i_o)
+    assert abs(area - 1.0) <= 1e-12
+    # int_{[0,1]^2} x y x^2 = 1/8
+    assert abs(integral - 0.125) <= 1e-12
+
+
+def test_p2_inner_product_rejects_bad_nodes(gpu_ctx):
+    dim, A, B = M.config_meshes("small2d_3x4")
+    e2a, fa, e2b, fb = _p2_fields(A, B)
+    e2a = e2a.copy()
+    e2a[0, 4] = len(fa) + 3
+    with pytest.raises(lsm.LsmError):
+        gpu_ctx.p2_inner_product(A, B, e2a, fa, e2b, fb)
+
+
 def test_empty_and_single_element_meshes(gpu_ctx):
     dim, A, B = M.config_meshes("small2d_3x4")
     empty = (A[0], np.zeros((0, 3), dtype=np.int32))

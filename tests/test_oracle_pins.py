@@ -248,3 +248,25 @@ def test_interval_basics(oracle_mod):
     assert np.array_equal(oracle_mod.intersect_intervals([0.0, 1.0], [1.0, 0.5]), [0.5, 1.0])
     assert oracle_mod.intersect_intervals([0.0, 1.0], [1.0, 2.0]).size == 0
     assert oracle_mod.intersect_intervals([0.0, 1.0], [1.0 - 2.0 ** -50, 2.0]).size == 0
+
+
+def _p2_fields(A, B):
+    from libsupermesh_b200 import meshes as M
+
+    e2a, na, eda = M.p2_space(A[1])
+    e2b, nb, edb = M.p2_space(B[1])
+    fa = M.p1_to_p2(A[0][:, 0], na, eda) * M.p1_to_p2(A[0][:, 1], na, eda)  # x y on A
+    fb = M.p1_to_p2(B[0][:, 0], nb, edb) ** 2                               # x^2 on B
+    return e2a, fa, e2b, fb
+
+
+def test_p2_inner_product_known_answer(oracle_mod, ref_meshes):
+    # src/tests/test_parallel_p2_inner_product_2d.F90:45-46, :151-152:
+    # area 0.5, integral 2.7083333333333272e-2 (run on the unpartitioned
+    # meshes: the supermesh of the whole domain is the union of the ranks')
+    A, B = ref_meshes("triangle_0_01"), ref_meshes("square_0_01")
+    e2a, fa, e2b, fb = _p2_fields(A, B)
+    ip, ind = oracle_mod.tree_finder(2, A, B)
+    integral, area, _ = oracle_mod.p2_inner_product(A, B, ip, ind, e2a, fa, e2b, fb)
+    assert oracle_mod.fequals(area, 0.5)
+    assert oracle_mod.fequals(integral, 2.7083333333333272e-2)
