@@ -532,9 +532,17 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per block
 constexpr int kWarpTile = 32 * kSortItems;             // contiguous per warp
 }  // namespace
 
+// Exclusive scan of the digit histograms, three passes over tiles of
+// kScanU32Tile entries (16 per thread, 128-bit loads): tile sums, a scan of
+// the tile sums, then each tile scanned with its prefix.
+constexpr int kScanU32Threads = 256;
+constexpr int kScanU32Items = 16;
+constexpr int kScanU32Tile = kScanU32Threads * kScanU32Items;
+
 int64_t radix_hist_entries(int64_t n) {
   const int64_t nb = (n + kSortTile - 1) / kSortTile;
-  return 256 * (nb > 0 ? nb : 1);
+  const int64_t count = 256 * (nb > 0 ? nb : 1);
+  return count + (count + kScanU32Tile - 1) / kScanU32Tile + 1;  // + tile sums
 }
 
 // Histogram of one digit per block: hist[d * nblocks + block].
@@ -585,6 +593,91 @@ __global__ void __launch_bounds__(1024) k_scan_u32_single(int64_t count, uint32_
     const uint32_t v = data[i];
     data[i] = run;
     run += v;
+  }
+}
+
+// Block-wide exclusive scan of one value per thread (kScanU32Threads).
+__device__ __forceinline__ uint32_t block_excl_scan_u32(uint32_t v, uint32_t* total) {
+  __shared__ uint32_t wt[kScanU32Threads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) wt[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = lane < kScanU32Threads / 32 ? wt[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    if (lane < kScanU32Threads / 32) wt[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t r = inc - v + (wid > 0 ? wt[wid - 1] : 0u);
+  if (total) *total = wt[kScanU32Threads / 32 - 1];
+  __syncthreads();
+  return r;
+}
+
+// count is a multiple of kScanU32Items (histograms hold 256 entries per
+// block); data 16-byte aligned.
+__global__ void __launch_bounds__(kScanU32Threads) k_scan_u32_tiles(int64_t count, const uint32_t* __restrict__ data,
+                                                                    uint32_t* tile_sums) {
+  const int64_t base = (int64_t)blockIdx.x * kScanU32Tile + (int64_t)threadIdx.x * kScanU32Items;
+  uint32_t v = 0;
+  if (base < count) {
+    const uint4* q = reinterpret_cast<const uint4*>(data + base);
+#pragma unroll
+    for (int k = 0; k < kScanU32Items / 4; ++k) {
+      const uint4 u = q[k];
+      v += u.x + u.y + u.z + u.w;
+    }
+  }
+  uint32_t total = 0;
+  block_excl_scan_u32(v, &total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanU32Threads) k_scan_u32_apply(int64_t count, uint32_t* data,
+                                                                    const uint32_t* __restrict__ tile_prefix) {
+  const int64_t base = (int64_t)blockIdx.x * kScanU32Tile + (int64_t)threadIdx.x * kScanU32Items;
+  uint32_t e[kScanU32Items];
+  uint32_t v = 0;
+  const bool in = base < count;
+  if (in) {
+    const uint4* q = reinterpret_cast<const uint4*>(data + base);
+#pragma unroll
+    for (int k = 0; k < kScanU32Items / 4; ++k) {
+      const uint4 u = q[k];
+      e[4 * k] = u.x;
+      e[4 * k + 1] = u.y;
+      e[4 * k + 2] = u.z;
+      e[4 * k + 3] = u.w;
+    }
+#pragma unroll
+    for (int k = 0; k < kScanU32Items; ++k) v += e[k];
+  }
+  uint32_t run = block_excl_scan_u32(v, nullptr) + tile_prefix[blockIdx.x];
+  if (in) {
+    uint4* q = reinterpret_cast<uint4*>(data + base);
+#pragma unroll
+    for (int k = 0; k < kScanU32Items / 4; ++k) {
+      uint4 u;
+      u.x = run;
+      run += e[4 * k];
+      u.y = run;
+      run += e[4 * k + 1];
+      u.z = run;
+      run += e[4 * k + 2];
+      u.w = run;
+      run += e[4 * k + 3];
+      q[k] = u;
+    }
   }
 }
 
@@ -645,9 +738,14 @@ cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals,
   int32_t *vi = vals, *vo = vals_tmp;
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
-    count_launch(3);
+    const int64_t count = (int64_t)256 * nb;
+    const int ntiles = (int)((count + kScanU32Tile - 1) / kScanU32Tile);
+    uint32_t* tile_sums = hist + count;
+    count_launch(5);
     k_radix_hist<<<nb, kSortThreads, 0, s>>>(n, shift, ki, hist);
-    k_scan_u32_single<<<1, 1024, 0, s>>>((int64_t)256 * nb, hist);
+    k_scan_u32_tiles<<<ntiles, kScanU32Threads, 0, s>>>(count, hist, tile_sums);
+    k_scan_u32_single<<<1, 1024, 0, s>>>(ntiles, tile_sums);
+    k_scan_u32_apply<<<ntiles, kScanU32Threads, 0, s>>>(count, hist, tile_sums);
     k_radix_scatter<<<nb, kSortThreads, 0, s>>>(n, shift, ki, vi, ko, vo, hist);
     uint32_t* tk = ki;
     ki = ko;
