@@ -1865,15 +1865,14 @@ __global__ void __launch_bounds__(kWqWarps * 32, kWqBlocksPerSm) k_clip_tets_wq(
 // and vertices are fetched by index with shared-memory loads instead of
 // chains of selects.
 constexpr int kIxPoints = 20;  // 4 + 4 per plane
-constexpr int kIxStack = 6;    // pending tets: 2 per plane for planes 0-2
 #ifndef LSM_IX_BLOCK
-#define LSM_IX_BLOCK 224
+#define LSM_IX_BLOCK 480
 #endif
 #ifndef LSM_IX_BPS
-#define LSM_IX_BPS 2
+#define LSM_IX_BPS 1
 #endif
-// 504 B of shared memory per lane: 2 blocks of 224 threads (14 warps) fill
-// the 228 KB of an SM.
+// 480 B of shared memory per lane (the point pool; pending tets are kept in
+// registers): one block of 480 threads (15 warps) fills the 228 KB of an SM.
 constexpr int kIxBlock = LSM_IX_BLOCK;
 constexpr int kIxBlocksPerSm = LSM_IX_BPS;
 
@@ -1986,7 +1985,10 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
     int32_t* pair_nout, unsigned long long* work) {
   extern __shared__ double ix_mem[];
   IxPool<kIxBlock> pool{ix_mem + threadIdx.x};
-  unsigned* stk = reinterpret_cast<unsigned*>(ix_mem + 3 * kIxPoints * kIxBlock) + threadIdx.x;
+  // pending tets: a 120-bit shift register of 20-bit index tuples (stk_hi:
+  // stk_lo, newest in the low bits) and their planes, 2 bits each (stk_lv)
+  unsigned long long stk_lo = 0, stk_hi = 0;
+  unsigned stk_lv = 0;
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -2025,6 +2027,8 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
       sp = 0;
       kept = 0;
       nstage = 0;
+      stk_lo = stk_hi = 0;
+      stk_lv = 0;
     }
     {
       const bool want = nstage == 0 && !exhausted;
@@ -2080,17 +2084,30 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
       k = 0;
     }
     if (k > 0) {
-      const unsigned lv = (unsigned)(L + 1) << 20;
-      if (k == 3) stk[(sp++) * kIxBlock] = c2 | lv;
-      if (k >= 2) stk[(sp++) * kIxBlock] = c1 | lv;
+      const unsigned lv = (unsigned)(L + 1);
+      if (k == 3) {
+        stk_hi = (stk_hi << 20) | (stk_lo >> 44);
+        stk_lo = (stk_lo << 20) | c2;
+        stk_lv = (stk_lv << 2) | lv;
+        ++sp;
+      }
+      if (k >= 2) {
+        stk_hi = (stk_hi << 20) | (stk_lo >> 44);
+        stk_lo = (stk_lo << 20) | c1;
+        stk_lv = (stk_lv << 2) | lv;
+        ++sp;
+      }
       cur = c0;
       ++L;
       continue;
     }
     if (sp > 0) {
-      const unsigned e = stk[(--sp) * kIxBlock];
-      cur = e & 0xfffffu;
-      L = (int)(e >> 20);
+      cur = (unsigned)(stk_lo & 0xfffffull);
+      L = (int)(stk_lv & 3u);
+      stk_lo = (stk_lo >> 20) | (stk_hi << 44);
+      stk_hi >>= 20;
+      stk_lv >>= 2;
+      --sp;
       continue;
     }
     pair_measure[p] = m;
@@ -2099,7 +2116,7 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
   }
 }
 
-size_t ix_smem_bytes() { return (size_t)kIxBlock * (3 * kIxPoints * sizeof(double) + kIxStack * sizeof(unsigned)); }
+size_t ix_smem_bytes() { return (size_t)kIxBlock * 3 * kIxPoints * sizeof(double); }
 
 int wq_grid_blocks() { return sm_count() * kWqBlocksPerSm; }
 
