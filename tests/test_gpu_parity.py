@@ -91,6 +91,29 @@ def test_config_tri2d_777x1024_rot7_full(gpu_ctx, oracle_mod):
     assert st.n_candidates > 10_000_000
 
 
+def test_config_tet3d_graded_full_properties(gpu_ctx):
+    # ~1.0M x ~0.8M graded tets (56M candidates): size-independent checks
+    # instead of the oracle: the total is the cube's volume and every target
+    # element is covered exactly once (its supermesh volume is its own)
+    dim, A, B = M.config_meshes("tet3d_graded_55x51")
+    st, em = gpu_ctx.supermesh(A, B, elem_measure=True)
+    assert st.n_candidates > 50_000_000
+    assert abs(st.total_measure - 1.0) <= REL_TOL
+    v = A[0][A[1]]
+    e1, e2, e3 = v[:, 1] - v[:, 0], v[:, 2] - v[:, 0], v[:, 3] - v[:, 0]
+    own = np.abs(np.einsum("ij,ij->i", e1, np.cross(e2, e3))) / 6.0
+    assert np.all(np.abs(em - own) <= 1e-12 * own)
+    # the per-pair results do not depend on the clipper variant
+    pm, pn = gpu_ctx.pair_results(st.n_candidates)
+    lsm.set_option("tet_clipper", 2)
+    try:
+        st2 = gpu_ctx.clip_candidates()
+        pm2, pn2 = gpu_ctx.pair_results(st.n_candidates)
+    finally:
+        lsm.set_option("tet_clipper", 0)
+    assert np.array_equal(pm, pm2) and np.array_equal(pn, pn2) and st2.total_measure == st.total_measure
+
+
 def test_config_tri2d_777x1024_rot7_p1_mass(gpu_ctx, oracle_mod):
     dim, A, B = M.config_meshes("tri2d_777x1024_rot7")
     u, v = A[0][:, 0], B[0][:, 1]
