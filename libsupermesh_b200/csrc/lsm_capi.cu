@@ -39,6 +39,7 @@ struct DevBuf {
 
 struct Ctx {
   int device = 0;
+  int64_t device_mem = 0;  // total device memory
   cudaStream_t stream = nullptr;
   std::string last_error;
   int64_t bytes = 0;
@@ -165,6 +166,9 @@ int init_ctx(int device, Ctx* c) {
   if (device < 0 || device >= n) return LSM_ERROR_INVALID_ARGUMENT;
   DeviceGuard g(device);
   c->device = device;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) c->device_mem = (int64_t)total_b;
+  (void)cudaGetLastError();
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMallocHost(&c->host_scalars, 4096) != cudaSuccess || lsm::init_device_attributes() != cudaSuccess ||
       cudaEventCreate(&c->clip_ev[0]) != cudaSuccess || cudaEventCreate(&c->clip_ev[1]) != cudaSuccess) {
@@ -247,6 +251,11 @@ MeshDev upload(Ctx* c, const lsm_gpu_mesh* m, int on_device, DevBuf& pos, DevBuf
 }
 
 int* bad_flag(Ctx* c) { return ensure<int>(c, c->misc, 64); }
+
+// Device memory the candidate-row cache of the search may hold: min(4 GiB,
+// 1/32 of the device).  Only rows' actual candidates are written (4 B each);
+// the cap only bounds the row length that avoids a second traversal.
+int64_t cache_budget(Ctx* c) { return std::min<int64_t>(4ll << 30, c->device_mem / 32); }
 
 // prep of the query mesh A: coords (simplices only), box64, tol
 void prep_a(Ctx* c, const MeshDev& a, bool simplex, cudaStream_t s) {
@@ -384,9 +393,8 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   int* counts = ensure<int>(c, c->counts, nel_a);
   int64_t* stmp = ensure<int64_t>(c, c->scan_tmp, lsm::scan_tmp_entries(nel_a) + 1);
   lsm::BVH bvh{};
-  // candidate cache of the count pass: up to kCacheBytes, at most 256 per row
-  constexpr int64_t kCacheBytes = 256ll << 20;
-  const int cap = nel_a > 0 ? (int)std::min<int64_t>(256, kCacheBytes / (4 * nel_a)) : 0;
+  // candidate cache of the count pass: at most 256 per row
+  const int cap = nel_a > 0 ? (int)std::min<int64_t>(256, cache_budget(c) / (4 * nel_a)) : 0;
   int32_t* cache = cap >= 8 ? ensure<int32_t>(c, c->q_cache, nel_a * cap) : nullptr;
   int* over = cache ? ensure<int>(c, c->q_over, nel_a + 1) : nullptr;
   if (b.nel > 0 && nel_a > 0) {
@@ -653,9 +661,15 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   int64_t* offsets = ensure<int64_t>(c, c->offsets, na + 1);
   int* counts = ensure<int>(c, c->counts, na);
   int64_t* stmp = ensure<int64_t>(c, c->scan_tmp, lsm::scan_tmp_entries(na) + 1);
-  if (na > 0 && nb > 0)
+  // candidate cache of the count pass, as in find_candidates
+  const int cap = na > 0 ? (int)std::min<int64_t>(256, cache_budget(c) / (4 * na)) : 0;
+  int32_t* cache = cap >= 8 ? ensure<int32_t>(c, c->q_cache, na * cap) : nullptr;
+  int* over = cache ? ensure<int>(c, c->q_over, na + 1) : nullptr;
+  if (na > 0 && nb > 0) {
+    if (over) CU(cudaMemsetAsync(over, 0, sizeof(int), s));
     CU(lsm::launch_query_batched(dim, false, na, a_box, pair_of_a, roots, stops, bvh, b_box, counts, nullptr,
-                                 nullptr, nullptr, s));
+                                 nullptr, nullptr, s, cache, cap, over));
+  }
   else if (na > 0)
     CU(cudaMemsetAsync(counts, 0, sizeof(int) * na, s));
   CU(lsm::launch_scan(na, counts, offsets, stmp, s));
@@ -669,8 +683,8 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   int32_t* pa = ensure<int32_t>(c, c->pair_a, nnz);
   int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);
   if (nnz > 0)
-    CU(lsm::launch_query_batched(dim, true, na, a_box, pair_of_a, roots, stops, bvh, b_box, nullptr, offsets,
-                                 pa, pb, s));
+    CU(lsm::launch_query_batched(dim, true, na, a_box, pair_of_a, roots, stops, bvh, b_box, counts, offsets,
+                                 pa, pb, s, cache, cap, over));
   c->dim = dim;
   c->loc_a = c->loc_b = loc;
   c->nel_a = na;
@@ -680,8 +694,9 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   narrow(c, s);
   lsm::Partial* tot = ensure<lsm::Partial>(c, c->bt_tot, nm);
   int64_t* nc = ensure<int64_t>(c, c->bt_ncand, nm);
+  lsm::Partial* pieces = ensure<lsm::Partial>(c, c->partials, lsm::mesh_totals_pieces(nm));
   CU(lsm::launch_mesh_totals(nm, d_eoa, offsets, static_cast<double*>(c->pair_measure.p),
-                             static_cast<int32_t*>(c->pair_nout.p), tot, nc, s));
+                             static_cast<int32_t*>(c->pair_nout.p), pieces, tot, nc, s));
   const size_t bytes = sizeof(lsm::Partial) * nm + sizeof(int64_t) * nm;
   char* hs = static_cast<char*>(host_stage(c, bytes));
   CU(cudaMemcpyAsync(hs, tot, sizeof(lsm::Partial) * nm, cudaMemcpyDeviceToHost, s));

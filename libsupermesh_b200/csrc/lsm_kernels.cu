@@ -2409,9 +2409,13 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
                                                        const float4* __restrict__ hi_esc, int n,
                                                        const double* __restrict__ box64_b, int* counts,
                                                        const int64_t* __restrict__ offsets, int32_t* pair_a,
-                                                       int32_t* pair_b) {
-  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < nel_a;
-       a += (int64_t)gridDim.x * blockDim.x) {
+                                                       int32_t* pair_b, int32_t* cache, int cap,
+                                                       const int32_t* __restrict__ rows, int* over_rows) {
+  // cache / rows / over_rows: as k_query
+  const int64_t nrows = rows ? (int64_t)*over_rows : nel_a;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = rows ? rows[r] : r;
     double lo[DIM], hi[DIM];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
@@ -2450,13 +2454,18 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
           if (FILL) {
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = w;
+          } else if (cache && cnt < cap) {
+            cache[a * cap + cnt] = w;
           }
           ++cnt;
         }
       }
       node = __float_as_int(H.w);
     }
-    if (!FILL) counts[a] = cnt;
+    if (!FILL) {
+      counts[a] = cnt;
+      if (cache && cnt > cap) over_rows[1 + atomicAdd(over_rows, 1)] = (int32_t)a;
+    }
   }
 }
 
@@ -2464,58 +2473,88 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
 cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double* box64_a,
                                  const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
-                                 int32_t* pair_b, cudaStream_t s) {
+                                 int32_t* pair_b, cudaStream_t s, int32_t* cache, int cap, int* over_rows) {
   if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
   const int B = query_block();
   const int g = grid_for(nel_a, B, 2048 / B);
-  count_launch();
+  if (fill && cache) {
+    count_launch(2);
+    k_fill_from_cache<<<grid_for(nel_a, 256, 8), 256, 0, s>>>(nel_a, counts, offsets, cache, cap, pair_a, pair_b);
+  } else {
+    count_launch();
+  }
+  const int32_t* rows = (fill && cache) ? over_rows + 1 : nullptr;
+  int32_t* cc = fill ? nullptr : cache;
+#define LSM_QUERY_ARGS                                                                                         \
+  nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, \
+      pair_b, cc, cap, rows, over_rows
   if (dim == 2) {
     if (fill)
-      k_query_batched<2, true><<<g, B, 0, s>>>(nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+      k_query_batched<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
     else
-      k_query_batched<2, false><<<g, B, 0, s>>>(nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+      k_query_batched<2, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
   } else {
     if (fill)
-      k_query_batched<3, true><<<g, B, 0, s>>>(nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+      k_query_batched<3, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
     else
-      k_query_batched<3, false><<<g, B, 0, s>>>(nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b);
+      k_query_batched<3, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
   }
+#undef LSM_QUERY_ARGS
   return cudaGetLastError();
 }
 
-// Per-mesh-pair totals: block p reduces the candidates of mesh pair p (CSR
-// rows elem_off_a[p] .. elem_off_a[p+1]-1) in a fixed order.
+// Per-mesh-pair totals of the batched path (mesh pair p owns the CSR rows
+// elem_off_a[p] .. elem_off_a[p+1]-1).  Mesh pairs differ in size by
+// 100x, so each pair's candidate range is split into kMeshSplit contiguous
+// pieces reduced by separate blocks (grid nm x kMeshSplit), and the pieces
+// are merged in piece order by k_mesh_combine: deterministic, and no block
+// walks a whole large mesh alone.
+constexpr int kMeshSplit = 32;
+
 __global__ void __launch_bounds__(256) k_mesh_totals(int nm, const int64_t* __restrict__ elem_off_a,
                                                      const int64_t* __restrict__ offsets,
                                                      const double* __restrict__ pm, const int32_t* __restrict__ pn,
-                                                     Partial* out, int64_t* ncand) {
-  const int p = blockIdx.x;
+                                                     Partial* pieces) {
+  const int p = blockIdx.x, g = blockIdx.y;
   if (p >= nm) return;
   const int64_t beg = offsets[elem_off_a[p]], end = offsets[elem_off_a[p + 1]];
+  const int64_t len = end - beg;
+  const int64_t b0 = beg + len * g / kMeshSplit, b1 = beg + len * (g + 1) / kMeshSplit;
   double sum = 0.0, err = 0.0;
   unsigned long long ni = 0, no = 0;
-  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
     cs_add(sum, err, pm[i]);
     const int k = pn[i];
     ni += k > 0;
     no += k;
   }
-  __shared__ Partial r;
-  block_reduce_partial<256>(sum, err, ni, no, &r);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    Partial q = r;
-    q.sum = q.sum + q.err;
-    out[p] = q;
-    ncand[p] = end - beg;
-  }
+  block_reduce_partial<256>(sum, err, ni, no, &pieces[(int64_t)p * kMeshSplit + g]);
 }
 
+__global__ void k_mesh_combine(int nm, const int64_t* __restrict__ elem_off_a, const int64_t* __restrict__ offsets,
+                               const Partial* __restrict__ pieces, Partial* out, int64_t* ncand) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nm) return;
+  Partial q = pieces[(int64_t)p * kMeshSplit];
+  for (int g = 1; g < kMeshSplit; ++g) {
+    const Partial r = pieces[(int64_t)p * kMeshSplit + g];
+    two_sum_merge(q.sum, q.err, r.sum, r.err);
+    q.n_int += r.n_int;
+    q.n_out += r.n_out;
+  }
+  q.sum = q.sum + q.err;
+  out[p] = q;
+  ncand[p] = offsets[elem_off_a[p + 1]] - offsets[elem_off_a[p]];
+}
+
+int64_t mesh_totals_pieces(int nm) { return (int64_t)nm * kMeshSplit; }
+
 cudaError_t launch_mesh_totals(int nm, const int64_t* elem_off_a, const int64_t* offsets, const double* pm,
-                               const int32_t* pn, Partial* out, int64_t* ncand, cudaStream_t s) {
+                               const int32_t* pn, Partial* pieces, Partial* out, int64_t* ncand, cudaStream_t s) {
   if (nm <= 0) return cudaSuccess;
-  count_launch();
-  k_mesh_totals<<<nm, 256, 0, s>>>(nm, elem_off_a, offsets, pm, pn, out, ncand);
+  count_launch(2);
+  k_mesh_totals<<<dim3(nm, kMeshSplit), 256, 0, s>>>(nm, elem_off_a, offsets, pm, pn, pieces);
+  k_mesh_combine<<<(nm + 127) / 128, 128, 0, s>>>(nm, elem_off_a, offsets, pieces, out, ncand);
   return cudaGetLastError();
 }
 

@@ -207,8 +207,10 @@ cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const
 cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double* box64_a,
                                  const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
-                                 int32_t* pair_b, cudaStream_t s);
+                                 int32_t* pair_b, cudaStream_t s, int32_t* cache = nullptr, int cap = 0,
+                                 int* over_rows = nullptr);
+int64_t mesh_totals_pieces(int nm);  // Partial scratch entries for launch_mesh_totals
 cudaError_t launch_mesh_totals(int nm, const int64_t* elem_off_a, const int64_t* offsets, const double* pm,
-                               const int32_t* pn, Partial* out, int64_t* ncand, cudaStream_t s);
+                               const int32_t* pn, Partial* pieces, Partial* out, int64_t* ncand, cudaStream_t s);
 
 }  // namespace lsm
