@@ -66,6 +66,10 @@ struct Ctx {
   void* host_scalars = nullptr;
   // events around the clip kernel of the last narrow phase (option time_kernels)
   cudaEvent_t clip_ev[2] = {nullptr, nullptr};
+  // side stream for mesh A's upload and prep (overlaps B's tree build) and
+  // the events that order it with the caller's stream
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_ev[2] = {nullptr, nullptr};
   bool clip_timed = false;
 
   // state of the last candidate search
@@ -171,7 +175,10 @@ int init_ctx(int device, Ctx* c) {
   (void)cudaGetLastError();
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMallocHost(&c->host_scalars, 4096) != cudaSuccess || lsm::init_device_attributes() != cudaSuccess ||
-      cudaEventCreate(&c->clip_ev[0]) != cudaSuccess || cudaEventCreate(&c->clip_ev[1]) != cudaSuccess) {
+      cudaEventCreate(&c->clip_ev[0]) != cudaSuccess || cudaEventCreate(&c->clip_ev[1]) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->side_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->side_ev[1], cudaEventDisableTiming) != cudaSuccess) {
     (void)cudaGetLastError();
     return LSM_ERROR_CUDA;
   }
@@ -198,6 +205,16 @@ void fini_ctx(Ctx* c) {
       cudaEventDestroy(e);
       e = nullptr;
     }
+  for (cudaEvent_t& e : c->side_ev)
+    if (e) {
+      cudaEventDestroy(e);
+      e = nullptr;
+    }
+  if (c->side) {
+    cudaStreamSynchronize(c->side);
+    cudaStreamDestroy(c->side);
+    c->side = nullptr;
+  }
   if (c->host_scalars) cudaFreeHost(c->host_scalars);
   if (c->host_stage) cudaFreeHost(c->host_stage);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -383,10 +400,15 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   c->ncand = -1;
   c->simplex_prep = false;
   simplex = simplex || (ma->loc == ma->dim + 1 && mb->loc == mb->dim + 1);
-  MeshDev a = upload(c, ma, on_device, c->a_pos, c->a_en, s);
-  MeshDev b = upload(c, mb, on_device, c->b_pos, c->b_en, s);
+  // A's upload and prep run on the side stream, overlapping B's upload,
+  // prep and tree build on s; s waits for them before the search.
   CU(cudaMemsetAsync(bad_flag(c), 0, sizeof(int) * 64, s));
-  prep_a(c, a, simplex, s);
+  CU(cudaEventRecord(c->side_ev[0], s));
+  CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
+  MeshDev b = upload(c, mb, on_device, c->b_pos, c->b_en, s);
+  MeshDev a = upload(c, ma, on_device, c->a_pos, c->a_en, c->side);
+  prep_a(c, a, simplex, c->side);
+  CU(cudaEventRecord(c->side_ev[1], c->side));
   prep_b(c, b, simplex, want_b_coords, s);
   const int64_t nel_a = a.nel;
   int64_t* offsets = ensure<int64_t>(c, c->offsets, nel_a + 1);
@@ -400,11 +422,13 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   if (b.nel > 0 && nel_a > 0) {
     bvh = build_tree(c, b, s);
     if (over) CU(cudaMemsetAsync(over, 0, sizeof(int), s));
+    CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
     CU(lsm::launch_query(a.dim, false, nel_a, static_cast<double*>(c->a_box64.p), bvh,
                          static_cast<double*>(c->b_box64.p), counts, nullptr, nullptr, nullptr, s, cache, cap,
                          over));
-  } else if (nel_a > 0) {
-    CU(cudaMemsetAsync(counts, 0, sizeof(int) * nel_a, s));
+  } else {
+    CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
+    if (nel_a > 0) CU(cudaMemsetAsync(counts, 0, sizeof(int) * nel_a, s));
   }
   CU(lsm::launch_scan(nel_a, counts, offsets, stmp, s));
   int64_t* h = static_cast<int64_t*>(c->host_scalars) + 8;
