@@ -167,6 +167,24 @@ def test_autotuner_keeps_results(gpu_ctx, tmp_path, monkeypatch):
         lsm.set_option(n, v)
 
 
+def test_clip_kernel_timing_option(gpu_ctx):
+    """time_kernels records events around the clip kernel; without the
+    option the timing entry reports a state error."""
+    dim, A, B = M.config_meshes("small3d_8x9")
+    lsm.set_option("time_kernels", 0)
+    gpu_ctx.supermesh(A, B)
+    with pytest.raises(lsm.LsmError) as e:
+        gpu_ctx.clip_kernel_ms()
+    assert e.value.status == 6  # LSM_ERROR_STATE
+    lsm.set_option("time_kernels", 1)
+    try:
+        st = gpu_ctx.clip_candidates()
+        ms = gpu_ctx.clip_kernel_ms()
+    finally:
+        lsm.set_option("time_kernels", 0)
+    assert st.n_candidates > 0 and 0.0 < ms < 1000.0
+
+
 def test_int64_and_int32_enlists_agree(gpu_ctx):
     dim, A, B = M.config_meshes("small3d_5x6")
     s32, _ = gpu_ctx.supermesh(A, B)
