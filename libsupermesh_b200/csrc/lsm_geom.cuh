@@ -142,6 +142,33 @@ __device__ __forceinline__ void poly_lines(const double* v, double* nx, double* 
   }
 }
 
+// Keep test of a final tet (vol_v4 >= tol) and its vertex-1 volume, with
+// the vertex-4 volume evaluated only when needed.  Both volumes are |det|/6
+// of the same four points through different edges; each computed det is
+// within 8u T of the exact one, T the sum of the absolute monomials, T <= L^3
+// for the vertex-1 edges and <= 4 L^3 for the vertex-4 edges (L the largest
+// L1 length of the vertex-1 edges, u = 2^-53), so |v1 - v4| <= 7.4u L^3 + 2u
+// v1.  bnd = 64u L^3 (+ an absolute term for subnormal results) bounds it
+// with room to spare: if v1 clears tol by bnd the outcome of v4 >= tol is
+// known; otherwise v4 is computed and compared as the reference does.
+// Overflow or NaN make both quick comparisons false and take the exact path.
+__device__ __forceinline__ bool final_tet_keep(const Tet& t, double tol, double& v1) {
+  const double e1x = t.x[1] - t.x[0], e1y = t.y[1] - t.y[0], e1z = t.z[1] - t.z[0];
+  const double e2x = t.x[2] - t.x[0], e2y = t.y[2] - t.y[0], e2z = t.z[2] - t.z[0];
+  const double e3x = t.x[3] - t.x[0], e3y = t.y[3] - t.y[0], e3z = t.z[3] - t.z[0];
+  double s = e1x * (e2y * e3z - e2z * e3y) + e1y * (e2z * e3x - e2x * e3z);
+  s = s + e1z * (e2x * e3y - e2y * e3x);
+  v1 = (1.0 / 6.0) * fabs(s);
+  const double l1 = (fabs(e1x) + fabs(e1y)) + fabs(e1z);
+  const double l2 = (fabs(e2x) + fabs(e2y)) + fabs(e2z);
+  const double l3 = (fabs(e3x) + fabs(e3y)) + fabs(e3z);
+  const double L = fmax(l1, fmax(l2, l3));
+  const double bnd = 0x1p-47 * (L * L * L) + 0x1p-1016;
+  if (v1 >= tol + bnd) return true;
+  if (v1 < tol - bnd) return false;
+  return tet_volume_v4(t) >= tol;
+}
+
 // ------------------------------------------------------------- tet setup
 struct Planes {
   double nx[4], ny[4], nz[4], c[4];

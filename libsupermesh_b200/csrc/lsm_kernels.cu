@@ -1392,8 +1392,11 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 // them (a schedule); survivors are appended in that order, warp by warp.
 // RECORDS: survivors are written as {pair, a, b, 0} so that the clipper gets
 // the element numbers with the pair number in one load.
+#ifndef LSM_PREFILTER_BPS
+#define LSM_PREFILTER_BPS 1
+#endif
 template <bool RECORDS>
-__global__ void __launch_bounds__(256) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ order,
+__global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ order,
                                                         const int32_t* __restrict__ pa,
                                                         const int32_t* __restrict__ pb,
                                                         const double* __restrict__ coords_a,
@@ -2075,8 +2078,9 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
         if (j < k) {
           Tet o;
           ix_gather(pool, j == 0 ? c0 : (j == 1 ? c1 : c2), o);
-          if (tet_volume_v4(o) >= tol) {
-            m = m + tet_volume_v1(o);
+          double v1;
+          if (final_tet_keep(o, tol, v1)) {
+            m = m + v1;
             ++kept;
           }
         }
