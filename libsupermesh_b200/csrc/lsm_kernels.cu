@@ -3,17 +3,27 @@
 //   K1  k_prep          element gather, FP64/FP32 boxes, measures, tolerances,
 //                       B-element clip setup (lines / unit-normal planes)
 //   K1b k_root_*        root box reduction;  k_morton  Morton keys
-//   K2  radix sort      stable LSD, 8-bit digits, warp-match ranking
+//   K2  radix sort      stable LSD, 8-bit digits, warp-match ranking;
+//                       coalesced three-pass histogram scan
 //   K3  k_bvh_internal  Karras LBVH hierarchy + rope table;
 //       k_bvh_refit     bottom-up FP32 box refit, escape links
 //   K4  k_query         stackless LBVH traversal per A element (FP32,
-//                       outward-rounded boxes) + exact strict FP64 box test
+//                       outward-rounded boxes) + exact strict FP64 box test;
+//                       the count pass caches rows, k_fill_from_cache copies
 //   K5  k_clip_tris     one candidate pair per thread, polygon in shared
 //                       memory, FP64 Sutherland-Hodgman
-//   K6  k_clip_tets     one candidate pair per thread, depth-first plane
-//                       clipping with a shared-memory tet stack
-//   K7  compensated reductions (per-block (sum, err), then final)
-//   K8  k_p1_mass       P1-P1 mixed mass blocks + u^T M v
+//   K6  k_prefilter_tets exact early-out; k_clip_tets_ix (default) depth-first
+//                       clipping over point indices with a refill pipeline;
+//                       k_clip_tets (tets in registers), k_clip_tets_wq
+//                       (per-warp task queues) as alternatives
+//   K7  compensated reductions (per-block (sum, err), then final; per mesh
+//                       pair for the batched path)
+//   K8  k_p1_mass       P1-P1 mixed mass blocks + u^T M v;  k_p2_inner  P2
+//                       inner product
+//   K9  1D sort finder  k_prep_1d, 64-bit stable sort, max segment tree,
+//                       k_rows_1d, k_sweep_1d, k_emit_1d;  k_clip_intervals
+//   K10 explicit pairs  k_pairs_tris / _tets and the mixed element pairs
+//                       (intervals, tri-quad, quad-quad, tet-hex, hex-hex)
 //
 // Everything FP64 is compiled with -fmad=false so that each +,-,*,/ is a
 // separately rounded IEEE operation, matching libsupermesh's gfortran build.
@@ -36,9 +46,9 @@ namespace {
 int g_tet_bps = 0;
 }  // namespace
 
-// Blocks per SM of the persistent tet clipper (3: up to 170 registers per
-// thread, no spills; 4: up to 128, spills).  Default 3 (measured faster on
-// B200); LSM_TET_BLOCKS_PER_SM overrides it.
+// Blocks per SM of the register tet clipper, variant 2 (3: up to 170
+// registers per thread, no spills; 4: up to 128, spills).  Default 3
+// (measured faster on B200); LSM_TET_BLOCKS_PER_SM overrides it.
 int tet_blocks_per_sm() {
   if (g_tet_bps == 0) {
     const char* e = getenv("LSM_TET_BLOCKS_PER_SM");
