@@ -79,6 +79,9 @@ int64_t libsupermesh_gpu_kernel_launches(void);
  *   "query_block"        64, 128 (default) or 256 threads per block (candidate search)
  *   "time_kernels"       1: record CUDA events around the clip kernel of every
  *                        narrow phase (read with libsupermesh_gpu_clip_kernel_ms); 0 (default)
+ *   "tet_screen"         1 (default): tet pairs whose B lies beyond a face plane of A by a
+ *                        proven rounding margin skip the clipper (exact: the reference
+ *                        returns no tets for them); 0: only the A-beyond-a-face-of-B test
  * Unknown names or values return LSM_ERROR_INVALID_ARGUMENT. */
 int libsupermesh_gpu_set_option(const char *name, int64_t value);
 int libsupermesh_gpu_get_option(const char *name, int64_t *value);
@@ -87,6 +90,12 @@ int libsupermesh_gpu_get_option(const char *name, int64_t *value);
  * CUDA events recorded on its stream (needs option time_kernels = 1 during
  * that phase; waits for the kernel to finish). */
 int libsupermesh_gpu_clip_kernel_ms(lsm_gpu_context *ctx, double *ms);
+
+/* Pairs of the last 3D narrow phase on ctx that the exact early-outs left
+ * for the clipper (the others were proven to give no tets).  Waits for the
+ * device.  LSM_ERROR_STATE if no 3D narrow phase ran since the last
+ * candidate search. */
+int libsupermesh_gpu_clip_survivors(lsm_gpu_context *ctx, int64_t *n);
 
 /* Candidate search only (tree finder): the work of
  * tree_intersection_finder_set_input_c (C_bindings.F90:346-366) on the GPU.

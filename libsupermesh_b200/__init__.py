@@ -100,6 +100,8 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_kernel_launches.argtypes = []
     L.libsupermesh_gpu_clip_kernel_ms.argtypes = [vp, _dp]
     L.libsupermesh_gpu_clip_kernel_ms.restype = ctypes.c_int
+    L.libsupermesh_gpu_clip_survivors.argtypes = [vp, _i64p]
+    L.libsupermesh_gpu_clip_survivors.restype = ctypes.c_int
     L.libsupermesh_gpu_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
     L.libsupermesh_gpu_set_option.restype = ctypes.c_int
     L.libsupermesh_gpu_get_option.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
@@ -246,6 +248,13 @@ class Context:
         time_kernels must have been on)."""
         r = ctypes.c_double(0.0)
         self._check(self.lib.libsupermesh_gpu_clip_kernel_ms(self._h, ctypes.byref(r)))
+        return r.value
+
+    def clip_survivors(self) -> int:
+        """Pairs of the last 3D narrow phase that the exact early-outs left
+        for the clipper."""
+        r = ctypes.c_int64(0)
+        self._check(self.lib.libsupermesh_gpu_clip_survivors(self._h, ctypes.byref(r)))
         return r.value
 
     def pair_results(self, n: int):

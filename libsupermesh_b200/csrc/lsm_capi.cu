@@ -30,6 +30,8 @@ namespace {
 // Option time_kernels: record events around the clip kernel of every narrow
 // phase (libsupermesh_gpu_clip_kernel_ms reads them).
 bool g_time_kernels = false;
+// second exact early-out of the tet clipper (B beyond a face of A)
+bool g_tet_screen = true;
 
 // ------------------------------------------------------------------ buffers
 struct DevBuf {
@@ -45,9 +47,9 @@ struct Ctx {
   int64_t bytes = 0;
 
   // mesh A (query side)
-  DevBuf a_pos, a_en, a_coords, a_box64, a_tol;
+  DevBuf a_pos, a_en, a_coords, a_box64, a_tol, a_faces, surv;
   // mesh B (tree side)
-  DevBuf b_pos, b_en, b_coords, b_box64, b_box32, b_setup;
+  DevBuf b_pos, b_en, b_coords, b_box64, b_box32, b_setup, b_screen;
   // tree
   DevBuf keys, vals, keys_tmp, vals_tmp, hist, root_partial, rootbox, bvh_lo, bvh_hi, bvh_work;
   // candidates
@@ -71,6 +73,7 @@ struct Ctx {
   cudaStream_t side = nullptr;
   cudaEvent_t side_ev[2] = {nullptr, nullptr};
   bool clip_timed = false;
+  bool surv_valid = false;  // surv holds the clipper's pair count of the last 3D narrow phase
 
   // state of the last candidate search
   int dim = 0;
@@ -198,7 +201,8 @@ void fini_ctx(Ctx* c) {
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
                    &c->bt_ncand, &c->bt_stage_pa, &c->bt_stage_ea, &c->bt_stage_pb, &c->bt_stage_eb,
                    &c->d1_keyhi, &c->d1_perm_a, &c->d1_perm_b, &c->d1_lo_a, &c->d1_hi_a, &c->d1_lo_b,
-                   &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over};
+                   &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over,
+                   &c->a_faces, &c->b_screen, &c->surv};
   for (DevBuf* b : all) free_buf(*b);
   for (cudaEvent_t& e : c->clip_ev)
     if (e) {
@@ -274,13 +278,15 @@ int* bad_flag(Ctx* c) { return ensure<int>(c, c->misc, 64); }
 // the cap only bounds the row length that avoids a second traversal.
 int64_t cache_budget(Ctx* c) { return std::min<int64_t>(4ll << 30, c->device_mem / 32); }
 
-// prep of the query mesh A: coords (simplices only), box64, tol
+// prep of the query mesh A: coords (simplices only), box64, tol; tets also
+// get their face planes for the clipper's separation screen
 void prep_a(Ctx* c, const MeshDev& a, bool simplex, cudaStream_t s) {
   double* coords = simplex ? ensure<double>(c, c->a_coords, a.nel * a.loc * a.dim) : nullptr;
   double* box = ensure<double>(c, c->a_box64, a.nel * 2 * a.dim);
   double* tol = simplex ? ensure<double>(c, c->a_tol, a.nel) : nullptr;
+  double* faces = simplex && a.dim == 3 ? ensure<double>(c, c->a_faces, a.nel * lsm::kScreen3) : nullptr;
   CU(lsm::launch_prep(a.dim, a.loc, a.nel, a.pos, a.en, a.idx_bytes, coords, box, nullptr, tol, nullptr,
-                      bad_flag(c), a.nnodes, s));
+                      bad_flag(c), a.nnodes, s, faces));
 }
 
 void prep_b(Ctx* c, const MeshDev& b, bool simplex, bool want_coords, cudaStream_t s) {
@@ -289,8 +295,9 @@ void prep_b(Ctx* c, const MeshDev& b, bool simplex, bool want_coords, cudaStream
   float* box32 = ensure<float>(c, c->b_box32, b.nel * 8);
   double* setup = nullptr;
   if (simplex) setup = ensure<double>(c, c->b_setup, b.nel * (b.dim == 2 ? lsm::kSetup2 : lsm::kSetup3));
+  double* screen = simplex && b.dim == 3 ? ensure<double>(c, c->b_screen, b.nel * lsm::kScreen3) : nullptr;
   CU(lsm::launch_prep(b.dim, b.loc, b.nel, b.pos, b.en, b.idx_bytes, coords, box, box32, nullptr, setup,
-                      bad_flag(c), b.nnodes, s));
+                      bad_flag(c), b.nnodes, s, nullptr, screen));
 }
 
 lsm::BVH build_tree(Ctx* c, const MeshDev& b, cudaStream_t s) {
@@ -384,6 +391,7 @@ void find_candidates_1d(Ctx* c, const MeshDev& a, const MeshDev& b, cudaStream_t
 void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int on_device, bool simplex,
                      bool want_b_coords, cudaStream_t s, bool intervals = false) {
   intervals = intervals || (ma && ma->dim == 1);
+  c->surv_valid = false;
   check_mesh(c, ma, "A", simplex, intervals);
   check_mesh(c, mb, "B", simplex, intervals);
   c->have_pairs = false;
@@ -478,12 +486,15 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
     return;
   }
   bool queued = false;
+  const bool screen = c->dim == 3 && g_tet_screen;
   if (c->dim == 3 && lsm::tet_clipper_variant() == 1) {
     int* err = bad_flag(c) + 16;
     unsigned char* scr = ensure<unsigned char>(c, c->wq_scratch, (int64_t)lsm::wq_scratch_bytes());
     CU(lsm::launch_clip_tets_wq(nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                                 static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
-                                static_cast<double*>(c->b_setup.p), pm, pn, ovf, work, scr, err, s, order));
+                                static_cast<double*>(c->b_setup.p), pm, pn, ovf, work, scr, err, s, order,
+                                screen ? static_cast<double*>(c->a_faces.p) : nullptr,
+                                screen ? static_cast<double*>(c->b_screen.p) : nullptr));
     int* h = static_cast<int*>(c->host_scalars) + 4;
     CU(cudaMemcpyAsync(h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(h + 2, work, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -497,8 +508,15 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
     CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                         static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                         static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order,
-                        g_time_kernels ? c->clip_ev[0] : nullptr, g_time_kernels ? c->clip_ev[1] : nullptr));
+                        g_time_kernels ? c->clip_ev[0] : nullptr, g_time_kernels ? c->clip_ev[1] : nullptr,
+                        screen ? static_cast<double*>(c->a_faces.p) : nullptr,
+                        screen ? static_cast<double*>(c->b_screen.p) : nullptr));
   c->clip_timed = !queued && g_time_kernels;
+  if (c->dim == 3) {
+    CU(cudaMemcpyAsync(ensure<unsigned long long>(c, c->surv, 1), work, sizeof(unsigned long long),
+                       cudaMemcpyDeviceToDevice, s));
+    c->surv_valid = true;
+  }
   if (c->dim == 2)
     CU(lsm::launch_clip_tris_wide(ovf, ovf_count, nnz, static_cast<int32_t*>(c->pair_a.p),
                                   static_cast<int32_t*>(c->pair_b.p), static_cast<double*>(c->a_coords.p),
@@ -564,6 +582,7 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   const int nm = (int)idx.size();
   const int ib = ma[idx[0]].index_bytes;
   const int loc = dim + 1;
+  c->surv_valid = false;
   // host tables: elem_off_a[nm+1] elem_off_b[nm+1] nnodes_a[nm] nnodes_b[nm]
   //              pos_a[nm] en_a[nm] pos_b[nm] en_b[nm]
   const size_t tab_words = 2 * (nm + 1) + 6 * (size_t)nm;
@@ -645,10 +664,12 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   float* b_box32 = ensure<float>(c, c->b_box32, nb * 8);
   double* b_setup = ensure<double>(c, c->b_setup, nb * (dim == 2 ? lsm::kSetup2 : lsm::kSetup3));
   int32_t* pair_of_b = ensure<int32_t>(c, c->bt_pair_b, nb);
+  double* a_faces = dim == 3 ? ensure<double>(c, c->a_faces, na * lsm::kScreen3) : nullptr;
+  double* b_screen = dim == 3 ? ensure<double>(c, c->b_screen, nb * lsm::kScreen3) : nullptr;
   CU(lsm::launch_prep_batched(dim, na, nm, d_eoa, d_pta, d_eta, d_nna, ib, a_coords, a_box, nullptr, a_tol,
-                              nullptr, pair_of_a, bad, s));
+                              nullptr, pair_of_a, bad, s, a_faces));
   CU(lsm::launch_prep_batched(dim, nb, nm, d_eob, d_ptb, d_etb, d_nnb, ib, nullptr, b_box, b_box32, nullptr,
-                              b_setup, pair_of_b, bad, s));
+                              b_setup, pair_of_b, bad, s, nullptr, b_screen));
   // tree over all B meshes
   lsm::BVH bvh;
   bvh.n = (int)nb;
@@ -1006,6 +1027,8 @@ int libsupermesh_gpu_set_option(const char* name, int64_t value) {
     lsm::set_query_block((int)value);
   } else if (n == "time_kernels" && (value == 0 || value == 1)) {
     g_time_kernels = value == 1;
+  } else if (n == "tet_screen" && (value == 0 || value == 1)) {
+    g_tet_screen = value == 1;
   } else {
     return LSM_ERROR_INVALID_ARGUMENT;
   }
@@ -1025,6 +1048,8 @@ int libsupermesh_gpu_get_option(const char* name, int64_t* value) {
     *value = lsm::query_block();
   else if (n == "time_kernels")
     *value = g_time_kernels ? 1 : 0;
+  else if (n == "tet_screen")
+    *value = g_tet_screen ? 1 : 0;
   else
     return LSM_ERROR_INVALID_ARGUMENT;
   return LSM_SUCCESS;
@@ -1042,6 +1067,21 @@ int libsupermesh_gpu_clip_kernel_ms(lsm_gpu_context* ctx, double* ms) {
     float f = 0.0f;
     CU(cudaEventElapsedTime(&f, c->clip_ev[0], c->clip_ev[1]));
     *ms = (double)f;
+  });
+}
+
+int libsupermesh_gpu_clip_survivors(lsm_gpu_context* ctx, int64_t* n) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(n != nullptr, "NULL output");
+    if (!c->surv_valid) {
+      set_error(c, "no 3D narrow phase since the last candidate search");
+      throw Fail{LSM_ERROR_STATE};
+    }
+    CU(cudaDeviceSynchronize());
+    unsigned long long v = 0;
+    CU(cudaMemcpy(&v, c->surv.p, sizeof(v), cudaMemcpyDeviceToHost));
+    *n = (int64_t)v;
   });
 }
 

@@ -209,6 +209,112 @@ __device__ __forceinline__ void tet_planes(const Tet& t, Planes& P) {
   for (int i = 0; i < 4; ++i) P.c[i] = (t.x[i] * P.nx[i] + t.y[i] * P.ny[i]) + t.z[i] * P.nz[i];
 }
 
+// ------------------------------------------------ separation screen (3D)
+// Data for the second exact early-out of the tet clipper, which proves that
+// B lies beyond a face plane of A (the first one, in the prefilter, proves
+// that A lies beyond a face plane of B).  Notation: u = 2^-53, M bounds the
+// coordinates of A and B and the plane offsets c of B.
+//
+// (1) Every vertex the reference's clipping of A creates is a rounded convex
+//     combination of A's vertices: one interpolation w0*vp + w1*vn has
+//     w0, w1 in [0, 1+3u], w0 + w1 = 1 +- 3u and 2u rounding per coordinate,
+//     so it lies within 8.7u*M' of an exact convex combination; four nested
+//     levels stay within 36u*M.  For any direction n (|n| <= 1 + 6u),
+//     n.p <= max_k n.a_k + 40u*M.  faces_a keeps h = that maximum plus
+//     128*eps*(1 + M) (eps = 2u), which also covers the rounding of n.a_k.
+// (2) Every vertex of every tet left after B's four planes satisfies
+//     n_L.v - c_L <= e for all four planes (exact arithmetic on the stored
+//     plane coefficients) with e = 2^-52 + 48u(M + |c|): it was classified
+//     non-positive (computed d < 2^-52), or created on plane L (exact d
+//     within 19u(M+|c|) of 0), and later interpolations of such vertices add
+//     at most 7u(M+|c|) each.  So those vertices lie in
+//     B+ = {x : n_L.x <= c_L + e, L = 0..3}.
+// (3) If the four stored normals positively span R^3 (the signed 3x3
+//     cofactors D_k all share one sign), B+ is bounded, and each of its
+//     vertices is some v+_k = M_k^-1 (c + e), M_k = the three normals through
+//     vertex k; |v+_k - b_k| <= sqrt3 |M_k^-1| (e + tau)
+//     <= 3.01 (e + tau) / |det M_k|, tau = the largest residual
+//     |n_L.b_k - c_L| of a stored plane at one of its own vertices.
+//     screen_b keeps g = 3.02 / (min|D_k| - 1e-14) (+inf when the sign test
+//     or the margin fails) and tau plus its own rounding.
+// (4) If min_j n.b_j - 1.01 g (tau + e) > h for a face n of A, B+ and the
+//     derived vertices are disjoint: no tet survives B's four planes and the
+//     reference returns 0 tets.  The prefilter applies this with e bounded
+//     by 2^-52 + 128*eps*(1 + 2M) and an extra 16*eps*(1 + M) for the
+//     rounding of n.b_j.
+//
+// faces_a [nel][16]: 4 x (nx, ny, nz, h) of A's outward face planes.
+// screen_b [nel][16]: B's 4 vertices (x, y, z), g, tau, M_B, 0.
+__device__ __forceinline__ double max_abs_tet(const Tet& t) {
+  double M = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) M = fmax(M, fmax(fabs(t.x[k]), fmax(fabs(t.y[k]), fabs(t.z[k]))));
+  return M;
+}
+
+__device__ __forceinline__ double pos_inf() { return __longlong_as_double(0x7ff0000000000000ll); }
+
+__device__ __forceinline__ void tet_faces_screen(const Tet& t, double* o) {
+  Planes P;
+  tet_planes(t, P);
+  const double drift = 128.0 * kEps * (1.0 + max_abs_tet(t));
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double h = -pos_inf();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) h = fmax(h, (P.nx[i] * t.x[k] + P.ny[i] * t.y[k]) + P.nz[i] * t.z[k]);
+    o[4 * i + 0] = P.nx[i];
+    o[4 * i + 1] = P.ny[i];
+    o[4 * i + 2] = P.nz[i];
+    o[4 * i + 3] = h + drift;
+  }
+}
+
+__device__ __forceinline__ double det3(double ax, double ay, double az, double bx, double by, double bz,
+                                       double cx, double cy, double cz) {
+  return (ax * (by * cz - bz * cy) + ay * (bz * cx - bx * cz)) + az * (bx * cy - by * cx);
+}
+
+__device__ __forceinline__ void tet_screen_b(const Tet& t, const Planes& P, double* o) {
+  double M = max_abs_tet(t);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) M = fmax(M, fabs(P.c[i]));
+  // residuals of each plane at its three own vertices (plane f omits vertex 3-f)
+  double tau = 0.0;
+#pragma unroll
+  for (int f = 0; f < 4; ++f)
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k != 3 - f)
+        tau = fmax(tau, fabs(((P.nx[f] * t.x[k] + P.ny[f] * t.y[k]) + P.nz[f] * t.z[k]) - P.c[f]));
+  // D_j = (-1)^j det(normals other than j, in index order); sum_j D_j n_j = 0
+  double D[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int r0 = j == 0 ? 1 : 0;
+    const int r1 = j <= 1 ? 2 : 1;
+    const int r2 = j <= 2 ? 3 : 2;
+    const double d = det3(P.nx[r0], P.ny[r0], P.nz[r0], P.nx[r1], P.ny[r1], P.nz[r1], P.nx[r2], P.ny[r2],
+                          P.nz[r2]);
+    D[j] = (j & 1) ? -d : d;
+  }
+  const double kDetErr = 1e-14;
+  const bool pos = D[0] > kDetErr && D[1] > kDetErr && D[2] > kDetErr && D[3] > kDetErr;
+  const bool neg = D[0] < -kDetErr && D[1] < -kDetErr && D[2] < -kDetErr && D[3] < -kDetErr;
+  const double dmin = fmin(fmin(fabs(D[0]), fabs(D[1])), fmin(fabs(D[2]), fabs(D[3])));
+  const double g = (pos || neg) ? 3.02 / (dmin - kDetErr) : pos_inf();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    o[3 * k + 0] = t.x[k];
+    o[3 * k + 1] = t.y[k];
+    o[3 * k + 2] = t.z[k];
+  }
+  o[12] = g;
+  o[13] = tau + 16.0 * kEps * (1.0 + 2.0 * M);
+  o[14] = M;
+  o[15] = 0.0;
+}
+
 // Face planes of a hexahedron in Gmsh node order (Supermesh.F90:262-280):
 // plane f = unit_cross(h[a] - h[b], h[c] - h[d]) with offset h[b] . n; no
 // orientation fix-up.

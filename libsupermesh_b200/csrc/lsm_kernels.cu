@@ -172,7 +172,7 @@ template <int DIM, int LOC, typename IDX>
 __device__ __forceinline__ void prep_element(int64_t e, const double* __restrict__ pos,
                                              const IDX* __restrict__ row, int64_t nnodes, double* coords,
                                              double* box64, float* box32, double* tolv, double* setup,
-                                             int* bad) {
+                                             int* bad, double* faces = nullptr, double* screen = nullptr) {
   constexpr bool SIMPLEX = LOC == DIM + 1;
   double v[LOC * DIM];
   bool ok = true;
@@ -266,17 +266,22 @@ __device__ __forceinline__ void prep_element(int64_t e, const double* __restrict
       o[17] = 0.0;
       o[18] = 0.0;
       o[19] = 0.0;
+      if (screen) tet_screen_b(t, P, screen + e * kScreen3);
     }
+  }
+  if constexpr (DIM == 3) {
+    if (faces) tet_faces_screen(t, faces + e * kScreen3);
   }
 }
 
 template <int DIM, int LOC, typename IDX>
 __global__ void k_prep(int64_t nel, const double* __restrict__ pos, const IDX* __restrict__ en,
                        double* coords, double* box64, float* box32, double* tolv, double* setup,
-                       int* bad, int64_t nnodes) {
+                       int* bad, int64_t nnodes, double* faces, double* screen) {
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
        e += (int64_t)gridDim.x * blockDim.x)
-    prep_element<DIM, LOC, IDX>(e, pos, en + e * LOC, nnodes, coords, box64, box32, tolv, setup, bad);
+    prep_element<DIM, LOC, IDX>(e, pos, en + e * LOC, nnodes, coords, box64, box32, tolv, setup, bad, faces,
+                                screen);
 }
 
 // Batched prep over the concatenation of many meshes.  Element e belongs to
@@ -299,7 +304,8 @@ __global__ void k_prep_batched(int64_t nel, int nm, const int64_t* __restrict__ 
                                const unsigned long long* __restrict__ pos_ptr,
                                const unsigned long long* __restrict__ en_ptr,
                                const int64_t* __restrict__ nnodes, double* coords, double* box64,
-                               float* box32, double* tolv, double* setup, int32_t* pair_of, int* bad) {
+                               float* box32, double* tolv, double* setup, int32_t* pair_of, int* bad,
+                               double* faces, double* screen) {
   constexpr int LOC = DIM + 1;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
        e += (int64_t)gridDim.x * blockDim.x) {
@@ -307,7 +313,8 @@ __global__ void k_prep_batched(int64_t nel, int nm, const int64_t* __restrict__ 
     const int64_t local = e - elem_off[p];
     const double* pos = reinterpret_cast<const double*>(pos_ptr[p]);
     const IDX* en = reinterpret_cast<const IDX*>(en_ptr[p]);
-    prep_element<DIM, LOC, IDX>(e, pos, en + local * LOC, nnodes[p], coords, box64, box32, tolv, setup, bad);
+    prep_element<DIM, LOC, IDX>(e, pos, en + local * LOC, nnodes[p], coords, box64, box32, tolv, setup, bad,
+                                faces, screen);
     pair_of[e] = p;
   }
 }
@@ -315,28 +322,35 @@ __global__ void k_prep_batched(int64_t nel, int nm, const int64_t* __restrict__ 
 template <int DIM, int LOC>
 static void prep_dispatch_idx(int g, int B, cudaStream_t s, int64_t nel, const double* pos,
                               const void* enlist, int idx_bytes, double* coords, double* box64,
-                              float* box32, double* tolv, double* setup, int* bad, int64_t nnodes) {
+                              float* box32, double* tolv, double* setup, int* bad, int64_t nnodes,
+                              double* faces, double* screen) {
   count_launch();
   if (idx_bytes == 4)
-    k_prep<DIM, LOC, int32_t><<<g, B, 0, s>>>(nel, pos, (const int32_t*)enlist, coords, box64, box32, tolv, setup, bad, nnodes);
+    k_prep<DIM, LOC, int32_t><<<g, B, 0, s>>>(nel, pos, (const int32_t*)enlist, coords, box64, box32, tolv, setup, bad,
+                                              nnodes, faces, screen);
   else
-    k_prep<DIM, LOC, int64_t><<<g, B, 0, s>>>(nel, pos, (const int64_t*)enlist, coords, box64, box32, tolv, setup, bad, nnodes);
+    k_prep<DIM, LOC, int64_t><<<g, B, 0, s>>>(nel, pos, (const int64_t*)enlist, coords, box64, box32, tolv, setup, bad,
+                                              nnodes, faces, screen);
 }
 
 cudaError_t launch_prep(int dim, int loc, int64_t nel, const double* pos, const void* enlist, int idx_bytes,
                         double* coords, double* box64, float* box32, double* tolv, double* setup,
-                        int* bad_index, int64_t nnodes, cudaStream_t s) {
+                        int* bad_index, int64_t nnodes, cudaStream_t s, double* faces, double* screen) {
   if (nel <= 0) return cudaSuccess;
   const int B = 256;
   const int g = grid_for(nel, B, 8);
   if (dim == 2 && loc == 3)
-    prep_dispatch_idx<2, 3>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes);
+    prep_dispatch_idx<2, 3>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes,
+                            nullptr, nullptr);
   else if (dim == 2 && loc == 4)
-    prep_dispatch_idx<2, 4>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes);
+    prep_dispatch_idx<2, 4>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes,
+                            nullptr, nullptr);
   else if (dim == 3 && loc == 4)
-    prep_dispatch_idx<3, 4>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes);
+    prep_dispatch_idx<3, 4>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes,
+                            faces, screen);
   else if (dim == 3 && loc == 8)
-    prep_dispatch_idx<3, 8>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes);
+    prep_dispatch_idx<3, 8>(g, B, s, nel, pos, enlist, idx_bytes, coords, box64, box32, tolv, setup, bad_index, nnodes,
+                            nullptr, nullptr);
   else
     return cudaErrorInvalidValue;
   return cudaGetLastError();
@@ -346,19 +360,23 @@ cudaError_t launch_prep_batched(int dim, int64_t nel, int nm, const int64_t* ele
                                 const unsigned long long* pos_ptr, const unsigned long long* en_ptr,
                                 const int64_t* nnodes, int idx_bytes, double* coords, double* box64,
                                 float* box32, double* tolv, double* setup, int32_t* pair_of, int* bad,
-                                cudaStream_t s) {
+                                cudaStream_t s, double* faces, double* screen) {
   if (nel <= 0) return cudaSuccess;
   const int B = 256;
   const int g = grid_for(nel, B, 8);
   count_launch();
   if (dim == 2 && idx_bytes == 4)
-    k_prep_batched<2, int32_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32, tolv, setup, pair_of, bad);
+    k_prep_batched<2, int32_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32,
+                                                 tolv, setup, pair_of, bad, nullptr, nullptr);
   else if (dim == 2)
-    k_prep_batched<2, int64_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32, tolv, setup, pair_of, bad);
+    k_prep_batched<2, int64_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32,
+                                                 tolv, setup, pair_of, bad, nullptr, nullptr);
   else if (idx_bytes == 4)
-    k_prep_batched<3, int32_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32, tolv, setup, pair_of, bad);
+    k_prep_batched<3, int32_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32,
+                                                 tolv, setup, pair_of, bad, faces, screen);
   else
-    k_prep_batched<3, int64_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32, tolv, setup, pair_of, bad);
+    k_prep_batched<3, int64_t><<<g, B, 0, s>>>(nel, nm, elem_off, pos_ptr, en_ptr, nnodes, coords, box64, box32,
+                                                 tolv, setup, pair_of, bad, faces, screen);
   return cudaGetLastError();
 }
 
@@ -1398,6 +1416,9 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 // plane and discarded, so the reference returns no tets: the pair's result is
 // written here (0 tets, measure 0) and only the remaining pairs are listed
 // for the clipper.
+// With faces_a / screen_b (optional) a pair that passes this test gets the
+// second one: B beyond a face plane of A by the margin derived next to
+// tet_screen_b, which again proves that the reference returns no tets.
 // `order` (optional) lists the pairs in the order the clipper should take
 // them (a schedule); survivors are appended in that order, warp by warp.
 // RECORDS: survivors are written as {pair, a, b, 0} so that the clipper gets
@@ -1412,7 +1433,9 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
                                                         const double* __restrict__ coords_a,
                                                         const double* __restrict__ setup_b,
                                                         double* pair_measure, int32_t* pair_nout,
-                                                        int32_t* survivors, unsigned long long* nsurv) {
+                                                        int32_t* survivors, unsigned long long* nsurv,
+                                                        const double* __restrict__ faces_a,
+                                                        const double* __restrict__ screen_b) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < npairs; base += (int64_t)gridDim.x * blockDim.x) {
@@ -1440,6 +1463,26 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
 #pragma unroll
         for (int k = 0; k < 4; ++k) dmin = fmin(dmin, ((nx * t.x[k] + ny * t.y[k]) + nz * t.z[k]) - c);
         reject = reject || dmin >= thr;
+      }
+      if (!reject && faces_a) {
+        const double2* sb = reinterpret_cast<const double2*>(screen_b + (int64_t)b * kScreen3);
+        const double2 gt = __ldg(sb + 6), mz = __ldg(sb + 7);
+        if (gt.x < DBL_MAX) {  // B's planes bound a proper tet
+          Tet u;
+          load_tet(screen_b + (int64_t)b * kScreen3, u);
+          const double Mp = fmax(M, mz.x);
+          const double e = kEps + 128.0 * kEps * (1.0 + 2.0 * Mp);
+          const double slack = 1.01 * gt.x * (gt.y + e) + 16.0 * kEps * (1.0 + Mp);
+          const double2* fa = reinterpret_cast<const double2*>(faces_a + (int64_t)a * kScreen3);
+#pragma unroll
+          for (int P = 0; P < 4; ++P) {
+            const double2 n01 = __ldg(fa + 2 * P), n2h = __ldg(fa + 2 * P + 1);
+            double m = DBL_MAX;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) m = fmin(m, (n01.x * u.x[k] + n01.y * u.y[k]) + n2h.x * u.z[k]);
+            reject = reject || m >= n2h.y + slack;
+          }
+        }
       }
       if (reject) {
         pair_measure[i] = 0.0;
@@ -2163,7 +2206,8 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         const double* coords_a, const double* tol_a, const double* setup_b,
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
-                        const int32_t* order, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
+                        const int32_t* order, cudaEvent_t ev_begin, cudaEvent_t ev_end, const double* faces_a,
+                        const double* screen_b) {
   const int g = clip_grid_blocks(dim);
   count_launch();
   if (dim == 2) {
@@ -2176,11 +2220,13 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
     count_launch();
     if (tet_clipper_variant() == 0)
-      k_prefilter_tets<true><<<grid_for(npairs, 256, 8), 256, 0, s>>>(
-          npairs, order, pair_a, pair_b, coords_a, setup_b, pair_measure, pair_nout, overflow_list, work);
+      k_prefilter_tets<true><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
+                                                                      setup_b, pair_measure, pair_nout,
+                                                                      overflow_list, work, faces_a, screen_b);
     else
-      k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(
-          npairs, order, pair_a, pair_b, coords_a, setup_b, pair_measure, pair_nout, overflow_list, work);
+      k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
+                                                                       setup_b, pair_measure, pair_nout,
+                                                                       overflow_list, work, faces_a, screen_b);
     if (ev_begin) cudaEventRecord(ev_begin, s);
     if (tet_clipper_variant() == 0)
       k_clip_tets_ix<<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
@@ -2201,14 +2247,14 @@ cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int
                                 const double* coords_a, const double* tol_a, const double* setup_b,
                                 double* pair_measure, int32_t* pair_nout, int32_t* survivors,
                                 unsigned long long* work, unsigned char* scratch, int* err, cudaStream_t s,
-                                const int32_t* order) {
+                                const int32_t* order, const double* faces_a, const double* screen_b) {
   // work[0]: survivors, work[1]: admitted pairs, work[2]: deepest clip stack
   cudaMemsetAsync(work, 0, 3 * sizeof(unsigned long long), s);
   cudaMemsetAsync(err, 0, sizeof(int), s);
   count_launch(2);
   k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
                                                                    setup_b, pair_measure, pair_nout, survivors,
-                                                                   work);
+                                                                   work, faces_a, screen_b);
   k_clip_tets_wq<<<wq_grid_blocks(), kWqWarps * 32, 0, s>>>(survivors, work, pair_a, pair_b, coords_a, tol_a,
                                                             setup_b, pair_measure, pair_nout, work, scratch, err);
   return cudaGetLastError();

@@ -17,6 +17,12 @@ namespace lsm {
 //   tolv    [nel]           10*spacing(measure) (A elements)
 constexpr int kSetup2 = 14;  // 3 lines x (nx, ny, px, py), tol, pad
 constexpr int kSetup3 = 20;  // 4 planes x (nx, ny, nz, c), tol, pad (16-byte aligned rows)
+// Separation screen of the tet clipper (3D simplices, optional):
+//   faces   [nel][kScreen3]  A: 4 outward face planes (nx, ny, nz, h), h
+//                            bounding n.x over every vertex clipping derives
+//   screen  [nel][kScreen3]  B: 4 vertices, dilation factor g, residual tau,
+//                            coordinate bound M, pad
+constexpr int kScreen3 = 16;
 
 // Per-block partial of a narrow-phase launch: compensated measure sum,
 // intersecting pairs and output simplices.
@@ -53,7 +59,8 @@ struct BVH {
 // idx_bytes selects the enlist element type (4 = int32, 8 = int64).
 cudaError_t launch_prep(int dim, int loc, int64_t nel, const double* pos, const void* enlist, int idx_bytes,
                         double* coords, double* box64, float* box32, double* tolv, double* setup,
-                        int* bad_index, int64_t nnodes, cudaStream_t s);
+                        int* bad_index, int64_t nnodes, cudaStream_t s, double* faces = nullptr,
+                        double* screen = nullptr);
 
 // Root box (float64) of a set of element boxes: rootbox[2*dim].
 cudaError_t launch_root_box(int dim, int64_t nel, const double* box64, double* partial,
@@ -94,13 +101,16 @@ cudaError_t launch_scan(int64_t n, const int* counts, int64_t* offsets, int64_t*
 // holds two counters (survivors, clipper progress), reset by the launch.
 // `order` (optional, npairs entries) is the schedule: the pairs in the order
 // in which the clipper takes them.  Results do not depend on it.
+// faces_a / screen_b (3D, optional, kScreen3 rows from the prep) enable the
+// second exact early-out (B beyond a face of A).
 int clip_grid_blocks(int dim);
 cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                         const double* coords_a, const double* tol_a, const double* setup_b,
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
                         const int32_t* order = nullptr, cudaEvent_t ev_begin = nullptr,
-                        cudaEvent_t ev_end = nullptr);
+                        cudaEvent_t ev_end = nullptr, const double* faces_a = nullptr,
+                        const double* screen_b = nullptr);
 // Opt-in shared-memory limits for the clip kernels on the current device.
 cudaError_t init_device_attributes();
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
@@ -117,7 +127,8 @@ cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int
                                 const double* coords_a, const double* tol_a, const double* setup_b,
                                 double* pair_measure, int32_t* pair_nout, int32_t* survivors,
                                 unsigned long long* work, unsigned char* scratch, int* err, cudaStream_t s,
-                                const int32_t* order = nullptr);
+                                const int32_t* order = nullptr, const double* faces_a = nullptr,
+                                const double* screen_b = nullptr);
 
 // Per-block partials of the pair measures/counts in a fixed order
 // (reduce_pairs_blocks() entries).
@@ -194,7 +205,7 @@ cudaError_t launch_prep_batched(int dim, int64_t nel, int nm, const int64_t* ele
                                 const unsigned long long* pos_ptr, const unsigned long long* en_ptr,
                                 const int64_t* nnodes, int idx_bytes, double* coords, double* box64,
                                 float* box32, double* tolv, double* setup, int32_t* pair_of, int* bad,
-                                cudaStream_t s);
+                                cudaStream_t s, double* faces = nullptr, double* screen = nullptr);
 // keys[i] = pair_of[vals[i]] (second sort pass: by mesh)
 cudaError_t launch_pair_keys(int64_t n, const int32_t* vals, const int32_t* pair_of, uint32_t* keys,
                              cudaStream_t s);

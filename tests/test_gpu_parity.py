@@ -185,6 +185,84 @@ def test_clip_kernel_timing_option(gpu_ctx):
     assert st.n_candidates > 0 and 0.0 < ms < 1000.0
 
 
+def _near_touching_tets(gaps, per_gap, seed):
+    """A: random tets spread over a box; B: for each A tet a tet whose tip
+    sits at a signed gap beyond the centroid of one of A's faces (negative:
+    it pokes into A) and whose base lies farther out, so that B's own face
+    planes do not separate the pair and only the B-beyond-a-face-of-A test
+    can.  Returns ((pos_a, en_a), (pos_b, en_b), gap per pair)."""
+    rng = np.random.default_rng(seed)
+    ta, tb, gs = [], [], []
+    for gap in gaps:
+        for _ in range(per_gap):
+            while True:
+                a = rng.random((4, 3)) + rng.random(3) * 40.0
+                vol = abs(np.linalg.det(a[1:] - a[0])) / 6.0
+                if vol > 0.02:
+                    break
+            f = int(rng.integers(4))
+            face = [k for k in range(4) if k != f]
+            q = a[face].mean(axis=0)
+            n = np.cross(a[face[1]] - a[face[0]], a[face[2]] - a[face[0]])
+            n /= np.linalg.norm(n)
+            if np.dot(n, a[f] - q) > 0:
+                n = -n
+            u = np.cross(n, [1.0, 0.0, 0.0] if abs(n[0]) < 0.9 else [0.0, 1.0, 0.0])
+            u /= np.linalg.norm(u)
+            v = np.cross(n, u)
+            size = vol ** (1.0 / 3.0)
+            th = rng.random() * 2 * np.pi + np.arange(3) * 2 * np.pi / 3
+            base = q + 0.6 * size * n + 0.7 * size * (np.cos(th)[:, None] * u + np.sin(th)[:, None] * v)
+            b = np.vstack([q + gap * n, base])[rng.permutation(4)]
+            ta.append(a)
+            tb.append(b)
+            gs.append(gap)
+    ta, tb = np.array(ta), np.array(tb)
+    en = np.arange(4 * len(ta), dtype=np.int64).reshape(-1, 4)
+    return (ta.reshape(-1, 3), en), (tb.reshape(-1, 3), en.copy()), np.array(gs)
+
+
+def test_separation_screen_near_touching(gpu_ctx, oracle_mod):
+    """Pairs separated by a face plane of A by gaps from far below to far
+    above the screen's rounding margin, and overlapping ones: per-pair
+    results equal the oracle's (check_pipeline) with the screen on and off,
+    and the screen takes pairs away from the clipper where the gap is wide."""
+    gaps = [-1e-3, -1e-9, -1e-13, 0.0, 1e-300, 1e-17, 1e-15, 1e-13, 1e-11, 1e-9, 1e-6, 1e-3]
+    A, B, g = _near_touching_tets(gaps, 24, 21)
+    lsm.set_option("tet_screen", 1)
+    st = check_pipeline(gpu_ctx, oracle_mod, 3, A, B)
+    with_screen = gpu_ctx.clip_survivors()
+    lsm.set_option("tet_screen", 0)
+    try:
+        st0 = check_pipeline(gpu_ctx, oracle_mod, 3, A, B)
+        without = gpu_ctx.clip_survivors()
+    finally:
+        lsm.set_option("tet_screen", 1)
+    assert st.as_dict() == st0.as_dict()
+    # every pair with a gap >= 1e-9 is screened out; the overlapping ones stay
+    assert without - with_screen >= int((g >= 1e-9).sum())
+    assert with_screen >= int((g < 0).sum())
+
+
+def test_separation_screen_keeps_results(gpu_ctx):
+    """Screen on and off give bit-identical per-pair results on a mesh pair,
+    and the screen removes pairs from the clipper."""
+    dim, A, B = M.config_meshes("small3d_10x12")
+    lsm.set_option("tet_screen", 0)
+    try:
+        st0, em0 = gpu_ctx.supermesh(A, B, elem_measure=True)
+        pm0, pn0 = gpu_ctx.pair_results(st0.n_candidates)
+        s0 = gpu_ctx.clip_survivors()
+    finally:
+        lsm.set_option("tet_screen", 1)
+    st1, em1 = gpu_ctx.supermesh(A, B, elem_measure=True)
+    pm1, pn1 = gpu_ctx.pair_results(st1.n_candidates)
+    s1 = gpu_ctx.clip_survivors()
+    assert st0.as_dict() == st1.as_dict()
+    assert np.array_equal(pm0, pm1) and np.array_equal(pn0, pn1) and np.array_equal(em0, em1)
+    assert st1.n_intersecting <= s1 < s0
+
+
 def test_int64_and_int32_enlists_agree(gpu_ctx):
     dim, A, B = M.config_meshes("small3d_5x6")
     s32, _ = gpu_ctx.supermesh(A, B)
