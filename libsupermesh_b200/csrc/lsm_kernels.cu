@@ -1421,16 +1421,22 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 // tet_screen_b, which again proves that the reference returns no tets.
 // `order` (optional) lists the pairs in the order the clipper should take
 // them (a schedule); survivors are appended in that order, warp by warp.
-// RECORDS: survivors are written as {pair, a, b, 0} so that the clipper gets
-// the element numbers with the pair number in one load.
+// A plane of B with every vertex of A at distance <= -(eps + margin) keeps
+// every tet derived from A whole (all its vertices classify negative), so it
+// changes nothing in the reference's result; such planes form the pair's
+// no-op mask.  With all four planes no-op the reference returns A itself,
+// which is settled here (volume test and measure as in the clipper).
+// RECORDS: survivors are written as {pair, a, b, no-op mask} so that the
+// clipper gets the element numbers and the planes to skip in one load.
 #ifndef LSM_PREFILTER_BPS
-#define LSM_PREFILTER_BPS 1
+#define LSM_PREFILTER_BPS 2
 #endif
 template <bool RECORDS>
 __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ order,
                                                         const int32_t* __restrict__ pa,
                                                         const int32_t* __restrict__ pb,
                                                         const double* __restrict__ coords_a,
+                                                        const double* __restrict__ tol_a,
                                                         const double* __restrict__ setup_b,
                                                         double* pair_measure, int32_t* pair_nout,
                                                         int32_t* survivors, unsigned long long* nsurv,
@@ -1442,7 +1448,7 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
     const int64_t j = base + threadIdx.x;
     bool live = false;
     int64_t i = j;
-    int a = 0, b = 0;
+    int a = 0, b = 0, noop = 0;
     if (j < npairs) {
       if (order) i = order[j];
       a = pa[i];
@@ -1459,10 +1465,15 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
         double nx, ny, nz, c;
         load_plane(pl, L, nx, ny, nz, c);
         const double thr = kEps + 64.0 * kEps * (1.0 + 2.0 * fmax(M, fabs(c)));
-        double dmin = DBL_MAX;
+        double dmin = DBL_MAX, dmax = -DBL_MAX;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) dmin = fmin(dmin, ((nx * t.x[k] + ny * t.y[k]) + nz * t.z[k]) - c);
+        for (int k = 0; k < 4; ++k) {
+          const double d = ((nx * t.x[k] + ny * t.y[k]) + nz * t.z[k]) - c;
+          dmin = fmin(dmin, d);
+          dmax = fmax(dmax, d);
+        }
         reject = reject || dmin >= thr;
+        noop |= dmax <= -thr ? 1 << L : 0;
       }
       if (!reject && faces_a) {
         const double2* sb = reinterpret_cast<const double2*>(screen_b + (int64_t)b * kScreen3);
@@ -1487,6 +1498,12 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
       if (reject) {
         pair_measure[i] = 0.0;
         pair_nout[i] = 0;
+      } else if (noop == 15) {
+        // A inside all four planes: the reference keeps A as its one tet
+        double v1;
+        const bool keep = final_tet_keep(t, fmin(tol_a[a], pl[16]), v1);
+        pair_measure[i] = keep ? v1 : 0.0;
+        pair_nout[i] = keep ? 1 : 0;
       } else {
         live = true;
       }
@@ -1500,7 +1517,7 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
       if (live) {
         const int64_t o = (int64_t)off + __popc(mask & lt);
         if (RECORDS)
-          reinterpret_cast<int4*>(survivors)[o] = make_int4((int)i, a, b, 0);
+          reinterpret_cast<int4*>(survivors)[o] = make_int4((int)i, a, b, noop);
         else
           survivors[o] = (int32_t)i;
       }
@@ -2064,6 +2081,10 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
   unsigned cur = 0;
   double tol = 0.0, m = 0.0;
   int L = 0, sp = 0, kept = 0;
+  // planes this pair clips at (bit L; the prefilter's no-op planes are
+  // skipped) and the last of them
+  unsigned act = 15u;
+  int lastL = 3;
   for (;;) {
     // ---- prefetch pipeline
     if (nstage == 1) {
@@ -2079,7 +2100,9 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
       tol = ntol;
       cur = ix_pack(0, 1, 2, 3);
       m = 0.0;
-      L = 0;
+      act = ~(unsigned)nrec.w & 15u;  // never 0: the prefilter settles those pairs
+      L = __ffs(act) - 1;
+      lastL = 31 - __clz(act);
       sp = 0;
       kept = 0;
       nstage = 0;
@@ -2124,7 +2147,7 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
     int k = 0;
     unsigned c0 = cur, c1 = 0, c2 = 0;
     if (cls.nn > 0) k = cls.np == 0 ? 1 : ix_split(cur, cls, pool, 4 + 4 * L, c0, c1, c2);
-    if (L == 3) {
+    if (L == lastL) {
       // final tets, in the reference's order
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
@@ -2141,7 +2164,7 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
       k = 0;
     }
     if (k > 0) {
-      const unsigned lv = (unsigned)(L + 1);
+      const unsigned lv = (unsigned)(__ffs(act & (~0u << (L + 1))) - 1);  // next plane clipped at
       if (k == 3) {
         stk_hi = (stk_hi << 20) | (stk_lo >> 44);
         stk_lo = (stk_lo << 20) | c2;
@@ -2155,7 +2178,7 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
         ++sp;
       }
       cur = c0;
-      ++L;
+      L = (int)lv;
       continue;
     }
     if (sp > 0) {
@@ -2221,11 +2244,11 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     count_launch();
     if (tet_clipper_variant() == 0)
       k_prefilter_tets<true><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
-                                                                      setup_b, pair_measure, pair_nout,
+                                                                      tol_a, setup_b, pair_measure, pair_nout,
                                                                       overflow_list, work, faces_a, screen_b);
     else
       k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
-                                                                       setup_b, pair_measure, pair_nout,
+                                                                       tol_a, setup_b, pair_measure, pair_nout,
                                                                        overflow_list, work, faces_a, screen_b);
     if (ev_begin) cudaEventRecord(ev_begin, s);
     if (tet_clipper_variant() == 0)
@@ -2253,7 +2276,7 @@ cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int
   cudaMemsetAsync(err, 0, sizeof(int), s);
   count_launch(2);
   k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
-                                                                   setup_b, pair_measure, pair_nout, survivors,
+                                                                   tol_a, setup_b, pair_measure, pair_nout, survivors,
                                                                    work, faces_a, screen_b);
   k_clip_tets_wq<<<wq_grid_blocks(), kWqWarps * 32, 0, s>>>(survivors, work, pair_a, pair_b, coords_a, tol_a,
                                                             setup_b, pair_measure, pair_nout, work, scratch, err);

@@ -263,6 +263,18 @@ def test_separation_screen_keeps_results(gpu_ctx):
     assert st1.n_intersecting <= s1 < s0
 
 
+@pytest.mark.parametrize("na,nb", [(12, 3), (3, 12)])
+def test_nested_meshes_plane_skipping(gpu_ctx, oracle_mod, na, nb):
+    """A fine mesh inside a coarse one (and the reverse): many pairs have
+    planes of B that keep A whole, which the clipper skips, and pairs with A
+    inside all four planes, which the prefilter settles; per-pair results
+    match the oracle."""
+    A = M.grid3d(na, 3, 0.25)
+    B = M.grid3d(nb, 2, 0.25)
+    st = check_pipeline(gpu_ctx, oracle_mod, 3, A, B, domain=1.0)
+    assert st.n_intersecting > 0
+
+
 def test_int64_and_int32_enlists_agree(gpu_ctx):
     dim, A, B = M.config_meshes("small3d_5x6")
     s32, _ = gpu_ctx.supermesh(A, B)
