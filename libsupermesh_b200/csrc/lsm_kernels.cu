@@ -849,8 +849,8 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
   float4 lo = box32[2 * elem], hi = box32[2 * elem + 1];
   lo.w = __int_as_float(elem);
   hi.w = __int_as_float(bvh_escape(n, node, rope, last));
-  lo_left[node] = lo;
-  hi_esc[node] = hi;
+  lo_left[2 * node] = lo;
+  hi_esc[2 * node] = hi;
   if (n == 1) return;
   int p = parent[node];
   for (int guard = 0; guard < 128 && p >= 0; ++guard) {
@@ -858,8 +858,8 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
     if (atomicAdd(&visit[p], 1) == 0) return;  // sibling not done yet
     __threadfence();
     const int lc = left[p], rc = right[p];
-    const float4 a0 = __ldcg(&lo_left[lc]), a1 = __ldcg(&hi_esc[lc]);
-    const float4 b0 = __ldcg(&lo_left[rc]), b1 = __ldcg(&hi_esc[rc]);
+    const float4 a0 = __ldcg(&lo_left[2 * lc]), a1 = __ldcg(&hi_esc[2 * lc]);
+    const float4 b0 = __ldcg(&lo_left[2 * rc]), b1 = __ldcg(&hi_esc[2 * rc]);
     float4 l, h;
     l.x = fminf(a0.x, b0.x);
     l.y = fminf(a0.y, b0.y);
@@ -869,8 +869,8 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
     h.y = fmaxf(a1.y, b1.y);
     h.z = fmaxf(a1.z, b1.z);
     h.w = __int_as_float(bvh_escape(n, p, rope, last));
-    __stcg(&lo_left[p], l);
-    __stcg(&hi_esc[p], h);
+    __stcg(&lo_left[2 * p], l);
+    __stcg(&hi_esc[2 * p], h);
     if (p == 0) return;
     p = parent[p];
   }
@@ -937,8 +937,8 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
     const int nodes = 2 * n - 1;
     for (int guard = 0; node >= 0 && guard < 2 * n + 1; ++guard) {
       if (node >= nodes) break;  // never taken for a well-formed hierarchy
-      const float4 L = __ldg(&lo_left[node]);
-      const float4 H = __ldg(&hi_esc[node]);
+      const float4 L = __ldg(&lo_left[2 * node]);
+      const float4 H = __ldg(&hi_esc[2 * node]);
       bool ov = H.x > ql[0] && L.x < qh[0] && H.y > ql[1] && L.y < qh[1];
       if (DIM == 3) ov = ov && H.z > ql[2] && L.z < qh[2];
       if (ov) {
@@ -2519,8 +2519,8 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
     const int nodes = 2 * n - 1;
     for (int guard = 0; node >= 0 && node != stop && guard < 2 * n + 1; ++guard) {
       if (node >= nodes) break;  // never taken for a well-formed hierarchy
-      const float4 L = __ldg(&lo_left[node]);
-      const float4 H = __ldg(&hi_esc[node]);
+      const float4 L = __ldg(&lo_left[2 * node]);
+      const float4 H = __ldg(&hi_esc[2 * node]);
       bool ov = H.x > ql[0] && L.x < qh[0] && H.y > ql[1] && L.y < qh[1];
       if (DIM == 3) ov = ov && H.z > ql[2] && L.z < qh[2];
       if (ov) {

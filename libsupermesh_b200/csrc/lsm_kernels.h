@@ -51,8 +51,10 @@ void set_query_block(int v);
 
 struct BVH {
   int n = 0;                 // leaves
-  float4* lo_left = nullptr;  // [2n-1]: lo.xyz, .w = left child / element (int bits)
-  float4* hi_esc = nullptr;   // [2n-1]: hi.xyz, .w = escape node (int bits), -1 = end
+  // Node k (2n-1 nodes) is the 32-byte pair lo_left[2k], hi_esc[2k] of one
+  // interleaved array (hi_esc = lo_left + 1), so a visit reads one sector.
+  float4* lo_left = nullptr;  // lo.xyz, .w = left child / element (int bits)
+  float4* hi_esc = nullptr;   // hi.xyz, .w = escape node (int bits), -1 = end
 };
 
 // Mesh prep: gather coordinates, boxes, measures/tolerances, B clip setup.
