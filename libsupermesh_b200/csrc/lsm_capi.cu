@@ -51,7 +51,7 @@ struct Ctx {
   // mesh B (tree side)
   DevBuf b_pos, b_en, b_coords, b_box64, b_box32, b_setup, b_screen;
   // tree
-  DevBuf keys, vals, keys_tmp, vals_tmp, hist, root_partial, rootbox, bvh_lo, bvh_work;
+  DevBuf keys, vals, keys_tmp, vals_tmp, hist, root_partial, rootbox, bvh_lo, bvh_work, bvh_leaf;
   // candidates
   DevBuf counts, offsets, scan_tmp, pair_a, pair_b, i64_tmp, q_cache, q_over;
   // narrow phase
@@ -194,7 +194,7 @@ void fini_ctx(Ctx* c) {
   DevBuf* all[] = {&c->a_pos, &c->a_en, &c->a_coords, &c->a_box64, &c->a_tol, &c->b_pos, &c->b_en,
                    &c->b_coords, &c->b_box64, &c->b_box32, &c->b_setup, &c->keys, &c->vals,
                    &c->keys_tmp, &c->vals_tmp, &c->hist, &c->root_partial, &c->rootbox, &c->bvh_lo,
-                   &c->bvh_work, &c->counts, &c->offsets, &c->scan_tmp, &c->pair_a,
+                   &c->bvh_work, &c->bvh_leaf, &c->counts, &c->offsets, &c->scan_tmp, &c->pair_a,
                    &c->pair_b, &c->i64_tmp, &c->pair_measure, &c->pair_nout, &c->partials,
                    &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->wq_scratch, &c->x_a, &c->x_b, &c->x_measure,
                    &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
@@ -319,8 +319,10 @@ lsm::BVH build_tree(Ctx* c, const MeshDev& b, cudaStream_t s) {
   CU(lsm::radix_sort_pairs(n, dim == 2 ? 32 : 30, keys, vals, kt, vt, hist, s));
   bvh.lo_left = ensure<float4>(c, c->bvh_lo, 2 * (2 * n - 1));
   bvh.hi_esc = bvh.lo_left + 1;
+  bvh.leaf = ensure<double>(c, c->bvh_leaf, 8 * n);
   int* work = ensure<int>(c, c->bvh_work, 8 * n);
-  CU(lsm::launch_bvh_build(dim, (int)n, keys, vals, static_cast<float*>(c->b_box32.p), bvh, work, s));
+  CU(lsm::launch_bvh_build(dim, (int)n, keys, vals, static_cast<float*>(c->b_box32.p), bvh, work, s,
+                           static_cast<double*>(c->b_box64.p)));
   return bvh;
 }
 

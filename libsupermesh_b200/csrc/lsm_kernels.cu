@@ -841,7 +841,8 @@ __device__ __forceinline__ int bvh_escape(int n, int node, const int* __restrict
 __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, const float4* __restrict__ box32,
                             const int* __restrict__ parent, const int* __restrict__ rope,
                             const int* __restrict__ last, const int* __restrict__ left,
-                            const int* __restrict__ right, int* visit, float4* lo_left, float4* hi_esc) {
+                            const int* __restrict__ right, int* visit, float4* lo_left, float4* hi_esc,
+                            int dim, const double* __restrict__ box64, double* leaf) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int elem = sorted_vals[k];
@@ -851,6 +852,16 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
   hi.w = __int_as_float(bvh_escape(n, node, rope, last));
   lo_left[2 * node] = lo;
   hi_esc[2 * node] = hi;
+  if (leaf) {
+    // leaf record in sorted order: FP64 box (lo at 0.., hi at 3..), element, escape
+    double* o = leaf + (int64_t)k * 8;
+    for (int c = 0; c < 3; ++c) {
+      o[c] = c < dim ? box64[(int64_t)elem * 2 * dim + c] : 0.0;
+      o[3 + c] = c < dim ? box64[(int64_t)elem * 2 * dim + dim + c] : 0.0;
+    }
+    reinterpret_cast<int2*>(o + 6)[0] = make_int2(elem, __float_as_int(hi.w));
+    o[7] = 0.0;
+  }
   if (n == 1) return;
   int p = parent[node];
   for (int guard = 0; guard < 128 && p >= 0; ++guard) {
@@ -877,8 +888,7 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
 }
 
 cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const int32_t* sorted_vals,
-                             const float* box32, BVH bvh, int* work, cudaStream_t s) {
-  (void)dim;
+                             const float* box32, BVH bvh, int* work, cudaStream_t s, const double* box64) {
   if (n <= 0) return cudaSuccess;
   int* parent = work;
   int* rope = parent + (2 * n - 1);
@@ -894,7 +904,8 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
   }
   cudaMemsetAsync(parent, 0xff, sizeof(int), s);  // parent[root] = -1
   k_bvh_refit<<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
-                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc);
+                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim, box64,
+                                              box64 ? bvh.leaf : nullptr);
   return cudaGetLastError();
 }
 
@@ -906,6 +917,10 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
 // more than cap candidates in over_rows; the fill then copies cached rows
 // (k_fill_from_cache) and traverses again only for the listed rows
 // (FILL = true with `rows`).
+// With leaf records (`leaf`, in sorted order: FP64 box, element, escape) a
+// leaf visit is one load that gives the exact box test and the next node;
+// without them it reads the leaf's FP32 node and then the element's FP64
+// box, two dependent loads.  Both give the same candidates in the same order.
 template <int DIM, bool FILL>
 __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __restrict__ box64_a,
                                                const float4* __restrict__ lo_left,
@@ -913,7 +928,8 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
                                                const double* __restrict__ box64_b, int* counts,
                                                const int64_t* __restrict__ offsets, int32_t* pair_a,
                                                int32_t* pair_b, int32_t* cache, int cap,
-                                               const int32_t* __restrict__ rows, int* over_rows) {
+                                               const int32_t* __restrict__ rows, int* over_rows,
+                                               const double* __restrict__ leaf) {
   const int64_t nrows = rows ? (int64_t)*over_rows : nel_a;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
        r += (int64_t)gridDim.x * blockDim.x) {
@@ -937,6 +953,26 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
     const int nodes = 2 * n - 1;
     for (int guard = 0; node >= 0 && guard < 2 * n + 1; ++guard) {
       if (node >= nodes) break;  // never taken for a well-formed hierarchy
+      if (leaf && node >= n - 1) {
+        const double2* q = reinterpret_cast<const double2*>(leaf + (int64_t)(node - (n - 1)) * 8);
+        const double2 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
+        const double blo[3] = {q0.x, q0.y, q1.x}, bhi[3] = {q1.y, q2.x, q2.y};
+        const int2 meta = make_int2(__double2loint(q3.x), __double2hiint(q3.x));
+        bool ex = true;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) ex = ex && (hi[c] > blo[c]) && (lo[c] < bhi[c]);
+        if (ex) {
+          if (FILL) {
+            pair_a[out + cnt] = (int32_t)a;
+            pair_b[out + cnt] = meta.x;
+          } else if (cache && cnt < cap) {
+            cache[a * cap + cnt] = meta.x;
+          }
+          ++cnt;
+        }
+        node = meta.y;
+        continue;
+      }
       const float4 L = __ldg(&lo_left[2 * node]);
       const float4 H = __ldg(&hi_esc[2 * node]);
       bool ov = H.x > ql[0] && L.x < qh[0] && H.y > ql[1] && L.y < qh[1];
@@ -1017,7 +1053,7 @@ cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_
   int32_t* cc = fill ? nullptr : cache;
 #define LSM_QUERY_ARGS                                                                                    \
   nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b, cc, cap, rows, \
-      over_rows
+      over_rows, bvh.leaf
   if (dim == 2) {
     if (fill)
       k_query<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
@@ -2472,7 +2508,7 @@ cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const
   cudaMemsetAsync(parent, 0xff, sizeof(int), s);
   k_mesh_roots<<<(nm + 255) / 256, 256, 0, s>>>(nm, n, mesh_off_b, rope, last, roots, stops);
   k_bvh_refit<<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
-                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc);
+                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, 3, nullptr, nullptr);
   return cudaGetLastError();
 }
 

@@ -55,6 +55,9 @@ struct BVH {
   // interleaved array (hi_esc = lo_left + 1), so a visit reads one sector.
   float4* lo_left = nullptr;  // lo.xyz, .w = left child / element (int bits)
   float4* hi_esc = nullptr;   // hi.xyz, .w = escape node (int bits), -1 = end
+  // optional [n][8] f64 leaf records in sorted order: lo (3), hi (3),
+  // {element, escape} as two ints, pad
+  double* leaf = nullptr;
 };
 
 // Mesh prep: gather coordinates, boxes, measures/tolerances, B clip setup.
@@ -80,7 +83,8 @@ cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals,
 
 // LBVH over sorted Morton codes.  work_int needs 8*n ints.
 cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const int32_t* sorted_vals,
-                             const float* box32, BVH bvh, int* work_int, cudaStream_t s);
+                             const float* box32, BVH bvh, int* work_int, cudaStream_t s,
+                             const double* box64 = nullptr);
 
 // Candidate search.  Pass 1 (fill=false) writes counts[nel_a]; pass 2 writes
 // pair_a/pair_b at offsets[a].  With a cache ([nel_a][cap] int32) pass 1 also
