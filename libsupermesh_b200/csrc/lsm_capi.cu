@@ -697,10 +697,11 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
     CU(lsm::radix_sort_pairs(nb, mbits, keys, vals, kt, vt, hist, s));
     bvh.lo_left = ensure<float4>(c, c->bvh_lo, 2 * (2 * nb - 1));
     bvh.hi_esc = bvh.lo_left + 1;
+    bvh.leaf = ensure<double>(c, c->bvh_leaf, 8 * nb);
     int* work = ensure<int>(c, c->bvh_work, 8 * nb);
     unsigned long long* codes = ensure<unsigned long long>(c, c->bt_codes, nb);
     CU(lsm::launch_batched_tree((int)nb, nm, vals, pair_of_b, mort, codes, b_box32, d_eob, bvh, work, roots,
-                                stops, s));
+                                stops, s, dim, b_box));
   } else {
     CU(cudaMemsetAsync(roots, 0xff, sizeof(int) * nm, s));
     CU(cudaMemsetAsync(stops, 0xff, sizeof(int) * nm, s));

@@ -2491,7 +2491,7 @@ __global__ void k_mesh_roots(int nm, int n, const int64_t* __restrict__ mesh_off
 cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const int32_t* pair_of_b,
                                 const uint32_t* mort, unsigned long long* codes, const float* box32,
                                 const int64_t* mesh_off_b, BVH bvh, int* work, int* roots, int* stops,
-                                cudaStream_t s) {
+                                cudaStream_t s, int dim, const double* box64) {
   if (n <= 0) return cudaSuccess;
   int* parent = work;
   int* rope = parent + (2 * n - 1);
@@ -2508,7 +2508,8 @@ cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const
   cudaMemsetAsync(parent, 0xff, sizeof(int), s);
   k_mesh_roots<<<(nm + 255) / 256, 256, 0, s>>>(nm, n, mesh_off_b, rope, last, roots, stops);
   k_bvh_refit<<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
-                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, 3, nullptr, nullptr);
+                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim, box64,
+                                              box64 ? bvh.leaf : nullptr);
   return cudaGetLastError();
 }
 
@@ -2529,8 +2530,9 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
                                                        const double* __restrict__ box64_b, int* counts,
                                                        const int64_t* __restrict__ offsets, int32_t* pair_a,
                                                        int32_t* pair_b, int32_t* cache, int cap,
-                                                       const int32_t* __restrict__ rows, int* over_rows) {
-  // cache / rows / over_rows: as k_query
+                                                       const int32_t* __restrict__ rows, int* over_rows,
+                                                       const double* __restrict__ leaf) {
+  // cache / rows / over_rows / leaf: as k_query
   const int64_t nrows = rows ? (int64_t)*over_rows : nel_a;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
        r += (int64_t)gridDim.x * blockDim.x) {
@@ -2555,6 +2557,26 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
     const int nodes = 2 * n - 1;
     for (int guard = 0; node >= 0 && node != stop && guard < 2 * n + 1; ++guard) {
       if (node >= nodes) break;  // never taken for a well-formed hierarchy
+      if (leaf && node >= n - 1) {
+        const double2* q = reinterpret_cast<const double2*>(leaf + (int64_t)(node - (n - 1)) * 8);
+        const double2 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
+        const double blo[3] = {q0.x, q0.y, q1.x}, bhi[3] = {q1.y, q2.x, q2.y};
+        const int2 meta = make_int2(__double2loint(q3.x), __double2hiint(q3.x));
+        bool ex = true;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) ex = ex && (hi[c] > blo[c]) && (lo[c] < bhi[c]);
+        if (ex) {
+          if (FILL) {
+            pair_a[out + cnt] = (int32_t)a;
+            pair_b[out + cnt] = meta.x;
+          } else if (cache && cnt < cap) {
+            cache[a * cap + cnt] = meta.x;
+          }
+          ++cnt;
+        }
+        node = meta.y;
+        continue;
+      }
       const float4 L = __ldg(&lo_left[2 * node]);
       const float4 H = __ldg(&hi_esc[2 * node]);
       bool ov = H.x > ql[0] && L.x < qh[0] && H.y > ql[1] && L.y < qh[1];
@@ -2606,7 +2628,7 @@ cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double
   int32_t* cc = fill ? nullptr : cache;
 #define LSM_QUERY_ARGS                                                                                         \
   nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, \
-      pair_b, cc, cap, rows, over_rows
+      pair_b, cc, cap, rows, over_rows, bvh.leaf
   if (dim == 2) {
     if (fill)
       k_query_batched<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);

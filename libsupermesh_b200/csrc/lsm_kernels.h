@@ -220,7 +220,8 @@ cudaError_t launch_pair_keys(int64_t n, const int32_t* vals, const int32_t* pair
 cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const int32_t* pair_of_b,
                                 const uint32_t* mort, unsigned long long* codes, const float* box32,
                                 const int64_t* mesh_off_b, BVH bvh, int* work, int* roots, int* stops,
-                                cudaStream_t s);
+                                cudaStream_t s, int dim = 3,
+                                const double* box64 = nullptr);
 cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double* box64_a,
                                  const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
