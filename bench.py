@@ -13,8 +13,11 @@ set (the tree finder's set); pairs/s = candidates / step time.
   e2e        the same call with host (pinned) inputs: H2D of positions and
              element lists and D2H of the per-element measure in the timed
              region
-  roofline   the dominant kernel (tet clipping), timed alone over the same
-             candidates, against the measured FP64 DADD/DMUL issue rate
+  roofline   the dominant kernels (3D: the exact early-out pass and the tet
+             clipper, which together settle every candidate; 2D: the
+             triangle clipper), timed alone over the same candidates, with
+             the reference algorithm's FLOP count for all candidates,
+             against the measured FP64 DADD/DMUL issue rate
   cpu_baseline  the oracle restatement of the reference algorithm
              (quadtree/octree + breadth-first clipping), one thread, full
              workload, on this host
@@ -176,12 +179,18 @@ def load_probe():
 
 
 def profile_traffic(kernel: str, workload: str):
-    """dram bytes per launch from the committed ncu summary, if present."""
-    f = ROOT / "profiles" / f"{kernel}_{workload}.md"
-    if not f.exists():
-        return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
-    return float(m.group(1)) if m else None
+    """dram bytes per launch from the committed ncu summaries, if present
+    (summed over the kernels of a 'k1+k2' span)."""
+    total = 0.0
+    for k in kernel.split("+"):
+        f = ROOT / "profiles" / f"{k}_{workload}.md"
+        if not f.exists():
+            return None
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
+        if not m:
+            return None
+        total += float(m.group(1))
+    return total
 
 
 def measured_peaks():
@@ -431,8 +440,8 @@ def run_ours(args, world, rank, local):
         kernel_ms.append(ctx.clip_kernel_ms())
     lsm.set_option("time_kernels", 0)
     clip_ms = all_max(sum(kernel_ms), world) / args.steps
-    clip_kernel = ({0: "k_clip_tets_ix", 1: "k_clip_tets_wq", 2: "k_clip_tets"}[lsm.get_option("tet_clipper")]
-                   if dim == 3 else "k_clip_tris")
+    clip_kernel = ("k_prefilter_tets+" + {0: "k_clip_tets_ix", 1: "k_clip_tets_wq", 2: "k_clip_tets"}[
+        lsm.get_option("tet_clipper")] if dim == 3 else "k_clip_tris")
 
     line = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,

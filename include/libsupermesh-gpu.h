@@ -86,9 +86,11 @@ int64_t libsupermesh_gpu_kernel_launches(void);
 int libsupermesh_gpu_set_option(const char *name, int64_t value);
 int libsupermesh_gpu_get_option(const char *name, int64_t *value);
 
-/* Device time (ms) of the clip kernel of the last narrow phase on ctx, from
- * CUDA events recorded on its stream (needs option time_kernels = 1 during
- * that phase; waits for the kernel to finish). */
+/* Device time (ms) of the clipping kernels of the last narrow phase on ctx
+ * (2D: the triangle clipper; 3D: the exact early-out pass and the tet
+ * clipper, which together settle every candidate), from CUDA events recorded
+ * on its stream (needs option time_kernels = 1 during that phase; waits for
+ * the kernels to finish). */
 int libsupermesh_gpu_clip_kernel_ms(lsm_gpu_context *ctx, double *ms);
 
 /* Pairs of the last 3D narrow phase on ctx that the exact early-outs left

@@ -2276,6 +2276,9 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
   } else {
     // work[0]: survivor count, work[1]: clipper pair counter
     const size_t smem = sizeof(double) * (kTetSmemSlots * 12 + 16) * kTetBlock;
+    // the timed span covers the early-out pass and the clipper: together
+    // they settle every candidate
+    if (ev_begin) cudaEventRecord(ev_begin, s);
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
     count_launch();
     if (tet_clipper_variant() == 0)
@@ -2286,7 +2289,6 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
       k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
                                                                        tol_a, setup_b, pair_measure, pair_nout,
                                                                        overflow_list, work, faces_a, screen_b);
-    if (ev_begin) cudaEventRecord(ev_begin, s);
     if (tet_clipper_variant() == 0)
       k_clip_tets_ix<<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
           reinterpret_cast<const int4*>(overflow_list), work, coords_a, tol_a, setup_b, pair_measure, pair_nout,
