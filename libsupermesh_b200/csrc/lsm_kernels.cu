@@ -30,6 +30,8 @@
 #include "lsm_geom.cuh"
 #include "lsm_kernels.h"
 
+#include <cuda/atomic>
+
 #include <cfloat>
 #include <cstdio>
 #include <cstdlib>
@@ -865,9 +867,9 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
   if (n == 1) return;
   int p = parent[node];
   for (int guard = 0; guard < 128 && p >= 0; ++guard) {
-    __threadfence();
-    if (atomicAdd(&visit[p], 1) == 0) return;  // sibling not done yet
-    __threadfence();
+    // release: this thread's node boxes; acquire: the sibling's
+    cuda::atomic_ref<int, cuda::thread_scope_device> vis(visit[p]);
+    if (vis.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;  // sibling not done yet
     const int lc = left[p], rc = right[p];
     const float4 a0 = __ldcg(&lo_left[2 * lc]), a1 = __ldcg(&hi_esc[2 * lc]);
     const float4 b0 = __ldcg(&lo_left[2 * rc]), b1 = __ldcg(&hi_esc[2 * rc]);
