@@ -316,7 +316,7 @@ lsm::BVH build_tree(Ctx* c, const MeshDev& b, cudaStream_t s) {
   double* root = ensure<double>(c, c->rootbox, 2 * dim);
   CU(lsm::launch_root_box(dim, n, static_cast<double*>(c->b_box64.p), part, pcap, root, s));
   CU(lsm::launch_morton(dim, n, static_cast<double*>(c->b_box64.p), root, keys, vals, s));
-  CU(lsm::radix_sort_pairs(n, dim == 2 ? 32 : 30, keys, vals, kt, vt, hist, s));
+  CU(lsm::radix_sort_pairs(n, dim == 2 ? 32 : 30, keys, vals, kt, vt, hist, s, bad_flag(c) + 3));
   bvh.lo_left = ensure<float4>(c, c->bvh_lo, 2 * (2 * n - 1));
   bvh.hi_esc = bvh.lo_left + 1;
   bvh.leaf = ensure<double>(c, c->bvh_leaf, 8 * n);
@@ -444,9 +444,13 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   int64_t* h = static_cast<int64_t*>(c->host_scalars) + 8;
   CU(cudaMemcpyAsync(h, offsets + nel_a, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   int* hb = static_cast<int*>(c->host_scalars);
-  CU(cudaMemcpyAsync(hb, c->misc.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(hb, c->misc.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   REQUIRE(hb[0] == 0, "Invalid node index in an element list");
+  if (hb[3] != 0) {
+    set_error(c, "tree build: the sort's look-back wait gave up");
+    throw Fail{LSM_ERROR_CUDA};
+  }
   const int64_t nnz = *h;
   int32_t* pa = ensure<int32_t>(c, c->pair_a, nnz);
   int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);

@@ -4,16 +4,19 @@
 //                       B-element clip setup (lines / unit-normal planes)
 //   K1b k_root_*        root box reduction;  k_morton  Morton keys
 //   K2  radix sort      stable LSD, 8-bit digits, warp-match ranking;
-//                       coalesced three-pass histogram scan
+//                       one digit-count kernel, then one kernel per pass
+//                       with decoupled look-back (k_radix_onesweep)
 //   K3  k_bvh_internal  Karras LBVH hierarchy + rope table;
-//       k_bvh_refit     bottom-up FP32 box refit, escape links
+//       k_bvh_refit     bottom-up FP32 box refit, escape links, leaf records
 //   K4  k_query         stackless LBVH traversal per A element (FP32,
-//                       outward-rounded boxes) + exact strict FP64 box test;
-//                       the count pass caches rows, k_fill_from_cache copies
+//                       outward-rounded boxes) + exact strict FP64 box test
+//                       at the leaf records; the count pass caches rows,
+//                       k_fill_from_cache copies
 //   K5  k_clip_tris     one candidate pair per thread, polygon in shared
 //                       memory, FP64 Sutherland-Hodgman
-//   K6  k_prefilter_tets exact early-out; k_clip_tets_ix (default) depth-first
-//                       clipping over point indices with a refill pipeline;
+//   K6  k_prefilter_tets two exact early-outs and the no-op plane mask;
+//                       k_clip_tets_ix (default) depth-first clipping over
+//                       point indices with a refill pipeline;
 //                       k_clip_tets (tets in registers), k_clip_tets_wq
 //                       (per-warp task queues) as alternatives
 //   K7  compensated reductions (per-block (sum, err), then final; per mesh
@@ -552,7 +555,7 @@ cudaError_t launch_morton(int dim, int64_t nel, const double* box64, const doubl
 }
 
 // ======================================================================
-// K2: stable LSD radix sort (8-bit digits)
+// K2: stable LSD radix sort (8-bit digits, one kernel per pass)
 // ======================================================================
 namespace {
 constexpr int kSortThreads = 256;
@@ -562,166 +565,66 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per block
 constexpr int kWarpTile = 32 * kSortItems;             // contiguous per warp
 }  // namespace
 
-// Exclusive scan of the digit histograms, three passes over tiles of
-// kScanU32Tile entries (16 per thread, 128-bit loads): tile sums, a scan of
-// the tile sums, then each tile scanned with its prefix.
-constexpr int kScanU32Threads = 256;
-constexpr int kScanU32Items = 16;
-constexpr int kScanU32Tile = kScanU32Threads * kScanU32Items;
+// Single-pass digit binning per pass ("onesweep"): one kernel counts every
+// digit of every pass over all keys; each pass is then one kernel in which
+// block b (in ticket order) ranks its 2048 keys, publishes its digit counts,
+// looks back over the blocks before it for their prefix (decoupled
+// look-back: a block publishes its local count first and its inclusive
+// prefix once known) and scatters.  Stable: ranks follow key order within a
+// block and blocks follow key order.
+//
+// Scratch layout (uint32, radix_hist_entries(n)): counts[4][256] |
+// tickets[4] | err | pad | status[4][nblocks][256].  A status word holds a
+// 2-bit flag (0 not ready, 1 local count, 2 inclusive prefix) over a 30-bit
+// count (n < 2^30).  Waits are bounded: a block that gives up sets err and
+// treats the missing prefix as 0 (wrong order, never a hang); forward
+// progress does not need the bound, since a block only waits for blocks
+// that took earlier tickets and are running or done.
+namespace {
+constexpr int kSortPassesMax = 4;
+constexpr int kSortHdr = kSortPassesMax * 256 + 8;
+constexpr uint32_t kFlagLocal = 1u << 30, kFlagIncl = 2u << 30, kFlagMask = 3u << 30;
+}  // namespace
 
 int64_t radix_hist_entries(int64_t n) {
   const int64_t nb = (n + kSortTile - 1) / kSortTile;
-  const int64_t count = 256 * (nb > 0 ? nb : 1);
-  return count + (count + kScanU32Tile - 1) / kScanU32Tile + 1;  // + tile sums
+  return kSortHdr + (int64_t)kSortPassesMax * 256 * (nb > 0 ? nb : 1);
 }
 
-// Histogram of one digit per block: hist[d * nblocks + block].
-__global__ void __launch_bounds__(kSortThreads) k_radix_hist(int64_t n, int shift, const uint32_t* __restrict__ keys,
-                                                             uint32_t* hist) {
-  __shared__ uint32_t h[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+__global__ void __launch_bounds__(kSortThreads) k_radix_counts(int64_t n, int passes,
+                                                               const uint32_t* __restrict__ keys, uint32_t* counts) {
+  __shared__ uint32_t h[kSortPassesMax][256];
+  for (int i = threadIdx.x; i < kSortPassesMax * 256; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
-  const int64_t base = (int64_t)blockIdx.x * kSortTile;
-  for (int r = 0; r < kSortItems; ++r) {
-    const int64_t i = base + (int64_t)r * kSortThreads + threadIdx.x;
-    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 255u], 1u);
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[(int64_t)d * gridDim.x + blockIdx.x] = h[d];
-}
-
-// Exclusive scan of `count` uint32 entries in place by one block of 1024.
-__global__ void __launch_bounds__(1024) k_scan_u32_single(int64_t count, uint32_t* data) {
-  __shared__ uint32_t warp_tot[32];
-  const int64_t per = (count + blockDim.x - 1) / blockDim.x;
-  const int64_t beg = (int64_t)threadIdx.x * per;
-  const int64_t end = beg + per < count ? beg + per : count;
-  uint32_t local = 0;
-  for (int64_t i = beg; i < end; ++i) local += data[i];
-  // block exclusive scan of `local`
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  uint32_t inc = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += t;
-  }
-  if (lane == 31) warp_tot[wid] = inc;
-  __syncthreads();
-  if (wid == 0) {
-    uint32_t w = warp_tot[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += t;
-    }
-    warp_tot[lane] = w;
-  }
-  __syncthreads();
-  uint32_t run = inc - local + (wid > 0 ? warp_tot[wid - 1] : 0u);
-  for (int64_t i = beg; i < end; ++i) {
-    const uint32_t v = data[i];
-    data[i] = run;
-    run += v;
+  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+    const uint32_t v = (&h[0][0])[i];
+    if (v) atomicAdd(&counts[i], v);
   }
 }
 
-// Block-wide exclusive scan of one value per thread (kScanU32Threads).
-__device__ __forceinline__ uint32_t block_excl_scan_u32(uint32_t v, uint32_t* total) {
-  __shared__ uint32_t wt[kScanU32Threads / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  uint32_t inc = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += t;
-  }
-  if (lane == 31) wt[wid] = inc;
-  __syncthreads();
-  if (wid == 0) {
-    uint32_t w = lane < kScanU32Threads / 32 ? wt[lane] : 0u;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += t;
-    }
-    if (lane < kScanU32Threads / 32) wt[lane] = w;
-  }
-  __syncthreads();
-  const uint32_t r = inc - v + (wid > 0 ? wt[wid - 1] : 0u);
-  if (total) *total = wt[kScanU32Threads / 32 - 1];
-  __syncthreads();
-  return r;
-}
-
-// count is a multiple of kScanU32Items (histograms hold 256 entries per
-// block); data 16-byte aligned.
-__global__ void __launch_bounds__(kScanU32Threads) k_scan_u32_tiles(int64_t count, const uint32_t* __restrict__ data,
-                                                                    uint32_t* tile_sums) {
-  const int64_t base = (int64_t)blockIdx.x * kScanU32Tile + (int64_t)threadIdx.x * kScanU32Items;
-  uint32_t v = 0;
-  if (base < count) {
-    const uint4* q = reinterpret_cast<const uint4*>(data + base);
-#pragma unroll
-    for (int k = 0; k < kScanU32Items / 4; ++k) {
-      const uint4 u = q[k];
-      v += u.x + u.y + u.z + u.w;
-    }
-  }
-  uint32_t total = 0;
-  block_excl_scan_u32(v, &total);
-  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
-}
-
-__global__ void __launch_bounds__(kScanU32Threads) k_scan_u32_apply(int64_t count, uint32_t* data,
-                                                                    const uint32_t* __restrict__ tile_prefix) {
-  const int64_t base = (int64_t)blockIdx.x * kScanU32Tile + (int64_t)threadIdx.x * kScanU32Items;
-  uint32_t e[kScanU32Items];
-  uint32_t v = 0;
-  const bool in = base < count;
-  if (in) {
-    const uint4* q = reinterpret_cast<const uint4*>(data + base);
-#pragma unroll
-    for (int k = 0; k < kScanU32Items / 4; ++k) {
-      const uint4 u = q[k];
-      e[4 * k] = u.x;
-      e[4 * k + 1] = u.y;
-      e[4 * k + 2] = u.z;
-      e[4 * k + 3] = u.w;
-    }
-#pragma unroll
-    for (int k = 0; k < kScanU32Items; ++k) v += e[k];
-  }
-  uint32_t run = block_excl_scan_u32(v, nullptr) + tile_prefix[blockIdx.x];
-  if (in) {
-    uint4* q = reinterpret_cast<uint4*>(data + base);
-#pragma unroll
-    for (int k = 0; k < kScanU32Items / 4; ++k) {
-      uint4 u;
-      u.x = run;
-      run += e[4 * k];
-      u.y = run;
-      run += e[4 * k + 1];
-      u.z = run;
-      run += e[4 * k + 2];
-      u.w = run;
-      run += e[4 * k + 3];
-      q[k] = u;
-    }
-  }
-}
-
-// Stable scatter: each warp owns a contiguous 256-key sub-tile.
-__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(int64_t n, int shift, const uint32_t* __restrict__ keys_in,
-                                                                const int32_t* __restrict__ vals_in,
-                                                                uint32_t* keys_out, int32_t* vals_out,
-                                                                const uint32_t* __restrict__ hist) {
+__global__ void __launch_bounds__(kSortThreads) k_radix_onesweep(int64_t n, int shift,
+                                                                 const uint32_t* __restrict__ keys_in,
+                                                                 const int32_t* __restrict__ vals_in,
+                                                                 uint32_t* keys_out, int32_t* vals_out,
+                                                                 const uint32_t* __restrict__ counts,
+                                                                 uint32_t* status, uint32_t* ticket,
+                                                                 uint32_t* err) {
   __shared__ uint32_t wh[kSortWarps][256];
+  __shared__ uint32_t base_s[256];
+  __shared__ uint32_t wt[kSortWarps];
+  __shared__ int bid_s;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
+  if (threadIdx.x == 0) bid_s = (int)atomicAdd(ticket, 1u);
   for (int i = lane; i < 256; i += 32) wh[wid][i] = 0;
-  __syncwarp();
-  const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)wid * kWarpTile;
+  __syncthreads();
+  const int b = bid_s;
+  const int64_t base = (int64_t)b * kSortTile + (int64_t)wid * kWarpTile;
   uint32_t k[kSortItems];
   int dg[kSortItems];
 #pragma unroll
@@ -734,9 +637,49 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(int64_t n, int s
     __syncwarp();
   }
   __syncthreads();
-  // cross-warp exclusive offsets per digit, plus the global digit/block base
-  for (int d = threadIdx.x; d < 256; d += blockDim.x) {
-    uint32_t run = hist[(int64_t)d * gridDim.x + blockIdx.x];
+  // thread d: this block's count of digit d, published, then the prefix of
+  // the blocks before it; the warps' offsets within the block
+  const int d = threadIdx.x;  // blockDim.x == 256
+  uint32_t local = 0;
+  for (int w = 0; w < kSortWarps; ++w) local += wh[w][d];
+  cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(status[(int64_t)b * 256 + d]);
+  mine.store((b == 0 ? kFlagIncl : kFlagLocal) | local, cuda::memory_order_relaxed);
+  uint32_t prefix = 0;
+  for (int j = b - 1; j >= 0;) {
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> st(status[(int64_t)j * 256 + d]);
+    uint32_t v = st.load(cuda::memory_order_relaxed);
+    for (int spin = 0; (v & kFlagMask) == 0; ++spin) {
+      if (spin > (1 << 22)) {
+        atomicExch(err, 1u);
+        v = kFlagIncl;
+        break;
+      }
+      __nanosleep(64);
+      v = st.load(cuda::memory_order_relaxed);
+    }
+    prefix += v & ~kFlagMask;
+    if ((v & kFlagMask) == kFlagIncl) break;
+    --j;
+  }
+  if (b > 0) mine.store(kFlagIncl | (prefix + local), cuda::memory_order_relaxed);
+  // global start of digit d: exclusive scan of the pass's digit counts
+  {
+    const uint32_t c = counts[d];
+    uint32_t inc = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    if (lane == 31) wt[wid] = inc;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < wid; ++w) before += wt[w];
+    base_s[d] = before + inc - c + prefix;
+  }
+  __syncthreads();
+  {
+    uint32_t run = base_s[d];
     for (int w = 0; w < kSortWarps; ++w) {
       const uint32_t c = wh[w][d];
       wh[w][d] = run;
@@ -760,23 +703,23 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(int64_t n, int s
 }
 
 cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals, uint32_t* keys_tmp,
-                             int32_t* vals_tmp, uint32_t* hist, cudaStream_t s) {
+                             int32_t* vals_tmp, uint32_t* hist, cudaStream_t s, int* err) {
   if (n <= 1) return cudaSuccess;
+  if (n >= (int64_t)1 << 30 || bits > 32) return cudaErrorInvalidValue;
   const int nb = (int)((n + kSortTile - 1) / kSortTile);
   const int passes = (bits + 7) / 8;
+  uint32_t* counts = hist;
+  uint32_t* tickets = hist + kSortPassesMax * 256;
+  uint32_t* errw = err ? reinterpret_cast<uint32_t*>(err) : tickets + kSortPassesMax;
+  uint32_t* status = hist + kSortHdr;
+  cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (kSortHdr - 4 + (int64_t)passes * 256 * nb + 4), s);
   uint32_t *ki = keys, *ko = keys_tmp;
   int32_t *vi = vals, *vo = vals_tmp;
+  count_launch(1 + passes);
+  k_radix_counts<<<grid_for(n, kSortThreads, 4), kSortThreads, 0, s>>>(n, passes, ki, counts);
   for (int p = 0; p < passes; ++p) {
-    const int shift = 8 * p;
-    const int64_t count = (int64_t)256 * nb;
-    const int ntiles = (int)((count + kScanU32Tile - 1) / kScanU32Tile);
-    uint32_t* tile_sums = hist + count;
-    count_launch(5);
-    k_radix_hist<<<nb, kSortThreads, 0, s>>>(n, shift, ki, hist);
-    k_scan_u32_tiles<<<ntiles, kScanU32Threads, 0, s>>>(count, hist, tile_sums);
-    k_scan_u32_single<<<1, 1024, 0, s>>>(ntiles, tile_sums);
-    k_scan_u32_apply<<<ntiles, kScanU32Threads, 0, s>>>(count, hist, tile_sums);
-    k_radix_scatter<<<nb, kSortThreads, 0, s>>>(n, shift, ki, vi, ko, vo, hist);
+    k_radix_onesweep<<<nb, kSortThreads, 0, s>>>(n, 8 * p, ki, vi, ko, vo, counts + 256 * p,
+                                                 status + (int64_t)p * 256 * nb, tickets + p, errw);
     uint32_t* tk = ki;
     ki = ko;
     ko = tk;

@@ -75,11 +75,13 @@ cudaError_t launch_morton(int dim, int64_t nel, const double* box64, const doubl
                           uint32_t* keys, int32_t* vals, cudaStream_t s);
 
 // Stable LSD radix sort of (key, val) pairs, 8 bits per pass over the low
-// `bits` bits.  tmp buffers must hold n entries; hist must hold
-// radix_hist_entries(n).  Result ends in keys/vals.
+// `bits` bits (at most 32), n < 2^30.  tmp buffers must hold n entries; hist
+// (scratch: digit counts, block tickets, look-back status) must hold
+// radix_hist_entries(n).  Result ends in keys/vals.  *err (optional) becomes
+// nonzero if a look-back wait gave up (bounded; not expected to happen).
 int64_t radix_hist_entries(int64_t n);
 cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals, uint32_t* keys_tmp,
-                             int32_t* vals_tmp, uint32_t* hist, cudaStream_t s);
+                             int32_t* vals_tmp, uint32_t* hist, cudaStream_t s, int* err = nullptr);
 
 // LBVH over sorted Morton codes.  work_int needs 8*n ints.
 cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const int32_t* sorted_vals,
