@@ -410,12 +410,13 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   c->ncand = -1;
   c->simplex_prep = false;
   simplex = simplex || (ma->loc == ma->dim + 1 && mb->loc == mb->dim + 1);
-  // A's upload and prep run on the side stream, overlapping B's upload,
-  // prep and tree build on s; s waits for them before the search.
+  // A's upload and prep run on the side stream, overlapping B's prep and
+  // tree build on s; s waits for them before the search.  A's copies start
+  // once B's are done, so B's (on the critical path) get the whole link.
   CU(cudaMemsetAsync(bad_flag(c), 0, sizeof(int) * 64, s));
+  MeshDev b = upload(c, mb, on_device, c->b_pos, c->b_en, s);
   CU(cudaEventRecord(c->side_ev[0], s));
   CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
-  MeshDev b = upload(c, mb, on_device, c->b_pos, c->b_en, s);
   MeshDev a = upload(c, ma, on_device, c->a_pos, c->a_en, c->side);
   prep_a(c, a, simplex, c->side);
   CU(cudaEventRecord(c->side_ev[1], c->side));
