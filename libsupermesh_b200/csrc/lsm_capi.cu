@@ -53,7 +53,7 @@ struct Ctx {
   // tree
   DevBuf keys, vals, keys_tmp, vals_tmp, hist, root_partial, rootbox, bvh_lo, bvh_work, bvh_leaf;
   // candidates
-  DevBuf counts, offsets, scan_tmp, pair_a, pair_b, i64_tmp, q_cache, q_over;
+  DevBuf counts, offsets, scan_tmp, pair_a, pair_b, i64_tmp, q_cache, q_over, q_pool, q_next, q_first;
   // narrow phase
   DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals, wq_scratch;
   // explicit pairs / p1 / batched
@@ -201,7 +201,7 @@ void fini_ctx(Ctx* c) {
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
                    &c->bt_ncand, &c->bt_stage_pa, &c->bt_stage_ea, &c->bt_stage_pb, &c->bt_stage_eb,
                    &c->d1_keyhi, &c->d1_perm_a, &c->d1_perm_b, &c->d1_lo_a, &c->d1_hi_a, &c->d1_lo_b,
-                   &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over,
+                   &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over, &c->q_pool, &c->q_next, &c->q_first,
                    &c->a_faces, &c->b_screen, &c->surv};
   for (DevBuf* b : all) free_buf(*b);
   for (cudaEvent_t& e : c->clip_ev)
@@ -277,6 +277,25 @@ int* bad_flag(Ctx* c) { return ensure<int>(c, c->misc, 64); }
 // 1/32 of the device).  Only rows' actual candidates are written (4 B each);
 // the cap only bounds the row length that avoids a second traversal.
 int64_t cache_budget(Ctx* c) { return std::min<int64_t>(4ll << 30, c->device_mem / 32); }
+
+// Spill pool for rows longer than the cache: what the budget leaves after
+// the dense part, at most 4 chunks (256 candidates) per row on average.  Its
+// chunk counter is bad_flag(c)[4], zeroed with the flags.  row_chunk needs no
+// clearing: the count pass writes it for every row longer than the cache,
+// and only those rows read it.
+lsm::Spill make_spill(Ctx* c, int64_t nel, int cap) {
+  lsm::Spill sp;
+  const int64_t chunk_bytes = sizeof(int32_t) * lsm::kSpillChunk + sizeof(int);
+  int64_t chunks = (cache_budget(c) - (int64_t)sizeof(int32_t) * nel * cap) / chunk_bytes;
+  chunks = std::min<int64_t>(std::min<int64_t>(chunks, 4 * nel), INT32_MAX);
+  if (nel <= 0 || chunks < 1) return sp;
+  sp.pool = ensure<int32_t>(c, c->q_pool, chunks * lsm::kSpillChunk);
+  sp.chunk_next = ensure<int>(c, c->q_next, chunks);
+  sp.row_chunk = ensure<int>(c, c->q_first, nel);
+  sp.next = bad_flag(c) + 4;
+  sp.chunks = (int)chunks;
+  return sp;
+}
 
 // prep of the query mesh A: coords (simplices only), box64, tol; tets also
 // get their face planes for the clipper's separation screen
@@ -430,13 +449,16 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   const int cap = nel_a > 0 ? (int)std::min<int64_t>(256, cache_budget(c) / (4 * nel_a)) : 0;
   int32_t* cache = cap >= 8 ? ensure<int32_t>(c, c->q_cache, nel_a * cap) : nullptr;
   int* over = cache ? ensure<int>(c, c->q_over, nel_a + 1) : nullptr;
+  // (the single-mesh search keeps the tighter walk of a cache without spill
+  // chunks: its long rows are traversed again)
+  const lsm::Spill spill{};
   if (b.nel > 0 && nel_a > 0) {
     bvh = build_tree(c, b, s);
     if (over) CU(cudaMemsetAsync(over, 0, sizeof(int), s));
     CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
     CU(lsm::launch_query(a.dim, false, nel_a, static_cast<double*>(c->a_box64.p), bvh,
                          static_cast<double*>(c->b_box64.p), counts, nullptr, nullptr, nullptr, s, cache, cap,
-                         over));
+                         over, spill));
   } else {
     CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
     if (nel_a > 0) CU(cudaMemsetAsync(counts, 0, sizeof(int) * nel_a, s));
@@ -457,7 +479,8 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);
   if (nnz > 0)
     CU(lsm::launch_query(a.dim, true, nel_a, static_cast<double*>(c->a_box64.p), bvh,
-                         static_cast<double*>(c->b_box64.p), counts, offsets, pa, pb, s, cache, cap, over));
+                         static_cast<double*>(c->b_box64.p), counts, offsets, pa, pb, s, cache, cap, over,
+                         spill));
   c->dim = a.dim;
   c->loc_a = a.loc;
   c->loc_b = b.loc;
@@ -718,10 +741,11 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   const int cap = na > 0 ? (int)std::min<int64_t>(256, cache_budget(c) / (4 * na)) : 0;
   int32_t* cache = cap >= 8 ? ensure<int32_t>(c, c->q_cache, na * cap) : nullptr;
   int* over = cache ? ensure<int>(c, c->q_over, na + 1) : nullptr;
+  const lsm::Spill spill = cache ? make_spill(c, na, cap) : lsm::Spill{};
   if (na > 0 && nb > 0) {
     if (over) CU(cudaMemsetAsync(over, 0, sizeof(int), s));
     CU(lsm::launch_query_batched(dim, false, na, a_box, pair_of_a, roots, stops, bvh, b_box, counts, nullptr,
-                                 nullptr, nullptr, s, cache, cap, over));
+                                 nullptr, nullptr, s, cache, cap, over, spill));
   }
   else if (na > 0)
     CU(cudaMemsetAsync(counts, 0, sizeof(int) * na, s));
@@ -737,7 +761,7 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);
   if (nnz > 0)
     CU(lsm::launch_query_batched(dim, true, na, a_box, pair_of_a, roots, stops, bvh, b_box, counts, offsets,
-                                 pa, pb, s, cache, cap, over));
+                                 pa, pb, s, cache, cap, over, spill));
   c->dim = dim;
   c->loc_a = c->loc_b = loc;
   c->nel_a = na;

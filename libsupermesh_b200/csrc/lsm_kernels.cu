@@ -857,6 +857,42 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
 // ======================================================================
 // K4: candidate search
 // ======================================================================
+// Row cache of the count pass: the first `cap` candidates of row a at
+// cache[a * cap ..]; later ones spill into chunks of kSpillChunk entries
+// taken from a pool (sp.next counts the chunks handed out), chained per row
+// (sp.row_chunk[a] = first chunk, sp.chunk_next[c] = the next one) in
+// traversal order.  A row that finds the pool exhausted, or runs without a
+// pool, is `lost`: it is listed for a second traversal instead.  SPILL is
+// on in the batched search, whose mesh pairs of unrelated resolutions give
+// many long rows; the single-mesh search keeps the tighter walk and lists
+// its (rare) long rows.
+template <bool SPILL>
+__device__ __forceinline__ void cache_put(int32_t* cache, int cap, const Spill& sp, int64_t a, int cnt, int w,
+                                          int& ch, bool& lost) {
+  if (cnt < cap) {
+    cache[a * cap + cnt] = w;
+    return;
+  }
+  if (!SPILL || lost || !sp.pool) {
+    lost = true;
+    return;
+  }
+  const int q = cnt - cap, o = q & (kSpillChunk - 1);
+  if (o == 0) {
+    const int nc = atomicAdd(sp.next, 1);
+    if (nc >= sp.chunks) {
+      lost = true;
+      return;
+    }
+    if (q == 0)
+      sp.row_chunk[a] = nc;
+    else
+      sp.chunk_next[ch] = nc;
+    ch = nc;
+  }
+  sp.pool[(int64_t)ch * kSpillChunk + o] = w;
+}
+
 // The count pass (FILL = false) also keeps the first `cap` candidates of
 // every row in cache[a * cap ..] (when cache is given) and lists rows with
 // more than cap candidates in over_rows; the fill then copies cached rows
@@ -874,7 +910,7 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
                                                const int64_t* __restrict__ offsets, int32_t* pair_a,
                                                int32_t* pair_b, int32_t* cache, int cap,
                                                const int32_t* __restrict__ rows, int* over_rows,
-                                               const double* __restrict__ leaf) {
+                                               const double* __restrict__ leaf, Spill sp) {
   const int64_t nrows = rows ? (int64_t)*over_rows : nel_a;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
        r += (int64_t)gridDim.x * blockDim.x) {
@@ -893,6 +929,8 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
     }
     int cnt = 0;
     int64_t out = FILL ? offsets[a] : 0;
+    int chunk = -1;     // current spill chunk of this row
+    bool lost = false;  // the row goes to the second traversal
     int node = 0;
     // Each step moves forward in depth-first order; 2n-1 nodes bound it.
     const int nodes = 2 * n - 1;
@@ -910,8 +948,8 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
           if (FILL) {
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = meta.x;
-          } else if (cache && cnt < cap) {
-            cache[a * cap + cnt] = meta.x;
+          } else if (cache) {
+            cache_put<false>(cache, cap, sp, a, cnt, meta.x, chunk, lost);
           }
           ++cnt;
         }
@@ -936,8 +974,8 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
           if (FILL) {
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = w;
-          } else if (cache && cnt < cap) {
-            cache[a * cap + cnt] = w;
+          } else if (cache) {
+            cache_put<false>(cache, cap, sp, a, cnt, w, chunk, lost);
           }
           ++cnt;
         }
@@ -946,7 +984,10 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
     }
     if (!FILL) {
       counts[a] = cnt;
-      if (cache && cnt > cap) over_rows[1 + atomicAdd(over_rows, 1)] = (int32_t)a;
+      if (cache && lost) {
+        if (sp.row_chunk) sp.row_chunk[a] = -2;
+        over_rows[1 + atomicAdd(over_rows, 1)] = (int32_t)a;
+      }
     }
   }
 }
@@ -957,7 +998,7 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
 __global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const int* __restrict__ counts,
                                                          const int64_t* __restrict__ offsets,
                                                          const int32_t* __restrict__ cache, int cap,
-                                                         int32_t* pair_a, int32_t* pair_b) {
+                                                         int32_t* pair_a, int32_t* pair_b, Spill sp) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < nel_a;
@@ -972,8 +1013,26 @@ __global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const in
     for (int r = 0; r < 32; ++r) {
       const int c = __shfl_sync(0xffffffffu, cnt, r);
       const int64_t o = __shfl_sync(0xffffffffu, off, r);
-      if (c > cap) continue;  // filled by the traversal over the listed rows
       const int64_t row = base + r;
+      if (c > cap) {
+        // the cached head, then the row's chain of spill chunks; rows that
+        // lost theirs (-2) are filled by the traversal over the listed rows
+        const int first = sp.row_chunk ? sp.row_chunk[row] : -2;
+        if (first < 0) continue;
+        for (int k = lane; k < cap; k += 32) {
+          pair_a[o + k] = (int32_t)row;
+          pair_b[o + k] = cache[row * cap + k];
+        }
+        int ch = first;
+        for (int k0 = cap; k0 < c; k0 += kSpillChunk) {
+          for (int k = lane; k < kSpillChunk && k0 + k < c; k += 32) {
+            pair_a[o + k0 + k] = (int32_t)row;
+            pair_b[o + k0 + k] = sp.pool[(int64_t)ch * kSpillChunk + k];
+          }
+          if (k0 + kSpillChunk < c) ch = sp.chunk_next[ch];
+        }
+        continue;
+      }
       for (int k = lane; k < c; k += 32) {
         pair_a[o + k] = (int32_t)row;
         pair_b[o + k] = cache[row * cap + k];
@@ -984,13 +1043,14 @@ __global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const in
 
 cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_a, BVH bvh,
                          const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
-                         int32_t* pair_b, cudaStream_t s, int32_t* cache, int cap, int* over_rows) {
+                         int32_t* pair_b, cudaStream_t s, int32_t* cache, int cap, int* over_rows, Spill sp) {
   if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
   const int B = query_block();
   const int g = grid_for(nel_a, B, 2048 / B);
   if (fill && cache) {
     count_launch(2);
-    k_fill_from_cache<<<grid_for(nel_a, 256, 8), 256, 0, s>>>(nel_a, counts, offsets, cache, cap, pair_a, pair_b);
+    k_fill_from_cache<<<grid_for(nel_a, 256, 8), 256, 0, s>>>(nel_a, counts, offsets, cache, cap, pair_a, pair_b,
+                                                              sp);
   } else {
     count_launch();
   }
@@ -998,7 +1058,7 @@ cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_
   int32_t* cc = fill ? nullptr : cache;
 #define LSM_QUERY_ARGS                                                                                    \
   nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b, cc, cap, rows, \
-      over_rows, bvh.leaf
+      over_rows, bvh.leaf, sp
   if (dim == 2) {
     if (fill)
       k_query<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
@@ -2478,7 +2538,7 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
                                                        const int64_t* __restrict__ offsets, int32_t* pair_a,
                                                        int32_t* pair_b, int32_t* cache, int cap,
                                                        const int32_t* __restrict__ rows, int* over_rows,
-                                                       const double* __restrict__ leaf) {
+                                                       const double* __restrict__ leaf, Spill sp) {
   // cache / rows / over_rows / leaf: as k_query
   const int64_t nrows = rows ? (int64_t)*over_rows : nel_a;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
@@ -2501,6 +2561,8 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
     const int stop = stops[mesh];
     int cnt = 0;
     int64_t out = FILL ? offsets[a] : 0;
+    int chunk = -1;     // current spill chunk of this row
+    bool lost = false;  // the row goes to the second traversal
     const int nodes = 2 * n - 1;
     for (int guard = 0; node >= 0 && node != stop && guard < 2 * n + 1; ++guard) {
       if (node >= nodes) break;  // never taken for a well-formed hierarchy
@@ -2516,8 +2578,8 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
           if (FILL) {
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = meta.x;
-          } else if (cache && cnt < cap) {
-            cache[a * cap + cnt] = meta.x;
+          } else if (cache) {
+            cache_put<true>(cache, cap, sp, a, cnt, meta.x, chunk, lost);
           }
           ++cnt;
         }
@@ -2542,8 +2604,8 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
           if (FILL) {
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = w;
-          } else if (cache && cnt < cap) {
-            cache[a * cap + cnt] = w;
+          } else if (cache) {
+            cache_put<true>(cache, cap, sp, a, cnt, w, chunk, lost);
           }
           ++cnt;
         }
@@ -2552,7 +2614,10 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
     }
     if (!FILL) {
       counts[a] = cnt;
-      if (cache && cnt > cap) over_rows[1 + atomicAdd(over_rows, 1)] = (int32_t)a;
+      if (cache && lost) {
+        if (sp.row_chunk) sp.row_chunk[a] = -2;
+        over_rows[1 + atomicAdd(over_rows, 1)] = (int32_t)a;
+      }
     }
   }
 }
@@ -2561,13 +2626,15 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
 cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double* box64_a,
                                  const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
-                                 int32_t* pair_b, cudaStream_t s, int32_t* cache, int cap, int* over_rows) {
+                                 int32_t* pair_b, cudaStream_t s, int32_t* cache, int cap, int* over_rows,
+                                 Spill sp) {
   if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
   const int B = query_block();
   const int g = grid_for(nel_a, B, 2048 / B);
   if (fill && cache) {
     count_launch(2);
-    k_fill_from_cache<<<grid_for(nel_a, 256, 8), 256, 0, s>>>(nel_a, counts, offsets, cache, cap, pair_a, pair_b);
+    k_fill_from_cache<<<grid_for(nel_a, 256, 8), 256, 0, s>>>(nel_a, counts, offsets, cache, cap, pair_a, pair_b,
+                                                              sp);
   } else {
     count_launch();
   }
@@ -2575,7 +2642,7 @@ cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double
   int32_t* cc = fill ? nullptr : cache;
 #define LSM_QUERY_ARGS                                                                                         \
   nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, \
-      pair_b, cc, cap, rows, over_rows, bvh.leaf
+      pair_b, cc, cap, rows, over_rows, bvh.leaf, sp
   if (dim == 2) {
     if (fill)
       k_query_batched<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);

@@ -88,15 +88,31 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
                              const float* box32, BVH bvh, int* work_int, cudaStream_t s,
                              const double* box64 = nullptr);
 
+// Spill pool of the count pass's row cache: rows longer than the cache
+// continue in chunks of kSpillChunk candidates (pool[chunks][kSpillChunk]),
+// chained per row (row_chunk[nel_a]: first chunk, or -2 for a row that
+// could not keep all its candidates; written for every row longer than the
+// cache; chunk_next[chunks]); *next (zeroed by the caller) counts the chunks
+// handed out.
+constexpr int kSpillChunk = 64;
+struct Spill {
+  int32_t* pool = nullptr;
+  int* next = nullptr;
+  int* chunk_next = nullptr;
+  int* row_chunk = nullptr;
+  int chunks = 0;
+};
+
 // Candidate search.  Pass 1 (fill=false) writes counts[nel_a]; pass 2 writes
 // pair_a/pair_b at offsets[a].  With a cache ([nel_a][cap] int32) pass 1 also
-// keeps each row's first cap candidates and lists the longer rows in
-// over_rows ({count, rows...}, count zeroed by the caller, nel_a + 1 ints);
-// pass 2 then copies the cached rows and traverses only the listed ones.
+// keeps each row's first cap candidates, the rest in spill chunks (sp), and
+// lists the rows that could not keep them all in over_rows ({count,
+// rows...}, count zeroed by the caller, nel_a + 1 ints); pass 2 then copies
+// the kept rows and traverses only the listed ones.
 cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_a, BVH bvh,
                          const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
                          int32_t* pair_b, cudaStream_t s, int32_t* cache = nullptr, int cap = 0,
-                         int* over_rows = nullptr);
+                         int* over_rows = nullptr, Spill sp = Spill{});
 
 // Exclusive scan of int32 counts into int64 offsets[n+1] (offsets[n] = total).
 int64_t scan_tmp_entries(int64_t n);
@@ -228,7 +244,7 @@ cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double
                                  const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
                                  int32_t* pair_b, cudaStream_t s, int32_t* cache = nullptr, int cap = 0,
-                                 int* over_rows = nullptr);
+                                 int* over_rows = nullptr, Spill sp = Spill{});
 int64_t mesh_totals_pieces(int nm);  // Partial scratch entries for launch_mesh_totals
 cudaError_t launch_mesh_totals(int nm, const int64_t* elem_off_a, const int64_t* offsets, const double* pm,
                                const int32_t* pn, Partial* pieces, Partial* out, int64_t* ncand, cudaStream_t s);
