@@ -79,6 +79,9 @@ int64_t libsupermesh_gpu_kernel_launches(void);
  *   "query_block"        64, 128 (default) or 256 threads per block (candidate search)
  *   "time_kernels"       1: record CUDA events around the clip kernel of every
  *                        narrow phase (read with libsupermesh_gpu_clip_kernel_ms); 0 (default)
+ *   "spill_chunks"       -1 (default, automatic), 0 or n > 0: chunks of 64 candidates that the
+ *                        batched search's row cache may take for rows longer than 256 (rows
+ *                        that find none are traversed a second time)
  *   "tet_screen"         1 (default): tet pairs whose B lies beyond a face plane of A by a
  *                        proven rounding margin skip the clipper (exact: the reference
  *                        returns no tets for them); 0: only the A-beyond-a-face-of-B test

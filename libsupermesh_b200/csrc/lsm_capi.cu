@@ -32,6 +32,9 @@ namespace {
 bool g_time_kernels = false;
 // second exact early-out of the tet clipper (B beyond a face of A)
 bool g_tet_screen = true;
+// spill chunks of the batched search's row cache: -1 automatic, 0 none (long
+// rows traversed again), n > 0 at most n
+int64_t g_spill_chunks = -1;
 
 // ------------------------------------------------------------------ buffers
 struct DevBuf {
@@ -288,6 +291,7 @@ lsm::Spill make_spill(Ctx* c, int64_t nel, int cap) {
   const int64_t chunk_bytes = sizeof(int32_t) * lsm::kSpillChunk + sizeof(int);
   int64_t chunks = (cache_budget(c) - (int64_t)sizeof(int32_t) * nel * cap) / chunk_bytes;
   chunks = std::min<int64_t>(std::min<int64_t>(chunks, 4 * nel), INT32_MAX);
+  if (g_spill_chunks >= 0) chunks = std::min<int64_t>(chunks, g_spill_chunks);
   if (nel <= 0 || chunks < 1) return sp;
   sp.pool = ensure<int32_t>(c, c->q_pool, chunks * lsm::kSpillChunk);
   sp.chunk_next = ensure<int>(c, c->q_next, chunks);
@@ -1061,6 +1065,8 @@ int libsupermesh_gpu_set_option(const char* name, int64_t value) {
     g_time_kernels = value == 1;
   } else if (n == "tet_screen" && (value == 0 || value == 1)) {
     g_tet_screen = value == 1;
+  } else if (n == "spill_chunks" && value >= -1 && value <= INT32_MAX) {
+    g_spill_chunks = value;
   } else {
     return LSM_ERROR_INVALID_ARGUMENT;
   }
@@ -1082,6 +1088,8 @@ int libsupermesh_gpu_get_option(const char* name, int64_t* value) {
     *value = g_time_kernels ? 1 : 0;
   else if (n == "tet_screen")
     *value = g_tet_screen ? 1 : 0;
+  else if (n == "spill_chunks")
+    *value = g_spill_chunks;
   else
     return LSM_ERROR_INVALID_ARGUMENT;
   return LSM_SUCCESS;

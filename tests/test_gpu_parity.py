@@ -521,6 +521,35 @@ def test_batched_matches_single(gpu_ctx):
         assert abs(totals[i] - 1.0) <= 1e-12
 
 
+def test_batched_spill_chunks_keep_results(gpu_ctx):
+    """Mesh pairs of unrelated resolutions give rows longer than the search's
+    256-entry row cache: with spill chunks, with a pool too small for all of
+    them (the rest traversed again) and with none, the candidate counts and
+    totals are identical."""
+    pairs = [(3, M.grid3d(3, 3, 0.25), M.grid3d(14, 2, 0.25)),
+             (3, M.grid3d(4, 5, 0.25), M.grid3d(13, 4, 0.25)),
+             (2, M.grid2d(4, 1, 0.3), M.grid2d(60, 0, 0.3)),
+             (2, M.grid2d(5, 3, 0.3), M.grid2d(45, 2, 0.3))]
+    results = []
+    try:
+        for chunks in (-1, 7, 0):
+            lsm.set_option("spill_chunks", chunks)
+            for dim in (2, 3):
+                sub = [(A, B) for d, A, B in pairs if d == dim]
+                results.append((chunks, dim, gpu_ctx.supermesh_batched(sub)))
+    finally:
+        lsm.set_option("spill_chunks", -1)
+    ref = {dim: r for ch, dim, r in results if ch == -1}
+    for ch, dim, (tot, nc, ni) in results:
+        rt, rc, ri = ref[dim]
+        assert list(nc) == list(rc) and list(ni) == list(ri)
+        assert list(tot) == list(rt)
+    for d, A, B in pairs:
+        st, _ = gpu_ctx.supermesh(A, B)
+        assert abs(st.total_measure - 1.0) <= 1e-12
+        assert st.n_candidates > 256 * len(A[1]) // 2  # long rows
+
+
 def test_batched_vs_oracle(gpu_ctx, oracle_mod):
     pairs = M.batched_pairs(24, seed=16, emin=1e2, emax=3e3)
     totals, nc, ni = gpu_ctx.supermesh_batched([(A, B) for _, A, B in pairs])
