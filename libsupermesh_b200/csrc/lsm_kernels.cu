@@ -1485,12 +1485,17 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
                                                         const double* __restrict__ screen_b) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < npairs; base += (int64_t)gridDim.x * blockDim.x) {
+  // each block takes one contiguous range of pairs (consecutive iterations
+  // then share A rows and most B elements in L1)
+  const int64_t per = ((npairs + gridDim.x - 1) / gridDim.x + blockDim.x - 1) / blockDim.x * blockDim.x;
+  const int64_t beg = (int64_t)blockIdx.x * per;
+  const int64_t end = beg + per < npairs ? beg + per : npairs;
+  for (int64_t base = beg; base < end; base += blockDim.x) {
     const int64_t j = base + threadIdx.x;
     bool live = false;
     int64_t i = j;
     int a = 0, b = 0, noop = 0;
-    if (j < npairs) {
+    if (j < end) {
       if (order) i = order[j];
       a = pa[i];
       b = pb[i];
