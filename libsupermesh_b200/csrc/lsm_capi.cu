@@ -722,11 +722,11 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
     CU(lsm::launch_root_box(dim, nb, b_box, part, pcap, root, s));
     CU(lsm::launch_morton(dim, nb, b_box, root, keys, vals, s));
     CU(cudaMemcpyAsync(mort, keys, sizeof(uint32_t) * nb, cudaMemcpyDeviceToDevice, s));
-    CU(lsm::radix_sort_pairs(nb, dim == 2 ? 32 : 30, keys, vals, kt, vt, hist, s));
+    CU(lsm::radix_sort_pairs(nb, dim == 2 ? 32 : 30, keys, vals, kt, vt, hist, s, bad + 3));
     int mbits = 1;
     while ((1 << mbits) < nm) ++mbits;
     CU(lsm::launch_pair_keys(nb, vals, pair_of_b, keys, s));
-    CU(lsm::radix_sort_pairs(nb, mbits, keys, vals, kt, vt, hist, s));
+    CU(lsm::radix_sort_pairs(nb, mbits, keys, vals, kt, vt, hist, s, bad + 3));
     bvh.lo_left = ensure<float4>(c, c->bvh_lo, 2 * (2 * nb - 1));
     bvh.hi_esc = bvh.lo_left + 1;
     bvh.leaf = ensure<double>(c, c->bvh_leaf, 8 * nb);
@@ -757,9 +757,13 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   int64_t* h = static_cast<int64_t*>(c->host_scalars) + 8;
   int* hb = static_cast<int*>(c->host_scalars);
   CU(cudaMemcpyAsync(h, offsets + na, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  CU(cudaMemcpyAsync(hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(hb, bad, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   REQUIRE(hb[0] == 0, "Invalid node index in an element list");
+  if (hb[3] != 0) {
+    set_error(c, "tree build: the sort's look-back wait gave up");
+    throw Fail{LSM_ERROR_CUDA};
+  }
   const int64_t nnz = *h;
   int32_t* pa = ensure<int32_t>(c, c->pair_a, nnz);
   int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);
