@@ -862,18 +862,17 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
 // taken from a pool (sp.next counts the chunks handed out), chained per row
 // (sp.row_chunk[a] = first chunk, sp.chunk_next[c] = the next one) in
 // traversal order.  A row that finds the pool exhausted, or runs without a
-// pool, is `lost`: it is listed for a second traversal instead.  SPILL is
-// on in the batched search, whose mesh pairs of unrelated resolutions give
-// many long rows; the single-mesh search keeps the tighter walk and lists
-// its (rare) long rows.
-template <bool SPILL>
+// pool, is `lost`: it is listed for a second traversal instead.  Only the
+// batched search spills (its mesh pairs of unrelated resolutions give many
+// long rows); the single-mesh search (k_query) keeps the tighter walk, with
+// fewer registers, and lists its (rare) long rows.
 __device__ __forceinline__ void cache_put(int32_t* cache, int cap, const Spill& sp, int64_t a, int cnt, int w,
                                           int& ch, bool& lost) {
   if (cnt < cap) {
     cache[a * cap + cnt] = w;
     return;
   }
-  if (!SPILL || lost || !sp.pool) {
+  if (lost || !sp.pool) {
     lost = true;
     return;
   }
@@ -910,7 +909,7 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
                                                const int64_t* __restrict__ offsets, int32_t* pair_a,
                                                int32_t* pair_b, int32_t* cache, int cap,
                                                const int32_t* __restrict__ rows, int* over_rows,
-                                               const double* __restrict__ leaf, Spill sp) {
+                                               const double* __restrict__ leaf) {
   const int64_t nrows = rows ? (int64_t)*over_rows : nel_a;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
        r += (int64_t)gridDim.x * blockDim.x) {
@@ -929,8 +928,6 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
     }
     int cnt = 0;
     int64_t out = FILL ? offsets[a] : 0;
-    int chunk = -1;     // current spill chunk of this row
-    bool lost = false;  // the row goes to the second traversal
     int node = 0;
     // Each step moves forward in depth-first order; 2n-1 nodes bound it.
     const int nodes = 2 * n - 1;
@@ -949,7 +946,7 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = meta.x;
           } else if (cache) {
-            cache_put<false>(cache, cap, sp, a, cnt, meta.x, chunk, lost);
+            if (cnt < cap) cache[a * cap + cnt] = meta.x;
           }
           ++cnt;
         }
@@ -975,7 +972,7 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = w;
           } else if (cache) {
-            cache_put<false>(cache, cap, sp, a, cnt, w, chunk, lost);
+            if (cnt < cap) cache[a * cap + cnt] = w;
           }
           ++cnt;
         }
@@ -984,10 +981,7 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
     }
     if (!FILL) {
       counts[a] = cnt;
-      if (cache && lost) {
-        if (sp.row_chunk) sp.row_chunk[a] = -2;
-        over_rows[1 + atomicAdd(over_rows, 1)] = (int32_t)a;
-      }
+      if (cache && cnt > cap) over_rows[1 + atomicAdd(over_rows, 1)] = (int32_t)a;
     }
   }
 }
@@ -1058,7 +1052,7 @@ cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_
   int32_t* cc = fill ? nullptr : cache;
 #define LSM_QUERY_ARGS                                                                                    \
   nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b, cc, cap, rows, \
-      over_rows, bvh.leaf, sp
+      over_rows, bvh.leaf
   if (dim == 2) {
     if (fill)
       k_query<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
@@ -2584,7 +2578,7 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = meta.x;
           } else if (cache) {
-            cache_put<true>(cache, cap, sp, a, cnt, meta.x, chunk, lost);
+            cache_put(cache, cap, sp, a, cnt, meta.x, chunk, lost);
           }
           ++cnt;
         }
@@ -2610,7 +2604,7 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
             pair_a[out + cnt] = (int32_t)a;
             pair_b[out + cnt] = w;
           } else if (cache) {
-            cache_put<true>(cache, cap, sp, a, cnt, w, chunk, lost);
+            cache_put(cache, cap, sp, a, cnt, w, chunk, lost);
           }
           ++cnt;
         }
