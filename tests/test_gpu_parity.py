@@ -71,6 +71,21 @@ def test_small_configs(gpu_ctx, oracle_mod, name):
     check_pipeline(gpu_ctx, oracle_mod, dim, A, B, domain=1.0)
 
 
+@pytest.mark.parametrize("name", ["small2d_20x17", "small3d_7x6"])
+@pytest.mark.parametrize("scale,shift", [(1.0, 1.0e6), (1.0, -3.5e4), (1.0e-6, 0.0)])
+def test_far_and_tiny_coordinates(gpu_ctx, oracle_mod, name, scale, shift):
+    """Meshes far from the origin or scaled far below unit size: the
+    rounding margins of the exact early-outs and of the final-tet test grow
+    with the coordinates or are dominated by their absolute terms; per-pair
+    results still match the oracle."""
+    dim, (pa, ea), (pb, eb) = M.config_meshes(name)
+    A = (pa * scale + shift, ea)
+    B = (pb * scale + shift, eb)
+    st = check_pipeline(gpu_ctx, oracle_mod, dim, A, B)
+    assert st.n_intersecting > 0
+    assert abs(st.total_measure - scale ** dim) <= 1e-9 * scale ** dim
+
+
 def test_config_tri2d_73x100_full(gpu_ctx, oracle_mod):
     dim, A, B = M.config_meshes("tri2d_73x100")
     st = check_pipeline(gpu_ctx, oracle_mod, dim, A, B, domain=1.0)
