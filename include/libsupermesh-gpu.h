@@ -209,7 +209,10 @@ int libsupermesh_gpu_p2_inner_product(lsm_gpu_context *ctx, const lsm_gpu_mesh *
 /* Many independent mesh pairs in one call.  totals[npairs] receives each
  * pair's supermesh measure
  * and n_candidates[npairs] / n_intersecting[npairs] (optional) its counts.
- * All meshes live in the memory space given by on_device. */
+ * All meshes live in the memory space given by on_device.  Host meshes are
+ * copied in per dimension group; the 3D group's copies run on the context's
+ * second stream while the 2D group computes (pinned host memory lets them
+ * overlap).  The call returns with all its work on the device done. */
 int libsupermesh_gpu_supermesh_batched(lsm_gpu_context *ctx, int npairs,
                                        const lsm_gpu_mesh *a, const lsm_gpu_mesh *b,
                                        int on_device, double *totals,

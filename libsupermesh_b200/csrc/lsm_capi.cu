@@ -62,7 +62,9 @@ struct Ctx {
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
   DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand;
-  DevBuf bt_stage_pa, bt_stage_ea, bt_stage_pb, bt_stage_eb;
+  // host meshes of a batch staged on the device, one set per dimension (the
+  // 3D set is copied on the side stream while the 2D group computes)
+  DevBuf bt_stage_pa[2], bt_stage_ea[2], bt_stage_pb[2], bt_stage_eb[2];
   // 1D sort finder
   DevBuf d1_keyhi, d1_perm_a, d1_perm_b, d1_lo_a, d1_hi_a, d1_lo_b, d1_hi_b, d1_tree, d1_e, d1_l, d1_js;
   void* host_stage = nullptr;  // pinned, grow-only
@@ -202,7 +204,9 @@ void fini_ctx(Ctx* c) {
                    &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->wq_scratch, &c->x_a, &c->x_b, &c->x_measure,
                    &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
-                   &c->bt_ncand, &c->bt_stage_pa, &c->bt_stage_ea, &c->bt_stage_pb, &c->bt_stage_eb,
+                   &c->bt_ncand, &c->bt_stage_pa[0], &c->bt_stage_ea[0], &c->bt_stage_pb[0],
+                   &c->bt_stage_eb[0], &c->bt_stage_pa[1], &c->bt_stage_ea[1], &c->bt_stage_pb[1],
+                   &c->bt_stage_eb[1],
                    &c->d1_keyhi, &c->d1_perm_a, &c->d1_perm_b, &c->d1_lo_a, &c->d1_hi_a, &c->d1_lo_b,
                    &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over, &c->q_pool, &c->q_next, &c->q_first,
                    &c->a_faces, &c->b_screen, &c->surv};
@@ -606,13 +610,57 @@ void* host_stage(Ctx* c, size_t bytes) {
   return c->host_stage;
 }
 
+// Copies the host meshes of one batch group into the context's staging
+// buffers for that dimension (one copy per array and mesh, issued on st).
+// ptr receives their device addresses as four tables of idx.size() entries:
+// A's positions, A's element lists, B's positions, B's element lists.
+void stage_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu_mesh* ma,
+                       const lsm_gpu_mesh* mb, cudaStream_t st, std::vector<uint64_t>& ptr) {
+  const int nm = (int)idx.size();
+  const int ib = ma[idx[0]].index_bytes;
+  const int loc = dim + 1;
+  const int g = dim - 2;
+  int64_t na = 0, nb = 0, va = 0, vb = 0;
+  for (int i : idx) {
+    na += ma[i].nelements;
+    nb += mb[i].nelements;
+    va += ma[i].nnodes;
+    vb += mb[i].nnodes;
+  }
+  REQUIRE(na < (int64_t)0x7fffffff && nb < (int64_t)0x7fffffff, "batch has more than 2^31-1 elements");
+  double* spa = ensure<double>(c, c->bt_stage_pa[g], va * dim);
+  double* spb = ensure<double>(c, c->bt_stage_pb[g], vb * dim);
+  char* sea = ensure<char>(c, c->bt_stage_ea[g], na * loc * ib);
+  char* seb = ensure<char>(c, c->bt_stage_eb[g], nb * loc * ib);
+  ptr.assign(4 * (size_t)nm, 0);
+  int64_t oa = 0, ob = 0, ea = 0, eb = 0;
+  for (int i = 0; i < nm; ++i) {
+    const lsm_gpu_mesh& A = ma[idx[i]];
+    const lsm_gpu_mesh& B = mb[idx[i]];
+    ptr[i] = (uint64_t)(spa + oa * dim);
+    ptr[nm + i] = (uint64_t)(sea + ea * loc * ib);
+    ptr[2 * nm + i] = (uint64_t)(spb + ob * dim);
+    ptr[3 * nm + i] = (uint64_t)(seb + eb * loc * ib);
+    if (A.nnodes) CU(cudaMemcpyAsync(spa + oa * dim, A.positions, sizeof(double) * A.nnodes * dim, cudaMemcpyHostToDevice, st));
+    if (B.nnodes) CU(cudaMemcpyAsync(spb + ob * dim, B.positions, sizeof(double) * B.nnodes * dim, cudaMemcpyHostToDevice, st));
+    if (A.nelements) CU(cudaMemcpyAsync(sea + ea * loc * ib, A.enlist, (size_t)A.nelements * loc * ib, cudaMemcpyHostToDevice, st));
+    if (B.nelements) CU(cudaMemcpyAsync(seb + eb * loc * ib, B.enlist, (size_t)B.nelements * loc * ib, cudaMemcpyHostToDevice, st));
+    oa += A.nnodes;
+    ob += B.nnodes;
+    ea += A.nelements;
+    eb += B.nelements;
+  }
+}
+
 // All mesh pairs of one dimension through each phase in one launch:
 // batched prep (pointer tables), one sort by (mesh, Morton), one LBVH with a
 // subtree per mesh, one traversal, the usual clipper over all candidates,
 // and a per-mesh-pair reduction.  One host synchronisation (candidate count).
+// staged: the device addresses from stage_batch_group (host meshes), or
+// null when the meshes are on the device.
 void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu_mesh* ma,
-                     const lsm_gpu_mesh* mb, int on_device, double* totals, int64_t* ncand, int64_t* nint,
-                     cudaStream_t s) {
+                     const lsm_gpu_mesh* mb, const uint64_t* staged, double* totals, int64_t* ncand,
+                     int64_t* nint, cudaStream_t s) {
   const int nm = (int)idx.size();
   const int ib = ma[idx[0]].index_bytes;
   const int loc = dim + 1;
@@ -629,7 +677,7 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   uint64_t* eta = pta + nm;
   uint64_t* ptb = eta + nm;
   uint64_t* etb = ptb + nm;
-  int64_t na = 0, nb = 0, va = 0, vb = 0;
+  int64_t na = 0, nb = 0;
   for (int i = 0; i < nm; ++i) {
     const lsm_gpu_mesh& A = ma[idx[i]];
     const lsm_gpu_mesh& B = mb[idx[i]];
@@ -639,13 +687,11 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
     nnb[i] = B.nnodes;
     na += A.nelements;
     nb += B.nelements;
-    va += A.nnodes;
-    vb += B.nnodes;
   }
   eoa[nm] = na;
   eob[nm] = nb;
   REQUIRE(na < (int64_t)0x7fffffff && nb < (int64_t)0x7fffffff, "batch has more than 2^31-1 elements");
-  if (on_device) {
+  if (!staged) {
     for (int i = 0; i < nm; ++i) {
       pta[i] = (uint64_t)ma[idx[i]].positions;
       eta[i] = (uint64_t)ma[idx[i]].enlist;
@@ -653,26 +699,8 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
       etb[i] = (uint64_t)mb[idx[i]].enlist;
     }
   } else {
-    // stage host meshes into device buffers (one copy per array and mesh)
-    double* spa = ensure<double>(c, c->bt_stage_pa, va * dim);
-    double* spb = ensure<double>(c, c->bt_stage_pb, vb * dim);
-    char* sea = ensure<char>(c, c->bt_stage_ea, na * loc * ib);
-    char* seb = ensure<char>(c, c->bt_stage_eb, nb * loc * ib);
-    int64_t oa = 0, ob = 0;
-    for (int i = 0; i < nm; ++i) {
-      const lsm_gpu_mesh& A = ma[idx[i]];
-      const lsm_gpu_mesh& B = mb[idx[i]];
-      pta[i] = (uint64_t)(spa + oa * dim);
-      ptb[i] = (uint64_t)(spb + ob * dim);
-      eta[i] = (uint64_t)(sea + eoa[i] * loc * ib);
-      etb[i] = (uint64_t)(seb + eob[i] * loc * ib);
-      if (A.nnodes) CU(cudaMemcpyAsync(spa + oa * dim, A.positions, sizeof(double) * A.nnodes * dim, cudaMemcpyHostToDevice, s));
-      if (B.nnodes) CU(cudaMemcpyAsync(spb + ob * dim, B.positions, sizeof(double) * B.nnodes * dim, cudaMemcpyHostToDevice, s));
-      if (A.nelements) CU(cudaMemcpyAsync(sea + eoa[i] * loc * ib, A.enlist, (size_t)A.nelements * loc * ib, cudaMemcpyHostToDevice, s));
-      if (B.nelements) CU(cudaMemcpyAsync(seb + eob[i] * loc * ib, B.enlist, (size_t)B.nelements * loc * ib, cudaMemcpyHostToDevice, s));
-      oa += A.nnodes;
-      ob += B.nnodes;
-    }
+    // pta, eta, ptb, etb are consecutive tables of nm entries, as in staged
+    memcpy(pta, staged, sizeof(uint64_t) * 4 * (size_t)nm);
   }
   int64_t* dtab = ensure<int64_t>(c, c->bt_tabs, (int64_t)tab_words);
   void* htab = host_stage(c, sizeof(int64_t) * tab_words);
@@ -1426,8 +1454,28 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context* ctx, int npairs, const l
     }
     c->have_pairs = false;
     c->ncand = -1;
-    if (!g2.empty()) run_batch_group(c, 2, g2, a, b, on_device, totals, n_candidates, n_intersecting, s);
-    if (!g3.empty()) run_batch_group(c, 3, g3, a, b, on_device, totals, n_candidates, n_intersecting, s);
+    // Host meshes: the 2D group's copies go on the caller's stream; the 3D
+    // group's go on the side stream, where they overlap the 2D group's work
+    // (the side stream first waits for earlier work on s, which may still
+    // read the 3D staging buffers).
+    std::vector<uint64_t> st2, st3;
+    const bool side3 = !on_device && !g2.empty() && !g3.empty();
+    CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));  // side-stream copies of a call that failed midway
+    if (!on_device && !g2.empty()) stage_batch_group(c, 2, g2, a, b, s, st2);
+    if (!on_device && !g3.empty()) {
+      if (side3) {
+        CU(cudaEventRecord(c->side_ev[0], s));
+        CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
+      }
+      stage_batch_group(c, 3, g3, a, b, side3 ? c->side : s, st3);
+      if (side3) CU(cudaEventRecord(c->side_ev[1], c->side));
+    }
+    if (!g2.empty())
+      run_batch_group(c, 2, g2, a, b, on_device ? nullptr : st2.data(), totals, n_candidates, n_intersecting, s);
+    if (!g3.empty()) {
+      if (side3) CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
+      run_batch_group(c, 3, g3, a, b, on_device ? nullptr : st3.data(), totals, n_candidates, n_intersecting, s);
+    }
   });
 }
 

@@ -575,6 +575,26 @@ def test_batched_vs_oracle(gpu_ctx, oracle_mod):
         assert abs(totals[i] - st.total) <= REL_TOL
 
 
+def test_batched_host_calls_back_to_back(gpu_ctx):
+    """Host-buffer batches of both dimensions, called back to back with
+    growing meshes (the 3D group's meshes are copied on a second stream
+    while the 2D group computes, into staging buffers the previous call
+    used), give exactly the results of device-resident inputs."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda:0")
+    for seed, emax in ((31, 1e3), (32, 4e3), (33, 2e3)):
+        pairs = M.batched_pairs(10, seed=seed, emin=1e2, emax=emax)
+        assert {d for d, _, _ in pairs} == {2, 3}
+        host = [(A, B) for _, A, B in pairs]
+        t_h, nc_h, ni_h = gpu_ctx.supermesh_batched(host)
+        tdev = [tuple((torch.from_numpy(np.ascontiguousarray(x[0])).to(dev),
+                       torch.from_numpy(np.ascontiguousarray(x[1])).to(dev)) for x in pr) for pr in host]
+        torch.cuda.synchronize()
+        t_d, nc_d, ni_d = gpu_ctx.supermesh_batched(tdev, on_device=True)
+        assert np.array_equal(nc_h, nc_d) and np.array_equal(ni_h, ni_d) and np.array_equal(t_h, t_d)
+        assert np.abs(t_h - 1.0).max() <= 1e-12
+
+
 def test_batched_device_inputs_and_empty_mesh(gpu_ctx):
     torch = pytest.importorskip("torch")
     pairs = M.batched_pairs(8, seed=26, emin=1e2, emax=1e3)
