@@ -1484,15 +1484,30 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
   const int64_t per = ((npairs + gridDim.x - 1) / gridDim.x + blockDim.x - 1) / blockDim.x * blockDim.x;
   const int64_t beg = (int64_t)blockIdx.x * per;
   const int64_t end = beg + per < npairs ? beg + per : npairs;
+  // the pair indices stream from DRAM: each iteration loads the next one's
+  // (ni, na, nb) while it tests its own pair
+  int64_t ni = beg + threadIdx.x;
+  int na = 0, nb = 0;
+  if (ni < end) {
+    if (order) ni = order[ni];
+    na = pa[ni];
+    nb = pb[ni];
+  }
   for (int64_t base = beg; base < end; base += blockDim.x) {
     const int64_t j = base + threadIdx.x;
     bool live = false;
-    int64_t i = j;
-    int a = 0, b = 0, noop = 0;
+    const int64_t i = ni;
+    const int a = na, b = nb;
+    int noop = 0;
+    {
+      const int64_t jn = j + blockDim.x;
+      if (jn < end) {
+        ni = order ? (int64_t)order[jn] : jn;
+        na = pa[ni];
+        nb = pb[ni];
+      }
+    }
     if (j < end) {
-      if (order) i = order[j];
-      a = pa[i];
-      b = pb[i];
       Tet t;
       load_tet(coords_a + (int64_t)a * 12, t);
       const double* pl = setup_b + (int64_t)b * kSetup3;
