@@ -3397,53 +3397,8 @@ __device__ __forceinline__ int64_t node_of(const void* en, int64_t e, int loc, i
   return (int64_t)((const IDX*)en)[e * loc + k];
 }
 
-constexpr int kP1Block = 128;
-
-// One supermesh triangle's contribution to a 2D P1 block: area/3 times the
-// outer product of both elements' basis values at the three points (4,1,1)/6
-// (test_parallel_p1_inner_product_2d.F90:62-68, 283-297).
-__device__ __forceinline__ void p1_tri_2d(const double* ca, const double* cb, double x0, double y0, double x1,
-                                          double y1, double x2, double y2, double (&blk)[9]) {
-  const double qp0 = 4.0 / 6.0, qp1 = 1.0 / 6.0;
-  const double meas = tri_area(x0, y0, x1, y1, x2, y2);
-  const double w = (1.0 / 3.0) * meas;
-#pragma unroll
-  for (int qq = 0; qq < 3; ++qq) {
-    const double w0 = qq == 0 ? qp0 : qp1;
-    const double w1 = qq == 1 ? qp0 : qp1;
-    const double w2 = qq == 2 ? qp0 : qp1;
-    const double x = (w0 * x0 + w1 * x1) + w2 * x2;
-    const double y = (w0 * y0 + w1 * y1) + w2 * y2;
-    double fa[3], fb[3];
-    p1_basis_2d(ca, x, y, fa);
-    p1_basis_2d(cb, x, y, fb);
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) blk[r * 3 + c] += w * fa[r] * fb[c];
-  }
-}
-
-// The rare 2D pair whose clip needs more than kTriCap polygon slots: the
-// same clip on the reference's full buffer in local memory, out of line so
-// that the common path keeps its registers.
-__device__ __noinline__ void p1_block_2d_wide(const double* ca, const double* cb, const Lines& L, double tol,
-                                              double* out) {
-  double blk[9];
-#pragma unroll
-  for (int j = 0; j < 9; ++j) blk[j] = 0.0;
-  LocalPoly<kTriWideCap> p, q;
-  double m;
-  clip_tri(ca[0], ca[1], ca[2], ca[3], ca[4], ca[5], L, tol, p, q, kTriWideCap, m,
-           [&](int, double x0, double y0, double x1, double y1, double x2, double y2) {
-             p1_tri_2d(ca, cb, x0, y0, x1, y1, x2, y2, blk);
-           });
-#pragma unroll
-  for (int j = 0; j < 9; ++j) out[j] = blk[j];
-}
-
 template <int DIM, typename IDX>
-__global__ void __launch_bounds__(kP1Block) k_p1_mass(int64_t npairs, const int32_t* __restrict__ pa,
+__global__ void __launch_bounds__(128) k_p1_mass(int64_t npairs, const int32_t* __restrict__ pa,
                                                  const int32_t* __restrict__ pb,
                                                  const double* __restrict__ coords_a,
                                                  const double* __restrict__ tol_a,
@@ -3453,9 +3408,6 @@ __global__ void __launch_bounds__(kP1Block) k_p1_mass(int64_t npairs, const int3
                                                  const double* __restrict__ v_b, double* blocks,
                                                  Partial* partials) {
   constexpr int LOC = DIM + 1;
-  // 2D polygons in shared memory (kTriCap slots, as in k_clip_tris); only
-  // DIM == 2 launches size it
-  extern __shared__ double p1_poly[];
   double sum = 0.0, err = 0.0;
   unsigned long long ni = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npairs;
@@ -3466,25 +3418,34 @@ __global__ void __launch_bounds__(kP1Block) k_p1_mass(int64_t npairs, const int3
     double blk[LOC * LOC];
 #pragma unroll
     for (int j = 0; j < LOC * LOC; ++j) blk[j] = 0.0;
-    if constexpr (DIM == 2) {
+    if (DIM == 2) {
       Lines L;
       double tolb;
       load_lines(setup_b + (int64_t)b * kSetup2, L, tolb);
       const double tol = fmin(tol_a[a], tolb);
+      LocalPoly<kTriWideCap> p, q;
       double m;
-      SmemPoly<kP1Block> p{p1_poly + threadIdx.x}, q{p1_poly + 2 * kTriCap * kP1Block + threadIdx.x};
-      // clip_tri emits nothing before all three stages fit: a pair that
-      // needs more than kTriCap slots (degenerate touching) starts again on
-      // the reference's full buffer in local memory
-      if (clip_tri(ca[0], ca[1], ca[2], ca[3], ca[4], ca[5], L, tol, p, q, kTriCap, m,
-                   [&](int, double x0, double y0, double x1, double y1, double x2, double y2) {
-                     p1_tri_2d(ca, cb, x0, y0, x1, y1, x2, y2, blk);
-                   }) < 0) {
-        double wide[9];
-        p1_block_2d_wide(ca, cb, L, tol, wide);
+      const double qp0 = 4.0 / 6.0, qp1 = 1.0 / 6.0;
+      clip_tri(ca[0], ca[1], ca[2], ca[3], ca[4], ca[5], L, tol, p, q, kTriWideCap, m,
+               [&](int, double x0, double y0, double x1, double y1, double x2, double y2) {
+                 const double meas = tri_area(x0, y0, x1, y1, x2, y2);
+                 const double w = (1.0 / 3.0) * meas;
 #pragma unroll
-        for (int j = 0; j < 9; ++j) blk[j] = wide[j];
-      }
+                 for (int qq = 0; qq < 3; ++qq) {
+                   const double w0 = qq == 0 ? qp0 : qp1;
+                   const double w1 = qq == 1 ? qp0 : qp1;
+                   const double w2 = qq == 2 ? qp0 : qp1;
+                   const double x = (w0 * x0 + w1 * x1) + w2 * x2;
+                   const double y = (w0 * y0 + w1 * y1) + w2 * y2;
+                   double fa[3], fb[3];
+                   p1_basis_2d(ca, x, y, fa);
+                   p1_basis_2d(cb, x, y, fb);
+#pragma unroll
+                   for (int r = 0; r < 3; ++r)
+#pragma unroll
+                     for (int c = 0; c < 3; ++c) blk[r * 3 + c] += w * fa[r] * fb[c];
+                 }
+               });
     } else {
       Tet t;
       load_tet(ca, t);
@@ -3676,16 +3637,15 @@ cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const
                            int idx_bytes, const double* u_a, const double* v_b, double* blocks,
                            Partial* partials, cudaStream_t s) {
   const int g = p1_grid_blocks(dim);
-  const size_t poly = sizeof(double) * 2 * 2 * kTriCap * kP1Block;
   count_launch();
   if (dim == 2 && idx_bytes == 4)
-    k_p1_mass<2, int32_t><<<g, kP1Block, poly, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+    k_p1_mass<2, int32_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
   else if (dim == 2)
-    k_p1_mass<2, int64_t><<<g, kP1Block, poly, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+    k_p1_mass<2, int64_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
   else if (idx_bytes == 4)
-    k_p1_mass<3, int32_t><<<g, kP1Block, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+    k_p1_mass<3, int32_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
   else
-    k_p1_mass<3, int64_t><<<g, kP1Block, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+    k_p1_mass<3, int64_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
   return cudaGetLastError();
 }
 
