@@ -292,11 +292,21 @@ class Context:
                                                                     None))
         return m[:n], k[:n], (e[:n] if e is not None else None)
 
-    def p1_mass(self, mesh_a, mesh_b, u_a=None, v_b=None, want_blocks: bool = False):
-        """Returns (u^T M v or None, blocks or None) for host meshes."""
-        ma, mb = _mesh(*mesh_a, False), _mesh(*mesh_b, False)
+    def p1_mass(self, mesh_a, mesh_b, u_a=None, v_b=None, want_blocks: bool = False,
+                on_device: bool = False, stream: int | None = None):
+        """Returns (u^T M v or None, blocks or None).  Host meshes and fields,
+        or with on_device meshes and fields in device memory (torch tensors;
+        blocks then not available)."""
+        ma, mb = _mesh(*mesh_a, on_device), _mesh(*mesh_b, on_device)
         if ma.index_bytes != mb.index_bytes:
             raise ValueError("A and B must use the same index width")
+        if on_device:
+            if want_blocks:
+                raise ValueError("want_blocks needs host meshes")
+            integral = ctypes.c_double(0.0)
+            self._check(self.lib.libsupermesh_gpu_p1_mass(self._h, ctypes.byref(ma), ctypes.byref(mb), _ptr(u_a),
+                                                          _ptr(v_b), None, ctypes.byref(integral), 1, stream))
+            return (integral.value if u_a is not None and v_b is not None else None), None
         u = np.ascontiguousarray(u_a, dtype=np.float64) if u_a is not None else None
         v = np.ascontiguousarray(v_b, dtype=np.float64) if v_b is not None else None
         blocks, n = None, 0
@@ -306,7 +316,7 @@ class Context:
             blocks = np.zeros((max(n, 1), loc, loc))
         integral = ctypes.c_double(0.0)
         self._check(self.lib.libsupermesh_gpu_p1_mass(self._h, ctypes.byref(ma), ctypes.byref(mb), _ptr(u),
-                                                      _ptr(v), _ptr(blocks), ctypes.byref(integral), 0, None))
+                                                      _ptr(v), _ptr(blocks), ctypes.byref(integral), 0, stream))
         return (integral.value if u is not None else None), (blocks[:n] if blocks is not None else None)
 
     def p2_inner_product(self, mesh_a, mesh_b, enlist_p2_a, field_a, enlist_p2_b, field_b,

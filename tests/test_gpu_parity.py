@@ -395,6 +395,24 @@ def test_legacy_single_pair_entries(oracle_mod):
         assert lsm.tetrahedron_volume(a[i]) == oracle_mod.tetrahedron_volume(a[i])
 
 
+@pytest.mark.parametrize("name", ["small2d_12x17", "small3d_4x5"])
+def test_p1_mass_device_inputs(gpu_ctx, name):
+    """Device-resident meshes and fields give the host call's u^T M v, bit
+    for bit."""
+    torch = pytest.importorskip("torch")
+    dim, A, B = M.config_meshes(name)
+    u = np.cos(3 * A[0][:, 0]) + A[0][:, 1]
+    v = np.sin(2 * B[0][:, 1]) - B[0][:, 0]
+    ref, _ = gpu_ctx.p1_mass(A, B, u, v)
+    dev = torch.device("cuda:0")
+    tA = tuple(torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in A)
+    tB = tuple(torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in B)
+    tu, tv = torch.from_numpy(u).to(dev), torch.from_numpy(v).to(dev)
+    torch.cuda.synchronize()
+    val, blocks = gpu_ctx.p1_mass(tA, tB, tu, tv, on_device=True)
+    assert blocks is None and val == ref
+
+
 def test_p1_mass_reference_answers(gpu_ctx, oracle_mod, ref_meshes):
     A, B = ref_meshes("triangle_0_01"), ref_meshes("square_0_01")
     integral, _ = gpu_ctx.p1_mass(A, B, A[0][:, 0], B[0][:, 1])
