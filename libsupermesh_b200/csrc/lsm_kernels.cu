@@ -3410,9 +3410,23 @@ __global__ void __launch_bounds__(128) k_p1_mass(int64_t npairs, const int32_t* 
   constexpr int LOC = DIM + 1;
   double sum = 0.0, err = 0.0;
   unsigned long long ni = 0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npairs;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int a = pa[i], b = pb[i];
+  // each iteration loads the next one's pair indices (which stream from
+  // DRAM) before it works on its own pair
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int na = 0, nb = 0;
+  {
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i0 < npairs) {
+      na = pa[i0];
+      nb = pb[i0];
+    }
+  }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npairs; i += stride) {
+    const int a = na, b = nb;
+    if (i + stride < npairs) {
+      na = pa[i + stride];
+      nb = pb[i + stride];
+    }
     const double* ca = coords_a + (int64_t)a * LOC * DIM;
     const double* cb = coords_b + (int64_t)b * LOC * DIM;
     double blk[LOC * LOC];
