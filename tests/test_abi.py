@@ -86,6 +86,26 @@ def test_legacy_api_without_gpu_aborts_loudly():
     assert "libsupermesh (B200) error" in r.stderr
 
 
+def test_missing_library_raises_instead_of_falling_back(tmp_path):
+    """Without the CUDA library every entry of the Python package raises;
+    nothing computes on the CPU in its place."""
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "from pathlib import Path\n"
+        "import libsupermesh_b200 as L\n"
+        "L._LIB = Path(%r)\n"
+        "for f in (L.load, lambda: L.Context(0), lambda: L.triangle_area([[0,0],[1,0],[0,1]])):\n"
+        "    try:\n"
+        "        f()\n"
+        "    except RuntimeError as e:\n"
+        "        assert 'no CPU implementation' in str(e), e\n"
+        "    else:\n"
+        "        raise SystemExit('no error')\n"
+        "print('ok')\n" % (str(ROOT), str(tmp_path / "missing.so")))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stderr
+
+
 def test_tuning_options_host_side(lib):
     """Options are process-wide host settings: valid values round-trip,
     invalid names/values are rejected (no GPU needed)."""
