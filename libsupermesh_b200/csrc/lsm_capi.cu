@@ -1460,21 +1460,30 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context* ctx, int npairs, const l
     // read the 3D staging buffers).
     std::vector<uint64_t> st2, st3;
     const bool side3 = !on_device && !g2.empty() && !g3.empty();
-    CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));  // side-stream copies of a call that failed midway
-    if (!on_device && !g2.empty()) stage_batch_group(c, 2, g2, a, b, s, st2);
-    if (!on_device && !g3.empty()) {
-      if (side3) {
-        CU(cudaEventRecord(c->side_ev[0], s));
-        CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
+    try {
+      if (!on_device && !g2.empty()) stage_batch_group(c, 2, g2, a, b, s, st2);
+      if (!on_device && !g3.empty()) {
+        if (side3) {
+          CU(cudaEventRecord(c->side_ev[0], s));
+          CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
+        }
+        stage_batch_group(c, 3, g3, a, b, side3 ? c->side : s, st3);
+        if (side3) CU(cudaEventRecord(c->side_ev[1], c->side));
       }
-      stage_batch_group(c, 3, g3, a, b, side3 ? c->side : s, st3);
-      if (side3) CU(cudaEventRecord(c->side_ev[1], c->side));
-    }
-    if (!g2.empty())
-      run_batch_group(c, 2, g2, a, b, on_device ? nullptr : st2.data(), totals, n_candidates, n_intersecting, s);
-    if (!g3.empty()) {
-      if (side3) CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
-      run_batch_group(c, 3, g3, a, b, on_device ? nullptr : st3.data(), totals, n_candidates, n_intersecting, s);
+      if (!g2.empty())
+        run_batch_group(c, 2, g2, a, b, on_device ? nullptr : st2.data(), totals, n_candidates, n_intersecting, s);
+      if (!g3.empty()) {
+        if (side3) CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
+        run_batch_group(c, 3, g3, a, b, on_device ? nullptr : st3.data(), totals, n_candidates, n_intersecting, s);
+      }
+    } catch (...) {
+      // a failed call returns only when no copy still reads the caller's
+      // host meshes or writes the staging buffers
+      if (!on_device) {
+        cudaStreamSynchronize(s);
+        if (side3) cudaStreamSynchronize(c->side);
+      }
+      throw;
     }
   });
 }
