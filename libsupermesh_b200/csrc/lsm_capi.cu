@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -120,6 +121,20 @@ void set_error(Ctx* c, const char* fmt, ...) {
       throw Fail{LSM_ERROR_INVALID_ARGUMENT}; \
     }                              \
   } while (0)
+
+// When an exception leaves its scope, waits for both streams, so that a
+// failed call returns with no copy or kernel of its own still reading the
+// caller's meshes.
+struct SyncOnThrow {
+  cudaStream_t s0, s1;
+  int depth = std::uncaught_exceptions();
+  ~SyncOnThrow() {
+    if (std::uncaught_exceptions() > depth) {
+      cudaStreamSynchronize(s0);
+      cudaStreamSynchronize(s1);
+    }
+  }
+};
 
 template <class T>
 T* ensure(Ctx* c, DevBuf& b, int64_t count) {
@@ -440,6 +455,7 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   // A's upload and prep run on the side stream, overlapping B's prep and
   // tree build on s; s waits for them before the search.  A's copies start
   // once B's are done, so B's (on the critical path) get the whole link.
+  SyncOnThrow sync_on_throw{s, c->side};
   CU(cudaMemsetAsync(bad_flag(c), 0, sizeof(int) * 64, s));
   MeshDev b = upload(c, mb, on_device, c->b_pos, c->b_en, s);
   CU(cudaEventRecord(c->side_ev[0], s));
@@ -1460,30 +1476,21 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context* ctx, int npairs, const l
     // read the 3D staging buffers).
     std::vector<uint64_t> st2, st3;
     const bool side3 = !on_device && !g2.empty() && !g3.empty();
-    try {
-      if (!on_device && !g2.empty()) stage_batch_group(c, 2, g2, a, b, s, st2);
-      if (!on_device && !g3.empty()) {
-        if (side3) {
-          CU(cudaEventRecord(c->side_ev[0], s));
-          CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
-        }
-        stage_batch_group(c, 3, g3, a, b, side3 ? c->side : s, st3);
-        if (side3) CU(cudaEventRecord(c->side_ev[1], c->side));
+    SyncOnThrow sync_on_throw{s, c->side};
+    if (!on_device && !g2.empty()) stage_batch_group(c, 2, g2, a, b, s, st2);
+    if (!on_device && !g3.empty()) {
+      if (side3) {
+        CU(cudaEventRecord(c->side_ev[0], s));
+        CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
       }
-      if (!g2.empty())
-        run_batch_group(c, 2, g2, a, b, on_device ? nullptr : st2.data(), totals, n_candidates, n_intersecting, s);
-      if (!g3.empty()) {
-        if (side3) CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
-        run_batch_group(c, 3, g3, a, b, on_device ? nullptr : st3.data(), totals, n_candidates, n_intersecting, s);
-      }
-    } catch (...) {
-      // a failed call returns only when no copy still reads the caller's
-      // host meshes or writes the staging buffers
-      if (!on_device) {
-        cudaStreamSynchronize(s);
-        if (side3) cudaStreamSynchronize(c->side);
-      }
-      throw;
+      stage_batch_group(c, 3, g3, a, b, side3 ? c->side : s, st3);
+      if (side3) CU(cudaEventRecord(c->side_ev[1], c->side));
+    }
+    if (!g2.empty())
+      run_batch_group(c, 2, g2, a, b, on_device ? nullptr : st2.data(), totals, n_candidates, n_intersecting, s);
+    if (!g3.empty()) {
+      if (side3) CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
+      run_batch_group(c, 3, g3, a, b, on_device ? nullptr : st3.data(), totals, n_candidates, n_intersecting, s);
     }
   });
 }
