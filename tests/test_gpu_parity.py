@@ -613,6 +613,30 @@ def test_batched_host_calls_back_to_back(gpu_ctx):
         assert np.abs(t_h - 1.0).max() <= 1e-12
 
 
+def test_batched_host_error_then_recovery(gpu_ctx):
+    """An invalid node index in a 2D mesh fails the batch while the 3D
+    group's copies may still be running on the second stream; the call
+    reports it (the kernels' bounds checks turn it into a status), and the
+    next batch on the same context gives the expected results."""
+    pairs = M.batched_pairs(8, seed=41, emin=1e2, emax=2e3)
+    host = [(A, B) for _, A, B in pairs]
+    i2 = next(i for i, (d, _, _) in enumerate(pairs) if d == 2)
+    assert any(d == 3 for d, _, _ in pairs)
+    A0, B0 = host[i2]
+    en = A0[1].copy()
+    en[0, 0] = len(A0[0]) + 7
+    bad = list(host)
+    bad[i2] = ((A0[0], en), B0)
+    with pytest.raises(lsm.LsmError) as e:
+        gpu_ctx.supermesh_batched(bad)
+    assert e.value.status == 1
+    t, nc, ni = gpu_ctx.supermesh_batched(host)
+    for i, (dim, A, B) in enumerate(pairs):
+        st, _ = gpu_ctx.supermesh(A, B)
+        assert nc[i] == st.n_candidates and ni[i] == st.n_intersecting
+        assert abs(t[i] - 1.0) <= 1e-12
+
+
 def test_batched_device_inputs_and_empty_mesh(gpu_ctx):
     torch = pytest.importorskip("torch")
     pairs = M.batched_pairs(8, seed=26, emin=1e2, emax=1e3)
