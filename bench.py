@@ -455,6 +455,7 @@ def run_ours(args, world, rank, local):
                    "tuning": (tuning or {}).get("setting")},
         "total_measure": st.total_measure,
         "measure_err_vs_domain": abs(st.total_measure - 1.0),
+        "intersecting_pairs_per_s": whole_job_rate(st.n_intersecting, args.steps, world, ms_dev),
         "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": ms_e2e / args.steps},
         "gpu_launches": per_step_launches * args.steps,
