@@ -4,29 +4,39 @@ One step = one pass of the hot path over one pair of meshes: candidate
 search (LBVH build + traversal), intersection of every candidate pair, and
 the compensated measure reduction, through libsupermesh_gpu_supermesh.
 
-Workload (default): 3D plain supermesh, target 27^3 x 6 = 118,098 Kuhn tets
-(seed 3) against source 32^3 x 6 = 196,608 tets (seed 2), jitter 0.25h,
-FP64.  The unit of work is one candidate pair of the strict-AABB candidate
-set (the tree finder's set); pairs/s = candidates / step time.
+Workload (default): 3D graded supermesh, target 55^3 x 6 = 998,250 Kuhn tets
+(seed 7) against source 51^3 x 6 = 795,906 tets (seed 8), coordinates graded
+x -> x^2 per axis, jitter 0.2h, FP64 (56.1M candidate pairs).  The unit of
+work is one candidate pair of the strict-AABB candidate set (the tree
+finder's set); pairs/s = candidates / step time.
 
-  value      device-resident inputs (positions/enlists already in HBM)
+  value      device-resident inputs (positions/enlists already in HBM), L2
+             flushed before every step
   e2e        the same call with host (pinned) inputs: H2D of positions and
              element lists and D2H of the per-element measure in the timed
              region
-  roofline   the dominant kernels (3D: the exact early-out pass and the tet
-             clipper, which together settle every candidate; 2D: the
-             triangle clipper), timed alone over the same candidates, with
-             the reference algorithm's FLOP count for all candidates,
-             against the measured FP64 DADD/DMUL issue rate
+  e2e_with_pairs  as e2e, plus the D2H of what a drop-in caller of the C API
+             reads per candidate: the CSR (ind_ptr, indices as int64, the
+             get_output layout) and per-pair measure and output count
+  roofline   narrow phase: the exact early-out pass and the tet clipper (3D;
+             together they settle every candidate) or the triangle clipper
+             (2D), timed by the library's CUDA events over the same
+             candidates, with the reference algorithm's FLOP count for all
+             candidates, against the measured FP64 DADD/DMUL issue rate;
+             broad_phase: the candidate search's algorithmic bytes over its
+             device time, against the measured HBM copy bandwidth
+  schedule   (3D) the narrow phase with the learned scheduler's bins beside
+             the plain order, when trained weights are present
   cpu_baseline  the oracle restatement of the reference algorithm
-             (quadtree/octree + breadth-first clipping), one thread, full
-             workload, on this host
+             (quadtree/octree + breadth-first clipping), one thread, on a
+             bounded sample of the workload (every k-th target element)
 
 Multi-GPU: the workload is replicated per rank (independent replicas, no
 collective on the data path); value = all ranks' pairs / max step time.
 
 `--impl reference` times the reference algorithm on the host CPU (the oracle
-restatement, all host threads; the Fortran reference cannot be built here).
+restatement, all host threads; the Fortran reference cannot be built here)
+on a bounded sample of the same workload per step.
 """
 from __future__ import annotations
 
@@ -57,7 +67,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", default="tet3d_27x32")
+    p.add_argument("--workload", default="tet3d_graded_55x51")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--kernel-only", action="store_true",
                    help="run only warm-up + timed steps (for profiler launch lists)")
@@ -205,13 +215,34 @@ def measured_peaks():
 
 def cpu_baseline(dim, A, B, threads: int = 1):
     """Oracle (reference algorithm) on this host: full pipeline as the C API
-    caller drives it.  Returns (pairs/s, seconds, stats, flops)."""
+    caller drives it.  Returns (pairs/s, seconds, stats)."""
     import oracle
 
     t0 = time.perf_counter()
     st = oracle.supermesh(dim, A, B, nthreads=threads)
     dt = time.perf_counter() - t0
     return st.n_candidates / dt, dt, st
+
+
+def corner_sample(dim, A, B, frac: float = 0.125):
+    """Bounded CPU sample of a workload: both meshes cut to the same corner
+    box [lo, X]^dim, X the per-axis quantile of A's element centroids that
+    keeps about `frac` of A's elements (B keeps about the same share, the
+    meshes being graded alike).  The octree build, the queries and the
+    clipping then shrink together, so pairs/s keeps the full workload's mix
+    of build, search and clipping cost."""
+    q = frac ** (1.0 / dim)
+    ca = A[0][A[1]].mean(axis=1)
+    X = float(np.quantile(ca[:, 0], q))
+
+    def cut(m):
+        inside = np.all(m[0][m[1]].max(axis=1) <= X, axis=1)
+        return (m[0], np.ascontiguousarray(m[1][inside]))
+
+    As, Bs = cut(A), cut(B)
+    desc = (f"corner box x,y,z <= {X:.4g}: {len(As[1])} of {len(A[1])} target and {len(Bs[1])} of {len(B[1])} "
+            f"source elements")
+    return As, Bs, desc
 
 
 def algorithmic_flops(dim, A, B):
@@ -225,32 +256,43 @@ def algorithmic_flops(dim, A, B):
     return st.flops, st
 
 
+def workload_config(args, dim, A, B, n_cand, world):
+    """The `config` object of both arms' lines (identical for the same workload)."""
+    return {"workload": args.workload, "dim": dim, "elements_a": int(len(A[1])), "elements_b": int(len(B[1])),
+            "candidates": int(n_cand), "parallelism": f"replicas x{world}",
+            "l2": "GPU arm: flushed before every timed step (256 MiB write, outside the events)"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
+    import oracle
+
     from libsupermesh_b200 import meshes as M
 
     dim, A, B = M.config_meshes(args.workload)
+    As, Bs, desc = corner_sample(dim, A, B) if len(A[1]) > 200_000 else (A, B, "full workload")
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        cpu_baseline(dim, A, B, threads)
+        cpu_baseline(dim, As, Bs, threads)
     times, st = [], None
     for _ in range(args.steps):
-        _, dt, st = cpu_baseline(dim, A, B, threads)
+        _, dt, st = cpu_baseline(dim, As, Bs, threads)
         times.append(dt)
     total = sum(times)
     value = st.n_candidates * args.steps / total
+    ip, ind = oracle.tree_finder(dim, A, B) if desc != "full workload" else (None, np.zeros(st.n_candidates))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "candidates": st.n_candidates},
+        "config": workload_config(args, dim, A, B, len(ind), world),
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
-                         "sample": "full workload per step: oracle quadtree/octree finder (1 thread) + "
-                                   "breadth-first clipping (OpenMP over A rows)"},
+                         "sample": f"per step: {desc} ({st.n_candidates} candidates); oracle quadtree/octree "
+                                   f"finder (1 thread) + breadth-first clipping (OpenMP over A rows)"},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "total_measure": st.total,
+        "sample_total_measure": st.total,
     }
     print(json.dumps(line), flush=True)
 
@@ -342,6 +384,16 @@ def run_batched(args, world, rank, local):
     ctx.close()
 
 
+def broad_phase_bytes(dim, A, B, n_cand):
+    """Algorithmic bytes of the candidate search: both meshes' positions and
+    element lists read once, 8 B per candidate pair written, and the radix
+    sort of B's Morton keys (4 passes x (4 B key + 4 B value) read and
+    written per element)."""
+    pos = A[0].nbytes + B[0].nbytes
+    en = len(A[1]) * A[1].shape[1] * 8 + len(B[1]) * B[1].shape[1] * 8
+    return pos + en + 8 * n_cand + 4 * 16 * len(B[1])
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -374,7 +426,7 @@ def run_ours(args, world, rank, local):
     def step_device():
         return ctx.supermesh(tA, tB, elem_measure=True, on_device=True, out=em_dev, stream=sp)[0]
 
-    # pinned host inputs for the end-to-end leg
+    # pinned host inputs and outputs for the end-to-end legs
     def pinned(a):
         t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
         return t.numpy()
@@ -427,9 +479,31 @@ def run_ours(args, world, rank, local):
     e2e = whole_job_rate(n_cand, args.steps, world, ms_e2e)
     assert st_e2e.n_candidates == n_cand and st_e2e.total_measure == st.total_measure
 
-    # dominant kernel alone: the clip kernel over the same candidates, timed
-    # by the library with CUDA events on its stream around that launch
-    step_device()
+    # e2e with the per-candidate outputs a drop-in caller reads: the CSR
+    # (get_output layout, int64) and each pair's measure and output count
+    nel_a = len(A[1])
+    csr_out = (pinned(np.zeros(nel_a + 1, dtype=np.int64)), pinned(np.zeros(max(n_cand, 1), dtype=np.int64)))
+    pair_out = (pinned(np.zeros(max(n_cand, 1))), pinned(np.zeros(max(n_cand, 1), dtype=np.int32)))
+
+    def step_e2e_pairs():
+        r = ctx.supermesh(hA, hB, elem_measure=True, on_device=False, out=em_host, stream=sp)[0]
+        ctx.get_candidates(nel_a, n_cand, out=csr_out, stream=sp)
+        ctx.pair_results(n_cand, out=pair_out, stream=sp)
+        return r
+
+    pair_steps = max(3, args.steps // 4)
+    ms_e2e_p, st_p = timed(step_e2e_pairs, pair_steps, 2)
+    ms_e2e_p = all_max(ms_e2e_p, world)
+    assert st_p.total_measure == st.total_measure
+    d2h_pairs = d2h + (nel_a + 1) * 8 + n_cand * (8 + 8 + 4)
+
+    # broad phase alone (device-resident meshes): search time with events
+    ms_bp, _ = timed(lambda: ctx.find_candidates(tA, tB, on_device=True, stream=sp), args.steps, 2)
+    ms_bp = all_max(ms_bp, world) / args.steps
+    step_device()  # leave the full pipeline's candidates and per-pair results current
+
+    # narrow phase alone: the clipping kernels over the same candidates,
+    # timed by the library with CUDA events on its stream
     lsm.set_option("time_kernels", 1)
     for _ in range(3):
         ctx.clip_candidates(stream=sp)
@@ -440,27 +514,31 @@ def run_ours(args, world, rank, local):
         kernel_ms.append(ctx.clip_kernel_ms())
     lsm.set_option("time_kernels", 0)
     clip_ms = all_max(sum(kernel_ms), world) / args.steps
-    clip_kernel = ("k_prefilter_tets+" + {0: "k_clip_tets_ix", 1: "k_clip_tets_wq", 2: "k_clip_tets"}[
-        lsm.get_option("tet_clipper")] if dim == 3 else "k_clip_tris")
+    clip_kernel = "k_prefilter_tets+k_clip_tets_ix" if dim == 3 else "k_clip_tris"
 
     line = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "dim": dim, "elements_a": int(len(A[1])),
-                   "elements_b": int(len(B[1])), "candidates": n_cand,
-                   "intersecting": st.n_intersecting, "out_simplices": st.n_out_simplices,
-                   "l2": "flushed before every timed step (256 MiB write, outside the events)",
-                   "parallelism": f"replicas x{world}",
-                   "tuning": (tuning or {}).get("setting")},
-        "total_measure": st.total_measure,
-        "measure_err_vs_domain": abs(st.total_measure - 1.0),
+        "config": workload_config(args, dim, A, B, n_cand, world),
+        "results": {"intersecting": st.n_intersecting, "out_simplices": st.n_out_simplices,
+                    "total_measure": st.total_measure, "measure_err_vs_domain": abs(st.total_measure - 1.0)},
+        "tuning": (tuning or {}).get("setting"),
         "intersecting_pairs_per_s": whole_job_rate(st.n_intersecting, args.steps, world, ms_dev),
         "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": ms_e2e / args.steps},
+        "e2e_with_pairs": {"value": whole_job_rate(n_cand, pair_steps, world, ms_e2e_p), "unit": "pairs/s",
+                           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h_pairs,
+                           "ms_per_step": ms_e2e_p / pair_steps,
+                           "outputs": "per-element measure + CSR ind_ptr/indices (int64) + per-pair measure "
+                                      "(f64) and output count (i32), into pinned host arrays"},
         "gpu_launches": per_step_launches * args.steps,
         "clocks": clock_rec,
     }
+    if dim == 3:
+        sched = schedule_legs(ctx, sp, flush, args.steps, world)
+        if sched:
+            line["schedule"] = sched
     if rank == 0:
         peak_rate = probe.lsm_probe_fp64_rate(0, 5)
         fma_rate = probe.lsm_probe_fp64_rate(1, 5)
@@ -468,14 +546,17 @@ def run_ours(args, world, rank, local):
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             flops, _ = algorithmic_flops(dim, A, B)
-            v, dt, st_cpu = cpu_baseline(dim, A, B, 1)
+            As, Bs, desc = corner_sample(dim, A, B) if len(A[1]) > 200_000 else (A, B, "full workload")
+            v, dt, st_cpu = cpu_baseline(dim, As, Bs, 1)
             cpu = {"value": v, "unit": "pairs/s", "cores": 1, "kind": "port",
-                   "sample": f"full workload ({st_cpu.n_candidates} candidates), oracle quadtree/octree "
+                   "sample": f"{desc} ({st_cpu.n_candidates} candidates), oracle quadtree/octree "
                              f"finder + breadth-first clipping, 1 thread, {dt:.2f} s"}
-            assert st_cpu.n_candidates == n_cand
-            line["cpu_total_measure"] = st_cpu.total
         achieved = flops / (clip_ms * 1e-3) / 1e12 if flops else None
         peak = peak_rate / 1e12 if peak_rate > 0 else None
+        pk = measured_peaks()
+        hbm = pk.get("hbm_gbs")
+        bp_bytes = broad_phase_bytes(dim, A, B, n_cand)
+        bp_gbs = bp_bytes / (ms_bp * 1e-3) / 1e9
         line["roofline"] = {
             "kernel": clip_kernel,
             "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -485,14 +566,22 @@ def run_ours(args, world, rank, local):
             "flops_per_launch": flops,
             "peak_source": "measured in-run: DADD+DMUL issue rate, 1 op each (the clipper is FMA-free); "
                            f"DFMA rate for context {fma_rate / 1e12:.1f} TFLOP/s",
+            "broad_phase": {"bound": "hbm", "achieved": bp_gbs, "peak": hbm, "unit": "GB/s",
+                            "frac": (bp_gbs / hbm) if hbm else None, "ms": ms_bp, "bytes": bp_bytes,
+                            "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)",
+                            "note": "search time includes the host read of the candidate count"},
         }
-        pk = measured_peaks()
-        line["roofline"]["hbm_peak_gbs"] = pk.get("hbm_gbs")
         line["cpu_baseline"] = cpu
         if dim == 2:
             line["p1_mass"] = p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush)
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def schedule_legs(ctx, sp, flush, steps, world):
+    """Learned-scheduler legs of the 3D narrow phase (filled in once the
+    scheduler exists)."""
+    return None
 
 
 def p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush):

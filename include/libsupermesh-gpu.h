@@ -85,6 +85,24 @@ int64_t libsupermesh_gpu_kernel_launches(void);
  *   "tet_screen"         1 (default): tet pairs whose B lies beyond a face plane of A by a
  *                        proven rounding margin skip the clipper (exact: the reference
  *                        returns no tets for them); 0: only the A-beyond-a-face-of-B test
+ *   "tet_schedule"       order of the 3D clipper's work list (never changes results):
+ *                        0 (default) plain: the early-out pass's survivors in candidate order;
+ *                        1 learned: survivors binned by the scheduler MLP's predicted output-size
+ *                          class within windows of sched_window survivors (needs weights,
+ *                          libsupermesh_gpu_sched_set_weights);
+ *                        2 true classes: binned by the output counts of the previous narrow phase
+ *                          over the same candidates (the best a predictor could do; a measurement)
+ *   "sched_window"       survivors per binning window: 256 .. 8192, a multiple of 256 (default 1024)
+ * Failure-injection hooks for tests (host side only; no GPU fault is made):
+ *   "fail_alloc_after"   -1 (default) off; n >= 0: the next n device allocations of any
+ *                        context succeed and the following one fails as cudaMalloc out of
+ *                        memory would (LSM_ERROR_OUT_OF_MEMORY; the hook then turns itself
+ *                        off and the context stays usable)
+ *   "sort_spin_limit"    polls (1 .. 2^22, default 2^22) before a look-back wait of the
+ *                        radix sort gives up
+ *   "sort_stall_block"   -1 (default) or b >= 1: block b of every pass of the tree build's
+ *                        sort never publishes its counts, so the waits after it give up;
+ *                        the search then returns LSM_ERROR_TIMEOUT ("look-back wait gave up")
  * Unknown names or values return LSM_ERROR_INVALID_ARGUMENT. */
 int libsupermesh_gpu_set_option(const char *name, int64_t value);
 int libsupermesh_gpu_get_option(const char *name, int64_t *value);
@@ -150,7 +168,9 @@ int libsupermesh_gpu_get_pair_results(lsm_gpu_context *ctx, double *measure,
 /* Batched form of the per-pair C API.  tri: a, b [n][3][2]; tet: a, b
  * [n][4][3].  measure[n] = sum of output simplex measures, n_out[n] = number
  * of output simplices; elems (optional) [n][22][3][2] or [n][81][4][3] in
- * the reference's output order. */
+ * the reference's output order.  With on_device = 1 and dim = 3, a and b
+ * must be 16-byte aligned (tetrahedra are read with 16-byte loads); other
+ * pointers return LSM_ERROR_INVALID_ARGUMENT before any launch. */
 int libsupermesh_gpu_intersect_pairs(lsm_gpu_context *ctx, int dim, int64_t n,
                                      const double *a, const double *b,
                                      double *measure, int32_t *n_out,
@@ -167,7 +187,9 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context *ctx, int dim, int64_t n,
  *   LSM_PAIR_HEX_HEX    a, b [n][8][3]  elems [n][3645][4][3] (intersect_hexes,
  *                       Supermesh.F90:303-334: A sliced into five tets)
  * measure[n] = sum of output measures, n_out[n] = number of outputs, elems
- * optional, in the reference's output order. */
+ * optional, in the reference's output order.  With on_device = 1 and kind
+ * LSM_PAIR_TET_HEX, a must be 16-byte aligned (as for
+ * libsupermesh_gpu_intersect_pairs). */
 enum {
   LSM_PAIR_INTERVALS = 0,
   LSM_PAIR_TRI_QUAD = 1,
@@ -206,6 +228,41 @@ int libsupermesh_gpu_p2_inner_product(lsm_gpu_context *ctx, const lsm_gpu_mesh *
                                       int64_t nnodes_p2_b, double *pair_values, double *integral,
                                       double *area, int on_device, void *stream);
 
+/* Learned scheduler of the 3D clipper (north-star pattern: a small BF16 MLP
+ * predicts each surviving candidate pair's output-size class -- 0: no tets,
+ * 1: 1-3, 2: 4-7, 3: 8 or more, the n_tets_c of intersect_tets_real,
+ * Tetrahedron_Intersection.F90:137-179 -- and is used only to order the
+ * clipper's work; every pair is still clipped exactly).  No counterpart in
+ * the reference.  Network 24 -> 64 -> 64 -> 4 (ReLU), BF16 weights, FP32
+ * accumulation on the tensor cores.  Parameters: LSM_SCHED_PARAMS FP32
+ * values, row-major [out][in] blocks W1 [64][32] (inputs 24..31 are padding),
+ * b1 [64], W2 [64][64], b2 [64], W3 [8][64] (rows 4..7 padding), b3 [8].
+ * Features: LSM_SCHED_FEATURES BF16 per pair, A's then B's four vertices
+ * (x, y, z) minus the mean of the eight, divided by the longest of the
+ * twelve edges; 24..31 zero.  All buffers below are device memory of the
+ * context's GPU, features 16-byte aligned. */
+#define LSM_SCHED_PARAMS 6792
+#define LSM_SCHED_FEATURES 32
+/* Load weights for tet_schedule 1 (params host or device memory). */
+int libsupermesh_gpu_sched_set_weights(lsm_gpu_context *ctx, const float *params, int on_device);
+/* Training samples from the last plain 3D narrow phase: the features of the
+ * first min(cap, survivors) pairs the early-out pass left for the clipper
+ * and the class of the clipper's output count; *n = survivors. */
+int libsupermesh_gpu_sched_samples(lsm_gpu_context *ctx, int64_t cap, void *features, int8_t *classes,
+                                   int64_t *n, void *stream);
+/* Inference: logits[n][4] (optional) and classes[n] of feature rows. */
+int libsupermesh_gpu_sched_predict(lsm_gpu_context *ctx, int64_t n, const void *features, float *logits,
+                                   int8_t *classes, void *stream);
+/* Training: `steps` Adam steps (betas 0.9 / 0.999) on the softmax
+ * cross-entropy, minibatches of 128 consecutive rows (row (128 step + i) mod
+ * n: shuffle the samples first).  params (in: initial, out: trained);
+ * loss_trace (optional) the minibatch loss of every trace_every-th step;
+ * grad_first (optional, LSM_SCHED_PARAMS) the gradient of the first
+ * minibatch.  Forward and backward products run on the tensor cores. */
+int libsupermesh_gpu_sched_train(lsm_gpu_context *ctx, int64_t n, const void *features,
+                                 const int8_t *classes, float *params, int steps, float lr,
+                                 float *loss_trace, int trace_every, float *grad_first, void *stream);
+
 /* Many independent mesh pairs in one call.  totals[npairs] receives each
  * pair's supermesh measure
  * and n_candidates[npairs] / n_intersecting[npairs] (optional) its counts.
@@ -225,9 +282,13 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context *ctx, int npairs,
  * and stream-overlapped loops where cudaFree's implicit device-wide
  * synchronisation would serialise other work.  Same results as
  * libsupermesh_gpu_intersect_pairs (dim 3) for measure[n] and n_out[n]; total
- * (host, optional) receives the compensated sum of measure.  tet_a, tet_b
- * ([n][4][3]), measure and n_out are device memory; n <= LSM_NOALLOC_MAX_PAIRS
- * (larger n returns LSM_ERROR_CAPACITY with a message on stderr).
+ * (host, optional) receives the compensated sum of measure; it makes the call
+ * wait for its stream (cudaStreamSynchronize), so a call issued inside stream
+ * capture must pass total = NULL and sum measure itself.  tet_a, tet_b
+ * ([n][4][3], 16-byte aligned), measure and n_out are device memory;
+ * n <= LSM_NOALLOC_MAX_PAIRS (larger n returns LSM_ERROR_CAPACITY, a
+ * misaligned tet_a or tet_b LSM_ERROR_INVALID_ARGUMENT, each with a message
+ * on stderr).
  * Scratch lives in one fixed device array of LSM_NOALLOC_SCRATCH_BYTES that
  * every GPU loading the library holds until exit; the first call on a device
  * looks up its address (make that first call before any stream capture).

@@ -25,6 +25,8 @@ _PKG = Path(__file__).resolve().parent
 _LIB = _PKG / "lib" / "libsupermesh.so"
 TRI_BUF_SIZE = 22
 TET_BUF_SIZE = 81
+SCHED_PARAMS = 6792    # LSM_SCHED_PARAMS
+SCHED_FEATURES = 32    # LSM_SCHED_FEATURES
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _i32p = ctypes.POINTER(ctypes.c_int32)
@@ -122,13 +124,20 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_p2_inner_product.argtypes = [vp, mp, mp, vp, vp, ctypes.c_int64, vp, vp, ctypes.c_int64, vp,
                                                     _dp, _dp, ctypes.c_int, vp]
     L.libsupermesh_gpu_supermesh_batched.argtypes = [vp, ctypes.c_int, mp, mp, ctypes.c_int, vp, vp, vp, vp]
+    L.libsupermesh_gpu_sched_set_weights.argtypes = [vp, vp, ctypes.c_int]
+    L.libsupermesh_gpu_sched_samples.argtypes = [vp, ctypes.c_int64, vp, vp, _i64p, vp]
+    L.libsupermesh_gpu_sched_predict.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp]
+    L.libsupermesh_gpu_sched_train.argtypes = [vp, ctypes.c_int64, vp, vp, vp, ctypes.c_int, ctypes.c_float, vp,
+                                               ctypes.c_int, vp, vp]
     for name in ("libsupermesh_gpu_context_create", "libsupermesh_gpu_context_destroy",
                  "libsupermesh_gpu_find_candidates", "libsupermesh_gpu_get_candidates",
                  "libsupermesh_gpu_supermesh", "libsupermesh_gpu_get_pair_results",
                  "libsupermesh_gpu_clip_candidates",
                  "libsupermesh_gpu_intersect_pairs", "libsupermesh_gpu_intersect_pairs_mixed",
                  "libsupermesh_gpu_p1_mass", "libsupermesh_gpu_p2_inner_product",
-                 "libsupermesh_gpu_supermesh_batched"):
+                 "libsupermesh_gpu_supermesh_batched", "libsupermesh_gpu_sched_set_weights",
+                 "libsupermesh_gpu_sched_samples", "libsupermesh_gpu_sched_predict",
+                 "libsupermesh_gpu_sched_train"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -208,11 +217,17 @@ class Context:
                                                               int(on_device), ctypes.byref(n), stream))
         return n.value
 
-    def get_candidates(self, nel_a: int, n: int):
-        indptr = np.zeros(nel_a + 1, dtype=np.int64)
-        indices = np.zeros(max(n, 1), dtype=np.int64)
+    def get_candidates(self, nel_a: int, n: int, out=None, stream: int | None = None):
+        """CSR of the last search: (ind_ptr[nel_a + 1], indices[n]), int64,
+        into `out` = (ind_ptr, indices) host arrays when given (pinned
+        arrays make the copies asynchronous DMA)."""
+        if out is None:
+            indptr = np.zeros(nel_a + 1, dtype=np.int64)
+            indices = np.zeros(max(n, 1), dtype=np.int64)
+        else:
+            indptr, indices = out
         self._check(self.lib.libsupermesh_gpu_get_candidates(self._h, indptr.ctypes.data, indices.ctypes.data,
-                                                             0, None))
+                                                             0, stream))
         return indptr, indices[:n]
 
     # -- whole supermesh --------------------------------------------------
@@ -257,10 +272,15 @@ class Context:
         self._check(self.lib.libsupermesh_gpu_clip_survivors(self._h, ctypes.byref(r)))
         return r.value
 
-    def pair_results(self, n: int):
-        m = np.zeros(max(n, 1), dtype=np.float64)
-        k = np.zeros(max(n, 1), dtype=np.int32)
-        self._check(self.lib.libsupermesh_gpu_get_pair_results(self._h, m.ctypes.data, k.ctypes.data, 0, None))
+    def pair_results(self, n: int, out=None, stream: int | None = None):
+        """Per-candidate (measure[n] float64, n_out[n] int32) of the last
+        narrow phase, in CSR order, into `out` = (measure, n_out) when given."""
+        if out is None:
+            m = np.zeros(max(n, 1), dtype=np.float64)
+            k = np.zeros(max(n, 1), dtype=np.int32)
+        else:
+            m, k = out
+        self._check(self.lib.libsupermesh_gpu_get_pair_results(self._h, m.ctypes.data, k.ctypes.data, 0, stream))
         return m[:n], k[:n]
 
     def intersect_pairs(self, dim: int, a, b, want_elems: bool = False):
@@ -341,6 +361,40 @@ class Context:
             e2b.ctypes.data, fb.ctypes.data, fb.size, _ptr(pv), ctypes.byref(integral), ctypes.byref(area), 0,
             None))
         return integral.value, area.value, (pv[:n] if pv is not None else None)
+
+    # -- learned scheduler (device buffers: torch tensors) -------------------
+    def sched_set_weights(self, params) -> None:
+        """Weights for option tet_schedule = 1: LSM_SCHED_PARAMS float32
+        values (numpy on the host, or a device tensor)."""
+        if hasattr(params, "data_ptr"):
+            self._check(self.lib.libsupermesh_gpu_sched_set_weights(self._h, params.data_ptr(), 1))
+        else:
+            p = np.ascontiguousarray(params, dtype=np.float32)
+            assert p.size == SCHED_PARAMS
+            self._check(self.lib.libsupermesh_gpu_sched_set_weights(self._h, p.ctypes.data, 0))
+
+    def sched_samples(self, cap: int, features, classes, stream: int | None = None) -> int:
+        """Features (device, [cap][32] 2-byte elements) and classes (device
+        int8 [cap]) of the survivors of the last plain 3D narrow phase;
+        returns the number of survivors."""
+        n = ctypes.c_int64(0)
+        self._check(self.lib.libsupermesh_gpu_sched_samples(self._h, cap, features.data_ptr(), classes.data_ptr(),
+                                                            ctypes.byref(n), stream))
+        return n.value
+
+    def sched_predict(self, n: int, features, logits, classes, stream: int | None = None) -> None:
+        self._check(self.lib.libsupermesh_gpu_sched_predict(
+            self._h, n, features.data_ptr(), logits.data_ptr() if logits is not None else None,
+            classes.data_ptr(), stream))
+
+    def sched_train(self, n: int, features, classes, params, steps: int, lr: float, loss_trace=None,
+                    trace_every: int = 0, grad_first=None, stream: int | None = None) -> None:
+        """Adam steps on device tensors; params (float32 [LSM_SCHED_PARAMS],
+        device) is updated in place."""
+        self._check(self.lib.libsupermesh_gpu_sched_train(
+            self._h, n, features.data_ptr(), classes.data_ptr(), params.data_ptr(), steps, lr,
+            loss_trace.data_ptr() if loss_trace is not None else None, trace_every,
+            grad_first.data_ptr() if grad_first is not None else None, stream))
 
     def supermesh_batched(self, pairs, on_device: bool = False, stream: int | None = None):
         """pairs: list of (mesh_a, mesh_b).  Returns (totals, n_candidates,

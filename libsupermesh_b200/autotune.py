@@ -25,7 +25,7 @@ import libsupermesh_b200 as lsm
 
 SPACE = {
     2: {"tri_blocks_per_sm": (4, 8, 16), "query_block": (64, 128, 256)},
-    3: {"tet_clipper": (0, 1, 2), "query_block": (64, 128, 256)},
+    3: {"query_block": (64, 128, 256)},
 }
 
 

@@ -20,8 +20,8 @@ ROOT = PKG.parent
 SRC = PKG / "csrc"
 OUT = PKG / "lib" / "libsupermesh.so"
 PROBE = PKG / "lib" / "liblsm_probe.so"
-SOURCES = ["lsm_kernels.cu", "lsm_capi.cu", "lsm_noalloc.cu"]
-HEADERS = ["lsm_geom.cuh", "lsm_kernels.h"]
+SOURCES = ["lsm_kernels.cu", "lsm_capi.cu", "lsm_noalloc.cu", "lsm_sched.cu"]
+HEADERS = ["lsm_geom.cuh", "lsm_kernels.h", "lsm_sched.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

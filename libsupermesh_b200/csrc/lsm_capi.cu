@@ -25,6 +25,7 @@
 #include "../../include/libsupermesh-c.h"
 #include "../../include/libsupermesh-gpu.h"
 #include "lsm_kernels.h"
+#include "lsm_sched.h"
 
 namespace {
 
@@ -36,6 +37,17 @@ bool g_tet_screen = true;
 // spill chunks of the batched search's row cache: -1 automatic, 0 none (long
 // rows traversed again), n > 0 at most n
 int64_t g_spill_chunks = -1;
+// Test hook of the allocation-failure path: -1 off; n >= 0: the next n
+// device allocations of the contexts succeed and the one after fails as if
+// cudaMalloc had run out of memory (the hook then switches itself off).
+int64_t g_fail_alloc_after = -1;
+// Schedule of the 3D clipper's work list: 0 plain (the early-out pass's
+// order), 1 learned (survivors binned by the MLP's predicted output-size
+// class within windows of g_sched_window), 2 true classes (binned by the
+// output counts of the previous narrow phase over the same candidates: the
+// best any predictor can do; a measurement, not a production mode).
+int g_tet_schedule = 0;
+int g_sched_window = 1024;
 
 // ------------------------------------------------------------------ buffers
 struct DevBuf {
@@ -66,6 +78,9 @@ struct Ctx {
   // host meshes of a batch staged on the device, one set per dimension (the
   // 3D set is copied on the side stream while the 2D group computes)
   DevBuf bt_stage_pa[2], bt_stage_ea[2], bt_stage_pb[2], bt_stage_eb[2];
+  // learned scheduler: BF16 weight image, binned survivor list, classes
+  DevBuf sched_w, sched_list, sched_cls, sched_adam;
+  bool have_sched = false;
   // 1D sort finder
   DevBuf d1_keyhi, d1_perm_a, d1_perm_b, d1_lo_a, d1_hi_a, d1_lo_b, d1_hi_b, d1_tree, d1_e, d1_l, d1_js;
   void* host_stage = nullptr;  // pinned, grow-only
@@ -148,6 +163,10 @@ T* ensure(Ctx* c, DevBuf& b, int64_t count) {
       b.cap = 0;
     }
     size_t want = need + need / 4;  // growth headroom
+    if (g_fail_alloc_after >= 0 && g_fail_alloc_after-- == 0) {
+      set_error(c, "cudaMalloc of %zu bytes failed: out of memory (forced by option fail_alloc_after)", want);
+      throw Fail{LSM_ERROR_OUT_OF_MEMORY};
+    }
     cudaError_t e = cudaMalloc(&b.p, want);
     if (e != cudaSuccess) {
       (void)cudaGetLastError();
@@ -224,7 +243,8 @@ void fini_ctx(Ctx* c) {
                    &c->bt_stage_eb[1],
                    &c->d1_keyhi, &c->d1_perm_a, &c->d1_perm_b, &c->d1_lo_a, &c->d1_hi_a, &c->d1_lo_b,
                    &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over, &c->q_pool, &c->q_next, &c->q_first,
-                   &c->a_faces, &c->b_screen, &c->surv};
+                   &c->a_faces, &c->b_screen, &c->surv, &c->sched_w, &c->sched_list, &c->sched_cls,
+                   &c->sched_adam};
   for (DevBuf* b : all) free_buf(*b);
   for (cudaEvent_t& e : c->clip_ev)
     if (e) {
@@ -496,7 +516,7 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   REQUIRE(hb[0] == 0, "Invalid node index in an element list");
   if (hb[3] != 0) {
     set_error(c, "tree build: the sort's look-back wait gave up");
-    throw Fail{LSM_ERROR_CUDA};
+    throw Fail{LSM_ERROR_TIMEOUT};
   }
   const int64_t nnz = *h;
   int32_t* pa = ensure<int32_t>(c, c->pair_a, nnz);
@@ -541,6 +561,28 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
   }
   bool queued = false;
   const bool screen = c->dim == 3 && g_tet_screen;
+  lsm::SchedBin bin;
+  const bool binned = c->dim == 3 && g_tet_schedule != 0 && lsm::tet_clipper_variant() == 0;
+  if (binned) {
+    if (g_tet_schedule == 1 && !c->have_sched) {
+      set_error(c, "tet_schedule 1 needs scheduler weights (libsupermesh_gpu_sched_set_weights)");
+      throw Fail{LSM_ERROR_STATE};
+    }
+    if (g_tet_schedule == 2) {
+      if (!c->have_pairs) {
+        set_error(c, "tet_schedule 2 needs a narrow phase over the same candidates first");
+        throw Fail{LSM_ERROR_STATE};
+      }
+      int8_t* cls = ensure<int8_t>(c, c->sched_cls, nnz);
+      CU(lsm::launch_sched_true_class(nnz, pn, cls, s));
+      bin.cls_of_pair = cls;
+    } else {
+      bin.weights = static_cast<const lsm::SchedWeights*>(c->sched_w.p);
+    }
+    bin.screen_b = static_cast<double*>(c->b_screen.p);
+    bin.out = ensure<int4>(c, c->sched_list, nnz);
+    bin.window = g_sched_window;
+  }
   if (c->dim == 3 && lsm::tet_clipper_variant() == 1) {
     int* err = bad_flag(c) + 16;
     unsigned char* scr = ensure<unsigned char>(c, c->wq_scratch, (int64_t)lsm::wq_scratch_bytes());
@@ -564,7 +606,7 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
                         static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order,
                         g_time_kernels ? c->clip_ev[0] : nullptr, g_time_kernels ? c->clip_ev[1] : nullptr,
                         screen ? static_cast<double*>(c->a_faces.p) : nullptr,
-                        screen ? static_cast<double*>(c->b_screen.p) : nullptr));
+                        screen ? static_cast<double*>(c->b_screen.p) : nullptr, binned ? &bin : nullptr));
   c->clip_timed = !queued && g_time_kernels;
   if (c->dim == 3) {
     CU(cudaMemcpyAsync(ensure<unsigned long long>(c, c->surv, 1), work, sizeof(unsigned long long),
@@ -777,7 +819,7 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
     int* work = ensure<int>(c, c->bvh_work, 8 * nb);
     unsigned long long* codes = ensure<unsigned long long>(c, c->bt_codes, nb);
     CU(lsm::launch_batched_tree((int)nb, nm, vals, pair_of_b, mort, codes, b_box32, d_eob, bvh, work, roots,
-                                stops, s, dim, b_box));
+                                stops, s, dim, b_box, bad + 3));
   } else {
     CU(cudaMemsetAsync(roots, 0xff, sizeof(int) * nm, s));
     CU(cudaMemsetAsync(stops, 0xff, sizeof(int) * nm, s));
@@ -806,7 +848,7 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   REQUIRE(hb[0] == 0, "Invalid node index in an element list");
   if (hb[3] != 0) {
     set_error(c, "tree build: the sort's look-back wait gave up");
-    throw Fail{LSM_ERROR_CUDA};
+    throw Fail{LSM_ERROR_TIMEOUT};
   }
   const int64_t nnz = *h;
   int32_t* pa = ensure<int32_t>(c, c->pair_a, nnz);
@@ -1115,6 +1157,16 @@ int libsupermesh_gpu_set_option(const char* name, int64_t value) {
     g_tet_screen = value == 1;
   } else if (n == "spill_chunks" && value >= -1 && value <= INT32_MAX) {
     g_spill_chunks = value;
+  } else if (n == "tet_schedule" && value >= 0 && value <= 2) {
+    g_tet_schedule = (int)value;
+  } else if (n == "sched_window" && value >= 256 && value <= lsm::kSchedMaxWindow && value % 256 == 0) {
+    g_sched_window = (int)value;
+  } else if (n == "fail_alloc_after" && value >= -1 && value <= INT32_MAX) {
+    g_fail_alloc_after = value;
+  } else if (n == "sort_spin_limit" && value >= 1 && value <= (1 << 22)) {
+    lsm::set_sort_spin_limit((int)value);
+  } else if (n == "sort_stall_block" && (value == -1 || (value >= 1 && value <= INT32_MAX))) {
+    lsm::set_sort_stall_block((int)value);
   } else {
     return LSM_ERROR_INVALID_ARGUMENT;
   }
@@ -1138,6 +1190,16 @@ int libsupermesh_gpu_get_option(const char* name, int64_t* value) {
     *value = g_tet_screen ? 1 : 0;
   else if (n == "spill_chunks")
     *value = g_spill_chunks;
+  else if (n == "fail_alloc_after")
+    *value = g_fail_alloc_after;
+  else if (n == "tet_schedule")
+    *value = g_tet_schedule;
+  else if (n == "sched_window")
+    *value = g_sched_window;
+  else if (n == "sort_spin_limit")
+    *value = lsm::sort_spin_limit();
+  else if (n == "sort_stall_block")
+    *value = lsm::sort_stall_block();
   else
     return LSM_ERROR_INVALID_ARGUMENT;
   return LSM_SUCCESS;
@@ -1282,6 +1344,8 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context* ctx, int dim, int64_t n, c
     REQUIRE(n >= 0, "negative pair count");
     if (n == 0) return;
     REQUIRE(a && b, "NULL element arrays");
+    REQUIRE(!on_device || dim == 2 || ((((uintptr_t)a | (uintptr_t)b) & 15u) == 0),
+            "device tetrahedron arrays must be 16-byte aligned (a %p, b %p)", (const void*)a, (const void*)b);
     cudaStream_t s = pick(c, stream);
     const int per = dim == 2 ? 6 : 12;
     const int64_t cap = dim == 2 ? 22 : 81;
@@ -1319,6 +1383,8 @@ int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context* ctx, int kind, int64
     REQUIRE(n >= 0, "negative pair count");
     if (n == 0) return;
     REQUIRE(a && b, "NULL element arrays");
+    REQUIRE(!on_device || kind != LSM_PAIR_TET_HEX || (((uintptr_t)a & 15u) == 0),
+            "device tetrahedron array a must be 16-byte aligned (%p)", (const void*)a);
     cudaStream_t s = pick(c, stream);
     const MixedShape m = mixed_shape(kind);
     const double *da = a, *db = b;
@@ -1448,6 +1514,77 @@ int libsupermesh_gpu_p2_inner_product(lsm_gpu_context* ctx, const lsm_gpu_mesh* 
     if (integral) *integral = h[0].sum;
     if (area) *area = h[1].sum;
     c->have_pairs = false;  // pair_measure now holds P2 contributions
+  });
+}
+
+int libsupermesh_gpu_sched_set_weights(lsm_gpu_context* ctx, const float* params, int on_device) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(params != nullptr, "NULL parameters");
+    cudaStream_t s = c->stream;
+    const float* d = params;
+    if (!on_device) {
+      float* t = ensure<float>(c, c->sched_adam, 2 * lsm::kSchedParams);
+      CU(cudaMemcpyAsync(t, params, sizeof(float) * lsm::kSchedParams, cudaMemcpyHostToDevice, s));
+      d = t;
+    }
+    lsm::SchedWeights* w = reinterpret_cast<lsm::SchedWeights*>(ensure<char>(c, c->sched_w, sizeof(lsm::SchedWeights)));
+    CU(lsm::launch_sched_pack(d, w, s));
+    CU(cudaStreamSynchronize(s));
+    c->have_sched = true;
+  });
+}
+
+int libsupermesh_gpu_sched_samples(lsm_gpu_context* ctx, int64_t cap, void* features, int8_t* classes, int64_t* n,
+                                   void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(cap >= 0 && (cap == 0 || (features && classes)), "invalid sample buffers");
+    REQUIRE((((uintptr_t)features) & 15u) == 0, "features must be 16-byte aligned");
+    if (!c->surv_valid || !c->have_pairs || c->dim != 3 || g_tet_schedule != 0 || lsm::tet_clipper_variant() != 0) {
+      set_error(c, "no plain 3D narrow phase (tet_schedule 0, tet_clipper 0) since the last candidate search");
+      throw Fail{LSM_ERROR_STATE};
+    }
+    cudaStream_t s = pick(c, stream);
+    const unsigned long long* nl = reinterpret_cast<const unsigned long long*>(bad_flag(c) + 8);
+    CU(lsm::launch_sched_samples(static_cast<const int4*>(c->ovf_list.p), nl, cap, static_cast<double*>(c->a_coords.p),
+                                 static_cast<double*>(c->b_screen.p), static_cast<int32_t*>(c->pair_nout.p), features,
+                                 classes, s));
+    unsigned long long* h = reinterpret_cast<unsigned long long*>(static_cast<char*>(c->host_scalars) + 512);
+    CU(cudaMemcpyAsync(h, nl, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (n) *n = (int64_t)*h;
+  });
+}
+
+int libsupermesh_gpu_sched_predict(lsm_gpu_context* ctx, int64_t n, const void* features, float* logits,
+                                   int8_t* classes, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(n >= 0 && (n == 0 || (features && classes)), "invalid buffers");
+    REQUIRE((((uintptr_t)features) & 15u) == 0, "features must be 16-byte aligned");
+    if (!c->have_sched) {
+      set_error(c, "no scheduler weights (libsupermesh_gpu_sched_set_weights)");
+      throw Fail{LSM_ERROR_STATE};
+    }
+    cudaStream_t s = pick(c, stream);
+    CU(lsm::launch_sched_predict(n, features, static_cast<const lsm::SchedWeights*>(c->sched_w.p), logits, classes, s));
+    CU(cudaStreamSynchronize(s));
+  });
+}
+
+int libsupermesh_gpu_sched_train(lsm_gpu_context* ctx, int64_t n, const void* features, const int8_t* classes,
+                                 float* params, int steps, float lr, float* loss_trace, int trace_every,
+                                 float* grad_first, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(n > 0 && features && classes && params, "invalid training buffers");
+    REQUIRE((((uintptr_t)features) & 15u) == 0, "features must be 16-byte aligned");
+    REQUIRE(steps >= 0 && lr > 0.0f, "invalid steps or learning rate");
+    cudaStream_t s = pick(c, stream);
+    float* adam = ensure<float>(c, c->sched_adam, 2 * lsm::kSchedParams);
+    CU(lsm::launch_sched_train(features, classes, n, params, adam, steps, lr, loss_trace, trace_every, grad_first, s));
+    CU(cudaStreamSynchronize(s));
   });
 }
 

@@ -32,6 +32,7 @@
 // separately rounded IEEE operation, matching libsupermesh's gfortran build.
 #include "lsm_geom.cuh"
 #include "lsm_kernels.h"
+#include "lsm_sched.h"
 
 #include <cuda/atomic>
 
@@ -93,9 +94,7 @@ void set_tri_blocks_per_sm(int v) { g_tri_bps = v; }
 int query_block() { return g_query_block; }
 void set_query_block(int v) { g_query_block = v; }
 
-namespace {
-
-inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+void count_launch(int n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 
 int sm_count() {
   static int cached = -1;
@@ -115,6 +114,8 @@ int grid_for(int64_t n, int block, int per_sm) {
   if (need < 1) need = 1;
   return (int)(need < cap ? need : cap);
 }
+
+namespace {
 
 // Compensated (sum, err) pair helpers: TwoSum-based merge.
 __device__ __forceinline__ void cs_add(double& sum, double& err, double x) {
@@ -579,12 +580,32 @@ constexpr int kWarpTile = 32 * kSortItems;             // contiguous per warp
 // count (n < 2^30).  Waits are bounded: a block that gives up sets err and
 // treats the missing prefix as 0 (wrong order, never a hang); forward
 // progress does not need the bound, since a block only waits for blocks
-// that took earlier tickets and are running or done.
+// that took earlier tickets and are running or done.  A partial prefix only
+// lowers the scatter positions, so they stay inside [0, n); some keys then
+// overwrite others, and k_sort_repair turns the output back into a
+// permutation (identity values, equal keys) so that the kernels after the
+// sort never read an element number that does not exist.  The caller sees
+// err and reports the failure.
+//
+// Test hooks (process-wide, off by default): the bound of each wait
+// (set_sort_spin_limit) and one block per pass that never publishes its
+// counts (set_sort_stall_block, sorts given an err word only), which makes
+// the waits of the blocks after it run out.
 namespace {
 constexpr int kSortPassesMax = 4;
 constexpr int kSortHdr = kSortPassesMax * 256 + 8;
 constexpr uint32_t kFlagLocal = 1u << 30, kFlagIncl = 2u << 30, kFlagMask = 3u << 30;
 }  // namespace
+
+namespace {
+int g_sort_spin_limit = 1 << 22;
+int g_sort_stall = -1;
+}  // namespace
+
+void set_sort_spin_limit(int v) { g_sort_spin_limit = v > 0 ? v : 1; }
+int sort_spin_limit() { return g_sort_spin_limit; }
+void set_sort_stall_block(int b) { g_sort_stall = b >= 1 ? b : -1; }
+int sort_stall_block() { return g_sort_stall; }
 
 int64_t radix_hist_entries(int64_t n) {
   const int64_t nb = (n + kSortTile - 1) / kSortTile;
@@ -613,7 +634,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_onesweep(int64_t n, int 
                                                                  uint32_t* keys_out, int32_t* vals_out,
                                                                  const uint32_t* __restrict__ counts,
                                                                  uint32_t* status, uint32_t* ticket,
-                                                                 uint32_t* err) {
+                                                                 uint32_t* err, int spin_limit, int stall) {
   __shared__ uint32_t wh[kSortWarps][256];
   __shared__ uint32_t base_s[256];
   __shared__ uint32_t wt[kSortWarps];
@@ -643,13 +664,14 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_onesweep(int64_t n, int 
   uint32_t local = 0;
   for (int w = 0; w < kSortWarps; ++w) local += wh[w][d];
   cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(status[(int64_t)b * 256 + d]);
-  mine.store((b == 0 ? kFlagIncl : kFlagLocal) | local, cuda::memory_order_relaxed);
+  const bool publish = b != stall;
+  if (publish) mine.store((b == 0 ? kFlagIncl : kFlagLocal) | local, cuda::memory_order_relaxed);
   uint32_t prefix = 0;
   for (int j = b - 1; j >= 0;) {
     cuda::atomic_ref<uint32_t, cuda::thread_scope_device> st(status[(int64_t)j * 256 + d]);
     uint32_t v = st.load(cuda::memory_order_relaxed);
     for (int spin = 0; (v & kFlagMask) == 0; ++spin) {
-      if (spin > (1 << 22)) {
+      if (spin > spin_limit) {
         atomicExch(err, 1u);
         v = kFlagIncl;
         break;
@@ -661,7 +683,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_onesweep(int64_t n, int 
     if ((v & kFlagMask) == kFlagIncl) break;
     --j;
   }
-  if (b > 0) mine.store(kFlagIncl | (prefix + local), cuda::memory_order_relaxed);
+  if (b > 0 && publish) mine.store(kFlagIncl | (prefix + local), cuda::memory_order_relaxed);
   // global start of digit d: exclusive scan of the pass's digit counts
   {
     const uint32_t c = counts[d];
@@ -702,6 +724,16 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_onesweep(int64_t n, int 
   }
 }
 
+// After a sort whose look-back gave up (*err != 0): identity values and
+// equal keys, a permutation that every later kernel can read safely.
+__global__ void k_sort_repair(int64_t n, const uint32_t* __restrict__ err, uint32_t* keys, int32_t* vals) {
+  if (*err == 0u) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    keys[i] = 0u;
+    vals[i] = (int32_t)i;
+  }
+}
+
 cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals, uint32_t* keys_tmp,
                              int32_t* vals_tmp, uint32_t* hist, cudaStream_t s, int* err) {
   if (n <= 1) return cudaSuccess;
@@ -719,7 +751,8 @@ cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals,
   k_radix_counts<<<grid_for(n, kSortThreads, 4), kSortThreads, 0, s>>>(n, passes, ki, counts);
   for (int p = 0; p < passes; ++p) {
     k_radix_onesweep<<<nb, kSortThreads, 0, s>>>(n, 8 * p, ki, vi, ko, vo, counts + 256 * p,
-                                                 status + (int64_t)p * 256 * nb, tickets + p, errw);
+                                                 status + (int64_t)p * 256 * nb, tickets + p, errw,
+                                                 g_sort_spin_limit, err ? g_sort_stall : -1);
     uint32_t* tk = ki;
     ki = ko;
     ko = tk;
@@ -730,6 +763,10 @@ cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals,
   if (ki != keys) {
     cudaMemcpyAsync(keys, ki, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(vals, vi, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s);
+  }
+  if (err) {
+    count_launch();
+    k_sort_repair<<<grid_for(n, 256, 4), 256, 0, s>>>(n, errw, keys, vals);
   }
   return cudaGetLastError();
 }
@@ -1179,7 +1216,6 @@ constexpr int kTriWideCap = 24;
 constexpr int kTetBlock = 128;
 constexpr int kTetStack = 6;      // max pending tets: 2 per level for planes 0-2
 constexpr int kTetSmemSlots = 3;  // stack slots kept in shared memory
-constexpr int kReduceBlocks = 1024;  // fixed: the totals' summation order
 }  // namespace
 
 // Polygon in shared memory: slot i, coord c at base[(2*i + c) * BLOCK].
@@ -2299,7 +2335,7 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
                         const int32_t* order, cudaEvent_t ev_begin, cudaEvent_t ev_end, const double* faces_a,
-                        const double* screen_b) {
+                        const double* screen_b, const SchedBin* bin) {
   const int g = clip_grid_blocks(dim);
   count_launch();
   if (dim == 2) {
@@ -2322,10 +2358,16 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
       k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
                                                                        tol_a, setup_b, pair_measure, pair_nout,
                                                                        overflow_list, work, faces_a, screen_b);
+    const int4* list = reinterpret_cast<const int4*>(overflow_list);
+    if (tet_clipper_variant() == 0 && bin) {
+      // the survivors reordered into class-uniform runs within windows
+      cudaError_t e = launch_sched_bin(*bin, list, work, bin->out, coords_a, s);
+      if (e != cudaSuccess) return e;
+      list = bin->out;
+    }
     if (tet_clipper_variant() == 0)
       k_clip_tets_ix<<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
-          reinterpret_cast<const int4*>(overflow_list), work, coords_a, tol_a, setup_b, pair_measure, pair_nout,
-          work + 1);
+          list, work, coords_a, tol_a, setup_b, pair_measure, pair_nout, work + 1);
     else if (tet_blocks_per_sm() == 3)
       k_clip_tets<3><<<sm_count() * 3, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,
                                                               setup_b, pair_measure, pair_nout, work + 1);
@@ -2369,7 +2411,9 @@ cudaError_t init_device_attributes() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_clip_tets<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_clip_tets_ix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
+  e = cudaFuncSetAttribute(k_clip_tets_ix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
+  if (e != cudaSuccess) return e;
+  return init_sched_attributes(kSchedMaxWindow);
 }
 
 
@@ -2457,11 +2501,17 @@ __global__ void k_pair_keys(int64_t n, const int32_t* __restrict__ vals, const i
     keys[i] = (uint32_t)pair_of[vals[i]];
 }
 
+// After a sort whose look-back wait gave up (*err != 0, values repaired to
+// the identity) the Morton part is left out: equal codes within a mesh give
+// a well-formed hierarchy (ties break by position), so the kernels after it
+// stay in bounds while the host reports the failure.
 __global__ void k_combined_codes(int64_t n, const int32_t* __restrict__ vals, const int32_t* __restrict__ pair_of,
-                                 const uint32_t* __restrict__ mort, unsigned long long* codes) {
+                                 const uint32_t* __restrict__ mort, unsigned long long* codes,
+                                 const uint32_t* __restrict__ err) {
+  const bool failed = err && *err != 0u;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int32_t v = vals[i];
-    codes[i] = ((unsigned long long)(uint32_t)pair_of[v] << 32) | (unsigned long long)mort[v];
+    codes[i] = ((unsigned long long)(uint32_t)pair_of[v] << 32) | (failed ? 0ull : (unsigned long long)mort[v]);
   }
 }
 
@@ -2526,7 +2576,7 @@ __global__ void k_mesh_roots(int nm, int n, const int64_t* __restrict__ mesh_off
 cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const int32_t* pair_of_b,
                                 const uint32_t* mort, unsigned long long* codes, const float* box32,
                                 const int64_t* mesh_off_b, BVH bvh, int* work, int* roots, int* stops,
-                                cudaStream_t s, int dim, const double* box64) {
+                                cudaStream_t s, int dim, const double* box64, const int* sort_err) {
   if (n <= 0) return cudaSuccess;
   int* parent = work;
   int* rope = parent + (2 * n - 1);
@@ -2535,7 +2585,8 @@ cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const
   int* left = last + n;
   int* right = left + n;
   count_launch(4);
-  k_combined_codes<<<grid_for(n, 256, 8), 256, 0, s>>>(n, sorted_vals, pair_of_b, mort, codes);
+  k_combined_codes<<<grid_for(n, 256, 8), 256, 0, s>>>(n, sorted_vals, pair_of_b, mort, codes,
+                                                       reinterpret_cast<const uint32_t*>(sort_err));
   cudaMemsetAsync(visit, 0, sizeof(int) * n, s);
   cudaMemsetAsync(rope, 0xff, sizeof(int) * n, s);
   cudaMemsetAsync(roots, 0xff, sizeof(int) * nm, s);

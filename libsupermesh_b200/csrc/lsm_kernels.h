@@ -33,8 +33,13 @@ struct Partial {
   unsigned long long n_out;
 };
 
-// Process-wide count of kernel launches issued by this library.
+// Process-wide count of kernel launches issued by this library (every
+// launcher adds its launches with count_launch).
 unsigned long long launches();
+void count_launch(int n = 1);
+// SMs of the current device; grid of at most per_sm blocks per SM for n items.
+int sm_count();
+int grid_for(int64_t n, int block, int per_sm);
 
 // Launch shape of the persistent tet clipper (3 or 4 blocks per SM).
 int tet_blocks_per_sm();
@@ -80,6 +85,14 @@ cudaError_t launch_morton(int dim, int64_t nel, const double* box64, const doubl
 // radix_hist_entries(n).  Result ends in keys/vals.  *err (optional) becomes
 // nonzero if a look-back wait gave up (bounded; not expected to happen).
 int64_t radix_hist_entries(int64_t n);
+// Test hooks of the sort's bounded waits (process-wide): the number of
+// polls before a look-back wait gives up (default 2^22), and a block (>= 1,
+// -1 = none) that never publishes its digit counts, so that the waits of the
+// blocks after it run out.  Only sorts given an err word take the stall.
+void set_sort_spin_limit(int v);
+int sort_spin_limit();
+void set_sort_stall_block(int b);
+int sort_stall_block();
 cudaError_t radix_sort_pairs(int64_t n, int bits, uint32_t* keys, int32_t* vals, uint32_t* keys_tmp,
                              int32_t* vals_tmp, uint32_t* hist, cudaStream_t s, int* err = nullptr);
 
@@ -127,6 +140,9 @@ cudaError_t launch_scan(int64_t n, const int* counts, int64_t* offsets, int64_t*
 // in which the clipper takes them.  Results do not depend on it.
 // faces_a / screen_b (3D, optional, kScreen3 rows from the prep) enable the
 // second exact early-out (B beyond a face of A).
+// bin (3D, optional): the learned scheduler's reordering of the survivors
+// between the early-out pass and the clipper (lsm_sched.h).
+struct SchedBin;
 int clip_grid_blocks(int dim);
 cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                         const double* coords_a, const double* tol_a, const double* setup_b,
@@ -134,7 +150,7 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
                         const int32_t* order = nullptr, cudaEvent_t ev_begin = nullptr,
                         cudaEvent_t ev_end = nullptr, const double* faces_a = nullptr,
-                        const double* screen_b = nullptr);
+                        const double* screen_b = nullptr, const SchedBin* bin = nullptr);
 // Opt-in shared-memory limits for the clip kernels on the current device.
 cudaError_t init_device_attributes();
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
@@ -155,7 +171,9 @@ cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int
                                 const double* screen_b = nullptr);
 
 // Per-block partials of the pair measures/counts in a fixed order
-// (reduce_pairs_blocks() entries).
+// (reduce_pairs_blocks() == kReduceBlocks entries; the block count is fixed
+// because it sets the totals' summation order).
+constexpr int kReduceBlocks = 1024;
 int reduce_pairs_blocks();
 cudaError_t launch_reduce_pairs(int64_t npairs, const double* pair_measure, const int32_t* pair_nout,
                                 Partial* partials, cudaStream_t s);
@@ -239,7 +257,7 @@ cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const
                                 const uint32_t* mort, unsigned long long* codes, const float* box32,
                                 const int64_t* mesh_off_b, BVH bvh, int* work, int* roots, int* stops,
                                 cudaStream_t s, int dim = 3,
-                                const double* box64 = nullptr);
+                                const double* box64 = nullptr, const int* sort_err = nullptr);
 cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double* box64_a,
                                  const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,

@@ -36,10 +36,11 @@ constexpr size_t kOffList = align_up(kOffIota + sizeof(int32_t) * kMaxPairs);   
 constexpr size_t kOffWork = align_up(kOffList + 4 * sizeof(int32_t) * kMaxPairs);        // misc counters
 constexpr size_t kWorkBytes = 256;
 constexpr size_t kOffPartials = align_up(kOffWork + kWorkBytes);                         // reduction partials
-constexpr size_t kOffTotal = align_up(kOffPartials + sizeof(lsm::Partial) * 1024);
+constexpr size_t kOffTotal = align_up(kOffPartials + sizeof(lsm::Partial) * lsm::kReduceBlocks);
 constexpr size_t kScratchBytes = align_up(kOffTotal + sizeof(lsm::Partial));
 
 static_assert(kScratchBytes == LSM_NOALLOC_SCRATCH_BYTES, "keep the header's scratch size in sync");
+static_assert(lsm::kReduceBlocks == 1024, "the partials region holds one Partial per reduce block");
 
 // Every GPU that loads the library holds this array until the process exits.
 // All calls share it: it keeps the previous call's contents, and calls that
@@ -119,6 +120,13 @@ extern "C" int libsupermesh_gpu_intersect_tets_noalloc(int64_t n, const double* 
     return LSM_ERROR_CAPACITY;
   }
   if (n > 0 && (!tet_a || !tet_b || !measure || !n_out)) return LSM_ERROR_INVALID_ARGUMENT;
+  // the clipper reads each tetrahedron as six 16-byte loads: a pair array
+  // that starts off a 16-byte boundary (a view at an odd double offset) is
+  // refused here instead of faulting on the device
+  if (n > 0 && (((uintptr_t)tet_a | (uintptr_t)tet_b) & 15u) != 0) {
+    fprintf(stderr, "libsupermesh_gpu_intersect_tets_noalloc: tet_a and tet_b must be 16-byte aligned\n");
+    return LSM_ERROR_INVALID_ARGUMENT;
+  }
   void* base = nullptr;
   const int st = scratch_address(&base);
   if (st != LSM_SUCCESS) return st;
@@ -134,6 +142,7 @@ extern "C" int libsupermesh_gpu_intersect_tets_noalloc(int64_t n, const double* 
   if (n > 0) {
     const int blocks = (int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184);
     k_setup_pairs<<<blocks, 256, 0, s>>>(n, tet_a, tet_b, setup, tol, iota);
+    if (cudaPeekAtLastError() != cudaSuccess) return LSM_ERROR_CUDA;
     // launch_clip clears the two work counters (survivors, progress) first
     if (lsm::launch_clip(3, n, iota, iota, tet_a, tol, setup, measure, n_out, list, nullptr, work, s) !=
         cudaSuccess)
@@ -149,5 +158,7 @@ extern "C" int libsupermesh_gpu_intersect_tets_noalloc(int64_t n, const double* 
       return LSM_ERROR_CUDA;
     *total = h.sum;
   }
-  return cudaGetLastError() == cudaSuccess ? LSM_SUCCESS : LSM_ERROR_CUDA;
+  // every launch above was checked where it was issued; an error pending
+  // from other work on this thread is left for its owner
+  return LSM_SUCCESS;
 }
