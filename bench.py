@@ -70,7 +70,11 @@ def parse_args():
     p.add_argument("--workload", default="tet3d_graded_55x51")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--kernel-only", action="store_true",
-                   help="run only warm-up + timed steps (for profiler launch lists)")
+                   help="run only warm-up + timed steps of --op (for profiler launch lists and captures)")
+    p.add_argument("--op", choices=["supermesh", "p1_mass", "p2_inner"], default="supermesh",
+                   help="with --kernel-only: the operation each step runs")
+    p.add_argument("--schedule", type=int, default=0,
+                   help="with --kernel-only: tet_schedule of the 3D narrow phase (1 needs the trained weights)")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the default launch shapes instead of running the autotuner first")
     return p.parse_args()
@@ -384,6 +388,51 @@ def run_batched(args, world, rank, local):
     ctx.close()
 
 
+def kernel_only(args, ctx, dim, A, B, tA, tB, step_device, timed, rank):
+    """Warm-up + timed steps of one operation and nothing else (no second
+    leg, no CPU work): the command that profiler launch lists and captures
+    run.  --op supermesh: the whole pipeline (with --schedule for 3D);
+    p1_mass: the P1-P1 product u^T M v (u = x on A, v = y on B, device
+    meshes and fields); p2_inner: the 2D P2 inner product of P1 fields
+    lifted to P2 (host arrays)."""
+    import libsupermesh_b200 as lsm
+    from libsupermesh_b200 import meshes as M
+
+    sp = None
+    if args.op == "supermesh":
+        if args.schedule:
+            from libsupermesh_b200 import scheduler
+
+            params, _ = scheduler.load()
+            if args.schedule == 1 and params is None:
+                raise SystemExit("--schedule 1 needs trained weights (python -m libsupermesh_b200.scheduler)")
+            if params is not None:
+                ctx.sched_set_weights(params)
+            step_device()  # a plain phase first: tet_schedule 2 takes its classes from it
+            lsm.set_option("tet_schedule", args.schedule)
+        fn = step_device
+    elif args.op == "p1_mass":
+        du, dv = tA[0][:, 0].contiguous(), tB[0][:, 1].contiguous()
+
+        def fn():
+            return ctx.p1_mass(tA, tB, du, dv, on_device=True, stream=sp)
+    else:
+        if dim != 2:
+            raise SystemExit("--op p2_inner needs a 2D workload")
+        e2a, na2, edges_a = M.p2_space(A[1])
+        e2b, nb2, edges_b = M.p2_space(B[1])
+        fa = M.p1_to_p2(A[0][:, 0], na2, edges_a)
+        fb = M.p1_to_p2(B[0][:, 1], nb2, edges_b)
+
+        def fn():
+            return ctx.p2_inner_product(A, B, e2a, fa, e2b, fb)
+    ms, _ = timed(fn, args.steps, args.warmup)
+    lsm.set_option("tet_schedule", 0)
+    if rank == 0:
+        print(json.dumps({"kernel_only": True, "workload": args.workload, "op": args.op, "schedule": args.schedule,
+                          "ms_per_step": ms / args.steps}), flush=True)
+
+
 def broad_phase_bytes(dim, A, B, n_cand):
     """Algorithmic bytes of the candidate search: both meshes' positions and
     element lists read once, 8 B per candidate pair written, and the radix
@@ -459,6 +508,9 @@ def run_ours(args, world, rank, local):
         ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
         return ms, st
 
+    if args.kernel_only:
+        return kernel_only(args, ctx, dim, A, B, tA, tB, step_device, timed, rank)
+
     launches0 = lsm.kernel_launches()
     clocks = ClockSampler(local)
     clocks.start()
@@ -469,10 +521,6 @@ def run_ours(args, world, rank, local):
     ms_dev = all_max(ms_dev, world)
     n_cand = st.n_candidates
     value = whole_job_rate(n_cand, args.steps, world, ms_dev)
-    if args.kernel_only:
-        if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": value, "kernel_only": True}), flush=True)
-        return
 
     ms_e2e, st_e2e = timed(step_e2e, args.steps, max(3, args.warmup // 2))
     ms_e2e = all_max(ms_e2e, world)
@@ -536,7 +584,8 @@ def run_ours(args, world, rank, local):
         "clocks": clock_rec,
     }
     if dim == 3:
-        sched = schedule_legs(ctx, sp, flush, args.steps, world)
+        pm0, pn0 = ctx.pair_results(n_cand)
+        sched = schedule_legs(ctx, sp, flush, args.steps, world, clip_ms, n_cand, pm0, pn0)
         if sched:
             line["schedule"] = sched
     if rank == 0:
@@ -578,10 +627,56 @@ def run_ours(args, world, rank, local):
     ctx.close()
 
 
-def schedule_legs(ctx, sp, flush, steps, world):
-    """Learned-scheduler legs of the 3D narrow phase (filled in once the
-    scheduler exists)."""
-    return None
+def schedule_legs(ctx, sp, flush, steps, world, plain_ms, n_cand, pm0, pn0):
+    """The metric's "chosen vs plain" comparison on the 3D narrow phase: the
+    early-out pass + clipper span (library CUDA events, L2 flushed before
+    each) with the plain work order, with the survivors binned by the learned
+    scheduler's predicted output-size class (tet_schedule 1), and binned by
+    the true classes (tet_schedule 2: a perfect predictor, the ceiling of
+    any scheduler).  The chosen form is the learned schedule where it is
+    faster than the plain one and the plain one otherwise.  Every form's
+    per-pair results are checked bit-identical to the plain run's."""
+    import libsupermesh_b200 as lsm
+    from libsupermesh_b200 import scheduler
+
+    params, meta = scheduler.load()
+    if params is None:
+        return None
+    ctx.sched_set_weights(params)
+
+    def span(mode):
+        lsm.set_option("tet_schedule", mode)
+        lsm.set_option("time_kernels", 1)
+        try:
+            ctx.clip_candidates(stream=sp)
+            ms = []
+            for _ in range(steps):
+                flush()
+                ctx.clip_candidates(stream=sp)
+                ms.append(ctx.clip_kernel_ms())
+            pm, pn = ctx.pair_results(n_cand)
+            assert np.array_equal(pm, pm0) and np.array_equal(pn, pn0), f"schedule {mode} changed results"
+        finally:
+            lsm.set_option("time_kernels", 0)
+            lsm.set_option("tet_schedule", 0)
+        return all_max(sum(ms), world) / steps
+
+    learned_ms = span(1)
+    true_ms = span(2)
+    chosen = "learned" if learned_ms < plain_ms else "plain"
+    chosen_ms = min(learned_ms, plain_ms)
+    return {"window": lsm.get_option("sched_window"),
+            "plain_ms": plain_ms, "learned_ms": learned_ms, "true_class_ms": true_ms,
+            "plain_pairs_per_s": n_cand / (plain_ms * 1e-3), "learned_pairs_per_s": n_cand / (learned_ms * 1e-3),
+            "true_class_pairs_per_s": n_cand / (true_ms * 1e-3),
+            "chosen": chosen, "chosen_pairs_per_s": n_cand / (chosen_ms * 1e-3),
+            "chosen_vs_plain": plain_ms / chosen_ms, "learned_vs_plain": plain_ms / learned_ms,
+            "true_class_vs_plain": plain_ms / true_ms,
+            "results": "per-pair measures and counts bit-identical in every schedule",
+            "model": {k: meta.get(k) for k in ("steps", "samples", "train_accuracy", "graded_accuracy",
+                                               "loss_first", "loss_last")} if meta else None,
+            "timing": "early-out pass + bin + clipper span, CUDA events on the library's stream, "
+                      "L2 flushed before each, mean of the timed repetitions"}
 
 
 def p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush):

@@ -69,12 +69,9 @@ int64_t libsupermesh_gpu_context_bytes(const lsm_gpu_context *ctx);
 /* Kernel launches issued by this library in this process so far. */
 int64_t libsupermesh_gpu_kernel_launches(void);
 
-/* Process-wide tuning options.  They change launch shapes and the 3D clipper
- * variant, never results (the autotuner in libsupermesh_b200/autotune.py
- * picks them per GPU and workload):
- *   "tet_clipper"        0 per-lane depth-first walk over point indices (default),
- *                        1 per-warp task queues, 2 per-lane walk over tets in registers
- *   "tet_blocks_per_sm"  3 (default) or 4 blocks of 128 threads per SM (clipper 2)
+/* Process-wide tuning options.  They change launch shapes and work order,
+ * never results (the autotuner in libsupermesh_b200/autotune.py picks the
+ * launch shapes per GPU and workload):
  *   "tri_blocks_per_sm"  4, 8 (default) or 16 blocks of 128 threads per SM (2D clipper)
  *   "query_block"        64, 128 (default) or 256 threads per block (candidate search)
  *   "time_kernels"       1: record CUDA events around the clip kernel of every
@@ -253,7 +250,8 @@ int libsupermesh_gpu_sched_samples(lsm_gpu_context *ctx, int64_t cap, void *feat
 /* Inference: logits[n][4] (optional) and classes[n] of feature rows. */
 int libsupermesh_gpu_sched_predict(lsm_gpu_context *ctx, int64_t n, const void *features, float *logits,
                                    int8_t *classes, void *stream);
-/* Training: `steps` Adam steps (betas 0.9 / 0.999) on the softmax
+/* Training: `steps` Adam steps (betas 0.9 / 0.999; learning rate decayed
+ * from lr to 0 along a half cosine) on the softmax
  * cross-entropy, minibatches of 128 consecutive rows (row (128 step + i) mod
  * n: shuffle the samples first).  params (in: initial, out: trained);
  * loss_trace (optional) the minibatch loss of every trace_every-th step;
@@ -275,6 +273,43 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context *ctx, int npairs,
                                        int on_device, double *totals,
                                        int64_t *n_candidates, int64_t *n_intersecting,
                                        void *stream);
+
+/* Batched supermesh with per-pair outputs: what a caller of the drop-in C
+ * API gets from one set_input / get_output round and the per-candidate
+ * intersect_*_real + measure calls, for every mesh pair of the batch (the
+ * loop of test_tri_intersector.F90:89-104 and C_bindings.F90:377-391, many
+ * mesh pairs at once).  No counterpart in the reference.
+ *   totals, n_candidates, n_intersecting  [npairs], host (optional)
+ *   cand_offset     [npairs], host (optional): first entry of pair i in the
+ *                   per-candidate arrays, or -1 if they could not hold it
+ *   total_candidates host (optional): entries written to them
+ *   ind_ptr         [sum_i (nelements_a(i) + 1)] (optional): pair i's CSR row
+ *                   pointers at offset sum_{j<i} (nelements_a(j) + 1),
+ *                   starting at 0 (get_output semantics)
+ *   indices         [cand_capacity] (optional): 0-based B element of the pair
+ *   pair_measure    [cand_capacity] (optional): measure of each candidate
+ *   pair_n_out      [cand_capacity] (optional): its number of output simplices
+ * ind_ptr, indices, pair_measure and pair_n_out follow on_device.  Each
+ * pair's candidates are contiguous and in its CSR order; 2D pairs come
+ * before 3D pairs in the arrays.  If they need more than cand_capacity
+ * entries the call still fills totals, counts and ind_ptr, sets cand_offset
+ * of the pairs that did not fit to -1 and returns LSM_ERROR_CAPACITY: retry
+ * with capacity >= the sum of n_candidates. */
+typedef struct {
+  double *totals;
+  int64_t *n_candidates;
+  int64_t *n_intersecting;
+  int64_t *cand_offset;
+  int64_t *total_candidates;
+  int64_t cand_capacity;
+  int64_t *ind_ptr;
+  int64_t *indices;
+  double *pair_measure;
+  int32_t *pair_n_out;
+} lsm_gpu_batch_out;
+int libsupermesh_gpu_supermesh_batched_ex(lsm_gpu_context *ctx, int npairs,
+                                          const lsm_gpu_mesh *a, const lsm_gpu_mesh *b,
+                                          int on_device, lsm_gpu_batch_out *out, void *stream);
 
 /* Allocation-free clipping of explicit tetrahedron pairs (no counterpart in
  * the reference).  For callers that cannot let a library allocate device

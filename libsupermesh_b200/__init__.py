@@ -63,6 +63,21 @@ class Mesh(ctypes.Structure):
     ]
 
 
+class BatchOut(ctypes.Structure):
+    _fields_ = [
+        ("totals", ctypes.c_void_p),
+        ("n_candidates", ctypes.c_void_p),
+        ("n_intersecting", ctypes.c_void_p),
+        ("cand_offset", ctypes.c_void_p),
+        ("total_candidates", ctypes.c_void_p),
+        ("cand_capacity", ctypes.c_int64),
+        ("ind_ptr", ctypes.c_void_p),
+        ("indices", ctypes.c_void_p),
+        ("pair_measure", ctypes.c_void_p),
+        ("pair_n_out", ctypes.c_void_p),
+    ]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("n_candidates", ctypes.c_int64),
@@ -124,6 +139,8 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_p2_inner_product.argtypes = [vp, mp, mp, vp, vp, ctypes.c_int64, vp, vp, ctypes.c_int64, vp,
                                                     _dp, _dp, ctypes.c_int, vp]
     L.libsupermesh_gpu_supermesh_batched.argtypes = [vp, ctypes.c_int, mp, mp, ctypes.c_int, vp, vp, vp, vp]
+    L.libsupermesh_gpu_supermesh_batched_ex.argtypes = [vp, ctypes.c_int, mp, mp, ctypes.c_int,
+                                                        ctypes.POINTER(BatchOut), vp]
     L.libsupermesh_gpu_sched_set_weights.argtypes = [vp, vp, ctypes.c_int]
     L.libsupermesh_gpu_sched_samples.argtypes = [vp, ctypes.c_int64, vp, vp, _i64p, vp]
     L.libsupermesh_gpu_sched_predict.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp]
@@ -135,7 +152,8 @@ def load() -> ctypes.CDLL:
                  "libsupermesh_gpu_clip_candidates",
                  "libsupermesh_gpu_intersect_pairs", "libsupermesh_gpu_intersect_pairs_mixed",
                  "libsupermesh_gpu_p1_mass", "libsupermesh_gpu_p2_inner_product",
-                 "libsupermesh_gpu_supermesh_batched", "libsupermesh_gpu_sched_set_weights",
+                 "libsupermesh_gpu_supermesh_batched", "libsupermesh_gpu_supermesh_batched_ex",
+                 "libsupermesh_gpu_sched_set_weights",
                  "libsupermesh_gpu_sched_samples", "libsupermesh_gpu_sched_predict",
                  "libsupermesh_gpu_sched_train"):
         getattr(L, name).restype = ctypes.c_int
@@ -361,6 +379,59 @@ class Context:
             e2b.ctypes.data, fb.ctypes.data, fb.size, _ptr(pv), ctypes.byref(integral), ctypes.byref(area), 0,
             None))
         return integral.value, area.value, (pv[:n] if pv is not None else None)
+
+    def supermesh_batched_pairs(self, pairs, capacity: int | None = None, on_device: bool = False, out=None,
+                                stream: int | None = None):
+        """Batched supermesh with per-pair outputs (host meshes and arrays
+        unless on_device).  Returns a dict with totals, n_candidates,
+        n_intersecting, cand_offset, total_candidates, and the arrays ind_ptr
+        (pair i's rows at row_offset[i]), indices, pair_measure, pair_n_out.
+        With capacity None the call is made twice if needed: the first
+        attempt's counts size the retry (LSM_ERROR_CAPACITY).  `out` (dict
+        of preallocated arrays, optional) is used as is."""
+        n = len(pairs)
+        A = (Mesh * max(n, 1))()
+        B = (Mesh * max(n, 1))()
+        keep = []
+        for i, (ma, mb) in enumerate(pairs):
+            a, b = _mesh(*ma, on_device), _mesh(*mb, on_device)
+            keep.append((a, b))
+            A[i], B[i] = a, b
+        rows = [int(ma[1].shape[0]) + 1 for ma, _ in pairs]
+        row_offset = np.concatenate([[0], np.cumsum(rows)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
+        cap = capacity if capacity is not None else (out["capacity"] if out else 0)
+        while True:
+            if out is None:
+                r = {"totals": np.zeros(max(n, 1)), "n_candidates": np.zeros(max(n, 1), dtype=np.int64),
+                     "n_intersecting": np.zeros(max(n, 1), dtype=np.int64),
+                     "cand_offset": np.zeros(max(n, 1), dtype=np.int64),
+                     "total_candidates": np.zeros(1, dtype=np.int64)}
+                if on_device:
+                    import torch
+
+                    dev = torch.device("cuda", torch.cuda.current_device())
+                    r["ind_ptr"] = torch.zeros(max(sum(rows), 1), dtype=torch.int64, device=dev)
+                    r["indices"] = torch.zeros(max(cap, 1), dtype=torch.int64, device=dev)
+                    r["pair_measure"] = torch.zeros(max(cap, 1), dtype=torch.float64, device=dev)
+                    r["pair_n_out"] = torch.zeros(max(cap, 1), dtype=torch.int32, device=dev)
+                else:
+                    r["ind_ptr"] = np.zeros(max(sum(rows), 1), dtype=np.int64)
+                    r["indices"] = np.zeros(max(cap, 1), dtype=np.int64)
+                    r["pair_measure"] = np.zeros(max(cap, 1))
+                    r["pair_n_out"] = np.zeros(max(cap, 1), dtype=np.int32)
+            else:
+                r = out
+            o = BatchOut(_ptr(r["totals"]), _ptr(r["n_candidates"]), _ptr(r["n_intersecting"]),
+                         _ptr(r["cand_offset"]), _ptr(r["total_candidates"]), cap, _ptr(r["ind_ptr"]),
+                         _ptr(r["indices"]), _ptr(r["pair_measure"]), _ptr(r["pair_n_out"]))
+            st = self.lib.libsupermesh_gpu_supermesh_batched_ex(self._h, n, A, B, int(on_device), ctypes.byref(o),
+                                                                stream)
+            if st == 3 and capacity is None and out is None:  # LSM_ERROR_CAPACITY: size the retry
+                cap = int(r["n_candidates"][:n].sum())
+                continue
+            self._check(st)
+            r["row_offset"] = row_offset
+            return r
 
     # -- learned scheduler (device buffers: torch tensors) -------------------
     def sched_set_weights(self, params) -> None:

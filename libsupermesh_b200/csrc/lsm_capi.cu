@@ -71,10 +71,10 @@ struct Ctx {
   // candidates
   DevBuf counts, offsets, scan_tmp, pair_a, pair_b, i64_tmp, q_cache, q_over, q_pool, q_next, q_first;
   // narrow phase
-  DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals, wq_scratch;
+  DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals;
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
-  DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand;
+  DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand, bt_indptr;
   // host meshes of a batch staged on the device, one set per dimension (the
   // 3D set is copied on the side stream while the 2D group computes)
   DevBuf bt_stage_pa[2], bt_stage_ea[2], bt_stage_pb[2], bt_stage_eb[2];
@@ -235,7 +235,7 @@ void fini_ctx(Ctx* c) {
                    &c->keys_tmp, &c->vals_tmp, &c->hist, &c->root_partial, &c->rootbox, &c->bvh_lo,
                    &c->bvh_work, &c->bvh_leaf, &c->counts, &c->offsets, &c->scan_tmp, &c->pair_a,
                    &c->pair_b, &c->i64_tmp, &c->pair_measure, &c->pair_nout, &c->partials,
-                   &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->wq_scratch, &c->x_a, &c->x_b, &c->x_measure,
+                   &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->x_a, &c->x_b, &c->x_measure,
                    &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
                    &c->bt_ncand, &c->bt_stage_pa[0], &c->bt_stage_ea[0], &c->bt_stage_pb[0],
@@ -244,7 +244,7 @@ void fini_ctx(Ctx* c) {
                    &c->d1_keyhi, &c->d1_perm_a, &c->d1_perm_b, &c->d1_lo_a, &c->d1_hi_a, &c->d1_lo_b,
                    &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over, &c->q_pool, &c->q_next, &c->q_first,
                    &c->a_faces, &c->b_screen, &c->surv, &c->sched_w, &c->sched_list, &c->sched_cls,
-                   &c->sched_adam};
+                   &c->sched_adam, &c->bt_indptr};
   for (DevBuf* b : all) free_buf(*b);
   for (cudaEvent_t& e : c->clip_ev)
     if (e) {
@@ -559,10 +559,9 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
     c->have_pairs = true;
     return;
   }
-  bool queued = false;
   const bool screen = c->dim == 3 && g_tet_screen;
   lsm::SchedBin bin;
-  const bool binned = c->dim == 3 && g_tet_schedule != 0 && lsm::tet_clipper_variant() == 0;
+  const bool binned = c->dim == 3 && g_tet_schedule != 0;
   if (binned) {
     if (g_tet_schedule == 1 && !c->have_sched) {
       set_error(c, "tet_schedule 1 needs scheduler weights (libsupermesh_gpu_sched_set_weights)");
@@ -583,31 +582,13 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
     bin.out = ensure<int4>(c, c->sched_list, nnz);
     bin.window = g_sched_window;
   }
-  if (c->dim == 3 && lsm::tet_clipper_variant() == 1) {
-    int* err = bad_flag(c) + 16;
-    unsigned char* scr = ensure<unsigned char>(c, c->wq_scratch, (int64_t)lsm::wq_scratch_bytes());
-    CU(lsm::launch_clip_tets_wq(nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
-                                static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
-                                static_cast<double*>(c->b_setup.p), pm, pn, ovf, work, scr, err, s, order,
-                                screen ? static_cast<double*>(c->a_faces.p) : nullptr,
-                                screen ? static_cast<double*>(c->b_screen.p) : nullptr));
-    int* h = static_cast<int*>(c->host_scalars) + 4;
-    CU(cudaMemcpyAsync(h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CU(cudaMemcpyAsync(h + 2, work, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
-    queued = h[0] == 0;  // on overflow the per-lane clipper redoes the pairs
-    if (getenv("LSM_DEBUG"))
-      fprintf(stderr, "task-queue clipper: err=%d survivors=%llu deepest clip stack=%llu\n", h[0],
-              reinterpret_cast<unsigned long long*>(h + 2)[0], reinterpret_cast<unsigned long long*>(h + 2)[2]);
-  }
-  if (!queued)
-    CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+  CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                         static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                         static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order,
                         g_time_kernels ? c->clip_ev[0] : nullptr, g_time_kernels ? c->clip_ev[1] : nullptr,
                         screen ? static_cast<double*>(c->a_faces.p) : nullptr,
                         screen ? static_cast<double*>(c->b_screen.p) : nullptr, binned ? &bin : nullptr));
-  c->clip_timed = !queued && g_time_kernels;
+  c->clip_timed = g_time_kernels;
   if (c->dim == 3) {
     CU(cudaMemcpyAsync(ensure<unsigned long long>(c, c->surv, 1), work, sizeof(unsigned long long),
                        cudaMemcpyDeviceToDevice, s));
@@ -710,6 +691,20 @@ void stage_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_g
   }
 }
 
+// Per-pair outputs of a batched call (libsupermesh_gpu_supermesh_batched_ex):
+// the caller's arrays, each pair's first CSR row in them (caller order), and
+// the next free slot of the per-candidate arrays (groups are written one
+// after the other).  ind_ptr of host calls goes through a device image of
+// the whole array, copied out once at the end.
+struct BatchOut {
+  const lsm_gpu_batch_out* o = nullptr;
+  std::vector<int64_t> rowbase;  // caller order
+  int64_t total_rows = 0;
+  int64_t next = 0;
+  bool overflow = false;
+  int64_t* dev_indptr = nullptr;  // where the kernels write ind_ptr
+};
+
 // All mesh pairs of one dimension through each phase in one launch:
 // batched prep (pointer tables), one sort by (mesh, Morton), one LBVH with a
 // subtree per mesh, one traversal, the usual clipper over all candidates,
@@ -718,14 +713,14 @@ void stage_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_g
 // null when the meshes are on the device.
 void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu_mesh* ma,
                      const lsm_gpu_mesh* mb, const uint64_t* staged, double* totals, int64_t* ncand,
-                     int64_t* nint, cudaStream_t s) {
+                     int64_t* nint, cudaStream_t s, BatchOut* bo = nullptr, int on_device = 0) {
   const int nm = (int)idx.size();
   const int ib = ma[idx[0]].index_bytes;
   const int loc = dim + 1;
   c->surv_valid = false;
   // host tables: elem_off_a[nm+1] elem_off_b[nm+1] nnodes_a[nm] nnodes_b[nm]
-  //              pos_a[nm] en_a[nm] pos_b[nm] en_b[nm]
-  const size_t tab_words = 2 * (nm + 1) + 6 * (size_t)nm;
+  //              pos_a[nm] en_a[nm] pos_b[nm] en_b[nm] rowbase[nm]
+  const size_t tab_words = 2 * (nm + 1) + 7 * (size_t)nm;
   std::vector<int64_t> tab(tab_words);
   int64_t* eoa = tab.data();
   int64_t* eob = eoa + (nm + 1);
@@ -735,6 +730,8 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   uint64_t* eta = pta + nm;
   uint64_t* ptb = eta + nm;
   uint64_t* etb = ptb + nm;
+  int64_t* rbase = reinterpret_cast<int64_t*>(etb + nm);
+  for (int i = 0; i < nm; ++i) rbase[i] = bo && bo->o ? bo->rowbase[idx[i]] : 0;
   int64_t na = 0, nb = 0;
   for (int i = 0; i < nm; ++i) {
     const lsm_gpu_mesh& A = ma[idx[i]];
@@ -773,6 +770,7 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   const unsigned long long* d_eta = d_pta + nm;
   const unsigned long long* d_ptb = d_eta + nm;
   const unsigned long long* d_etb = d_ptb + nm;
+  const int64_t* d_rbase = reinterpret_cast<const int64_t*>(d_etb + nm);
 
   int* bad = bad_flag(c);
   CU(cudaMemsetAsync(bad, 0, sizeof(int) * 64, s));
@@ -868,6 +866,31 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   lsm::Partial* pieces = ensure<lsm::Partial>(c, c->partials, lsm::mesh_totals_pieces(nm));
   CU(lsm::launch_mesh_totals(nm, d_eoa, offsets, static_cast<double*>(c->pair_measure.p),
                              static_cast<int32_t*>(c->pair_nout.p), pieces, tot, nc, s));
+  // per-pair outputs: CSR rows at the caller's row bases; the group's
+  // per-candidate arrays (pair-major, as the caller's) as one block at the
+  // next free slot, if they fit
+  int64_t group_base = -1;
+  if (bo && bo->o) {
+    const lsm_gpu_batch_out* o = bo->o;
+    const bool fits = bo->next + nnz <= o->cand_capacity;
+    if (!fits) bo->overflow = true;
+    const bool want_ind = fits && o->indices && nnz > 0;
+    int64_t* ind_dst = nullptr;
+    if (want_ind) ind_dst = on_device ? o->indices + bo->next : ensure<int64_t>(c, c->i64_tmp, nnz);
+    CU(lsm::launch_batch_csr(na, nm, pair_of_a, d_eoa, offsets, d_rbase, o->ind_ptr ? bo->dev_indptr : nullptr,
+                             want_ind ? nnz : 0, pb, pair_of_b, d_eob, ind_dst, s));
+    if (fits) {
+      const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+      if (want_ind && !on_device)
+        CU(cudaMemcpyAsync(o->indices + bo->next, ind_dst, sizeof(int64_t) * nnz, k, s));
+      if (o->pair_measure && nnz > 0)
+        CU(cudaMemcpyAsync(o->pair_measure + bo->next, c->pair_measure.p, sizeof(double) * nnz, k, s));
+      if (o->pair_n_out && nnz > 0)
+        CU(cudaMemcpyAsync(o->pair_n_out + bo->next, c->pair_nout.p, sizeof(int32_t) * nnz, k, s));
+      group_base = bo->next;
+      bo->next += nnz;
+    }
+  }
   const size_t bytes = sizeof(lsm::Partial) * nm + sizeof(int64_t) * nm;
   char* hs = static_cast<char*>(host_stage(c, bytes));
   CU(cudaMemcpyAsync(hs, tot, sizeof(lsm::Partial) * nm, cudaMemcpyDeviceToHost, s));
@@ -875,10 +898,13 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   CU(cudaStreamSynchronize(s));
   const lsm::Partial* ht = reinterpret_cast<const lsm::Partial*>(hs);
   const int64_t* hn = reinterpret_cast<const int64_t*>(hs + sizeof(lsm::Partial) * nm);
+  int64_t run = group_base;
   for (int i = 0; i < nm; ++i) {
     if (totals) totals[idx[i]] = ht[i].sum;
     if (ncand) ncand[idx[i]] = hn[i];
     if (nint) nint[idx[i]] = (int64_t)ht[i].n_int;
+    if (bo && bo->o && bo->o->cand_offset) bo->o->cand_offset[idx[i]] = group_base >= 0 ? run : -1;
+    if (group_base >= 0) run += hn[i];
   }
 }
 
@@ -997,6 +1023,79 @@ struct lsm_gpu_context {
 };
 
 static Ctx* C(lsm_gpu_context* p) { return p ? &p->c : nullptr; }
+
+// Both batched entries.
+static int batched(Ctx* c, int npairs, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b, int on_device, double* totals,
+            int64_t* n_candidates, int64_t* n_intersecting, const lsm_gpu_batch_out* out, void* stream) {
+  return guarded(c, [&] {
+    REQUIRE(npairs >= 0 && (npairs == 0 || (a && b)), "invalid batch");
+    cudaStream_t s = pick(c, stream);
+    std::vector<int> g2, g3;
+    for (int i = 0; i < npairs; ++i) {
+      check_mesh(c, &a[i], "A", true);
+      check_mesh(c, &b[i], "B", true);
+      REQUIRE(a[i].dim >= 2, "batched supermesh: pair %d is 1D (use libsupermesh_gpu_supermesh)", i);
+      REQUIRE(a[i].dim == b[i].dim, "Invalid dimension: pair %d mixes %dD and %dD", i, a[i].dim, b[i].dim);
+      REQUIRE(a[i].index_bytes == a[0].index_bytes && b[i].index_bytes == a[0].index_bytes,
+              "all meshes of a batch must use the same index width");
+      (a[i].dim == 2 ? g2 : g3).push_back(i);
+    }
+    BatchOut bo;
+    if (out) {
+      REQUIRE(out->cand_capacity >= 0, "negative candidate capacity");
+      bo.o = out;
+      bo.rowbase.resize(npairs);
+      for (int i = 0; i < npairs; ++i) {
+        bo.rowbase[i] = bo.total_rows;
+        bo.total_rows += a[i].nelements + 1;
+      }
+      if (out->ind_ptr)
+        bo.dev_indptr = on_device ? out->ind_ptr : ensure<int64_t>(c, c->bt_indptr, bo.total_rows);
+    }
+    c->have_pairs = false;
+    c->ncand = -1;
+    // Host meshes: the 2D group's copies go on the caller's stream; the 3D
+    // group's go on the side stream, where they overlap the 2D group's work
+    // (the side stream first waits for earlier work on s, which may still
+    // read the 3D staging buffers).
+    std::vector<uint64_t> st2, st3;
+    const bool side3 = !on_device && !g2.empty() && !g3.empty();
+    SyncOnThrow sync_on_throw{s, c->side};
+    if (!on_device && !g2.empty()) stage_batch_group(c, 2, g2, a, b, s, st2);
+    if (!on_device && !g3.empty()) {
+      if (side3) {
+        CU(cudaEventRecord(c->side_ev[0], s));
+        CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
+      }
+      stage_batch_group(c, 3, g3, a, b, side3 ? c->side : s, st3);
+      if (side3) CU(cudaEventRecord(c->side_ev[1], c->side));
+    }
+    BatchOut* bp = out ? &bo : nullptr;
+    if (!g2.empty())
+      run_batch_group(c, 2, g2, a, b, on_device ? nullptr : st2.data(), totals, n_candidates, n_intersecting, s, bp,
+                      on_device);
+    if (!g3.empty()) {
+      if (side3) CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
+      run_batch_group(c, 3, g3, a, b, on_device ? nullptr : st3.data(), totals, n_candidates, n_intersecting, s, bp,
+                      on_device);
+    }
+    if (out && out->ind_ptr && !on_device && bo.total_rows > 0) {
+      CU(cudaMemcpyAsync(out->ind_ptr, bo.dev_indptr, sizeof(int64_t) * bo.total_rows, cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+    }
+    if (out) {
+      if (out->total_candidates) *out->total_candidates = bo.next;
+      if (bo.overflow) {
+        int64_t need = 0;
+        if (n_candidates)
+          for (int i = 0; i < npairs; ++i) need += n_candidates[i];
+        set_error(c, "batched supermesh: %lld candidates do not fit the per-candidate arrays (capacity %lld)",
+                  (long long)need, (long long)out->cand_capacity);
+        throw Fail{LSM_ERROR_CAPACITY};
+      }
+    }
+  });
+}
 
 extern "C" {
 
@@ -1143,11 +1242,7 @@ int64_t libsupermesh_gpu_kernel_launches(void) { return (int64_t)lsm::launches()
 int libsupermesh_gpu_set_option(const char* name, int64_t value) {
   if (!name) return LSM_ERROR_INVALID_ARGUMENT;
   const std::string n(name);
-  if (n == "tet_clipper" && value >= 0 && value <= 2) {
-    lsm::set_tet_clipper_variant((int)value);
-  } else if (n == "tet_blocks_per_sm" && (value == 3 || value == 4)) {
-    lsm::set_tet_blocks_per_sm((int)value);
-  } else if (n == "tri_blocks_per_sm" && (value == 4 || value == 8 || value == 16)) {
+  if (n == "tri_blocks_per_sm" && (value == 4 || value == 8 || value == 16)) {
     lsm::set_tri_blocks_per_sm((int)value);
   } else if (n == "query_block" && (value == 64 || value == 128 || value == 256)) {
     lsm::set_query_block((int)value);
@@ -1176,11 +1271,7 @@ int libsupermesh_gpu_set_option(const char* name, int64_t value) {
 int libsupermesh_gpu_get_option(const char* name, int64_t* value) {
   if (!name || !value) return LSM_ERROR_INVALID_ARGUMENT;
   const std::string n(name);
-  if (n == "tet_clipper")
-    *value = lsm::tet_clipper_variant();
-  else if (n == "tet_blocks_per_sm")
-    *value = lsm::tet_blocks_per_sm();
-  else if (n == "tri_blocks_per_sm")
+  if (n == "tri_blocks_per_sm")
     *value = lsm::tri_blocks_per_sm();
   else if (n == "query_block")
     *value = lsm::query_block();
@@ -1541,8 +1632,8 @@ int libsupermesh_gpu_sched_samples(lsm_gpu_context* ctx, int64_t cap, void* feat
   return guarded(c, [&] {
     REQUIRE(cap >= 0 && (cap == 0 || (features && classes)), "invalid sample buffers");
     REQUIRE((((uintptr_t)features) & 15u) == 0, "features must be 16-byte aligned");
-    if (!c->surv_valid || !c->have_pairs || c->dim != 3 || g_tet_schedule != 0 || lsm::tet_clipper_variant() != 0) {
-      set_error(c, "no plain 3D narrow phase (tet_schedule 0, tet_clipper 0) since the last candidate search");
+    if (!c->surv_valid || !c->have_pairs || c->dim != 3) {
+      set_error(c, "no 3D narrow phase since the last candidate search");
       throw Fail{LSM_ERROR_STATE};
     }
     cudaStream_t s = pick(c, stream);
@@ -1591,45 +1682,26 @@ int libsupermesh_gpu_sched_train(lsm_gpu_context* ctx, int64_t n, const void* fe
 int libsupermesh_gpu_supermesh_batched(lsm_gpu_context* ctx, int npairs, const lsm_gpu_mesh* a,
                                        const lsm_gpu_mesh* b, int on_device, double* totals,
                                        int64_t* n_candidates, int64_t* n_intersecting, void* stream) {
+  return batched(C(ctx), npairs, a, b, on_device, totals, n_candidates, n_intersecting, nullptr, stream);
+}
+
+int libsupermesh_gpu_supermesh_batched_ex(lsm_gpu_context* ctx, int npairs, const lsm_gpu_mesh* a,
+                                          const lsm_gpu_mesh* b, int on_device, lsm_gpu_batch_out* out,
+                                          void* stream) {
   Ctx* c = C(ctx);
-  return guarded(c, [&] {
-    REQUIRE(npairs >= 0 && (npairs == 0 || (a && b)), "invalid batch");
-    cudaStream_t s = pick(c, stream);
-    std::vector<int> g2, g3;
-    for (int i = 0; i < npairs; ++i) {
-      check_mesh(c, &a[i], "A", true);
-      check_mesh(c, &b[i], "B", true);
-      REQUIRE(a[i].dim >= 2, "batched supermesh: pair %d is 1D (use libsupermesh_gpu_supermesh)", i);
-      REQUIRE(a[i].dim == b[i].dim, "Invalid dimension: pair %d mixes %dD and %dD", i, a[i].dim, b[i].dim);
-      REQUIRE(a[i].index_bytes == a[0].index_bytes && b[i].index_bytes == a[0].index_bytes,
-              "all meshes of a batch must use the same index width");
-      (a[i].dim == 2 ? g2 : g3).push_back(i);
-    }
-    c->have_pairs = false;
-    c->ncand = -1;
-    // Host meshes: the 2D group's copies go on the caller's stream; the 3D
-    // group's go on the side stream, where they overlap the 2D group's work
-    // (the side stream first waits for earlier work on s, which may still
-    // read the 3D staging buffers).
-    std::vector<uint64_t> st2, st3;
-    const bool side3 = !on_device && !g2.empty() && !g3.empty();
-    SyncOnThrow sync_on_throw{s, c->side};
-    if (!on_device && !g2.empty()) stage_batch_group(c, 2, g2, a, b, s, st2);
-    if (!on_device && !g3.empty()) {
-      if (side3) {
-        CU(cudaEventRecord(c->side_ev[0], s));
-        CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
-      }
-      stage_batch_group(c, 3, g3, a, b, side3 ? c->side : s, st3);
-      if (side3) CU(cudaEventRecord(c->side_ev[1], c->side));
-    }
-    if (!g2.empty())
-      run_batch_group(c, 2, g2, a, b, on_device ? nullptr : st2.data(), totals, n_candidates, n_intersecting, s);
-    if (!g3.empty()) {
-      if (side3) CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
-      run_batch_group(c, 3, g3, a, b, on_device ? nullptr : st3.data(), totals, n_candidates, n_intersecting, s);
-    }
-  });
+  if (!c) return LSM_ERROR_INVALID_ARGUMENT;
+  if (!out) {
+    set_error(c, "NULL output descriptor");
+    return LSM_ERROR_INVALID_ARGUMENT;
+  }
+  // counts are needed to report the size a retry needs
+  std::vector<int64_t> nc_local;
+  int64_t* nc = out->n_candidates;
+  if (!nc) {
+    nc_local.assign(npairs > 0 ? npairs : 1, 0);
+    nc = nc_local.data();
+  }
+  return batched(c, npairs, a, b, on_device, out->totals, nc, out->n_intersecting, out, stream);
 }
 
 }  // extern "C"

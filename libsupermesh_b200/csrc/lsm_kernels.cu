@@ -15,10 +15,8 @@
 //   K5  k_clip_tris     one candidate pair per thread, polygon in shared
 //                       memory, FP64 Sutherland-Hodgman
 //   K6  k_prefilter_tets two exact early-outs and the no-op plane mask;
-//                       k_clip_tets_ix (default) depth-first clipping over
-//                       point indices with a refill pipeline;
-//                       k_clip_tets (tets in registers), k_clip_tets_wq
-//                       (per-warp task queues) as alternatives
+//                       k_clip_tets_ix depth-first clipping over point
+//                       indices with a refill pipeline
 //   K7  compensated reductions (per-block (sum, err), then final; per mesh
 //                       pair for the batched path)
 //   K8  k_p1_mass       P1-P1 mixed mass blocks + u^T M v;  k_p2_inner  P2
@@ -47,42 +45,6 @@ unsigned long long g_launches = 0;
 }  // namespace
 
 unsigned long long launches() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
-
-namespace {
-int g_tet_bps = 0;
-}  // namespace
-
-// Blocks per SM of the register tet clipper, variant 2 (3: up to 170
-// registers per thread, no spills; 4: up to 128, spills).  Default 3
-// (measured faster on B200); LSM_TET_BLOCKS_PER_SM overrides it.
-int tet_blocks_per_sm() {
-  if (g_tet_bps == 0) {
-    const char* e = getenv("LSM_TET_BLOCKS_PER_SM");
-    g_tet_bps = (e && atoi(e) == 4) ? 4 : 3;
-  }
-  return g_tet_bps;
-}
-
-void set_tet_blocks_per_sm(int v) { g_tet_bps = (v == 3) ? 3 : 4; }
-
-namespace {
-int g_tet_variant = -1;
-}  // namespace
-
-// 3D clipper variant: 0 = per-lane depth-first walk over point indices
-// (k_clip_tets_ix, default), 1 = per-warp task queues in L2
-// (k_clip_tets_wq), 2 = per-lane depth-first walk over tets held in
-// registers (k_clip_tets).  LSM_TET_CLIPPER=index|queue|register.
-// Measured on B200 (tet3d_27x32): 3.0 ms, 6.3 ms and 4.6 ms.
-int tet_clipper_variant() {
-  if (g_tet_variant < 0) {
-    const char* e = getenv("LSM_TET_CLIPPER");
-    g_tet_variant = (e && e[0] == 'q') ? 1 : (e && e[0] == 'r') ? 2 : 0;
-  }
-  return g_tet_variant;
-}
-
-void set_tet_clipper_variant(int v) { g_tet_variant = (v == 1 || v == 2) ? v : 0; }
 
 namespace {
 int g_tri_bps = 8;
@@ -1213,9 +1175,7 @@ namespace {
 constexpr int kTriBlock = 128;
 constexpr int kTriCap = 8;  // fast-path polygon slots (geometric max is 6)
 constexpr int kTriWideCap = 24;
-constexpr int kTetBlock = 128;
 constexpr int kTetStack = 6;      // max pending tets: 2 per level for planes 0-2
-constexpr int kTetSmemSlots = 3;  // stack slots kept in shared memory
 }  // namespace
 
 // Polygon in shared memory: slot i, coord c at base[(2*i + c) * BLOCK].
@@ -1333,39 +1293,6 @@ __global__ void __launch_bounds__(32) k_clip_tris_wide(const int32_t* __restrict
 // ======================================================================
 // K6: tetrahedron clipping, depth-first
 // ======================================================================
-// Stack of pending tets.  Slots [0, kTetSmemSlots) live in shared memory
-// (slot s, component j at base[(s*12 + j) * BLOCK]); deeper slots, which
-// few pairs reach, live in per-thread local memory.
-template <int BLOCK>
-struct TetStack {
-  double* base;
-  Tet deep[kTetStack - kTetSmemSlots];
-  __device__ __forceinline__ void store(int s, const Tet& t) {
-    if (s < kTetSmemSlots) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        base[(s * 12 + 3 * k + 0) * BLOCK] = t.x[k];
-        base[(s * 12 + 3 * k + 1) * BLOCK] = t.y[k];
-        base[(s * 12 + 3 * k + 2) * BLOCK] = t.z[k];
-      }
-    } else {
-      deep[s - kTetSmemSlots] = t;
-    }
-  }
-  __device__ __forceinline__ void load(int s, Tet& t) const {
-    if (s < kTetSmemSlots) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        t.x[k] = base[(s * 12 + 3 * k + 0) * BLOCK];
-        t.y[k] = base[(s * 12 + 3 * k + 1) * BLOCK];
-        t.z[k] = base[(s * 12 + 3 * k + 2) * BLOCK];
-      }
-    } else {
-      t = deep[s - kTetSmemSlots];
-    }
-  }
-};
-
 struct TetStackLocal {
   Tet slot[kTetStack];
   __device__ __forceinline__ void store(int s, const Tet& t) { slot[s] = t; }
@@ -1511,12 +1438,11 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 // changes nothing in the reference's result; such planes form the pair's
 // no-op mask.  With all four planes no-op the reference returns A itself,
 // which is settled here (volume test and measure as in the clipper).
-// RECORDS: survivors are written as {pair, a, b, no-op mask} so that the
-// clipper gets the element numbers and the planes to skip in one load.
+// Survivors are written as {pair, a, b, no-op mask} so that the clipper
+// gets the element numbers and the planes to skip in one load.
 #ifndef LSM_PREFILTER_BPS
 #define LSM_PREFILTER_BPS 2
 #endif
-template <bool RECORDS>
 __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ order,
                                                         const int32_t* __restrict__ pa,
                                                         const int32_t* __restrict__ pb,
@@ -1621,420 +1547,18 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
       off = __shfl_sync(0xffffffffu, off, leader);
       if (live) {
         const int64_t o = (int64_t)off + __popc(mask & lt);
-        if (RECORDS)
-          reinterpret_cast<int4*>(survivors)[o] = make_int4((int)i, a, b, noop);
-        else
-          survivors[o] = (int32_t)i;
+        reinterpret_cast<int4*>(survivors)[o] = make_int4((int)i, a, b, noop);
       }
     }
-  }
-}
-
-// Persistent clipper over the surviving pairs: one pair per lane, one
-// tet-vs-plane clip per loop iteration (depth-first, children 1..k-1 parked
-// on the lane's stack).  A lane whose pair is finished takes the next pair
-// from a global counter (one atomic per warp per refill), so lanes stay busy
-// even though pairs differ in work by more than 10x.
-template <int BPS>
-__global__ void __launch_bounds__(kTetBlock, BPS) k_clip_tets(
-    const int32_t* __restrict__ list, const unsigned long long* __restrict__ nlist,
-    const int32_t* __restrict__ pa, const int32_t* __restrict__ pb, const double* __restrict__ coords_a,
-    const double* __restrict__ tol_a, const double* __restrict__ setup_b, double* pair_measure,
-    int32_t* pair_nout, unsigned long long* work) {
-  extern __shared__ double stack_mem[];
-  TetStack<kTetBlock> stk{stack_mem + threadIdx.x};
-  // the current pair's four planes, plane L component j at my_planes[(4L+j)*kTetBlock]
-  double* my_planes = stack_mem + kTetSmemSlots * 12 * kTetBlock + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  const unsigned lt = (1u << lane) - 1u;
-  const int64_t npairs = (int64_t)*nlist;
-  int64_t p = -1;
-  bool exhausted = false;
-  Tet t;
-  double tol = 0.0, m = 0.0;
-  int L = 0, sp = 0, kept = 0;
-  unsigned levels = 0;
-  for (;;) {
-    const bool need = p < 0 && !exhausted;
-    const unsigned needmask = __ballot_sync(0xffffffffu, need);
-    if (needmask) {
-      const int leader = __ffs(needmask) - 1;
-      unsigned long long base = 0;
-      if (lane == leader) base = atomicAdd(work, (unsigned long long)__popc(needmask));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (need) {
-        const int64_t q = (int64_t)(base + __popc(needmask & lt));
-        if (q < npairs) {
-          p = list[q];
-          const int a = pa[p], b = pb[p];
-          load_tet(coords_a + (int64_t)a * 12, t);
-          const double2* pl = reinterpret_cast<const double2*>(setup_b + (int64_t)b * kSetup3);
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const double2 v = __ldg(pl + j);
-            my_planes[(2 * j) * kTetBlock] = v.x;
-            my_planes[(2 * j + 1) * kTetBlock] = v.y;
-          }
-          tol = fmin(tol_a[a], setup_b[(int64_t)b * kSetup3 + 16]);
-          m = 0.0;
-          L = 0;
-          sp = 0;
-          kept = 0;
-          levels = 0;
-        } else {
-          exhausted = true;
-        }
-      }
-    }
-    if (__all_sync(0xffffffffu, p < 0)) break;
-    if (p < 0) continue;
-    const double nx = my_planes[(4 * L + 0) * kTetBlock], ny = my_planes[(4 * L + 1) * kTetBlock];
-    const double nz = my_planes[(4 * L + 2) * kTetBlock], c = my_planes[(4 * L + 3) * kTetBlock];
-    auto leaf = [&](const Tet& o) { m = m + tet_volume_v1(o); };
-    DfsSink<TetStack<kTetBlock>, decltype(leaf)> sink{stk, leaf, sp, L == 3, tol, 0, 0};
-    const int k = clip_tet_plane(t, nx, ny, nz, c, sink);
-    kept += sink.kept;
-    if (L < 3 && k > 0) {
-      if (k > 1) levels |= (unsigned)(L + 1) << (2 * sp);
-      if (k > 2) levels |= (unsigned)(L + 1) << (2 * (sp + 1));
-      sp += k - 1;
-      ++L;
-      continue;
-    }
-    if (sp > 0) {
-      --sp;
-      stk.load(sp, t);
-      L = (int)((levels >> (2 * sp)) & 3u);
-      levels &= ~(3u << (2 * sp));
-      continue;
-    }
-    pair_measure[p] = m;
-    pair_nout[p] = kept;
-    p = -1;
   }
 }
 
 // ----------------------------------------------------------------------
-// K6b: tet clipper with per-warp task queues
+// K6: depth-first tet clipper over point indices
 // ----------------------------------------------------------------------
-// Each warp works on up to kWqSlots pairs at a time and keeps three stacks of
-// tasks in global scratch (L2-resident): tets to classify against their next
-// plane (clip), tets to split (split), and final tets whose volume decides
-// whether they are kept (leaf).  Every phase takes up to 32 tasks of ONE kind,
-// one per lane, so the FP64-heavy split and leaf work runs with full warps
-// instead of the few lanes that happen to need it in a per-pair walk.
-//
-// Tasks are processed out of the reference's order, so each final tet
-// carries its rank in the reference's output order (its base-3 path of child
-// indices over the four planes, 0..80).  Kept volumes land in a per-pair
-// buffer indexed by rank and the pair's measure is summed in rank order when
-// its last task completes: the per-pair sums are the reference's, bit for
-// bit.
-namespace {
-constexpr int kWqWarps = 4;    // warps per block
-#ifndef LSM_WQ_BPS
-#define LSM_WQ_BPS 2
-#endif
-constexpr int kWqBlocksPerSm = LSM_WQ_BPS;
-constexpr int kWqSlots = 32;   // pairs in flight per warp
-constexpr int kWqCapC = 1024;  // clip stack entries
-constexpr int kWqCapS = 64;    // split stack entries (<= 31 + 32)
-constexpr int kWqCapL = 128;   // leaf stack entries (<= 31 + 96)
-constexpr size_t kWqClipD = 12 * (size_t)kWqCapC;
-constexpr size_t kWqSplitD = 16 * (size_t)kWqCapS;
-constexpr size_t kWqLeafD = 12 * (size_t)kWqCapL;
-constexpr size_t kWqVolD = (size_t)kWqSlots * 81;
-constexpr size_t kWqDoubles = kWqClipD + kWqSplitD + kWqLeafD + kWqVolD;
-constexpr size_t kWqInts = kWqCapC + 2 * kWqCapS + kWqCapL;
-constexpr size_t kWqWarpBytes = ((kWqDoubles * 8 + kWqInts * 4) + 255) / 256 * 256;
-}  // namespace
-
-size_t wq_scratch_bytes() { return (size_t)sm_count() * kWqBlocksPerSm * kWqWarps * kWqWarpBytes; }
-
-__device__ __forceinline__ void wq_store_tet(double* base, int cap, int i, const Tet& t) {
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    base[(3 * k + 0) * cap + i] = t.x[k];
-    base[(3 * k + 1) * cap + i] = t.y[k];
-    base[(3 * k + 2) * cap + i] = t.z[k];
-  }
-}
-
-__device__ __forceinline__ void wq_load_tet(const double* base, int cap, int i, Tet& t) {
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    t.x[k] = base[(3 * k + 0) * cap + i];
-    t.y[k] = base[(3 * k + 1) * cap + i];
-    t.z[k] = base[(3 * k + 2) * cap + i];
-  }
-}
-
-// warp prefix of per-lane counts 0..3
-__device__ __forceinline__ int wq_prefix(int cnt, unsigned lt, int& total) {
-  const unsigned b0 = __ballot_sync(0xffffffffu, cnt & 1), b1 = __ballot_sync(0xffffffffu, cnt & 2);
-  total = __popc(b0) + 2 * __popc(b1);
-  return __popc(b0 & lt) + 2 * __popc(b1 & lt);
-}
-
-__global__ void __launch_bounds__(kWqWarps * 32, kWqBlocksPerSm) k_clip_tets_wq(
-    const int32_t* __restrict__ list, const unsigned long long* __restrict__ nlist,
-    const int32_t* __restrict__ pa, const int32_t* __restrict__ pb, const double* __restrict__ coords_a,
-    const double* __restrict__ tol_a, const double* __restrict__ setup_b, double* pair_measure,
-    int32_t* pair_nout, unsigned long long* work, unsigned char* scratch, int* err) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const unsigned lt = (1u << lane) - 1u;
-  const size_t gw = (size_t)blockIdx.x * kWqWarps + wid;
-  double* clipD = reinterpret_cast<double*>(scratch + gw * kWqWarpBytes);
-  double* splitD = clipD + kWqClipD;
-  double* leafD = splitD + kWqSplitD;
-  double* vol = leafD + kWqLeafD;
-  int* clipM = reinterpret_cast<int*>(vol + kWqVolD);
-  int* splitM = clipM + kWqCapC;
-  int* splitC = splitM + kWqCapS;
-  int* leafM = splitC + kWqCapS;
-
-  __shared__ int s_pair[kWqWarps][kWqSlots], s_b[kWqWarps][kWqSlots], s_cnt[kWqWarps][kWqSlots];
-  __shared__ unsigned s_mask[kWqWarps][kWqSlots][3];
-  __shared__ double s_tol[kWqWarps][kWqSlots];
-  __shared__ int s_free[kWqWarps][kWqSlots];
-  __shared__ int s_nfree[kWqWarps];
-  s_free[wid][lane] = lane;
-  if (lane == 0) s_nfree[wid] = kWqSlots;
-  __syncwarp();
-
-  const int64_t npairs = (int64_t)*nlist;
-  int topC = 0, topS = 0, topL = 0;  // warp-uniform
-  bool exhausted = false;
-
-  // finish a pair: sum its kept volumes in rank order, free its slot
-  auto finalize = [&](int slot) {
-    const int p = s_pair[wid][slot];
-    double m = 0.0;
-    int nout = 0;
-    for (int w = 0; w < 3; ++w) {
-      unsigned bits = s_mask[wid][slot][w];
-      while (bits) {
-        const int r = __ffs(bits) - 1;
-        bits &= bits - 1u;
-        m = m + vol[slot * 81 + w * 32 + r];
-        ++nout;
-      }
-    }
-    pair_measure[p] = m;
-    pair_nout[p] = nout;
-    const int f = atomicAdd(&s_nfree[wid], 1);
-    s_free[wid][f] = slot;
-  };
-
-  int maxC = 0;
-  // every phase retires or creates at least one task; a pair creates at most
-  // 40 clip, 40 split and 81 leaf tasks
-  const long long guard_max = (long long)(npairs + kWqSlots) * 256 + 1024;
-  for (long long guard = 0;; ++guard) {
-    int phase;  // 0 leaf, 1 split, 2 clip, -1 done
-    if (topL >= 32) {
-      phase = 0;
-    } else if (topS >= 32) {
-      phase = 1;
-    } else {
-      const int nfree = s_nfree[wid];
-      if (topC < 32 && !exhausted && nfree > 0) {
-        // ---- admit new pairs
-        const int want = min(nfree, 32 - topC);
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(&work[1], (unsigned long long)want);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        const bool take = lane < want && (int64_t)(base + lane) < npairs;
-        const unsigned tk = __ballot_sync(0xffffffffu, take);
-        const int ntake = __popc(tk);
-        if ((int64_t)(base + want) >= npairs) exhausted = true;
-        if (take) {
-          const int p = list[base + lane];
-          const int slot = s_free[wid][nfree - 1 - lane];
-          const int a = pa[p], b = pb[p];
-          Tet t;
-          load_tet(coords_a + (int64_t)a * 12, t);
-          s_pair[wid][slot] = p;
-          s_b[wid][slot] = b;
-          s_tol[wid][slot] = fmin(tol_a[a], setup_b[(int64_t)b * kSetup3 + 16]);
-          s_cnt[wid][slot] = 1;
-          s_mask[wid][slot][0] = s_mask[wid][slot][1] = s_mask[wid][slot][2] = 0u;
-          wq_store_tet(clipD, kWqCapC, topC + lane, t);
-          clipM[topC + lane] = slot;  // level 0, rank 0
-        }
-        __syncwarp();
-        if (lane == 0) s_nfree[wid] = nfree - ntake;
-        topC += ntake;
-        __syncwarp();
-      }
-      if (topC > 0)
-        phase = 2;
-      else if (topS > 0)
-        phase = 1;
-      else if (topL > 0)
-        phase = 0;
-      else
-        phase = -1;
-    }
-    if (phase < 0) {
-      // all stacks empty: either every pair is done, or slots are held by
-      // pairs without tasks (cannot happen; reported, never waited on)
-      if ((!exhausted || s_nfree[wid] != kWqSlots) && lane == 0) atomicExch(err, 2);
-      break;
-    }
-    if (guard > guard_max) {
-      if (lane == 0) atomicExch(err, 3);
-      break;
-    }
-
-    if (phase == 2) {
-      // ---- clip: classify tets against their next plane
-      const int n = min(32, topC);
-      const bool act = lane < n;
-      Tet t;
-      TetClass cls;
-      int meta = 0, slot = 0, L = 0, rank = 0, type = -1;  // 0 drop, 1 keep, 2 split
-      if (act) {
-        const int idx = topC - n + lane;
-        wq_load_tet(clipD, kWqCapC, idx, t);
-        meta = clipM[idx];
-        slot = meta & 31;
-        L = (meta >> 5) & 3;
-        rank = meta >> 7;
-        const double* pl = setup_b + (int64_t)s_b[wid][slot] * kSetup3;
-        double nx, ny, nz, c;
-        load_plane(pl, L, nx, ny, nz, c);
-        classify_tet(t, nx, ny, nz, c, cls);
-        type = cls.nn == 0 ? 0 : (cls.np == 0 ? 1 : 2);
-      }
-      __syncwarp();
-      topC -= n;
-      const int pc = (type == 1 && L < 3) ? 1 : 0;
-      const int pl_ = (type == 1 && L == 3) ? 1 : 0;
-      const int ps = type == 2 ? 1 : 0;
-      int tc, tl, ts;
-      const int oc = wq_prefix(pc, lt, tc), ol = wq_prefix(pl_, lt, tl), os = wq_prefix(ps, lt, ts);
-      if (topC + tc > kWqCapC || topL + tl > kWqCapL || topS + ts > kWqCapS) {
-        if (lane == 0) atomicExch(err, 1);
-        break;
-      }
-      if (pc) {
-        wq_store_tet(clipD, kWqCapC, topC + oc, t);
-        clipM[topC + oc] = slot | ((L + 1) << 5) | ((rank * 3) << 7);
-      }
-      if (pl_) {
-        wq_store_tet(leafD, kWqCapL, topL + ol, t);
-        leafM[topL + ol] = slot | ((rank * 3) << 5);
-      }
-      if (ps) {
-        const int i = topS + os;
-        wq_store_tet(splitD, kWqCapS, i, t);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) splitD[(12 + q) * kWqCapS + i] = cls.d[q];
-        splitM[i] = meta;
-        splitC[i] = (int)(cls.negl | cls.posl << 6 | cls.zerl << 12 | (unsigned)cls.nn << 18 | (unsigned)cls.np << 21);
-      }
-      topC += tc;
-      topL += tl;
-      topS += ts;
-      __syncwarp();
-      if (type == 0 && atomicSub(&s_cnt[wid][slot], 1) == 1) finalize(slot);
-      __syncwarp();
-    } else if (phase == 1) {
-      // ---- split: interpolate and assemble children
-      const int n = min(32, topS);
-      const bool act = lane < n;
-      Tet t, c1, c2;
-      TetClass cls;
-      int meta = 0, k = 0;
-      if (act) {
-        const int idx = topS - n + lane;
-        wq_load_tet(splitD, kWqCapS, idx, t);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) cls.d[q] = splitD[(12 + q) * kWqCapS + idx];
-        meta = splitM[idx];
-        const unsigned cw = (unsigned)splitC[idx];
-        cls.negl = cw & 63u;
-        cls.posl = (cw >> 6) & 63u;
-        cls.zerl = (cw >> 12) & 63u;
-        cls.nn = (int)((cw >> 18) & 7u);
-        cls.np = (int)((cw >> 21) & 7u);
-      }
-      __syncwarp();
-      topS -= n;
-      if (act) k = split_tet(t, cls, c1, c2);
-      const int slot = meta & 31, L = (meta >> 5) & 3, rank = meta >> 7;
-      const int kc = (act && L < 3) ? k : 0;
-      const int kl = (act && L == 3) ? k : 0;
-      int tc, tl;
-      const int oc = wq_prefix(kc, lt, tc), ol = wq_prefix(kl, lt, tl);
-      if (topC + tc > kWqCapC || topL + tl > kWqCapL) {
-        if (lane == 0) atomicExch(err, 1);
-        break;
-      }
-      if (kc) {
-        const int m0 = slot | ((L + 1) << 5);
-        wq_store_tet(clipD, kWqCapC, topC + oc, t);
-        clipM[topC + oc] = m0 | ((rank * 3) << 7);
-        if (kc > 1) {
-          wq_store_tet(clipD, kWqCapC, topC + oc + 1, c1);
-          clipM[topC + oc + 1] = m0 | ((rank * 3 + 1) << 7);
-        }
-        if (kc > 2) {
-          wq_store_tet(clipD, kWqCapC, topC + oc + 2, c2);
-          clipM[topC + oc + 2] = m0 | ((rank * 3 + 2) << 7);
-        }
-      }
-      if (kl) {
-        wq_store_tet(leafD, kWqCapL, topL + ol, t);
-        leafM[topL + ol] = slot | ((rank * 3) << 5);
-        if (kl > 1) {
-          wq_store_tet(leafD, kWqCapL, topL + ol + 1, c1);
-          leafM[topL + ol + 1] = slot | ((rank * 3 + 1) << 5);
-        }
-        if (kl > 2) {
-          wq_store_tet(leafD, kWqCapL, topL + ol + 2, c2);
-          leafM[topL + ol + 2] = slot | ((rank * 3 + 2) << 5);
-        }
-      }
-      topC += tc;
-      topL += tl;
-      if (act && k != 1) atomicAdd(&s_cnt[wid][slot], k - 1);
-      __syncwarp();
-    } else {
-      // ---- leaf: tolerance test and volume of final tets
-      const int n = min(32, topL);
-      const bool act = lane < n;
-      Tet t;
-      int slot = 0, rank = 0;
-      if (act) {
-        const int idx = topL - n + lane;
-        wq_load_tet(leafD, kWqCapL, idx, t);
-        const int meta = leafM[idx];
-        slot = meta & 31;
-        rank = meta >> 5;
-      }
-      __syncwarp();
-      topL -= n;
-      if (act && tet_volume_v4(t) >= s_tol[wid][slot]) {
-        vol[slot * 81 + rank] = tet_volume_v1(t);
-        atomicOr(&s_mask[wid][slot][rank >> 5], 1u << (rank & 31));
-      }
-      __syncwarp();
-      if (act && atomicSub(&s_cnt[wid][slot], 1) == 1) finalize(slot);
-      __syncwarp();
-    }
-    maxC = max(maxC, topC);
-  }
-  if (lane == 0) atomicMax(&work[2], (unsigned long long)maxC);
-}
-
-// ----------------------------------------------------------------------
-// K6d: depth-first tet clipper over point indices
-// ----------------------------------------------------------------------
-// As K6 (one pair per lane, depth-first, lane refill), but a tet is four
-// 5-bit indices into the lane's point pool in shared memory instead of twelve
-// doubles in registers.  Pool slots 0-3 hold A's vertices; the split at
+// One pair per lane, depth-first, lanes refilled from the survivor list; a
+// tet is four 5-bit indices into the lane's point pool in shared memory
+// instead of twelve doubles in registers.  Pool slots 0-3 hold A's vertices; the split at
 // plane L writes its (at most four) new points to slots 4+4L .. 7+4L.  In
 // depth-first order that is safe: a tet at plane L references only points of
 // planes < L, and when a sibling is taken from the stack every point written
@@ -2303,7 +1827,6 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
 
 size_t ix_smem_bytes() { return (size_t)kIxBlock * 3 * kIxPoints * sizeof(double); }
 
-int wq_grid_blocks() { return sm_count() * kWqBlocksPerSm; }
 
 
 
@@ -2325,10 +1848,7 @@ __global__ void __launch_bounds__(256) k_reduce_pairs(int64_t npairs, const doub
   block_reduce_partial<256>(sum, err, ni, no, &partials[blockIdx.x]);
 }
 
-int clip_grid_blocks(int dim) {
-  if (dim == 2) return sm_count() * tri_blocks_per_sm();
-  return sm_count() * tet_blocks_per_sm();
-}
+int clip_grid_blocks(int dim) { return sm_count() * (dim == 2 ? tri_blocks_per_sm() : kIxBlocksPerSm); }
 
 cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                         const double* coords_a, const double* tol_a, const double* setup_b,
@@ -2344,55 +1864,25 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                                         pair_nout, overflow_list, overflow_count, order);
   } else {
     // work[0]: survivor count, work[1]: clipper pair counter
-    const size_t smem = sizeof(double) * (kTetSmemSlots * 12 + 16) * kTetBlock;
     // the timed span covers the early-out pass and the clipper: together
     // they settle every candidate
     if (ev_begin) cudaEventRecord(ev_begin, s);
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
     count_launch();
-    if (tet_clipper_variant() == 0)
-      k_prefilter_tets<true><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
-                                                                      tol_a, setup_b, pair_measure, pair_nout,
-                                                                      overflow_list, work, faces_a, screen_b);
-    else
-      k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
-                                                                       tol_a, setup_b, pair_measure, pair_nout,
-                                                                       overflow_list, work, faces_a, screen_b);
+    k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, tol_a,
+                                                              setup_b, pair_measure, pair_nout, overflow_list, work,
+                                                              faces_a, screen_b);
     const int4* list = reinterpret_cast<const int4*>(overflow_list);
-    if (tet_clipper_variant() == 0 && bin) {
+    if (bin) {
       // the survivors reordered into class-uniform runs within windows
       cudaError_t e = launch_sched_bin(*bin, list, work, bin->out, coords_a, s);
       if (e != cudaSuccess) return e;
       list = bin->out;
     }
-    if (tet_clipper_variant() == 0)
-      k_clip_tets_ix<<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
-          list, work, coords_a, tol_a, setup_b, pair_measure, pair_nout, work + 1);
-    else if (tet_blocks_per_sm() == 3)
-      k_clip_tets<3><<<sm_count() * 3, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,
-                                                              setup_b, pair_measure, pair_nout, work + 1);
-    else
-      k_clip_tets<4><<<sm_count() * 4, kTetBlock, smem, s>>>(overflow_list, work, pair_a, pair_b, coords_a, tol_a,
-                                                              setup_b, pair_measure, pair_nout, work + 1);
+    k_clip_tets_ix<<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
+        list, work, coords_a, tol_a, setup_b, pair_measure, pair_nout, work + 1);
   }
   if (ev_end) cudaEventRecord(ev_end, s);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
-                                const double* coords_a, const double* tol_a, const double* setup_b,
-                                double* pair_measure, int32_t* pair_nout, int32_t* survivors,
-                                unsigned long long* work, unsigned char* scratch, int* err, cudaStream_t s,
-                                const int32_t* order, const double* faces_a, const double* screen_b) {
-  // work[0]: survivors, work[1]: admitted pairs, work[2]: deepest clip stack
-  cudaMemsetAsync(work, 0, 3 * sizeof(unsigned long long), s);
-  cudaMemsetAsync(err, 0, sizeof(int), s);
-  count_launch(2);
-  k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a,
-                                                                   tol_a, setup_b, pair_measure, pair_nout, survivors,
-                                                                   work, faces_a, screen_b);
-  k_clip_tets_wq<<<wq_grid_blocks(), kWqWarps * 32, 0, s>>>(survivors, work, pair_a, pair_b, coords_a, tol_a,
-                                                            setup_b, pair_measure, pair_nout, work, scratch, err);
   return cudaGetLastError();
 }
 
@@ -2406,12 +1896,7 @@ cudaError_t launch_reduce_pairs(int64_t npairs, const double* pair_measure, cons
 }
 
 cudaError_t init_device_attributes() {
-  const int smem = (int)(sizeof(double) * (kTetSmemSlots * 12 + 16) * kTetBlock);
-  cudaError_t e = cudaFuncSetAttribute(k_clip_tets<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_clip_tets<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_clip_tets_ix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
+  cudaError_t e = cudaFuncSetAttribute(k_clip_tets_ix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
   if (e != cudaSuccess) return e;
   return init_sched_attributes(kSchedMaxWindow);
 }
@@ -2782,6 +2267,47 @@ __global__ void k_mesh_combine(int nm, const int64_t* __restrict__ elem_off_a, c
 }
 
 int64_t mesh_totals_pieces(int nm) { return (int64_t)nm * kMeshSplit; }
+
+// Per-pair CSR of a batch group in the get_output layout of the C API
+// (C_bindings.F90:377-391): mesh pair k owns rows eoa[k] .. eoa[k+1]-1 and
+// writes out[rowbase[k] + r] = offsets[eoa[k] + r] - offsets[eoa[k]] for
+// r = 0 .. nel_a(k) (the last entry is the pair's candidate count).
+__global__ void k_batch_indptr(int64_t na, int nm, const int32_t* __restrict__ pair_of_a,
+                               const int64_t* __restrict__ eoa, const int64_t* __restrict__ offsets,
+                               const int64_t* __restrict__ rowbase, int64_t* out) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < na + nm; e += (int64_t)gridDim.x * blockDim.x) {
+    if (e < na) {
+      const int k = pair_of_a[e];
+      out[rowbase[k] + (e - eoa[k])] = offsets[e] - offsets[eoa[k]];
+    } else {
+      const int k = (int)(e - na);
+      out[rowbase[k] + (eoa[k + 1] - eoa[k])] = offsets[eoa[k + 1]] - offsets[eoa[k]];
+    }
+  }
+}
+
+// Candidate B elements as numbers local to their mesh pair, int64.
+__global__ void k_batch_indices(int64_t n, const int32_t* __restrict__ pair_b, const int32_t* __restrict__ pair_of_b,
+                                const int64_t* __restrict__ eob, int64_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t b = pair_b[i];
+    out[i] = (int64_t)b - eob[pair_of_b[b]];
+  }
+}
+
+cudaError_t launch_batch_csr(int64_t na, int nm, const int32_t* pair_of_a, const int64_t* eoa, const int64_t* offsets,
+                             const int64_t* rowbase, int64_t* ind_ptr, int64_t ncand, const int32_t* pair_b,
+                             const int32_t* pair_of_b, const int64_t* eob, int64_t* indices, cudaStream_t s) {
+  if (ind_ptr && na + nm > 0) {
+    count_launch();
+    k_batch_indptr<<<grid_for(na + nm, 256, 8), 256, 0, s>>>(na, nm, pair_of_a, eoa, offsets, rowbase, ind_ptr);
+  }
+  if (indices && ncand > 0) {
+    count_launch();
+    k_batch_indices<<<grid_for(ncand, 256, 8), 256, 0, s>>>(ncand, pair_b, pair_of_b, eob, indices);
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t launch_mesh_totals(int nm, const int64_t* elem_off_a, const int64_t* offsets, const double* pm,
                                const int32_t* pn, Partial* pieces, Partial* out, int64_t* ncand, cudaStream_t s) {

@@ -41,13 +41,6 @@ void count_launch(int n = 1);
 int sm_count();
 int grid_for(int64_t n, int block, int per_sm);
 
-// Launch shape of the persistent tet clipper (3 or 4 blocks per SM).
-int tet_blocks_per_sm();
-void set_tet_blocks_per_sm(int v);
-// 3D clipper variant: 0 per-lane depth-first over point indices (default),
-// 1 per-warp task queues in L2, 2 per-lane depth-first over tets in registers.
-int tet_clipper_variant();
-void set_tet_clipper_variant(int v);
 // Grid of the 2D clipper (blocks per SM) and block size of the search.
 int tri_blocks_per_sm();
 void set_tri_blocks_per_sm(int v);
@@ -158,18 +151,6 @@ cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overf
                                   const double* coords_a, const double* tol_a,
                                   const double* setup_b, double* pair_measure, int32_t* pair_nout,
                                   cudaStream_t s);
-// Task-queue tet clipper (prefilter + k_clip_tets_wq).  scratch:
-// wq_scratch_bytes(); work: 3 counters; err != 0 after the launch means the
-// queues overflowed (results invalid: re-run with launch_clip).
-size_t wq_scratch_bytes();
-
-cudaError_t launch_clip_tets_wq(int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
-                                const double* coords_a, const double* tol_a, const double* setup_b,
-                                double* pair_measure, int32_t* pair_nout, int32_t* survivors,
-                                unsigned long long* work, unsigned char* scratch, int* err, cudaStream_t s,
-                                const int32_t* order = nullptr, const double* faces_a = nullptr,
-                                const double* screen_b = nullptr);
-
 // Per-block partials of the pair measures/counts in a fixed order
 // (reduce_pairs_blocks() == kReduceBlocks entries; the block count is fixed
 // because it sets the totals' summation order).
@@ -263,6 +244,12 @@ cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
                                  int32_t* pair_b, cudaStream_t s, int32_t* cache = nullptr, int cap = 0,
                                  int* over_rows = nullptr, Spill sp = Spill{});
+// Per-pair CSR of a batch group (get_output layout): ind_ptr rows of mesh
+// pair k at rowbase[k] (optional), candidate B elements local to their pair
+// as int64 (optional).
+cudaError_t launch_batch_csr(int64_t na, int nm, const int32_t* pair_of_a, const int64_t* eoa, const int64_t* offsets,
+                             const int64_t* rowbase, int64_t* ind_ptr, int64_t ncand, const int32_t* pair_b,
+                             const int32_t* pair_of_b, const int64_t* eob, int64_t* indices, cudaStream_t s);
 int64_t mesh_totals_pieces(int nm);  // Partial scratch entries for launch_mesh_totals
 cudaError_t launch_mesh_totals(int nm, const int64_t* elem_off_a, const int64_t* offsets, const double* pm,
                                const int32_t* pn, Partial* pieces, Partial* out, int64_t* ncand, cudaStream_t s);

@@ -419,7 +419,8 @@ __global__ void __launch_bounds__(256) k_sched_predict(int64_t n, const __nv_bfl
 //   dH1 = (dH2 W2) * [H1 > 0],  dW1 = dH1^T X,  db = column sums,
 // every product an mma.sync over 16-sample K blocks (BF16 operands, FP32
 // accumulation, summed over the warps in shared memory), then an Adam step
-// on the FP32 master weights (moments in `adam`, 2 * kSchedParams floats).
+// on the FP32 master weights (moments in `adam`, 2 * kSchedParams floats)
+// with the learning rate decayed from lr to 0 along a half cosine.
 // Padding entries (W1 columns 24..31, W3 rows 4..7, b3[4..7]) stay fixed.
 namespace {
 struct TrainWarp {
@@ -682,6 +683,7 @@ __global__ void __launch_bounds__(256, 1) k_sched_train(const __nv_bfloat16* __r
     b1t *= 0.9f;
     b2t *= 0.999f;
     const float c1 = 1.0f / (1.0f - b1t), c2 = 1.0f / (1.0f - b2t);
+    const float lr_t = 0.5f * lr * (1.0f + cospif((float)step / (float)steps));
     for (int i = threadIdx.x; i < kSchedParams; i += blockDim.x) {
       const float gi = G[i];
       G[i] = 0.0f;
@@ -691,7 +693,7 @@ __global__ void __launch_bounds__(256, 1) k_sched_train(const __nv_bfloat16* __r
       v = 0.999f * v + 0.001f * gi * gi;
       adam[i] = m;
       adam[kSchedParams + i] = v;
-      P[i] -= lr * (m * c1) / (sqrtf(v * c2) + 1e-8f);
+      P[i] -= lr_t * (m * c1) / (sqrtf(v * c2) + 1e-8f);
     }
     __syncthreads();
     if (threadIdx.x == 0) loss_sum = 0.0f;
@@ -739,7 +741,7 @@ cudaError_t launch_sched_true_class(int64_t n, const int32_t* n_out, int8_t* cls
 cudaError_t launch_sched_bin(const SchedBin& b, const int4* in, const unsigned long long* nlist, int4* out,
                              const double* coords_a, cudaStream_t s) {
   count_launch();
-  k_sched_bin<<<sm_count() * 2, 256, sched_bin_smem_bytes(b.window), s>>>(
+  k_sched_bin<<<sm_count() * 4, 256, sched_bin_smem_bytes(b.window), s>>>(
       in, nlist, out, coords_a, b.screen_b, b.weights, b.cls_of_pair, b.pred_of_pair, b.window);
   return cudaGetLastError();
 }

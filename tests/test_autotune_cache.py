@@ -19,7 +19,7 @@ def tuner(tmp_path, monkeypatch):
     import libsupermesh_b200 as lsm
 
     monkeypatch.setenv("LIBSUPERMESH_TUNING_CACHE", str(tmp_path / "tuning.json"))
-    names = ("query_block", "tet_clipper", "tri_blocks_per_sm")
+    names = ("query_block", "tri_blocks_per_sm")
     before = {n: lsm.get_option(n) for n in names}
     yield autotune, lsm
     for n, v in before.items():
@@ -28,7 +28,7 @@ def tuner(tmp_path, monkeypatch):
 
 def test_stored_choice_is_applied(tuner):
     autotune, lsm = tuner
-    setting = {"query_block": 64, "tet_clipper": 0}
+    setting = {"query_block": 64, "tri_blocks_per_sm": 8}
     db = {autotune._key(3, 1000, 2000): {"setting": setting, "ms": 1.0, "source": autotune._source_hash()}}
     autotune.cache_path().write_text(json.dumps(db))
     assert autotune.apply_cached(3, 1000, 2000) == setting

@@ -129,14 +129,14 @@ def test_config_tet3d_graded_full_properties(gpu_ctx):
     e1, e2, e3 = v[:, 1] - v[:, 0], v[:, 2] - v[:, 0], v[:, 3] - v[:, 0]
     own = np.abs(np.einsum("ij,ij->i", e1, np.cross(e2, e3))) / 6.0
     assert np.all(np.abs(em - own) <= 1e-12 * own)
-    # the per-pair results do not depend on the clipper variant
+    # the per-pair results do not depend on the work order (true-class bins)
     pm, pn = gpu_ctx.pair_results(st.n_candidates)
-    lsm.set_option("tet_clipper", 2)
+    lsm.set_option("tet_schedule", 2)
     try:
         st2 = gpu_ctx.clip_candidates()
         pm2, pn2 = gpu_ctx.pair_results(st.n_candidates)
     finally:
-        lsm.set_option("tet_clipper", 0)
+        lsm.set_option("tet_schedule", 0)
     assert np.array_equal(pm, pm2) and np.array_equal(pn, pn2) and st2.total_measure == st.total_measure
 
 
@@ -147,34 +147,6 @@ def test_config_tri2d_777x1024_rot7_p1_mass(gpu_ctx, oracle_mod):
     ip, ind = oracle_mod.tree_finder(dim, A, B)
     i_o, meas_o, _ = oracle_mod.p1_mass(dim, A, B, ip, ind, u, v)
     assert abs(integral - i_o) <= 1e-12 * abs(i_o)
-
-
-@pytest.mark.parametrize("variant", ["queue", "register"])
-def test_alternative_tet_clippers_match(oracle_mod, tmp_path, variant):
-    """The alternative tet clippers (task queues; tets held in registers)
-    give the same per-pair results, bit for bit."""
-    import subprocess
-    import sys
-
-    code = (
-        "import sys, numpy as np; sys.path.insert(0, %r)\n"
-        "import libsupermesh_b200 as L; from libsupermesh_b200 import meshes as M\n"
-        "dim, A, B = M.config_meshes('small3d_12x14')\n"
-        "c = L.Context(0); st, _ = c.supermesh(A, B); pm, pn = c.pair_results(st.n_candidates)\n"
-        "ip, ind = c.get_candidates(len(A[1]), st.n_candidates)\n"
-        "np.savez(%r, pm=pm, pn=pn, ip=ip, ind=ind, tot=st.total_measure)\n" % (str(ROOT), str(tmp_path / "q.npz")))
-    import os
-    env = dict(os.environ, LSM_TET_CLIPPER=variant)
-    subprocess.run([sys.executable, "-c", code], check=True, env=env, timeout=600)
-    q = np.load(tmp_path / "q.npz")
-    dim, A, B = M.config_meshes("small3d_12x14")
-    ip_o, ind_o = oracle_mod.tree_finder(dim, A, B)
-    pm_o, pn_o, _, st_o = oracle_mod.narrow(dim, A, B, ip_o, ind_o)
-    ro, bo, mo, no = pair_table(ip_o, ind_o, pm_o, pn_o)
-    rg, bg, mg, ng = pair_table(q["ip"], q["ind"], q["pm"], q["pn"])
-    assert np.array_equal(bo, bg) and np.array_equal(no, ng)
-    assert np.array_equal(mo, mg)  # sums in the reference's order: bit-identical
-    assert abs(float(q["tot"]) - st_o.total) <= REL_TOL
 
 
 def test_autotuner_keeps_results(gpu_ctx, tmp_path, monkeypatch):
@@ -189,7 +161,7 @@ def test_autotuner_keeps_results(gpu_ctx, tmp_path, monkeypatch):
         st, em = gpu_ctx.supermesh(A, B, elem_measure=True)
         assert st.as_dict() == ref.as_dict() and np.array_equal(em, em_ref)
         assert autotune.apply_cached(dim, len(A[1]), len(B[1])) == res["setting"]
-    for n, v in {"tet_clipper": 0, "tet_blocks_per_sm": 3, "tri_blocks_per_sm": 8, "query_block": 128}.items():
+    for n, v in {"tri_blocks_per_sm": 8, "query_block": 128}.items():
         lsm.set_option(n, v)
 
 
