@@ -433,6 +433,44 @@ def kernel_only(args, ctx, dim, A, B, tA, tB, step_device, timed, rank):
                           "ms_per_step": ms / args.steps}), flush=True)
 
 
+def drop_in_per_pair(ctx, dim, A, B, n_cand, n: int = 2000):
+    """Calls per second of the drop-in per-pair entry
+    (libsupermesh_intersect_tets_real / _tris_real: one copy in, one kernel
+    launch, one copy out and a host wait per call) against the oracle's
+    per-pair call (the reference algorithm on the host), on the first n
+    candidate pairs of the workload, both driven by the same ctypes loop with
+    preallocated arguments; host wall clock."""
+    import libsupermesh_b200 as lsm
+    import oracle
+
+    ip, ind = ctx.get_candidates(len(A[1]), n_cand)
+    n = min(n, n_cand)
+    rows = np.repeat(np.arange(len(ip) - 1), np.diff(ip))[:n]
+    ea = np.ascontiguousarray(A[0][A[1][rows]].reshape(n, -1))
+    eb = np.ascontiguousarray(B[0][B[1][ind[:n]]].reshape(n, -1))
+    cap = (lsm.TET_BUF_SIZE * 12) if dim == 3 else (lsm.TRI_BUF_SIZE * 6)
+    out = np.zeros(cap)
+    k = ctypes.c_int(0)
+    dp = ctypes.POINTER(ctypes.c_double)
+    args = [(ea[i].ctypes.data_as(dp), eb[i].ctypes.data_as(dp)) for i in range(n)]
+    po, pk = out.ctypes.data_as(dp), ctypes.byref(k)
+    g = getattr(lsm.load(), "libsupermesh_intersect_tets_real" if dim == 3 else "libsupermesh_intersect_tris_real")
+    o = getattr(oracle.lib(), "orc_intersect_tets" if dim == 3 else "orc_intersect_tris")
+
+    def rate(fn):
+        for a, b in args[:20]:
+            fn(a, b, po, pk)
+        t0 = time.perf_counter()
+        for a, b in args:
+            fn(a, b, po, pk)
+        return n / (time.perf_counter() - t0)
+
+    gpu, cpu = rate(g), rate(o)
+    return {"pairs": n, "gpu_calls_per_s": gpu, "oracle_calls_per_s": cpu, "gpu_vs_oracle": gpu / cpu,
+            "entry": "libsupermesh_intersect_tets_real" if dim == 3 else "libsupermesh_intersect_tris_real",
+            "timing": "host wall clock of a ctypes loop over the first candidate pairs (1 thread each)"}
+
+
 def broad_phase_bytes(dim, A, B, n_cand):
     """Algorithmic bytes of the candidate search: both meshes' positions and
     element lists read once, 8 B per candidate pair written, and the radix
@@ -621,6 +659,7 @@ def run_ours(args, world, rank, local):
                             "note": "search time includes the host read of the candidate count"},
         }
         line["cpu_baseline"] = cpu
+        line["drop_in_per_pair"] = drop_in_per_pair(ctx, dim, A, B, n_cand)
         if dim == 2:
             line["p1_mass"] = p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush)
         print(json.dumps(line), flush=True)
