@@ -90,6 +90,13 @@ int64_t libsupermesh_gpu_kernel_launches(void);
  *                        2 true classes: binned by the output counts of the previous narrow phase
  *                          over the same candidates (the best a predictor could do; a measurement)
  *   "sched_window"       survivors per binning window: 256 .. 8192, a multiple of 256 (default 1024)
+ *   "batch_graph"        0 (default) or 1: a device-resident libsupermesh_gpu_supermesh_batched
+ *                        call is captured into a CUDA graph after its first (eager) run; later
+ *                        calls with the same meshes (same arrays, sizes and options; coordinates
+ *                        may change in place) replay it with one graph launch and one host wait.
+ *                        Pair arrays are sized from the first run's counts plus 1/8; a batch whose
+ *                        candidates outgrow them, or a context that reallocated its buffers since
+ *                        the capture, runs eagerly and is captured again.  Results are identical.
  * Failure-injection hooks for tests (host side only; no GPU fault is made):
  *   "fail_alloc_after"   -1 (default) off; n >= 0: the next n device allocations of any
  *                        context succeed and the following one fails as cudaMalloc out of
@@ -142,6 +149,32 @@ int libsupermesh_gpu_supermesh(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
                                const lsm_gpu_mesh *b, int on_device,
                                double *elem_measure_a, lsm_gpu_stats *stats,
                                void *stream);
+
+/* Whole supermesh of one mesh pair with everything a drop-in caller reads:
+ * the work of set_input / get_output (C_bindings.F90:346-391) and of one
+ * intersect_*_real + measure call per candidate, in one call.
+ *   elem_measure    [nelements_a] (optional): supermesh measure inside each A element
+ *   ind_ptr         [nelements_a + 1] (optional): CSR row pointers (0-based, start at 0)
+ *   indices         [cand_capacity] (optional): 0-based B element of each candidate
+ *   pair_measure    [cand_capacity] (optional): measure of each candidate pair
+ *   pair_n_out      [cand_capacity] (optional): its number of output simplices
+ *   n_candidates    set by the call
+ * Arrays follow on_device (host arrays should be pinned: the CSR's copy runs
+ * on the context's second stream while the candidates are clipped).  If the
+ * candidates do not fit cand_capacity the call fills elem_measure, ind_ptr,
+ * n_candidates and stats and returns LSM_ERROR_CAPACITY. */
+typedef struct {
+  double *elem_measure;
+  int64_t *ind_ptr;
+  int64_t *indices;
+  double *pair_measure;
+  int32_t *pair_n_out;
+  int64_t cand_capacity;
+  int64_t n_candidates;
+} lsm_gpu_pair_out;
+int libsupermesh_gpu_supermesh_out(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
+                                   const lsm_gpu_mesh *b, int on_device, lsm_gpu_pair_out *out,
+                                   lsm_gpu_stats *stats, void *stream);
 
 /* Narrow phase alone: intersect and measure every candidate of the last
  * libsupermesh_gpu_find_candidates / libsupermesh_gpu_supermesh call on
@@ -289,12 +322,17 @@ int libsupermesh_gpu_supermesh_batched(lsm_gpu_context *ctx, int npairs,
  *   indices         [cand_capacity] (optional): 0-based B element of the pair
  *   pair_measure    [cand_capacity] (optional): measure of each candidate
  *   pair_n_out      [cand_capacity] (optional): its number of output simplices
- * ind_ptr, indices, pair_measure and pair_n_out follow on_device.  Each
- * pair's candidates are contiguous and in its CSR order; 2D pairs come
+ *   p1_blocks       [p1_capacity] doubles (optional): for every candidate its
+ *                   P1-P1 mixed mass block (loc x loc, row-major, loc = dim + 1;
+ *                   the integrand of test_parallel_p1_inner_product_{2d,3d}),
+ *                   pair i's blocks from p1_offset[i] (host, [npairs]) on
+ * ind_ptr, indices, pair_measure, pair_n_out and p1_blocks follow on_device.
+ * Each pair's candidates are contiguous and in its CSR order; 2D pairs come
  * before 3D pairs in the arrays.  If they need more than cand_capacity
- * entries the call still fills totals, counts and ind_ptr, sets cand_offset
- * of the pairs that did not fit to -1 and returns LSM_ERROR_CAPACITY: retry
- * with capacity >= the sum of n_candidates. */
+ * entries (or p1_capacity doubles) the call still fills totals, counts and
+ * ind_ptr, sets cand_offset / p1_offset of the pairs that did not fit to -1
+ * and returns LSM_ERROR_CAPACITY: retry with capacity >= the sum of
+ * n_candidates (p1: the sum of n_candidates(i) * (dim(i) + 1)^2). */
 typedef struct {
   double *totals;
   int64_t *n_candidates;
@@ -306,6 +344,9 @@ typedef struct {
   int64_t *indices;
   double *pair_measure;
   int32_t *pair_n_out;
+  int64_t *p1_offset;
+  int64_t p1_capacity;
+  double *p1_blocks;
 } lsm_gpu_batch_out;
 int libsupermesh_gpu_supermesh_batched_ex(lsm_gpu_context *ctx, int npairs,
                                           const lsm_gpu_mesh *a, const lsm_gpu_mesh *b,

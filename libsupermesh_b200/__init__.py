@@ -75,6 +75,21 @@ class BatchOut(ctypes.Structure):
         ("indices", ctypes.c_void_p),
         ("pair_measure", ctypes.c_void_p),
         ("pair_n_out", ctypes.c_void_p),
+        ("p1_offset", ctypes.c_void_p),
+        ("p1_capacity", ctypes.c_int64),
+        ("p1_blocks", ctypes.c_void_p),
+    ]
+
+
+class PairOut(ctypes.Structure):
+    _fields_ = [
+        ("elem_measure", ctypes.c_void_p),
+        ("ind_ptr", ctypes.c_void_p),
+        ("indices", ctypes.c_void_p),
+        ("pair_measure", ctypes.c_void_p),
+        ("pair_n_out", ctypes.c_void_p),
+        ("cand_capacity", ctypes.c_int64),
+        ("n_candidates", ctypes.c_int64),
     ]
 
 
@@ -129,6 +144,9 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_supermesh.argtypes = [vp, mp, mp, ctypes.c_int, vp, ctypes.POINTER(Stats), vp]
     L.libsupermesh_gpu_get_pair_results.argtypes = [vp, vp, vp, ctypes.c_int, vp]
     L.libsupermesh_gpu_clip_candidates.argtypes = [vp, ctypes.POINTER(Stats), vp]
+    L.libsupermesh_gpu_supermesh_out.argtypes = [vp, mp, mp, ctypes.c_int, ctypes.POINTER(PairOut),
+                                                 ctypes.POINTER(Stats), vp]
+    L.libsupermesh_gpu_supermesh_out.restype = ctypes.c_int
     L.libsupermesh_gpu_clip_candidates_ordered.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(Stats), vp]
     L.libsupermesh_gpu_clip_candidates_ordered.restype = ctypes.c_int
     L.libsupermesh_gpu_intersect_pairs.argtypes = [vp, ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp, vp,
@@ -261,6 +279,21 @@ class Context:
                                                         int(on_device), _ptr(em), ctypes.byref(st), stream))
         return st, em
 
+    def supermesh_out(self, mesh_a, mesh_b, out: dict, on_device: bool = False, stream: int | None = None):
+        """Whole supermesh plus the per-candidate outputs in one call
+        (libsupermesh_gpu_supermesh_out).  out: dict with any of
+        elem_measure, ind_ptr, indices, pair_measure, pair_n_out (arrays in
+        the memory space of on_device; host arrays should be pinned) and
+        capacity.  Returns (Stats, n_candidates)."""
+        ma, mb = _mesh(*mesh_a, on_device), _mesh(*mesh_b, on_device)
+        o = PairOut(_ptr(out.get("elem_measure")), _ptr(out.get("ind_ptr")), _ptr(out.get("indices")),
+                    _ptr(out.get("pair_measure")), _ptr(out.get("pair_n_out")), int(out.get("capacity", 0)), 0)
+        st = Stats()
+        self._check(self.lib.libsupermesh_gpu_supermesh_out(self._h, ctypes.byref(ma), ctypes.byref(mb),
+                                                            int(on_device), ctypes.byref(o), ctypes.byref(st),
+                                                            stream))
+        return st, o.n_candidates
+
     def clip_candidates(self, stream: int | None = None) -> Stats:
         """Re-run the narrow phase over the last candidate set."""
         st = Stats()
@@ -381,14 +414,15 @@ class Context:
         return integral.value, area.value, (pv[:n] if pv is not None else None)
 
     def supermesh_batched_pairs(self, pairs, capacity: int | None = None, on_device: bool = False, out=None,
-                                stream: int | None = None):
+                                stream: int | None = None, p1_blocks: bool = False):
         """Batched supermesh with per-pair outputs (host meshes and arrays
         unless on_device).  Returns a dict with totals, n_candidates,
         n_intersecting, cand_offset, total_candidates, and the arrays ind_ptr
         (pair i's rows at row_offset[i]), indices, pair_measure, pair_n_out.
         With capacity None the call is made twice if needed: the first
         attempt's counts size the retry (LSM_ERROR_CAPACITY).  `out` (dict
-        of preallocated arrays, optional) is used as is."""
+        of preallocated arrays, optional) is used as is.  p1_blocks: also
+        every candidate's P1-P1 mass block (p1_blocks from p1_offset[i])."""
         n = len(pairs)
         A = (Mesh * max(n, 1))()
         B = (Mesh * max(n, 1))()
@@ -400,6 +434,8 @@ class Context:
         rows = [int(ma[1].shape[0]) + 1 for ma, _ in pairs]
         row_offset = np.concatenate([[0], np.cumsum(rows)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
         cap = capacity if capacity is not None else (out["capacity"] if out else 0)
+        dims = [int(ma[0].shape[1]) for ma, _ in pairs]
+        p1cap = 16 * cap if p1_blocks else 0
         while True:
             if out is None:
                 r = {"totals": np.zeros(max(n, 1)), "n_candidates": np.zeros(max(n, 1), dtype=np.int64),
@@ -414,20 +450,26 @@ class Context:
                     r["indices"] = torch.zeros(max(cap, 1), dtype=torch.int64, device=dev)
                     r["pair_measure"] = torch.zeros(max(cap, 1), dtype=torch.float64, device=dev)
                     r["pair_n_out"] = torch.zeros(max(cap, 1), dtype=torch.int32, device=dev)
+                    r["p1_blocks"] = torch.zeros(max(p1cap, 1), dtype=torch.float64, device=dev) if p1_blocks else None
                 else:
                     r["ind_ptr"] = np.zeros(max(sum(rows), 1), dtype=np.int64)
                     r["indices"] = np.zeros(max(cap, 1), dtype=np.int64)
                     r["pair_measure"] = np.zeros(max(cap, 1))
                     r["pair_n_out"] = np.zeros(max(cap, 1), dtype=np.int32)
+                    r["p1_blocks"] = np.zeros(max(p1cap, 1)) if p1_blocks else None
+                r["p1_offset"] = np.zeros(max(n, 1), dtype=np.int64)
             else:
                 r = out
             o = BatchOut(_ptr(r["totals"]), _ptr(r["n_candidates"]), _ptr(r["n_intersecting"]),
                          _ptr(r["cand_offset"]), _ptr(r["total_candidates"]), cap, _ptr(r["ind_ptr"]),
-                         _ptr(r["indices"]), _ptr(r["pair_measure"]), _ptr(r["pair_n_out"]))
+                         _ptr(r["indices"]), _ptr(r["pair_measure"]), _ptr(r["pair_n_out"]),
+                         _ptr(r.get("p1_offset")), p1cap, _ptr(r.get("p1_blocks")))
             st = self.lib.libsupermesh_gpu_supermesh_batched_ex(self._h, n, A, B, int(on_device), ctypes.byref(o),
                                                                 stream)
             if st == 3 and capacity is None and out is None:  # LSM_ERROR_CAPACITY: size the retry
-                cap = int(r["n_candidates"][:n].sum())
+                nc = r["n_candidates"][:n]
+                cap = int(nc.sum())
+                p1cap = int(sum(int(k) * (d + 1) ** 2 for k, d in zip(nc, dims))) if p1_blocks else 0
                 continue
             self._check(st)
             r["row_offset"] = row_offset

@@ -48,6 +48,9 @@ int64_t g_fail_alloc_after = -1;
 // best any predictor can do; a measurement, not a production mode).
 int g_tet_schedule = 0;
 int g_sched_window = 1024;
+// Device-resident batched calls replay a CUDA graph of the whole batch when
+// the same meshes come again (1), or always run eagerly (0, default).
+int g_batch_graph = 0;
 
 // ------------------------------------------------------------------ buffers
 struct DevBuf {
@@ -87,6 +90,9 @@ struct Ctx {
   size_t host_stage_cap = 0;
   // pinned host scalars
   void* host_scalars = nullptr;
+  // pinned staging of the single-pair entries (inputs and the whole output
+  // buffer travel through it, one host wait per call)
+  void* pair_io = nullptr;
   // events around the clip kernel of the last narrow phase (option time_kernels)
   cudaEvent_t clip_ev[2] = {nullptr, nullptr};
   // side stream for mesh A's upload and prep (overlaps B's tree build) and
@@ -95,6 +101,23 @@ struct Ctx {
   cudaEvent_t side_ev[2] = {nullptr, nullptr};
   bool clip_timed = false;
   bool surv_valid = false;  // surv holds the clipper's pair count of the last 3D narrow phase
+  // bumped whenever a device buffer is (re)allocated: a captured graph holds
+  // buffer addresses and is only replayed while this is unchanged
+  uint64_t gen = 0;
+  // graph of a device-resident batched call (option batch_graph)
+  struct BatchGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> sig;
+    uint64_t gen = 0;
+    unsigned long long launches = 0;
+    void* host = nullptr;  // pinned: both groups' tables and result areas
+    size_t host_cap = 0;
+    std::vector<int> idx[2];
+    int64_t cap[2] = {0, 0};
+    size_t res_off[2] = {0, 0};
+    int last_dim = 0, last_loc = 0;
+    int64_t last_na = 0, last_nb = 0;
+  } bg;
 
   // state of the last candidate search
   int dim = 0;
@@ -180,6 +203,7 @@ T* ensure(Ctx* c, DevBuf& b, int64_t count) {
     }
     b.cap = want;
     c->bytes += (int64_t)want;
+    ++c->gen;
   }
   return static_cast<T*>(b.p);
 }
@@ -261,7 +285,13 @@ void fini_ctx(Ctx* c) {
     cudaStreamDestroy(c->side);
     c->side = nullptr;
   }
+  if (c->bg.exec) cudaGraphExecDestroy(c->bg.exec);
+  c->bg.exec = nullptr;
+  if (c->bg.host) cudaFreeHost(c->bg.host);
+  c->bg.host = nullptr;
   if (c->host_scalars) cudaFreeHost(c->host_scalars);
+  if (c->pair_io) cudaFreeHost(c->pair_io);
+  c->pair_io = nullptr;
   if (c->host_stage) cudaFreeHost(c->host_stage);
   if (c->stream) cudaStreamDestroy(c->stream);
   c->host_stage = nullptr;
@@ -536,7 +566,9 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
 
 // Narrow phase over the current candidates.  Leaves the merged totals in
 // c->totals (one lsm::Partial).
-void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
+// n_dev (optional): the candidate count on the device; c->ncand is then only
+// its upper bound, the capacity of the pair arrays.
+void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_t* n_dev = nullptr) {
   const int64_t nnz = c->ncand;
   double* pm = ensure<double>(c, c->pair_measure, nnz);
   int32_t* pn = ensure<int32_t>(c, c->pair_nout, nnz);
@@ -587,7 +619,7 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
                         static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order,
                         g_time_kernels ? c->clip_ev[0] : nullptr, g_time_kernels ? c->clip_ev[1] : nullptr,
                         screen ? static_cast<double*>(c->a_faces.p) : nullptr,
-                        screen ? static_cast<double*>(c->b_screen.p) : nullptr, binned ? &bin : nullptr));
+                        screen ? static_cast<double*>(c->b_screen.p) : nullptr, binned ? &bin : nullptr, n_dev));
   c->clip_timed = g_time_kernels;
   if (c->dim == 3) {
     CU(cudaMemcpyAsync(ensure<unsigned long long>(c, c->surv, 1), work, sizeof(unsigned long long),
@@ -599,7 +631,7 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr) {
                                   static_cast<int32_t*>(c->pair_b.p), static_cast<double*>(c->a_coords.p),
                                   static_cast<double*>(c->a_tol.p), static_cast<double*>(c->b_setup.p), pm,
                                   pn, s));
-  CU(lsm::launch_reduce_pairs(nnz, pm, pn, part, s));
+  CU(lsm::launch_reduce_pairs(nnz, pm, pn, part, s, n_dev));
   CU(lsm::launch_finalize(part, nred, tot, s));
   c->have_pairs = true;
 }
@@ -701,6 +733,7 @@ struct BatchOut {
   std::vector<int64_t> rowbase;  // caller order
   int64_t total_rows = 0;
   int64_t next = 0;
+  int64_t p1_next = 0;  // next free double of the P1 blocks
   bool overflow = false;
   int64_t* dev_indptr = nullptr;  // where the kernels write ind_ptr
 };
@@ -711,9 +744,63 @@ struct BatchOut {
 // and a per-mesh-pair reduction.  One host synchronisation (candidate count).
 // staged: the device addresses from stage_batch_group (host meshes), or
 // null when the meshes are on the device.
-void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu_mesh* ma,
+// Pinned area a launched group's results are copied to: totals[nm],
+// counts[nm], the candidate count, the error words.
+struct GroupRes {
+  lsm::Partial* tot;
+  int64_t* nc;
+  int64_t* count;
+  int* flags;
+};
+size_t group_res_bytes(int nm) { return (sizeof(lsm::Partial) + sizeof(int64_t)) * (size_t)nm + 64; }
+GroupRes group_res(char* base, int nm) {
+  GroupRes r;
+  r.tot = reinterpret_cast<lsm::Partial*>(base);
+  r.nc = reinterpret_cast<int64_t*>(base + sizeof(lsm::Partial) * nm);
+  r.count = r.nc + nm;
+  r.flags = reinterpret_cast<int*>(r.count + 1);
+  return r;
+}
+
+// The host half of a group: errors, overflow, per-pair results.  Returns
+// false if the candidates did not fit a capacity-mode launch (pair_cap).
+bool finish_batch_group(Ctx* c, const std::vector<int>& idx, int loc, const GroupRes& r, int64_t pair_cap,
+                        double* totals, int64_t* ncand, int64_t* nint, BatchOut* bo, int64_t group_base,
+                        int64_t p1_base) {
+  const int nm = (int)idx.size();
+  REQUIRE(r.flags[0] == 0, "Invalid node index in an element list");
+  if (r.flags[3] != 0) {
+    set_error(c, "tree build: the sort's look-back wait gave up");
+    throw Fail{LSM_ERROR_TIMEOUT};
+  }
+  if (pair_cap > 0 && *r.count > pair_cap) return false;
+  c->ncand = *r.count;
+  int64_t run = group_base;
+  for (int i = 0; i < nm; ++i) {
+    if (totals) totals[idx[i]] = r.tot[i].sum;
+    if (ncand) ncand[idx[i]] = r.nc[i];
+    if (nint) nint[idx[i]] = (int64_t)r.tot[i].n_int;
+    if (bo && bo->o && bo->o->cand_offset) bo->o->cand_offset[idx[i]] = group_base >= 0 ? run : -1;
+    if (bo && bo->o && bo->o->p1_offset)
+      bo->o->p1_offset[idx[i]] = p1_base >= 0 ? p1_base + (run - group_base) * loc * loc : -1;
+    if (group_base >= 0) run += r.nc[i];
+  }
+  return true;
+}
+
+// pair_cap > 0 (capacity mode): the pair arrays hold pair_cap candidates and
+// no count is read back mid-call: the fill and the narrow phase read the
+// count on the device and write nothing beyond the arrays; host_tab (pinned,
+// group-owned) holds the tables and res_area receives the results, which
+// finish_batch_group reads after the caller waits for the stream.  Nothing in
+// that mode synchronises or allocates once the buffers have their sizes, so
+// it can run under stream capture.  Returns false in capacity mode with the
+// results pending; true when the group is finished (sync mode).
+bool run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu_mesh* ma,
                      const lsm_gpu_mesh* mb, const uint64_t* staged, double* totals, int64_t* ncand,
-                     int64_t* nint, cudaStream_t s, BatchOut* bo = nullptr, int on_device = 0) {
+                     int64_t* nint, cudaStream_t s, BatchOut* bo = nullptr, int on_device = 0,
+                     int64_t pair_cap = 0, void* host_tab = nullptr, char* res_area = nullptr) {
+  REQUIRE(pair_cap == 0 || (!(bo && bo->o) && host_tab && res_area), "capacity mode without per-pair outputs");
   const int nm = (int)idx.size();
   const int ib = ma[idx[0]].index_bytes;
   const int loc = dim + 1;
@@ -758,8 +845,11 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
     memcpy(pta, staged, sizeof(uint64_t) * 4 * (size_t)nm);
   }
   int64_t* dtab = ensure<int64_t>(c, c->bt_tabs, (int64_t)tab_words);
-  void* htab = host_stage(c, sizeof(int64_t) * tab_words);
-  CU(cudaStreamSynchronize(s));  // the pinned stage may still feed a previous copy
+  void* htab = host_tab;
+  if (!htab) {
+    htab = host_stage(c, sizeof(int64_t) * tab_words);
+    CU(cudaStreamSynchronize(s));  // the pinned stage may still feed a previous copy
+  }
   memcpy(htab, tab.data(), sizeof(int64_t) * tab_words);
   CU(cudaMemcpyAsync(dtab, htab, sizeof(int64_t) * tab_words, cudaMemcpyHostToDevice, s));
   const int64_t* d_eoa = dtab;
@@ -782,11 +872,13 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   float* b_box32 = ensure<float>(c, c->b_box32, nb * 8);
   double* b_setup = ensure<double>(c, c->b_setup, nb * (dim == 2 ? lsm::kSetup2 : lsm::kSetup3));
   int32_t* pair_of_b = ensure<int32_t>(c, c->bt_pair_b, nb);
+  const bool want_p1 = bo && bo->o && bo->o->p1_blocks;
+  double* b_coords = want_p1 ? ensure<double>(c, c->b_coords, nb * loc * dim) : nullptr;
   double* a_faces = dim == 3 ? ensure<double>(c, c->a_faces, na * lsm::kScreen3) : nullptr;
   double* b_screen = dim == 3 ? ensure<double>(c, c->b_screen, nb * lsm::kScreen3) : nullptr;
   CU(lsm::launch_prep_batched(dim, na, nm, d_eoa, d_pta, d_eta, d_nna, ib, a_coords, a_box, nullptr, a_tol,
                               nullptr, pair_of_a, bad, s, a_faces));
-  CU(lsm::launch_prep_batched(dim, nb, nm, d_eob, d_ptb, d_etb, d_nnb, ib, nullptr, b_box, b_box32, nullptr,
+  CU(lsm::launch_prep_batched(dim, nb, nm, d_eob, d_ptb, d_etb, d_nnb, ib, b_coords, b_box, b_box32, nullptr,
                               b_setup, pair_of_b, bad, s, nullptr, b_screen));
   // tree over all B meshes
   lsm::BVH bvh;
@@ -838,38 +930,50 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
   else if (na > 0)
     CU(cudaMemsetAsync(counts, 0, sizeof(int) * na, s));
   CU(lsm::launch_scan(na, counts, offsets, stmp, s));
-  int64_t* h = static_cast<int64_t*>(c->host_scalars) + 8;
-  int* hb = static_cast<int*>(c->host_scalars);
-  CU(cudaMemcpyAsync(h, offsets + na, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  CU(cudaMemcpyAsync(hb, bad, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
-  CU(cudaStreamSynchronize(s));
-  REQUIRE(hb[0] == 0, "Invalid node index in an element list");
-  if (hb[3] != 0) {
-    set_error(c, "tree build: the sort's look-back wait gave up");
-    throw Fail{LSM_ERROR_TIMEOUT};
+  int64_t nnz = pair_cap;
+  if (pair_cap == 0) {
+    int64_t* h = static_cast<int64_t*>(c->host_scalars) + 8;
+    int* hb = static_cast<int*>(c->host_scalars);
+    CU(cudaMemcpyAsync(h, offsets + na, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(hb, bad, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    REQUIRE(hb[0] == 0, "Invalid node index in an element list");
+    if (hb[3] != 0) {
+      set_error(c, "tree build: the sort's look-back wait gave up");
+      throw Fail{LSM_ERROR_TIMEOUT};
+    }
+    nnz = *h;
   }
-  const int64_t nnz = *h;
   int32_t* pa = ensure<int32_t>(c, c->pair_a, nnz);
   int32_t* pb = ensure<int32_t>(c, c->pair_b, nnz);
   if (nnz > 0)
     CU(lsm::launch_query_batched(dim, true, na, a_box, pair_of_a, roots, stops, bvh, b_box, counts, offsets,
-                                 pa, pb, s, cache, cap, over, spill));
+                                 pa, pb, s, cache, cap, over, spill, pair_cap > 0 ? pair_cap : INT64_MAX));
   c->dim = dim;
   c->loc_a = c->loc_b = loc;
   c->nel_a = na;
   c->nel_b = nb;
   c->ncand = nnz;
   c->simplex_prep = true;
-  narrow(c, s);
+  narrow(c, s, nullptr, pair_cap > 0 ? offsets + na : nullptr);
   lsm::Partial* tot = ensure<lsm::Partial>(c, c->bt_tot, nm);
   int64_t* nc = ensure<int64_t>(c, c->bt_ncand, nm);
   lsm::Partial* pieces = ensure<lsm::Partial>(c, c->partials, lsm::mesh_totals_pieces(nm));
   CU(lsm::launch_mesh_totals(nm, d_eoa, offsets, static_cast<double*>(c->pair_measure.p),
-                             static_cast<int32_t*>(c->pair_nout.p), pieces, tot, nc, s));
+                             static_cast<int32_t*>(c->pair_nout.p), pieces, tot, nc, s,
+                             pair_cap > 0 ? pair_cap : INT64_MAX));
+  if (pair_cap > 0) {
+    const GroupRes r = group_res(res_area, nm);
+    CU(cudaMemcpyAsync(r.tot, tot, sizeof(lsm::Partial) * nm, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(r.nc, nc, sizeof(int64_t) * nm, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(r.count, offsets + na, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(r.flags, bad, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    return false;
+  }
   // per-pair outputs: CSR rows at the caller's row bases; the group's
   // per-candidate arrays (pair-major, as the caller's) as one block at the
   // next free slot, if they fit
-  int64_t group_base = -1;
+  int64_t group_base = -1, p1_base = -1;
   if (bo && bo->o) {
     const lsm_gpu_batch_out* o = bo->o;
     const bool fits = bo->next + nnz <= o->cand_capacity;
@@ -890,22 +994,33 @@ void run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
       group_base = bo->next;
       bo->next += nnz;
     }
+    // P1-P1 mass blocks of every candidate (a second clipping pass with the
+    // quadrature; blocks dense, loc x loc per candidate, CSR order)
+    const int64_t p1_need = nnz * loc * loc;
+    if (want_p1 && fits && bo->p1_next + p1_need <= o->p1_capacity) {
+      p1_base = bo->p1_next;
+      if (nnz > 0) {
+        double* dst = on_device ? o->p1_blocks + bo->p1_next : ensure<double>(c, c->blocks, p1_need);
+        lsm::Partial* pp = ensure<lsm::Partial>(c, c->partials, std::max<int64_t>(lsm::p1_grid_blocks(dim),
+                                                                                  lsm::mesh_totals_pieces(nm)));
+        CU(lsm::launch_p1_mass(dim, nnz, pa, pb, a_coords, a_tol, b_coords, b_setup, nullptr, nullptr, ib, nullptr,
+                               nullptr, dst, pp, s));
+        if (!on_device)
+          CU(cudaMemcpyAsync(o->p1_blocks + bo->p1_next, dst, sizeof(double) * p1_need, cudaMemcpyDeviceToHost, s));
+      }
+      bo->p1_next += p1_need;
+    } else if (want_p1) {
+      bo->overflow = true;
+    }
   }
-  const size_t bytes = sizeof(lsm::Partial) * nm + sizeof(int64_t) * nm;
-  char* hs = static_cast<char*>(host_stage(c, bytes));
-  CU(cudaMemcpyAsync(hs, tot, sizeof(lsm::Partial) * nm, cudaMemcpyDeviceToHost, s));
-  CU(cudaMemcpyAsync(hs + sizeof(lsm::Partial) * nm, nc, sizeof(int64_t) * nm, cudaMemcpyDeviceToHost, s));
+  const GroupRes r = group_res(static_cast<char*>(host_stage(c, group_res_bytes(nm))), nm);
+  CU(cudaMemcpyAsync(r.tot, tot, sizeof(lsm::Partial) * nm, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(r.nc, nc, sizeof(int64_t) * nm, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(r.count, offsets + na, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(r.flags, bad, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
-  const lsm::Partial* ht = reinterpret_cast<const lsm::Partial*>(hs);
-  const int64_t* hn = reinterpret_cast<const int64_t*>(hs + sizeof(lsm::Partial) * nm);
-  int64_t run = group_base;
-  for (int i = 0; i < nm; ++i) {
-    if (totals) totals[idx[i]] = ht[i].sum;
-    if (ncand) ncand[idx[i]] = hn[i];
-    if (nint) nint[idx[i]] = (int64_t)ht[i].n_int;
-    if (bo && bo->o && bo->o->cand_offset) bo->o->cand_offset[idx[i]] = group_base >= 0 ? run : -1;
-    if (group_base >= 0) run += hn[i];
-  }
+  finish_batch_group(c, idx, loc, r, 0, totals, ncand, nint, bo, group_base, p1_base);
+  return true;
 }
 
 // ------------------------------------------------------------- legacy API
@@ -935,6 +1050,22 @@ void legacy_check(Ctx* c, int st) {
   if (st != LSM_SUCCESS) legacy_abort(c->last_error.empty() ? "CUDA failure" : c->last_error.c_str());
 }
 
+// Pinned staging area of the single-pair entries: inputs at 0, the count
+// and the output simplices after them.
+constexpr size_t kPairIoBytes = 16384;
+char* pair_io(Ctx* c) {
+  if (!c->pair_io && cudaMallocHost(&c->pair_io, kPairIoBytes) != cudaSuccess) {
+    (void)cudaGetLastError();
+    c->pair_io = nullptr;
+    set_error(c, "pinned host allocation of %zu bytes failed", kPairIoBytes);
+    throw Fail{LSM_ERROR_OUT_OF_MEMORY};
+  }
+  return static_cast<char*>(c->pair_io);
+}
+
+// One pair through the batched kernels: inputs copied into pinned staging
+// and sent in one copy, the kernel, then the count and the whole output
+// buffer (at most cap simplices) back in one copy, one host wait.
 void single_pair(int dim, const double* a, const double* b, double* out_elems, int* n_out) {
   std::lock_guard<std::mutex> lk(g_mutex);
   Ctx* c = legacy_ctx();
@@ -942,21 +1073,22 @@ void single_pair(int dim, const double* a, const double* b, double* out_elems, i
   const int cap = dim == 2 ? 22 : 81;
   legacy_check(c, guarded(c, [&] {
     cudaStream_t s = c->stream;
-    double* da = ensure<double>(c, c->x_a, per);
-    double* db = ensure<double>(c, c->x_b, per);
-    int32_t* dn = ensure<int32_t>(c, c->x_nout, 1);
-    double* de = ensure<double>(c, c->x_elems, (int64_t)cap * per);
-    CU(cudaMemcpyAsync(da, a, sizeof(double) * per, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(db, b, sizeof(double) * per, cudaMemcpyHostToDevice, s));
-    CU(lsm::launch_pairs_explicit(dim, 1, da, db, nullptr, dn, de, s));
-    int32_t* hn = static_cast<int32_t*>(c->host_scalars);
-    CU(cudaMemcpyAsync(hn, dn, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    char* io = pair_io(c);
+    double* hin = reinterpret_cast<double*>(io);
+    memcpy(hin, a, sizeof(double) * per);
+    memcpy(hin + per, b, sizeof(double) * per);
+    double* din = ensure<double>(c, c->x_a, 2 * per);
+    const size_t out_bytes = 16 + sizeof(double) * (size_t)cap * per;
+    char* dout = ensure<char>(c, c->x_elems, (int64_t)out_bytes);
+    CU(cudaMemcpyAsync(din, hin, sizeof(double) * 2 * per, cudaMemcpyHostToDevice, s));
+    CU(lsm::launch_pairs_explicit(dim, 1, din, din + per, nullptr, reinterpret_cast<int32_t*>(dout),
+                                  reinterpret_cast<double*>(dout + 16), s));
+    char* hout = io + 1024;
+    CU(cudaMemcpyAsync(hout, dout, out_bytes, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
-    *n_out = hn[0];
-    if (hn[0] > 0) {
-      CU(cudaMemcpyAsync(out_elems, de, sizeof(double) * per * hn[0], cudaMemcpyDeviceToHost, s));
-      CU(cudaStreamSynchronize(s));
-    }
+    const int k = *reinterpret_cast<int32_t*>(hout);
+    *n_out = k;
+    if (k > 0) memcpy(out_elems, hout + 16, sizeof(double) * per * k);
   }));
 }
 
@@ -965,6 +1097,7 @@ void single_pair(int dim, const double* a, const double* b, double* out_elems, i
 struct MixedShape {
   int per_a, per_b, cap, per_out;
 };
+
 MixedShape mixed_shape(int kind) {
   if (kind == LSM_PAIR_INTERVALS) return {2, 2, 1, 2};
   if (kind == LSM_PAIR_TRI_QUAD) return {6, 8, 46, 6};
@@ -979,24 +1112,35 @@ void single_mixed(int kind, const double* a, const double* b, double* out_elems,
   const MixedShape m = mixed_shape(kind);
   legacy_check(c, guarded(c, [&] {
     cudaStream_t s = c->stream;
-    double* da = ensure<double>(c, c->x_a, m.per_a);
-    double* db = ensure<double>(c, c->x_b, m.per_b);
-    int32_t* dn = ensure<int32_t>(c, c->x_nout, 1);
-    double* de = ensure<double>(c, c->x_elems, (int64_t)m.cap * m.per_out);
-    CU(cudaMemcpyAsync(da, a, sizeof(double) * m.per_a, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(db, b, sizeof(double) * m.per_b, cudaMemcpyHostToDevice, s));
-    CU(lsm::launch_pairs_mixed(kind, 1, da, db, nullptr, dn, de, s));
-    int32_t* hn = static_cast<int32_t*>(c->host_scalars);
-    CU(cudaMemcpyAsync(hn, dn, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    char* io = pair_io(c);
+    double* hin = reinterpret_cast<double*>(io);
+    memcpy(hin, a, sizeof(double) * m.per_a);
+    memcpy(hin + m.per_a, b, sizeof(double) * m.per_b);
+    double* din = ensure<double>(c, c->x_a, m.per_a + m.per_b);
+    const size_t elem_bytes = sizeof(double) * (size_t)m.cap * m.per_out;
+    char* dout = ensure<char>(c, c->x_elems, (int64_t)(16 + elem_bytes));
+    CU(cudaMemcpyAsync(din, hin, sizeof(double) * (m.per_a + m.per_b), cudaMemcpyHostToDevice, s));
+    CU(lsm::launch_pairs_mixed(kind, 1, din, din + m.per_a, nullptr, reinterpret_cast<int32_t*>(dout),
+                               reinterpret_cast<double*>(dout + 16), s));
+    // small output buffers come back whole with the count; large ones
+    // (tet-hex, hex-hex) only up to the count, after a first wait
+    char* hout = io + 1024;
+    const bool whole = 16 + elem_bytes <= kPairIoBytes - 1024;
+    CU(cudaMemcpyAsync(hout, dout, whole ? 16 + elem_bytes : 16, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
-    *n_out = hn[0];
-    if (hn[0] > 0) {
-      CU(cudaMemcpyAsync(out_elems, de, sizeof(double) * m.per_out * hn[0], cudaMemcpyDeviceToHost, s));
-      CU(cudaStreamSynchronize(s));
+    const int k = *reinterpret_cast<int32_t*>(hout);
+    *n_out = k;
+    if (k > 0) {
+      const size_t bytes = sizeof(double) * m.per_out * (size_t)k;
+      if (whole) {
+        memcpy(out_elems, hout + 16, bytes);
+      } else {
+        CU(cudaMemcpyAsync(out_elems, dout + 16, bytes, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+      }
     }
   }));
 }
-
 double single_measure(int dim, const double* e) {
   std::lock_guard<std::mutex> lk(g_mutex);
   Ctx* c = legacy_ctx();
@@ -1006,7 +1150,9 @@ double single_measure(int dim, const double* e) {
     cudaStream_t s = c->stream;
     double* de = ensure<double>(c, c->x_a, per);
     double* dm = ensure<double>(c, c->x_measure, 1);
-    CU(cudaMemcpyAsync(de, e, sizeof(double) * per, cudaMemcpyHostToDevice, s));
+    double* hin = reinterpret_cast<double*>(pair_io(c));
+    memcpy(hin, e, sizeof(double) * per);
+    CU(cudaMemcpyAsync(de, hin, sizeof(double) * per, cudaMemcpyHostToDevice, s));
     CU(lsm::launch_measure_explicit(dim, 1, de, dm, s));
     double* h = static_cast<double*>(c->host_scalars);
     CU(cudaMemcpyAsync(h, dm, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1023,6 +1169,150 @@ struct lsm_gpu_context {
 };
 
 static Ctx* C(lsm_gpu_context* p) { return p ? &p->c : nullptr; }
+
+// ---------------------------------------------------- batched CUDA graph
+// Signature of a device-resident batch: the meshes' shapes and addresses and
+// the options that shape the launches.  A graph replays only for the same
+// signature (the caller may change the coordinates in place).
+std::vector<uint64_t> batch_signature(int npairs, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b) {
+  std::vector<uint64_t> v;
+  v.reserve(10 + 14 * (size_t)npairs);
+  v.push_back((uint64_t)npairs);
+  v.push_back((uint64_t)lsm::query_block());
+  v.push_back((uint64_t)lsm::tri_blocks_per_sm());
+  v.push_back((uint64_t)g_tet_screen);
+  v.push_back((uint64_t)g_tet_schedule);
+  v.push_back((uint64_t)g_sched_window);
+  v.push_back((uint64_t)g_spill_chunks);
+  v.push_back((uint64_t)lsm::sort_spin_limit());
+  v.push_back((uint64_t)(int64_t)lsm::sort_stall_block());
+  for (int i = 0; i < npairs; ++i)
+    for (const lsm_gpu_mesh* m : {&a[i], &b[i]}) {
+      v.push_back((uint64_t)m->dim);
+      v.push_back((uint64_t)m->loc);
+      v.push_back((uint64_t)m->nnodes);
+      v.push_back((uint64_t)m->nelements);
+      v.push_back((uint64_t)m->positions);
+      v.push_back((uint64_t)m->enlist);
+      v.push_back((uint64_t)m->index_bytes);
+    }
+  return v;
+}
+
+void drop_batch_graph(Ctx* c) {
+  if (c->bg.exec) cudaGraphExecDestroy(c->bg.exec);
+  c->bg.exec = nullptr;
+  c->bg.sig.clear();
+}
+
+// One launch of the batch's graph and one host wait.  False if there is no
+// graph for this signature, a device buffer was reallocated since its
+// capture, or the candidates outgrew its arrays (the caller then runs the
+// batch eagerly and captures again).
+bool replay_batch_graph(Ctx* c, const std::vector<uint64_t>& sig, cudaStream_t s, double* totals, int64_t* ncand,
+                        int64_t* nint) {
+  Ctx::BatchGraph& g = c->bg;
+  if (!g.exec || g.sig != sig || g.gen != c->gen) return false;
+  CU(cudaGraphLaunch(g.exec, s));
+  lsm::count_launch((int)g.launches);
+  CU(cudaStreamSynchronize(s));
+  char* host = static_cast<char*>(g.host);
+  for (int k = 0; k < 2; ++k) {
+    if (g.idx[k].empty()) continue;
+    const int nm = (int)g.idx[k].size();
+    if (!finish_batch_group(c, g.idx[k], k + 3, group_res(host + g.res_off[k], nm), g.cap[k], totals, ncand, nint,
+                            nullptr, -1, -1)) {
+      drop_batch_graph(c);
+      return false;
+    }
+  }
+  c->dim = g.last_dim;
+  c->loc_a = c->loc_b = g.last_loc;
+  c->nel_a = g.last_na;
+  c->nel_b = g.last_nb;
+  c->simplex_prep = true;
+  c->have_pairs = true;
+  c->surv_valid = g.last_dim == 3;
+  return true;
+}
+
+// Graph of a batch that has just run eagerly: pair arrays sized from that
+// run's counts (+1/8), a dry run in capacity mode (it sizes every buffer, so
+// the captured run allocates nothing) and the capture of the same launches.
+// Leaves no graph if anything in the capture would allocate.
+void capture_batch_graph(Ctx* c, std::vector<uint64_t> sig, const std::vector<int>& g2, const std::vector<int>& g3,
+                         const int64_t cnt[2], const lsm_gpu_mesh* a, const lsm_gpu_mesh* b, cudaStream_t s,
+                         double* totals, int64_t* ncand, int64_t* nint) {
+  drop_batch_graph(c);
+  Ctx::BatchGraph& g = c->bg;
+  const std::vector<int>* grp[2] = {&g2, &g3};
+  size_t tab_off[2] = {0, 0}, bytes = 0;
+  for (int k = 0; k < 2; ++k) {
+    const size_t nm = grp[k]->size();
+    tab_off[k] = bytes;
+    bytes += (sizeof(int64_t) * (2 * (nm + 1) + 7 * nm) + 255) & ~(size_t)255;
+    g.res_off[k] = bytes;
+    bytes += (group_res_bytes((int)nm) + 255) & ~(size_t)255;
+    g.idx[k] = *grp[k];
+    g.cap[k] = cnt[k] + cnt[k] / 8 + 1024;
+  }
+  if (g.host_cap < bytes) {
+    if (g.host) cudaFreeHost(g.host);
+    g.host = nullptr;
+    g.host_cap = 0;
+    if (cudaMallocHost(&g.host, bytes) != cudaSuccess) {
+      (void)cudaGetLastError();
+      set_error(c, "pinned host allocation of %zu bytes failed", bytes);
+      throw Fail{LSM_ERROR_OUT_OF_MEMORY};
+    }
+    g.host_cap = bytes;
+  }
+  char* host = static_cast<char*>(g.host);
+  auto run = [&]() {
+    for (int k = 0; k < 2; ++k)
+      if (!grp[k]->empty())
+        run_batch_group(c, k + 2, *grp[k], a, b, nullptr, nullptr, nullptr, nullptr, s, nullptr, 1, g.cap[k],
+                        host + tab_off[k], host + g.res_off[k]);
+  };
+  run();
+  CU(cudaStreamSynchronize(s));
+  for (int k = 0; k < 2; ++k)
+    if (!grp[k]->empty() && !finish_batch_group(c, *grp[k], k + 3, group_res(host + g.res_off[k], (int)grp[k]->size()),
+                                                g.cap[k], totals, ncand, nint, nullptr, -1, -1))
+      return;
+  const uint64_t gen0 = c->gen;
+  const unsigned long long l0 = lsm::launches();
+  CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  cudaGraph_t graph = nullptr;
+  try {
+    run();
+  } catch (...) {
+    cudaStreamEndCapture(s, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    (void)cudaGetLastError();
+    throw;
+  }
+  CU(cudaStreamEndCapture(s, &graph));
+  if (c->gen != gen0) {
+    cudaGraphDestroy(graph);
+    return;
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return;
+  }
+  g.exec = exec;
+  g.sig = std::move(sig);
+  g.gen = c->gen;
+  g.launches = lsm::launches() - l0;
+  g.last_dim = c->dim;
+  g.last_loc = c->loc_a;
+  g.last_na = c->nel_a;
+  g.last_nb = c->nel_b;
+}
 
 // Both batched entries.
 static int batched(Ctx* c, int npairs, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b, int on_device, double* totals,
@@ -1052,6 +1342,13 @@ static int batched(Ctx* c, int npairs, const lsm_gpu_mesh* a, const lsm_gpu_mesh
       if (out->ind_ptr)
         bo.dev_indptr = on_device ? out->ind_ptr : ensure<int64_t>(c, c->bt_indptr, bo.total_rows);
     }
+    // device-resident batches without per-pair outputs can replay a graph
+    const bool graph_mode = g_batch_graph && on_device && !out && !g_time_kernels;
+    std::vector<uint64_t> sig;
+    if (graph_mode) {
+      sig = batch_signature(npairs, a, b);
+      if (replay_batch_graph(c, sig, s, totals, n_candidates, n_intersecting)) return;
+    }
     c->have_pairs = false;
     c->ncand = -1;
     // Host meshes: the 2D group's copies go on the caller's stream; the 3D
@@ -1071,14 +1368,20 @@ static int batched(Ctx* c, int npairs, const lsm_gpu_mesh* a, const lsm_gpu_mesh
       if (side3) CU(cudaEventRecord(c->side_ev[1], c->side));
     }
     BatchOut* bp = out ? &bo : nullptr;
-    if (!g2.empty())
+    int64_t cnt[2] = {0, 0};
+    if (!g2.empty()) {
       run_batch_group(c, 2, g2, a, b, on_device ? nullptr : st2.data(), totals, n_candidates, n_intersecting, s, bp,
                       on_device);
+      cnt[0] = c->ncand;
+    }
     if (!g3.empty()) {
       if (side3) CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
       run_batch_group(c, 3, g3, a, b, on_device ? nullptr : st3.data(), totals, n_candidates, n_intersecting, s, bp,
                       on_device);
+      cnt[1] = c->ncand;
     }
+    if (graph_mode && npairs > 0)
+      capture_batch_graph(c, std::move(sig), g2, g3, cnt, a, b, s, totals, n_candidates, n_intersecting);
     if (out && out->ind_ptr && !on_device && bo.total_rows > 0) {
       CU(cudaMemcpyAsync(out->ind_ptr, bo.dev_indptr, sizeof(int64_t) * bo.total_rows, cudaMemcpyDeviceToHost, s));
       CU(cudaStreamSynchronize(s));
@@ -1086,11 +1389,16 @@ static int batched(Ctx* c, int npairs, const lsm_gpu_mesh* a, const lsm_gpu_mesh
     if (out) {
       if (out->total_candidates) *out->total_candidates = bo.next;
       if (bo.overflow) {
-        int64_t need = 0;
+        int64_t need = 0, need_p1 = 0;
         if (n_candidates)
-          for (int i = 0; i < npairs; ++i) need += n_candidates[i];
-        set_error(c, "batched supermesh: %lld candidates do not fit the per-candidate arrays (capacity %lld)",
-                  (long long)need, (long long)out->cand_capacity);
+          for (int i = 0; i < npairs; ++i) {
+            need += n_candidates[i];
+            need_p1 += n_candidates[i] * (a[i].dim + 1) * (a[i].dim + 1);
+          }
+        set_error(c,
+                  "batched supermesh: %lld candidates (%lld block doubles) do not fit the per-candidate arrays "
+                  "(capacity %lld, %lld)",
+                  (long long)need, (long long)need_p1, (long long)out->cand_capacity, (long long)out->p1_capacity);
         throw Fail{LSM_ERROR_CAPACITY};
       }
     }
@@ -1256,6 +1564,8 @@ int libsupermesh_gpu_set_option(const char* name, int64_t value) {
     g_tet_schedule = (int)value;
   } else if (n == "sched_window" && value >= 256 && value <= lsm::kSchedMaxWindow && value % 256 == 0) {
     g_sched_window = (int)value;
+  } else if (n == "batch_graph" && (value == 0 || value == 1)) {
+    g_batch_graph = (int)value;
   } else if (n == "fail_alloc_after" && value >= -1 && value <= INT32_MAX) {
     g_fail_alloc_after = value;
   } else if (n == "sort_spin_limit" && value >= 1 && value <= (1 << 22)) {
@@ -1287,6 +1597,8 @@ int libsupermesh_gpu_get_option(const char* name, int64_t* value) {
     *value = g_tet_schedule;
   else if (n == "sched_window")
     *value = g_sched_window;
+  else if (n == "batch_graph")
+    *value = g_batch_graph;
   else if (n == "sort_spin_limit")
     *value = lsm::sort_spin_limit();
   else if (n == "sort_stall_block")
@@ -1374,6 +1686,54 @@ int libsupermesh_gpu_supermesh(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, cons
         CU(cudaMemcpyAsync(elem_measure_a, em, sizeof(double) * c->nel_a, cudaMemcpyDeviceToHost, s));
     }
     read_stats(c, stats, s);
+  });
+}
+
+int libsupermesh_gpu_supermesh_out(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b,
+                                   int on_device, lsm_gpu_pair_out* out, lsm_gpu_stats* stats, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(out != nullptr, "NULL output descriptor");
+    cudaStream_t s = pick(c, stream);
+    SyncOnThrow sync_on_throw{s, c->side};
+    find_candidates(c, a, b, on_device, true, false, s);
+    const int64_t n = c->ncand, na = c->nel_a;
+    out->n_candidates = n;
+    const bool fits = n <= out->cand_capacity;
+    const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    // the CSR is final once the search is done: its conversion and copy run
+    // on the side stream while the narrow phase runs on s
+    const bool csr = out->ind_ptr || (fits && out->indices && n > 0);
+    if (csr) {
+      CU(cudaEventRecord(c->side_ev[0], s));
+      CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
+      if (out->ind_ptr)
+        CU(cudaMemcpyAsync(out->ind_ptr, c->offsets.p, sizeof(int64_t) * (na + 1), k, c->side));
+      if (fits && out->indices && n > 0) {
+        int64_t* dst = on_device ? out->indices : ensure<int64_t>(c, c->i64_tmp, n);
+        CU(lsm::launch_i32_to_i64(n, static_cast<int32_t*>(c->pair_b.p), dst, c->side));
+        if (!on_device) CU(cudaMemcpyAsync(out->indices, dst, sizeof(int64_t) * n, k, c->side));
+      }
+      CU(cudaEventRecord(c->side_ev[1], c->side));
+    }
+    narrow(c, s);
+    if (out->elem_measure && na > 0) {
+      double* em = on_device ? out->elem_measure : ensure<double>(c, c->elem_measure, na);
+      CU(lsm::launch_row_sums(na, static_cast<int64_t*>(c->offsets.p), static_cast<double*>(c->pair_measure.p), em,
+                              s));
+      if (!on_device) CU(cudaMemcpyAsync(out->elem_measure, em, sizeof(double) * na, cudaMemcpyDeviceToHost, s));
+    }
+    if (fits && out->pair_measure && n > 0)
+      CU(cudaMemcpyAsync(out->pair_measure, c->pair_measure.p, sizeof(double) * n, k, s));
+    if (fits && out->pair_n_out && n > 0)
+      CU(cudaMemcpyAsync(out->pair_n_out, c->pair_nout.p, sizeof(int32_t) * n, k, s));
+    if (csr) CU(cudaStreamWaitEvent(s, c->side_ev[1], 0));
+    read_stats(c, stats, s);
+    if (!fits && (out->indices || out->pair_measure || out->pair_n_out)) {
+      set_error(c, "supermesh: %lld candidates do not fit the per-candidate arrays (capacity %lld)", (long long)n,
+                (long long)out->cand_capacity);
+      throw Fail{LSM_ERROR_CAPACITY};
+    }
   });
 }
 

@@ -908,7 +908,7 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
                                                const int64_t* __restrict__ offsets, int32_t* pair_a,
                                                int32_t* pair_b, int32_t* cache, int cap,
                                                const int32_t* __restrict__ rows, int* over_rows,
-                                               const double* __restrict__ leaf) {
+                                               const double* __restrict__ leaf, int64_t pair_cap) {
   const int64_t nrows = rows ? (int64_t)*over_rows : nel_a;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
        r += (int64_t)gridDim.x * blockDim.x) {
@@ -942,8 +942,10 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
         for (int c = 0; c < DIM; ++c) ex = ex && (hi[c] > blo[c]) && (lo[c] < bhi[c]);
         if (ex) {
           if (FILL) {
-            pair_a[out + cnt] = (int32_t)a;
-            pair_b[out + cnt] = meta.x;
+            if (out + cnt < pair_cap) {
+              pair_a[out + cnt] = (int32_t)a;
+              pair_b[out + cnt] = meta.x;
+            }
           } else if (cache) {
             if (cnt < cap) cache[a * cap + cnt] = meta.x;
           }
@@ -968,8 +970,10 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
         for (int c = 0; c < DIM; ++c) ex = ex && (hi[c] > bb[c]) && (lo[c] < bb[DIM + c]);
         if (ex) {
           if (FILL) {
-            pair_a[out + cnt] = (int32_t)a;
-            pair_b[out + cnt] = w;
+            if (out + cnt < pair_cap) {
+              pair_a[out + cnt] = (int32_t)a;
+              pair_b[out + cnt] = w;
+            }
           } else if (cache) {
             if (cnt < cap) cache[a * cap + cnt] = w;
           }
@@ -991,7 +995,8 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
 __global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const int* __restrict__ counts,
                                                          const int64_t* __restrict__ offsets,
                                                          const int32_t* __restrict__ cache, int cap,
-                                                         int32_t* pair_a, int32_t* pair_b, Spill sp) {
+                                                         int32_t* pair_a, int32_t* pair_b, Spill sp,
+                                                         int64_t pair_cap) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < nel_a;
@@ -1012,13 +1017,13 @@ __global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const in
         // lost theirs (-2) are filled by the traversal over the listed rows
         const int first = sp.row_chunk ? sp.row_chunk[row] : -2;
         if (first < 0) continue;
-        for (int k = lane; k < cap; k += 32) {
+        for (int k = lane; k < cap && o + k < pair_cap; k += 32) {
           pair_a[o + k] = (int32_t)row;
           pair_b[o + k] = cache[row * cap + k];
         }
         int ch = first;
         for (int k0 = cap; k0 < c; k0 += kSpillChunk) {
-          for (int k = lane; k < kSpillChunk && k0 + k < c; k += 32) {
+          for (int k = lane; k < kSpillChunk && k0 + k < c && o + k0 + k < pair_cap; k += 32) {
             pair_a[o + k0 + k] = (int32_t)row;
             pair_b[o + k0 + k] = sp.pool[(int64_t)ch * kSpillChunk + k];
           }
@@ -1026,7 +1031,7 @@ __global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const in
         }
         continue;
       }
-      for (int k = lane; k < c; k += 32) {
+      for (int k = lane; k < c && o + k < pair_cap; k += 32) {
         pair_a[o + k] = (int32_t)row;
         pair_b[o + k] = cache[row * cap + k];
       }
@@ -1036,14 +1041,15 @@ __global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const in
 
 cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_a, BVH bvh,
                          const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
-                         int32_t* pair_b, cudaStream_t s, int32_t* cache, int cap, int* over_rows, Spill sp) {
+                         int32_t* pair_b, cudaStream_t s, int32_t* cache, int cap, int* over_rows, Spill sp,
+                         int64_t pair_cap) {
   if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
   const int B = query_block();
   const int g = grid_for(nel_a, B, 2048 / B);
   if (fill && cache) {
     count_launch(2);
     k_fill_from_cache<<<grid_for(nel_a, 256, 8), 256, 0, s>>>(nel_a, counts, offsets, cache, cap, pair_a, pair_b,
-                                                              sp);
+                                                              sp, pair_cap);
   } else {
     count_launch();
   }
@@ -1051,7 +1057,7 @@ cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_
   int32_t* cc = fill ? nullptr : cache;
 #define LSM_QUERY_ARGS                                                                                    \
   nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b, cc, cap, rows, \
-      over_rows, bvh.leaf
+      over_rows, bvh.leaf, pair_cap
   if (dim == 2) {
     if (fill)
       k_query<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
@@ -1223,7 +1229,10 @@ __global__ void __launch_bounds__(kTriBlock) k_clip_tris(int64_t npairs, const i
                                                          const double* __restrict__ setup_b,
                                                          double* pair_measure, int32_t* pair_nout,
                                                          int32_t* ovf_list, int* ovf_count,
-                                                         const int32_t* __restrict__ order) {
+                                                         const int32_t* __restrict__ order,
+                                                         const int64_t* __restrict__ n_dev) {
+  // n_dev (optional): the pair count on the device, npairs its upper bound
+  if (n_dev && *n_dev < npairs) npairs = *n_dev;
   __shared__ double poly[2 * 2 * kTriCap * kTriBlock];
   SmemPoly<kTriBlock> p{poly + threadIdx.x}, q{poly + 2 * kTriCap * kTriBlock + threadIdx.x};
   // each iteration loads the next one's pair indices (which stream from
@@ -1452,7 +1461,10 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
                                                         double* pair_measure, int32_t* pair_nout,
                                                         int32_t* survivors, unsigned long long* nsurv,
                                                         const double* __restrict__ faces_a,
-                                                        const double* __restrict__ screen_b) {
+                                                        const double* __restrict__ screen_b,
+                                                        const int64_t* __restrict__ n_dev) {
+  // n_dev (optional): the pair count on the device, npairs its upper bound
+  if (n_dev && *n_dev < npairs) npairs = *n_dev;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   // each block takes one contiguous range of pairs (consecutive iterations
@@ -1833,7 +1845,9 @@ size_t ix_smem_bytes() { return (size_t)kIxBlock * 3 * kIxPoints * sizeof(double
 // Deterministic per-block partials of the pair measures: block b reduces the
 // contiguous range [b*chunk, (b+1)*chunk) in a fixed thread order.
 __global__ void __launch_bounds__(256) k_reduce_pairs(int64_t npairs, const double* __restrict__ pm,
-                                                      const int32_t* __restrict__ pn, Partial* partials) {
+                                                      const int32_t* __restrict__ pn, Partial* partials,
+                                                      const int64_t* __restrict__ n_dev) {
+  if (n_dev && *n_dev < npairs) npairs = *n_dev;
   const int64_t chunk = (npairs + gridDim.x - 1) / gridDim.x;
   const int64_t beg = (int64_t)blockIdx.x * chunk;
   const int64_t end = beg + chunk < npairs ? beg + chunk : npairs;
@@ -1855,13 +1869,13 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
                         const int32_t* order, cudaEvent_t ev_begin, cudaEvent_t ev_end, const double* faces_a,
-                        const double* screen_b, const SchedBin* bin) {
+                        const double* screen_b, const SchedBin* bin, const int64_t* n_dev) {
   const int g = clip_grid_blocks(dim);
   count_launch();
   if (dim == 2) {
     if (ev_begin) cudaEventRecord(ev_begin, s);
     k_clip_tris<<<g, kTriBlock, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure,
-                                        pair_nout, overflow_list, overflow_count, order);
+                                        pair_nout, overflow_list, overflow_count, order, n_dev);
   } else {
     // work[0]: survivor count, work[1]: clipper pair counter
     // the timed span covers the early-out pass and the clipper: together
@@ -1871,7 +1885,7 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     count_launch();
     k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, tol_a,
                                                               setup_b, pair_measure, pair_nout, overflow_list, work,
-                                                              faces_a, screen_b);
+                                                              faces_a, screen_b, n_dev);
     const int4* list = reinterpret_cast<const int4*>(overflow_list);
     if (bin) {
       // the survivors reordered into class-uniform runs within windows
@@ -1889,9 +1903,9 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
 int reduce_pairs_blocks() { return kReduceBlocks; }
 
 cudaError_t launch_reduce_pairs(int64_t npairs, const double* pair_measure, const int32_t* pair_nout,
-                                Partial* partials, cudaStream_t s) {
+                                Partial* partials, cudaStream_t s, const int64_t* n_dev) {
   count_launch();
-  k_reduce_pairs<<<kReduceBlocks, 256, 0, s>>>(npairs, pair_measure, pair_nout, partials);
+  k_reduce_pairs<<<kReduceBlocks, 256, 0, s>>>(npairs, pair_measure, pair_nout, partials, n_dev);
   return cudaGetLastError();
 }
 
@@ -2102,7 +2116,8 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
                                                        const int64_t* __restrict__ offsets, int32_t* pair_a,
                                                        int32_t* pair_b, int32_t* cache, int cap,
                                                        const int32_t* __restrict__ rows, int* over_rows,
-                                                       const double* __restrict__ leaf, Spill sp) {
+                                                       const double* __restrict__ leaf, Spill sp,
+                                                       int64_t pair_cap) {
   // cache / rows / over_rows / leaf: as k_query
   const int64_t nrows = rows ? (int64_t)*over_rows : nel_a;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
@@ -2140,8 +2155,10 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
         for (int c = 0; c < DIM; ++c) ex = ex && (hi[c] > blo[c]) && (lo[c] < bhi[c]);
         if (ex) {
           if (FILL) {
-            pair_a[out + cnt] = (int32_t)a;
-            pair_b[out + cnt] = meta.x;
+            if (out + cnt < pair_cap) {
+              pair_a[out + cnt] = (int32_t)a;
+              pair_b[out + cnt] = meta.x;
+            }
           } else if (cache) {
             cache_put(cache, cap, sp, a, cnt, meta.x, chunk, lost);
           }
@@ -2166,8 +2183,10 @@ __global__ void __launch_bounds__(256) k_query_batched(int64_t nel_a, const doub
         for (int c = 0; c < DIM; ++c) ex = ex && (hi[c] > bb[c]) && (lo[c] < bb[DIM + c]);
         if (ex) {
           if (FILL) {
-            pair_a[out + cnt] = (int32_t)a;
-            pair_b[out + cnt] = w;
+            if (out + cnt < pair_cap) {
+              pair_a[out + cnt] = (int32_t)a;
+              pair_b[out + cnt] = w;
+            }
           } else if (cache) {
             cache_put(cache, cap, sp, a, cnt, w, chunk, lost);
           }
@@ -2191,14 +2210,14 @@ cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double
                                  const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
                                  int32_t* pair_b, cudaStream_t s, int32_t* cache, int cap, int* over_rows,
-                                 Spill sp) {
+                                 Spill sp, int64_t pair_cap) {
   if (nel_a <= 0 || bvh.n <= 0) return cudaSuccess;
   const int B = query_block();
   const int g = grid_for(nel_a, B, 2048 / B);
   if (fill && cache) {
     count_launch(2);
     k_fill_from_cache<<<grid_for(nel_a, 256, 8), 256, 0, s>>>(nel_a, counts, offsets, cache, cap, pair_a, pair_b,
-                                                              sp);
+                                                              sp, pair_cap);
   } else {
     count_launch();
   }
@@ -2206,7 +2225,7 @@ cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double
   int32_t* cc = fill ? nullptr : cache;
 #define LSM_QUERY_ARGS                                                                                         \
   nel_a, box64_a, pair_of_a, roots, stops, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, \
-      pair_b, cc, cap, rows, over_rows, bvh.leaf, sp
+      pair_b, cc, cap, rows, over_rows, bvh.leaf, sp, pair_cap
   if (dim == 2) {
     if (fill)
       k_query_batched<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
@@ -2233,10 +2252,12 @@ constexpr int kMeshSplit = 32;
 __global__ void __launch_bounds__(256) k_mesh_totals(int nm, const int64_t* __restrict__ elem_off_a,
                                                      const int64_t* __restrict__ offsets,
                                                      const double* __restrict__ pm, const int32_t* __restrict__ pn,
-                                                     Partial* pieces) {
+                                                     Partial* pieces, int64_t cap) {
   const int p = blockIdx.x, g = blockIdx.y;
   if (p >= nm) return;
-  const int64_t beg = offsets[elem_off_a[p]], end = offsets[elem_off_a[p + 1]];
+  // cap: entries the pair arrays hold (a count beyond it is reported by the
+  // host, which then runs the batch again with larger arrays)
+  const int64_t beg = min(offsets[elem_off_a[p]], cap), end = min(offsets[elem_off_a[p + 1]], cap);
   const int64_t len = end - beg;
   const int64_t b0 = beg + len * g / kMeshSplit, b1 = beg + len * (g + 1) / kMeshSplit;
   double sum = 0.0, err = 0.0;
@@ -2310,10 +2331,11 @@ cudaError_t launch_batch_csr(int64_t na, int nm, const int32_t* pair_of_a, const
 }
 
 cudaError_t launch_mesh_totals(int nm, const int64_t* elem_off_a, const int64_t* offsets, const double* pm,
-                               const int32_t* pn, Partial* pieces, Partial* out, int64_t* ncand, cudaStream_t s) {
+                               const int32_t* pn, Partial* pieces, Partial* out, int64_t* ncand, cudaStream_t s,
+                               int64_t cap) {
   if (nm <= 0) return cudaSuccess;
   count_launch(2);
-  k_mesh_totals<<<dim3(nm, kMeshSplit), 256, 0, s>>>(nm, elem_off_a, offsets, pm, pn, pieces);
+  k_mesh_totals<<<dim3(nm, kMeshSplit), 256, 0, s>>>(nm, elem_off_a, offsets, pm, pn, pieces, cap);
   k_mesh_combine<<<(nm + 127) / 128, 128, 0, s>>>(nm, elem_off_a, offsets, pieces, out, ncand);
   return cudaGetLastError();
 }

@@ -115,10 +115,12 @@ struct Spill {
 // lists the rows that could not keep them all in over_rows ({count,
 // rows...}, count zeroed by the caller, nel_a + 1 ints); pass 2 then copies
 // the kept rows and traverses only the listed ones.
+// pair_cap: entries pair_a / pair_b hold; the fill writes no pair beyond it
+// (the caller compares the count with it afterwards).
 cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_a, BVH bvh,
                          const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
                          int32_t* pair_b, cudaStream_t s, int32_t* cache = nullptr, int cap = 0,
-                         int* over_rows = nullptr, Spill sp = Spill{});
+                         int* over_rows = nullptr, Spill sp = Spill{}, int64_t pair_cap = INT64_MAX);
 
 // Exclusive scan of int32 counts into int64 offsets[n+1] (offsets[n] = total).
 int64_t scan_tmp_entries(int64_t n);
@@ -143,7 +145,8 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
                         const int32_t* order = nullptr, cudaEvent_t ev_begin = nullptr,
                         cudaEvent_t ev_end = nullptr, const double* faces_a = nullptr,
-                        const double* screen_b = nullptr, const SchedBin* bin = nullptr);
+                        const double* screen_b = nullptr, const SchedBin* bin = nullptr,
+                        const int64_t* n_dev = nullptr);
 // Opt-in shared-memory limits for the clip kernels on the current device.
 cudaError_t init_device_attributes();
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
@@ -156,8 +159,10 @@ cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overf
 // because it sets the totals' summation order).
 constexpr int kReduceBlocks = 1024;
 int reduce_pairs_blocks();
+// n_dev (optional): the pair count on the device; npairs is then its upper
+// bound (the pair arrays' capacity).  The same holds for launch_clip.
 cudaError_t launch_reduce_pairs(int64_t npairs, const double* pair_measure, const int32_t* pair_nout,
-                                Partial* partials, cudaStream_t s);
+                                Partial* partials, cudaStream_t s, const int64_t* n_dev = nullptr);
 
 // Totals: merge of the per-block partials into out[0] (in order).
 cudaError_t launch_finalize(const Partial* partials, int npartials, Partial* out, cudaStream_t s);
@@ -243,7 +248,7 @@ cudaError_t launch_query_batched(int dim, bool fill, int64_t nel_a, const double
                                  const int32_t* pair_of_a, const int* roots, const int* stops, BVH bvh,
                                  const double* box64_b, int* counts, const int64_t* offsets, int32_t* pair_a,
                                  int32_t* pair_b, cudaStream_t s, int32_t* cache = nullptr, int cap = 0,
-                                 int* over_rows = nullptr, Spill sp = Spill{});
+                                 int* over_rows = nullptr, Spill sp = Spill{}, int64_t pair_cap = INT64_MAX);
 // Per-pair CSR of a batch group (get_output layout): ind_ptr rows of mesh
 // pair k at rowbase[k] (optional), candidate B elements local to their pair
 // as int64 (optional).
@@ -252,6 +257,7 @@ cudaError_t launch_batch_csr(int64_t na, int nm, const int32_t* pair_of_a, const
                              const int32_t* pair_of_b, const int64_t* eob, int64_t* indices, cudaStream_t s);
 int64_t mesh_totals_pieces(int nm);  // Partial scratch entries for launch_mesh_totals
 cudaError_t launch_mesh_totals(int nm, const int64_t* elem_off_a, const int64_t* offsets, const double* pm,
-                               const int32_t* pn, Partial* pieces, Partial* out, int64_t* ncand, cudaStream_t s);
+                               const int32_t* pn, Partial* pieces, Partial* out, int64_t* ncand, cudaStream_t s,
+                               int64_t cap = INT64_MAX);
 
 }  // namespace lsm

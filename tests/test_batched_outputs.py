@@ -114,3 +114,24 @@ def test_config_batched256_per_pair_vs_oracle(gpu_ctx, oracle_mod):
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         counts = list(ex.map(check, range(len(pairs))))
     assert sum(counts) == res["total_candidates"][0] > 100_000_000
+
+
+def test_batched_p1_blocks_match_single_pair_entry(gpu_ctx):
+    """P1-P1 mass blocks through the batched entry equal the blocks of the
+    single-pair P1 entry, candidate by candidate (matched by (row, B
+    element): the two searches order each row's candidates differently)."""
+    pairs = _small_batch()
+    res = gpu_ctx.supermesh_batched_pairs(pairs, p1_blocks=True)
+    for i, (A, B) in enumerate(pairs):
+        loc = A[1].shape[1]
+        _, blk1 = gpu_ctx.p1_mass(A, B, want_blocks=True)
+        st, _ = gpu_ctx.supermesh(A, B)
+        ip1, ind1 = gpu_ctx.get_candidates(len(A[1]), st.n_candidates)
+        ip, ind, _, _ = _pair_view(res, pairs, i)
+        nc = int(res["n_candidates"][i])
+        o = int(res["p1_offset"][i])
+        blk = res["p1_blocks"][o:o + nc * loc * loc].reshape(nc, loc * loc)
+        a = _table(ip, ind, blk)
+        b = _table(ip1, ind1, blk1.reshape(-1, loc * loc))
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), i
