@@ -135,3 +135,22 @@ def test_batched_p1_blocks_match_single_pair_entry(gpu_ctx):
         b = _table(ip1, ind1, blk1.reshape(-1, loc * loc))
         for x, y in zip(a, b):
             assert np.array_equal(x, y), i
+
+
+def test_batched_with_empty_meshes_and_empty_batch(gpu_ctx):
+    """Mesh pairs with an empty side give no candidates and a zero total; an
+    empty batch is a no-op."""
+    _, A, B = M.config_meshes("small3d_5x6")
+    _, A2, B2 = M.config_meshes("small2d_12x17")
+    empty3 = (np.zeros((0, 3)), np.zeros((0, 4), dtype=A[1].dtype))
+    empty2 = (np.zeros((0, 2)), np.zeros((0, 3), dtype=A2[1].dtype))
+    pairs = [(A, B), (A, empty3), (empty3, B), (A2, empty2), (A2, B2)]
+    res = gpu_ctx.supermesh_batched_pairs(pairs)
+    nc = res["n_candidates"][: len(pairs)]
+    assert nc[1] == nc[2] == nc[3] == 0 and nc[0] > 0 and nc[4] > 0
+    assert res["totals"][1] == res["totals"][2] == res["totals"][3] == 0.0
+    for i in (0, 4):
+        assert abs(res["totals"][i] - 1.0) <= REL_TOL
+    assert np.all(res["ind_ptr"][res["row_offset"][1]:res["row_offset"][1] + len(A[1]) + 1] == 0)
+    empty = gpu_ctx.supermesh_batched_pairs([])
+    assert empty["total_candidates"][0] == 0
