@@ -344,6 +344,13 @@ def run_batched(args, world, rank, local):
         barrier(world)
         return sum(e0.elapsed_time(e1) for e0, e1 in evs), out
 
+    if args.kernel_only:
+        ms_k, _ = timed(lambda: ctx.supermesh_batched(tdev, on_device=True, stream=sp), args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"kernel_only": True, "workload": args.workload, "ms_per_step": ms_k / args.steps}),
+                  flush=True)
+        ctx.close()
+        return
     # eager: every phase launched by the host, one host wait per dimension
     # group for the candidate count; graph: the whole batch replayed from a
     # CUDA graph captured on the first call (option batch_graph)

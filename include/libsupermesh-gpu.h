@@ -74,6 +74,9 @@ int64_t libsupermesh_gpu_kernel_launches(void);
  * launch shapes per GPU and workload):
  *   "tri_blocks_per_sm"  4, 8 (default) or 16 blocks of 128 threads per SM (2D clipper)
  *   "query_block"        64, 128 (default) or 256 threads per block (candidate search)
+ *   "leaf_bucket"        1 (default), 2, 4 or 8: subtrees of the single-mesh search hierarchy with
+ *                        at most this many leaves are scanned as contiguous leaf records instead
+ *                        of being walked (same candidates, same order)
  *   "time_kernels"       1: record CUDA events around the clip kernel of every
  *                        narrow phase (read with libsupermesh_gpu_clip_kernel_ms); 0 (default)
  *   "spill_chunks"       -1 (default, automatic), 0 or n > 0: chunks of 64 candidates that the

@@ -24,8 +24,8 @@ from pathlib import Path
 import libsupermesh_b200 as lsm
 
 SPACE = {
-    2: {"tri_blocks_per_sm": (4, 8, 16), "query_block": (64, 128, 256)},
-    3: {"query_block": (64, 128, 256)},
+    2: {"tri_blocks_per_sm": (4, 8, 16), "query_block": (64, 128, 256), "leaf_bucket": (1, 4, 8)},
+    3: {"query_block": (64, 128, 256), "leaf_bucket": (1, 4, 8)},
 }
 
 

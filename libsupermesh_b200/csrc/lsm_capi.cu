@@ -1564,6 +1564,8 @@ int libsupermesh_gpu_set_option(const char* name, int64_t value) {
     g_tet_schedule = (int)value;
   } else if (n == "sched_window" && value >= 256 && value <= lsm::kSchedMaxWindow && value % 256 == 0) {
     g_sched_window = (int)value;
+  } else if (n == "leaf_bucket" && (value == 1 || value == 2 || value == 4 || value == 8)) {
+    lsm::set_leaf_bucket((int)value);
   } else if (n == "batch_graph" && (value == 0 || value == 1)) {
     g_batch_graph = (int)value;
   } else if (n == "fail_alloc_after" && value >= -1 && value <= INT32_MAX) {
@@ -1599,6 +1601,8 @@ int libsupermesh_gpu_get_option(const char* name, int64_t* value) {
     *value = g_sched_window;
   else if (n == "batch_graph")
     *value = g_batch_graph;
+  else if (n == "leaf_bucket")
+    *value = lsm::leaf_bucket();
   else if (n == "sort_spin_limit")
     *value = lsm::sort_spin_limit();
   else if (n == "sort_stall_block")

@@ -49,12 +49,15 @@ unsigned long long launches() { return __atomic_load_n(&g_launches, __ATOMIC_REL
 namespace {
 int g_tri_bps = 8;
 int g_query_block = 128;
+int g_leaf_bucket = 1;
 }  // namespace
 
 int tri_blocks_per_sm() { return g_tri_bps; }
 void set_tri_blocks_per_sm(int v) { g_tri_bps = v; }
 int query_block() { return g_query_block; }
 void set_query_block(int v) { g_query_block = v; }
+int leaf_bucket() { return g_leaf_bucket; }
+void set_leaf_bucket(int v) { g_leaf_bucket = v; }
 
 void count_launch(int n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 
@@ -744,9 +747,9 @@ __device__ __forceinline__ int bvh_delta(const uint32_t* __restrict__ codes, int
   return 32 + __clz((uint32_t)i ^ (uint32_t)j);
 }
 
-// work layout (ints): parent[2n-1] | rope[n] | visit[n] | last[n] | left[n] | right[n]
+// work layout (ints): parent[2n-1] | rope[n] | visit[n] | last[n] | left[n] | right[n] | first[n]
 __global__ void k_bvh_internal(int n, const uint32_t* __restrict__ codes, int* parent, int* rope,
-                               int* last, int* left, int* right) {
+                               int* last, int* left, int* right, int* first_leaf) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
   const int d = (bvh_delta(codes, n, i, i + 1) - bvh_delta(codes, n, i, i - 1)) >= 0 ? 1 : -1;
@@ -775,6 +778,7 @@ __global__ void k_bvh_internal(int n, const uint32_t* __restrict__ codes, int* p
   parent[rc] = i;
   rope[gamma + 1] = rc;
   last[i] = lst;
+  if (first_leaf) first_leaf[i] = first;
 }
 
 __device__ __forceinline__ int bvh_escape(int n, int node, const int* __restrict__ rope, const int* __restrict__ last) {
@@ -786,7 +790,8 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
                             const int* __restrict__ parent, const int* __restrict__ rope,
                             const int* __restrict__ last, const int* __restrict__ left,
                             const int* __restrict__ right, int* visit, float4* lo_left, float4* hi_esc,
-                            int dim, const double* __restrict__ box64, double* leaf) {
+                            int dim, const double* __restrict__ box64, double* leaf,
+                            const int* __restrict__ first_leaf, int bucket) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int elem = sorted_vals[k];
@@ -820,6 +825,13 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
     l.y = fminf(a0.y, b0.y);
     l.z = fminf(a0.z, b0.z);
     l.w = __int_as_float(lc);
+    if (first_leaf) {
+      // a subtree of at most `bucket` leaves becomes a bucket: the node
+      // records its first sorted leaf and leaf count instead of its left
+      // child, and the search scans those leaf records in order
+      const int f = first_leaf[p], cnt = last[p] - f + 1;
+      if (cnt <= bucket) l.w = __int_as_float((int)(0x80000000u | ((unsigned)(cnt - 1) << 27) | (unsigned)f));
+    }
     h.x = fmaxf(a1.x, b1.x);
     h.y = fmaxf(a1.y, b1.y);
     h.z = fmaxf(a1.z, b1.z);
@@ -843,13 +855,19 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
   cudaMemsetAsync(visit, 0, sizeof(int) * n, s);
   cudaMemsetAsync(rope, 0xff, sizeof(int) * n, s);  // unset ropes read as "end"
   count_launch(n > 1 ? 2 : 1);
+  // leaf buckets need the leaf records (box64) and fit the node encoding
+  // (first leaf below 2^27, at most 8 leaves)
+  int* first_leaf = right + n;
+  const bool buckets = box64 && g_leaf_bucket > 1 && n < (1 << 27);
   if (n > 1) {
-    k_bvh_internal<<<(n - 1 + 255) / 256, 256, 0, s>>>(n, sorted_keys, parent, rope, last, left, right);
+    k_bvh_internal<<<(n - 1 + 255) / 256, 256, 0, s>>>(n, sorted_keys, parent, rope, last, left, right,
+                                                       buckets ? first_leaf : nullptr);
   }
   cudaMemsetAsync(parent, 0xff, sizeof(int), s);  // parent[root] = -1
   k_bvh_refit<<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
                                               rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim, box64,
-                                              box64 ? bvh.leaf : nullptr);
+                                              box64 ? bvh.leaf : nullptr, buckets ? first_leaf : nullptr,
+                                              g_leaf_bucket);
   return cudaGetLastError();
 }
 
@@ -960,6 +978,33 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
       if (DIM == 3) ov = ov && H.z > ql[2] && L.z < qh[2];
       if (ov) {
         const int w = __float_as_int(L.w);
+        if (node < n - 1 && w < 0) {
+          // leaf bucket: its sorted leaves in order, exact FP64 test each
+          // (independent loads), then on past the subtree
+          const int f = w & 0x07ffffff, nl = ((w >> 27) & 7) + 1;
+          for (int k = 0; k < nl; ++k) {
+            const double2* q = reinterpret_cast<const double2*>(leaf + (int64_t)(f + k) * 8);
+            const double2 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
+            const double blo[3] = {q0.x, q0.y, q1.x}, bhi[3] = {q1.y, q2.x, q2.y};
+            bool ex = true;
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) ex = ex && (hi[c] > blo[c]) && (lo[c] < bhi[c]);
+            if (ex) {
+              const int e = __double2loint(q3.x);
+              if (FILL) {
+                if (out + cnt < pair_cap) {
+                  pair_a[out + cnt] = (int32_t)a;
+                  pair_b[out + cnt] = e;
+                }
+              } else if (cache) {
+                if (cnt < cap) cache[a * cap + cnt] = e;
+              }
+              ++cnt;
+            }
+          }
+          node = __float_as_int(H.w);
+          continue;
+        }
         if (node < n - 1) {
           node = w;
           continue;
@@ -2094,7 +2139,7 @@ cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const
   k_mesh_roots<<<(nm + 255) / 256, 256, 0, s>>>(nm, n, mesh_off_b, rope, last, roots, stops);
   k_bvh_refit<<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
                                               rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim, box64,
-                                              box64 ? bvh.leaf : nullptr);
+                                              box64 ? bvh.leaf : nullptr, nullptr, 1);
   return cudaGetLastError();
 }
 

@@ -46,6 +46,11 @@ int tri_blocks_per_sm();
 void set_tri_blocks_per_sm(int v);
 int query_block();
 void set_query_block(int v);
+// Leaves per bucket of the single-mesh hierarchy (1 = none; 2, 4 or 8):
+// subtrees of at most this many leaves are scanned as contiguous leaf
+// records instead of being walked.
+int leaf_bucket();
+void set_leaf_bucket(int v);
 
 struct BVH {
   int n = 0;                 // leaves

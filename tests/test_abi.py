@@ -114,12 +114,14 @@ def test_tuning_options_host_side(lib):
     for name, vals in {"tri_blocks_per_sm": (16, 8), "query_block": (256, 128), "tet_screen": (0, 1),
                        "time_kernels": (1, 0), "spill_chunks": (0, 5, -1), "tet_schedule": (1, 2, 0),
                        "sched_window": (256, 8192, 1024), "fail_alloc_after": (5, -1),
-                       "sort_spin_limit": (1000, 1 << 22), "sort_stall_block": (2, -1)}.items():
+                       "sort_spin_limit": (1000, 1 << 22), "sort_stall_block": (2, -1),
+                       "leaf_bucket": (1, 2, 8, 4), "batch_graph": (1, 0)}.items():
         for v in vals:
             L.set_option(name, v)
             assert L.get_option(name) == v
     for bad in (("tet_clipper", 0), ("query_block", 100), ("tet_screen", 2), ("spill_chunks", -2),
                 ("tet_schedule", 3), ("sched_window", 300), ("sched_window", 16384), ("sort_stall_block", 0),
-                ("sort_spin_limit", 0), ("fail_alloc_after", -2), ("nonsense", 1)):
+                ("sort_spin_limit", 0), ("fail_alloc_after", -2), ("leaf_bucket", 3), ("batch_graph", 2),
+                ("nonsense", 1)):
         with pytest.raises(L.LsmError):
             L.set_option(*bad)

@@ -19,7 +19,7 @@ def tuner(tmp_path, monkeypatch):
     import libsupermesh_b200 as lsm
 
     monkeypatch.setenv("LIBSUPERMESH_TUNING_CACHE", str(tmp_path / "tuning.json"))
-    names = ("query_block", "tri_blocks_per_sm")
+    names = ("query_block", "tri_blocks_per_sm", "leaf_bucket")
     before = {n: lsm.get_option(n) for n in names}
     yield autotune, lsm
     for n, v in before.items():

@@ -157,11 +157,11 @@ def test_autotuner_keeps_results(gpu_ctx, tmp_path, monkeypatch):
         dim, A, B = M.config_meshes(name)
         ref, em_ref = gpu_ctx.supermesh(A, B, elem_measure=True)
         res = autotune.tune(gpu_ctx, A, B, reps=1)
-        assert res["tried"] == (9 if dim == 2 else 3)
+        assert res["tried"] == (27 if dim == 2 else 9)
         st, em = gpu_ctx.supermesh(A, B, elem_measure=True)
         assert st.as_dict() == ref.as_dict() and np.array_equal(em, em_ref)
         assert autotune.apply_cached(dim, len(A[1]), len(B[1])) == res["setting"]
-    for n, v in {"tri_blocks_per_sm": 8, "query_block": 128}.items():
+    for n, v in {"tri_blocks_per_sm": 8, "query_block": 128, "leaf_bucket": 1}.items():
         lsm.set_option(n, v)
 
 
