@@ -682,8 +682,7 @@ def run_ours(args, world, rank, local):
         }
         line["cpu_baseline"] = cpu
         line["drop_in_per_pair"] = drop_in_per_pair(ctx, dim, A, B, n_cand)
-        if dim == 2:
-            line["p1_mass"] = p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush)
+        line["p1_mass"] = p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush)
         print(json.dumps(line), flush=True)
     ctx.close()
 
@@ -742,7 +741,8 @@ def schedule_legs(ctx, sp, flush, steps, world, plain_ms, n_cand, pm0, pn0):
 
 def p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush):
     """The P1-P1 mixed mass product u^T M v over the supermesh (search,
-    clipping and the 3-point-rule blocks), u = x on A, v = y on B, reported
+    clipping and the quadrature blocks: 3-point rule per triangle, 4-point
+    rule per tet), u = x on A, v = y on B, reported
     beside the main metric, not part of it: device-resident meshes and fields
     timed with CUDA events on the stream (L2 flushed before each call), and
     end to end from pinned host meshes and fields (copies inside the events).

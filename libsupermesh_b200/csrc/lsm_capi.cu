@@ -75,6 +75,7 @@ struct Ctx {
   DevBuf counts, offsets, scan_tmp, pair_a, pair_b, i64_tmp, q_cache, q_over, q_pool, q_next, q_first;
   // narrow phase
   DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals;
+  DevBuf p1_list;  // survivors of the P1 pass's early-out (kept apart from the narrow phase's)
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
   DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand, bt_indptr;
@@ -259,7 +260,7 @@ void fini_ctx(Ctx* c) {
                    &c->keys_tmp, &c->vals_tmp, &c->hist, &c->root_partial, &c->rootbox, &c->bvh_lo,
                    &c->bvh_work, &c->bvh_leaf, &c->counts, &c->offsets, &c->scan_tmp, &c->pair_a,
                    &c->pair_b, &c->i64_tmp, &c->pair_measure, &c->pair_nout, &c->partials,
-                   &c->ovf_list, &c->misc, &c->elem_measure, &c->totals, &c->x_a, &c->x_b, &c->x_measure,
+                   &c->ovf_list, &c->p1_list, &c->misc, &c->elem_measure, &c->totals, &c->x_a, &c->x_b, &c->x_measure,
                    &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
                    &c->bt_ncand, &c->bt_stage_pa[0], &c->bt_stage_ea[0], &c->bt_stage_pb[0],
@@ -344,6 +345,12 @@ MeshDev upload(Ctx* c, const lsm_gpu_mesh* m, int on_device, DevBuf& pos, DevBuf
 }
 
 int* bad_flag(Ctx* c) { return ensure<int>(c, c->misc, 64); }
+
+// P1 mass pass (3D): its survivor list and two counters (misc ints 16-19)
+int32_t* p1_survivors(Ctx* c, int dim, int64_t nnz) {
+  return dim == 3 ? ensure<int32_t>(c, c->p1_list, 4 * std::max<int64_t>(nnz, 1)) : nullptr;
+}
+unsigned long long* p1_work(Ctx* c) { return reinterpret_cast<unsigned long long*>(bad_flag(c) + 16); }
 
 // Device memory the candidate-row cache of the search may hold: min(4 GiB,
 // 1/32 of the device).  Only rows' actual candidates are written (4 B each);
@@ -1004,7 +1011,8 @@ bool run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
         lsm::Partial* pp = ensure<lsm::Partial>(c, c->partials, std::max<int64_t>(lsm::p1_grid_blocks(dim),
                                                                                   lsm::mesh_totals_pieces(nm)));
         CU(lsm::launch_p1_mass(dim, nnz, pa, pb, a_coords, a_tol, b_coords, b_setup, nullptr, nullptr, ib, nullptr,
-                               nullptr, dst, pp, s));
+                               nullptr, dst, pp, s, p1_survivors(c, dim, nnz), p1_work(c),
+                               g_tet_screen ? a_faces : nullptr, g_tet_screen ? b_screen : nullptr));
         if (!on_device)
           CU(cudaMemcpyAsync(o->p1_blocks + bo->p1_next, dst, sizeof(double) * p1_need, cudaMemcpyDeviceToHost, s));
       }
@@ -1897,7 +1905,9 @@ int libsupermesh_gpu_p1_mass(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const 
     CU(lsm::launch_p1_mass(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                            static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                            static_cast<double*>(c->b_coords.p), static_cast<double*>(c->b_setup.p), en_a, en_b,
-                           a->index_bytes, du, dv, dbk, part, s));
+                           a->index_bytes, du, dv, dbk, part, s, p1_survivors(c, c->dim, nnz), p1_work(c),
+                           c->dim == 3 && g_tet_screen ? static_cast<double*>(c->a_faces.p) : nullptr,
+                           c->dim == 3 && g_tet_screen ? static_cast<double*>(c->b_screen.p) : nullptr));
     CU(lsm::launch_finalize(part, nblk, tot, s));
     double* h = static_cast<double*>(c->host_scalars) + 64;
     CU(cudaMemcpyAsync(h, tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -19,8 +19,9 @@
 //                       indices with a refill pipeline
 //   K7  compensated reductions (per-block (sum, err), then final; per mesh
 //                       pair for the batched path)
-//   K8  k_p1_mass       P1-P1 mixed mass blocks + u^T M v;  k_p2_inner  P2
-//                       inner product
+//   K8  P1-P1 mixed mass blocks + u^T M v: 2D k_p1_mass; 3D the early-out
+//                       pass and k_clip_tets_ix with the quadrature sink;
+//                       k_p2_inner  P2 inner product
 //   K9  1D sort finder  k_prep_1d, 64-bit stable sort, max segment tree,
 //                       k_rows_1d, k_sweep_1d, k_emit_1d;  k_clip_intervals
 //   K10 explicit pairs  k_pairs_tris / _tets and the mixed element pairs
@@ -1389,15 +1390,8 @@ __device__ __forceinline__ void load_plane(const double* __restrict__ planes, in
   c = b.y;
 }
 
-// Plane sources for the depth-first walk.
-struct GlobalPlanes {  // B's planes in global memory (setup row, stride 4)
-  const double* p;
-  __device__ __forceinline__ void get(int L, double& nx, double& ny, double& nz, double& c) const {
-    load_plane(p, L, nx, ny, nz, c);
-  }
-};
-
-struct RegPlanes {  // planes computed in registers
+// Plane source for the depth-first walk: planes computed in registers.
+struct RegPlanes {
   const Planes& P;
   __device__ __forceinline__ void get(int L, double& nx, double& ny, double& nz, double& c) const {
     nx = sel4(L, P.nx[0], P.nx[1], P.nx[2], P.nx[3]);
@@ -1494,9 +1488,13 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 // which is settled here (volume test and measure as in the clipper).
 // Survivors are written as {pair, a, b, no-op mask} so that the clipper
 // gets the element numbers and the planes to skip in one load.
+// kSettle false (the P1 mass pass): nothing is written for rejected pairs
+// (their results are zero-filled by the caller) and pairs with all four
+// planes no-op are listed too, for the clipper to integrate A itself.
 #ifndef LSM_PREFILTER_BPS
 #define LSM_PREFILTER_BPS 2
 #endif
+template <bool kSettle>
 __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ order,
                                                         const int32_t* __restrict__ pa,
                                                         const int32_t* __restrict__ pb,
@@ -1583,7 +1581,9 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
           }
         }
       }
-      if (reject) {
+      if (!kSettle) {
+        live = !reject;
+      } else if (reject) {
         pair_measure[i] = 0.0;
         pair_nout[i] = 0;
       } else if (noop == 15) {
@@ -1738,12 +1738,41 @@ __device__ __forceinline__ int ix_split(unsigned cur, const TetClass& k, const P
 // atomic per chunk).
 constexpr int kIxChunk = 64;
 
-__global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
+// What the clipper does with a pair's kept output tets (each passed with
+// its vertex-1 volume, in the reference's output order).  kInside: the list
+// may hold pairs whose every plane is a no-op (A inside B: its one output
+// tet is A itself), which the supermesh's early-out pass settles itself.
+struct IxMeasureSink {
+  static constexpr bool kInside = false;
+  static constexpr int kLaneDoubles = 0;  // shared memory per lane behind the point pool
+  double* pair_measure;
+  int32_t* pair_nout;
+  double m;
+  int kept;
+  __device__ __forceinline__ void bind(double*) {}
+  __device__ __forceinline__ void begin(const int4&) {
+    m = 0.0;
+    kept = 0;
+  }
+  __device__ __forceinline__ void tet(const Tet&, double v1) {
+    m = m + v1;
+    ++kept;
+  }
+  __device__ __forceinline__ void end(int64_t p) {
+    pair_measure[p] = m;
+    pair_nout[p] = kept;
+  }
+  template <int BLOCK>
+  __device__ __forceinline__ void finish() {}
+};
+
+template <class Sink, int BLOCK, int BPS>
+__global__ void __launch_bounds__(BLOCK, BPS) k_clip_tets_ix(
     const int4* __restrict__ list, const unsigned long long* __restrict__ nlist, const double* __restrict__ coords_a,
-    const double* __restrict__ tol_a, const double* __restrict__ setup_b, double* pair_measure,
-    int32_t* pair_nout, unsigned long long* work) {
+    const double* __restrict__ tol_a, const double* __restrict__ setup_b, Sink sk, unsigned long long* work) {
   extern __shared__ double ix_mem[];
-  IxPool<kIxBlock> pool{ix_mem + threadIdx.x};
+  IxPool<BLOCK> pool{ix_mem + threadIdx.x};
+  sk.bind(ix_mem + 3 * kIxPoints * BLOCK + threadIdx.x);
   // pending tets: a 120-bit shift register of 20-bit index tuples (stk_hi:
   // stk_lo, newest in the low bits) and their planes, 2 bits each (stk_lv)
   unsigned long long stk_lo = 0, stk_hi = 0;
@@ -1765,8 +1794,8 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
   int64_t p = -1;
   const double* planes = setup_b;
   unsigned cur = 0;
-  double tol = 0.0, m = 0.0;
-  int L = 0, sp = 0, kept = 0;
+  double tol = 0.0;
+  int L = 0, sp = 0;
   // planes this pair clips at (bit L; the prefilter's no-op planes are
   // skipped) and the last of them
   unsigned act = 15u;
@@ -1785,15 +1814,23 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
       planes = setup_b + (int64_t)nrec.z * kSetup3;
       tol = ntol;
       cur = ix_pack(0, 1, 2, 3);
-      m = 0.0;
-      act = ~(unsigned)nrec.w & 15u;  // never 0: the prefilter settles those pairs
+      sk.begin(nrec);
+      act = ~(unsigned)nrec.w & 15u;  // never 0 unless Sink::kInside
       L = __ffs(act) - 1;
       lastL = 31 - __clz(act);
       sp = 0;
-      kept = 0;
       nstage = 0;
       stk_lo = stk_hi = 0;
       stk_lv = 0;
+      if (Sink::kInside && act == 0u) {
+        // A inside all four planes: the reference keeps A as its one tet
+        Tet o;
+        ix_gather(pool, cur, o);
+        double v1;
+        if (final_tet_keep(o, tol, v1)) sk.tet(o, v1);
+        sk.end(p);
+        p = -1;
+      }
     }
     {
       const bool want = nstage == 0 && !exhausted;
@@ -1841,10 +1878,7 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
           Tet o;
           ix_gather(pool, j == 0 ? c0 : (j == 1 ? c1 : c2), o);
           double v1;
-          if (final_tet_keep(o, tol, v1)) {
-            m = m + v1;
-            ++kept;
-          }
+          if (final_tet_keep(o, tol, v1)) sk.tet(o, v1);
         }
       }
       k = 0;
@@ -1876,10 +1910,10 @@ __global__ void __launch_bounds__(kIxBlock, kIxBlocksPerSm) k_clip_tets_ix(
       --sp;
       continue;
     }
-    pair_measure[p] = m;
-    pair_nout[p] = kept;
+    sk.end(p);
     p = -1;
   }
+  sk.template finish<BLOCK>();
 }
 
 size_t ix_smem_bytes() { return (size_t)kIxBlock * 3 * kIxPoints * sizeof(double); }
@@ -1928,7 +1962,7 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     if (ev_begin) cudaEventRecord(ev_begin, s);
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
     count_launch();
-    k_prefilter_tets<<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, tol_a,
+    k_prefilter_tets<true><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, tol_a,
                                                               setup_b, pair_measure, pair_nout, overflow_list, work,
                                                               faces_a, screen_b, n_dev);
     const int4* list = reinterpret_cast<const int4*>(overflow_list);
@@ -1938,8 +1972,8 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
       if (e != cudaSuccess) return e;
       list = bin->out;
     }
-    k_clip_tets_ix<<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
-        list, work, coords_a, tol_a, setup_b, pair_measure, pair_nout, work + 1);
+    k_clip_tets_ix<IxMeasureSink, kIxBlock, kIxBlocksPerSm><<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
+        list, work, coords_a, tol_a, setup_b, IxMeasureSink{pair_measure, pair_nout, 0.0, 0}, work + 1);
   }
   if (ev_end) cudaEventRecord(ev_end, s);
   return cudaGetLastError();
@@ -1954,8 +1988,12 @@ cudaError_t launch_reduce_pairs(int64_t npairs, const double* pair_measure, cons
   return cudaGetLastError();
 }
 
+cudaError_t init_p1_attributes();
+
 cudaError_t init_device_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(k_clip_tets_ix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
+  cudaError_t e = cudaFuncSetAttribute(k_clip_tets_ix<IxMeasureSink, kIxBlock, kIxBlocksPerSm>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
+  if (e == cudaSuccess) e = init_p1_attributes();
   if (e != cudaSuccess) return e;
   return init_sched_attributes(kSchedMaxWindow);
 }
@@ -2963,33 +3001,59 @@ cudaError_t launch_measure_explicit(int dim, int64_t n, const double* elems, dou
 // ======================================================================
 // K8: P1-P1 mixed mass matrix
 // ======================================================================
-// P1 basis on a triangle (test_parallel_p1_inner_product_2d.F90:206-229).
-__device__ __forceinline__ void p1_basis_2d(const double* cc, double x, double y, double f[3]) {
+// P1 basis on a triangle (test_parallel_p1_inner_product_2d.F90:206-229):
+// the inverse Jacobian (divided by the determinant entry by entry) depends
+// only on the element and is formed once per pair; each point then takes
+// the same products and sums as the reference.
+struct P1Fac2 {
+  double ox, oy, j11, j12, j21, j22;
+};
+
+__device__ __forceinline__ P1Fac2 p1_factor_2d(const double* cc) {
   const double e1x = cc[2] - cc[0], e1y = cc[3] - cc[1];
   const double e2x = cc[4] - cc[0], e2y = cc[5] - cc[1];
   double j11 = e2y, j12 = -e2x, j21 = -e1y, j22 = e1x;
   const double det = j11 * j22 - j12 * j21;
-  j11 = j11 / det;
-  j12 = j12 / det;
-  j21 = j21 / det;
-  j22 = j22 / det;
-  const double dx = x - cc[0], dy = y - cc[1];
-  f[1] = j11 * dx + j12 * dy;
-  f[2] = j21 * dx + j22 * dy;
+  return P1Fac2{cc[0], cc[1], j11 / det, j12 / det, j21 / det, j22 / det};
+}
+
+__device__ __forceinline__ void p1_apply_2d(const P1Fac2& F, double x, double y, double f[3]) {
+  const double dx = x - F.ox, dy = y - F.oy;
+  f[1] = F.j11 * dx + F.j12 * dy;
+  f[2] = F.j21 * dx + F.j22 * dy;
   f[0] = 1.0 - f[1] - f[2];
 }
 
-// P1 basis on a tetrahedron: Gaussian elimination with partial pivoting in
-// the order of test_parallel_p1_inner_product_3d.F90:215-250.
-__device__ __forceinline__ void p1_basis_3d(const double* cc, double x, double y, double z, double f[4]) {
-  double m[3][4];
-  const double xx[3] = {x, y, z};
+template <typename IDX>
+__device__ __forceinline__ int64_t node_of(const void* en, int64_t e, int loc, int k) {
+  return (int64_t)((const IDX*)en)[e * loc + k];
+}
+
+// P1 basis on a tetrahedron (test_parallel_p1_inner_product_3d.F90:215-250):
+// the local coordinates of point x solve [v1-v0 | v2-v0 | v3-v0] l = x - v0
+// by Gaussian elimination with partial pivoting on the augmented 3x4 matrix
+// (pivot search, row swap, pivot row divided by the pivot, rows below
+// reduced; then back substitution from the last row), f = (1 - l1 - l2 - l3,
+// l1, l2, l3).  The pivot choices, pivots and multipliers depend only on the
+// element's edge matrix, so p1_factor_3d runs that elimination on the three
+// matrix columns once per element and stores, at stride S: the origin v0
+// (3), the pivots (3), the forward multipliers of rows (1,0) (2,0) (2,1) and
+// the back-substitution multipliers of rows (1,2) (0,2) (0,1); it returns the
+// row swaps (row exchanged with row 0 in bits 0-1, with row 1 in bits 2-3).
+// p1_apply_3d applies to the point's right-hand side exactly the operations
+// the elimination applies to the augmented column, in the same order.
+constexpr int kP1Fac3 = 12;
+
+template <int S>
+__device__ __forceinline__ int p1_factor_3d(const double* cc, double* F) {
+  double m[3][3];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) m[r][c] = cc[3 * (c + 1) + r] - cc[r];
-    m[r][3] = xx[r] - cc[r];
+    F[r * S] = cc[r];
   }
+  int sw = 0, nl = 0;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     int j = i;
@@ -3000,48 +3064,154 @@ __device__ __forceinline__ void p1_basis_3d(const double* cc, double x, double y
         best = fabs(m[k][i]);
         j = k;
       }
-    // swap rows i and j (registers: select-based)
 #pragma unroll
     for (int k = i + 1; k < 3; ++k) {
       if (j == k) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < 3; ++c) {
           const double t = m[i][c];
           m[i][c] = m[k][c];
           m[k][c] = t;
         }
       }
     }
+    sw |= j << (2 * i);
     const double piv = m[i][i];
+    F[(3 + i) * S] = piv;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) m[i][c] = m[i][c] / piv;
+    for (int c = 0; c < 3; ++c) m[i][c] = m[i][c] / piv;
 #pragma unroll
     for (int k = i + 1; k < 3; ++k) {
       const double fk = m[k][i];
+      F[(6 + nl++) * S] = fk;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) m[k][c] = m[k][c] - fk * m[i][c];
+      for (int c = 0; c < 3; ++c) m[k][c] = m[k][c] - fk * m[i][c];
     }
   }
+  int nu = 0;
 #pragma unroll
   for (int i = 2; i >= 0; --i)
 #pragma unroll
     for (int k = i - 1; k >= 0; --k) {
       const double fk = m[k][i];
+      F[(9 + nu++) * S] = fk;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) m[k][c] = m[k][c] - fk * m[i][c];
+      for (int c = 0; c < 3; ++c) m[k][c] = m[k][c] - fk * m[i][c];
     }
-  f[1] = m[0][3];
-  f[2] = m[1][3];
-  f[3] = m[2][3];
+  return sw;
+}
+
+template <int S>
+__device__ __forceinline__ void p1_apply_3d(const double* F, int sw, double x, double y, double z, double f[4]) {
+  double r0 = x - F[0], r1 = y - F[S], r2 = z - F[2 * S];
+  const int j0 = sw & 3, j1 = (sw >> 2) & 3;
+  {
+    const double t0 = r0;
+    r0 = j0 == 1 ? r1 : (j0 == 2 ? r2 : r0);
+    r1 = j0 == 1 ? t0 : r1;
+    r2 = j0 == 2 ? t0 : r2;
+  }
+  r0 = r0 / F[3 * S];
+  r1 = r1 - F[6 * S] * r0;
+  r2 = r2 - F[7 * S] * r0;
+  {
+    const double t1 = r1;
+    r1 = j1 == 2 ? r2 : r1;
+    r2 = j1 == 2 ? t1 : r2;
+  }
+  r1 = r1 / F[4 * S];
+  r2 = r2 - F[8 * S] * r1;
+  r2 = r2 / F[5 * S];
+  r1 = r1 - F[9 * S] * r2;
+  r0 = r0 - F[10 * S] * r2;
+  r0 = r0 - F[11 * S] * r1;
+  f[1] = r0;
+  f[2] = r1;
+  f[3] = r2;
   f[0] = 1.0 - f[1] - f[2] - f[3];
 }
 
-template <typename IDX>
-__device__ __forceinline__ int64_t node_of(const void* en, int64_t e, int loc, int k) {
-  return (int64_t)((const IDX*)en)[e * loc + k];
-}
+// P1-P1 mixed mass block of a pair (test_parallel_p1_inner_product_3d.F90:
+// four-point rule, P1 bases of A and B by elimination at each point), per
+// kept output tet in the reference's order; at the end of the pair the block
+// is stored and u^T M v added to a compensated sum.  The per-element part of
+// both eliminations is done once per pair (p1_factor_3d) into the lane's
+// slice of shared memory behind the point pool (kLaneDoubles per lane).
+template <typename IDX, int BLOCK>
+struct IxP1Sink {
+  static constexpr bool kInside = true;
+  static constexpr int kLaneDoubles = 2 * kP1Fac3;
+  const double* coords_a;
+  const double* coords_b;
+  const void* en_a;
+  const void* en_b;
+  const double* u_a;
+  const double* v_b;
+  double* blocks;
+  Partial* partials;
+  double blk[16];
+  double* fac;  // this lane's factors: A's at fac, B's at fac + kP1Fac3 * BLOCK
+  int a, b, swa, swb;
+  double sum, err;
+  unsigned long long ni;
+  __device__ __forceinline__ void bind(double* lane_mem) { fac = lane_mem; }
+  __device__ __forceinline__ void begin(const int4& r) {
+    a = r.y;
+    b = r.z;
+    swa = p1_factor_3d<BLOCK>(coords_a + (int64_t)a * 12, fac);
+    swb = p1_factor_3d<BLOCK>(coords_b + (int64_t)b * 12, fac + kP1Fac3 * BLOCK);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) blk[j] = 0.0;
+  }
+  __device__ __forceinline__ void tet(const Tet& o, double v1) {
+    const double qa = 5.8541019662496852e-1, qb = 1.3819660112501050e-1;
+    const double w = 0.25 * v1;
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) {
+      double x = 0.0, y = 0.0, z = 0.0;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const double wv = v == qq ? qa : qb;
+        x = x + wv * o.x[v];
+        y = y + wv * o.y[v];
+        z = z + wv * o.z[v];
+      }
+      double fa[4], fb[4];
+      p1_apply_3d<BLOCK>(fac, swa, x, y, z, fa);
+      p1_apply_3d<BLOCK>(fac + kP1Fac3 * BLOCK, swb, x, y, z, fb);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) blk[r * 4 + c] += w * fa[r] * fb[c];
+    }
+  }
+  __device__ __forceinline__ void end(int64_t p) {
+    if (blocks) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) blocks[p * 16 + j] = blk[j];
+    }
+    if (u_a && v_b) {
+      double sv = 0.0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const double ur = u_a[node_of<IDX>(en_a, a, 4, r)];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) sv += ur * blk[r * 4 + c] * v_b[node_of<IDX>(en_b, b, 4, c)];
+      }
+      cs_add(sum, err, sv);
+    }
+    ++ni;
+  }
+  template <int NT>
+  __device__ __forceinline__ void finish() {
+    block_reduce_partial<NT>(sum, err, ni, 0ull, &partials[blockIdx.x]);
+  }
+};
 
-template <int DIM, typename IDX>
+
+// 2D: one pair per thread, clipped with the triangle clipper; per supermesh
+// triangle the degree-2 rule (three points), P1 bases of A and B, 3x3 block.
+template <typename IDX>
 __global__ void __launch_bounds__(128) k_p1_mass(int64_t npairs, const int32_t* __restrict__ pa,
                                                  const int32_t* __restrict__ pb,
                                                  const double* __restrict__ coords_a,
@@ -3051,7 +3221,6 @@ __global__ void __launch_bounds__(128) k_p1_mass(int64_t npairs, const int32_t* 
                                                  const void* en_b, const double* __restrict__ u_a,
                                                  const double* __restrict__ v_b, double* blocks,
                                                  Partial* partials) {
-  constexpr int LOC = DIM + 1;
   double sum = 0.0, err = 0.0;
   unsigned long long ni = 0;
   // each iteration loads the next one's pair indices (which stream from
@@ -3071,83 +3240,51 @@ __global__ void __launch_bounds__(128) k_p1_mass(int64_t npairs, const int32_t* 
       na = pa[i + stride];
       nb = pb[i + stride];
     }
-    const double* ca = coords_a + (int64_t)a * LOC * DIM;
-    const double* cb = coords_b + (int64_t)b * LOC * DIM;
-    double blk[LOC * LOC];
+    const double* ca = coords_a + (int64_t)a * 6;
+    double blk[9];
 #pragma unroll
-    for (int j = 0; j < LOC * LOC; ++j) blk[j] = 0.0;
-    if (DIM == 2) {
-      Lines L;
-      double tolb;
-      load_lines(setup_b + (int64_t)b * kSetup2, L, tolb);
-      const double tol = fmin(tol_a[a], tolb);
-      LocalPoly<kTriWideCap> p, q;
-      double m;
-      const double qp0 = 4.0 / 6.0, qp1 = 1.0 / 6.0;
-      clip_tri(ca[0], ca[1], ca[2], ca[3], ca[4], ca[5], L, tol, p, q, kTriWideCap, m,
-               [&](int, double x0, double y0, double x1, double y1, double x2, double y2) {
-                 const double meas = tri_area(x0, y0, x1, y1, x2, y2);
-                 const double w = (1.0 / 3.0) * meas;
+    for (int j = 0; j < 9; ++j) blk[j] = 0.0;
+    Lines L;
+    double tolb;
+    load_lines(setup_b + (int64_t)b * kSetup2, L, tolb);
+    const double tol = fmin(tol_a[a], tolb);
+    const P1Fac2 fa_ = p1_factor_2d(ca), fb_ = p1_factor_2d(coords_b + (int64_t)b * 6);
+    LocalPoly<kTriWideCap> p, q;
+    double m;
+    const double qp0 = 4.0 / 6.0, qp1 = 1.0 / 6.0;
+    clip_tri(ca[0], ca[1], ca[2], ca[3], ca[4], ca[5], L, tol, p, q, kTriWideCap, m,
+             [&](int, double x0, double y0, double x1, double y1, double x2, double y2) {
+               const double meas = tri_area(x0, y0, x1, y1, x2, y2);
+               const double w = (1.0 / 3.0) * meas;
 #pragma unroll
-                 for (int qq = 0; qq < 3; ++qq) {
-                   const double w0 = qq == 0 ? qp0 : qp1;
-                   const double w1 = qq == 1 ? qp0 : qp1;
-                   const double w2 = qq == 2 ? qp0 : qp1;
-                   const double x = (w0 * x0 + w1 * x1) + w2 * x2;
-                   const double y = (w0 * y0 + w1 * y1) + w2 * y2;
-                   double fa[3], fb[3];
-                   p1_basis_2d(ca, x, y, fa);
-                   p1_basis_2d(cb, x, y, fb);
+               for (int qq = 0; qq < 3; ++qq) {
+                 const double w0 = qq == 0 ? qp0 : qp1;
+                 const double w1 = qq == 1 ? qp0 : qp1;
+                 const double w2 = qq == 2 ? qp0 : qp1;
+                 const double x = (w0 * x0 + w1 * x1) + w2 * x2;
+                 const double y = (w0 * y0 + w1 * y1) + w2 * y2;
+                 double fa[3], fb[3];
+                 p1_apply_2d(fa_, x, y, fa);
+                 p1_apply_2d(fb_, x, y, fb);
 #pragma unroll
-                   for (int r = 0; r < 3; ++r)
+                 for (int r = 0; r < 3; ++r)
 #pragma unroll
-                     for (int c = 0; c < 3; ++c) blk[r * 3 + c] += w * fa[r] * fb[c];
-                 }
-               });
-    } else {
-      Tet t;
-      load_tet(ca, t);
-      const double* planes = setup_b + (int64_t)b * kSetup3;
-      const double tol = fmin(tol_a[a], planes[16]);
-      TetStackLocal stk;
-      const double qa = 5.8541019662496852e-1, qb = 1.3819660112501050e-1;
-      clip_tet_dfs(t, GlobalPlanes{planes}, tol, stk, [&](const Tet& o) {
-        const double meas = tet_volume_v1(o);
-        const double w = 0.25 * meas;
-#pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-          double xq[3];
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const double* comp = d == 0 ? o.x : (d == 1 ? o.y : o.z);
-            double s = 0.0;
-#pragma unroll
-            for (int v = 0; v < 4; ++v) s = s + (v == qq ? qa : qb) * comp[v];
-            xq[d] = s;
-          }
-          double fa[4], fb[4];
-          p1_basis_3d(ca, xq[0], xq[1], xq[2], fa);
-          p1_basis_3d(cb, xq[0], xq[1], xq[2], fb);
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) blk[r * 4 + c] += w * fa[r] * fb[c];
-        }
-      });
-    }
+                   for (int c = 0; c < 3; ++c) blk[r * 3 + c] += w * fa[r] * fb[c];
+               }
+             });
     if (blocks) {
 #pragma unroll
-      for (int j = 0; j < LOC * LOC; ++j) blocks[i * LOC * LOC + j] = blk[j];
+      for (int j = 0; j < 9; ++j) blocks[i * 9 + j] = blk[j];
     }
     if (u_a && v_b) {
-      double s = 0.0;
+      double sv = 0.0;
 #pragma unroll
-      for (int r = 0; r < LOC; ++r) {
-        const double ur = u_a[node_of<IDX>(en_a, a, LOC, r)];
+      for (int r = 0; r < 3; ++r) {
+        const double ur = u_a[node_of<IDX>(en_a, a, 3, r)];
 #pragma unroll
-        for (int c = 0; c < LOC; ++c) s += ur * blk[r * LOC + c] * v_b[node_of<IDX>(en_b, b, LOC, c)];
+        for (int c = 0; c < 3; ++c) sv += ur * blk[r * 3 + c] * v_b[node_of<IDX>(en_b, b, 3, c)];
       }
-      cs_add(sum, err, s);
+      cs_add(sum, err, sv);
     }
     ++ni;
   }
@@ -3287,24 +3424,75 @@ cudaError_t launch_p2_inner(int64_t npairs, const int32_t* pair_a, const int32_t
   return cudaGetLastError();
 }
 
-int p1_grid_blocks(int dim) { return sm_count() * (dim == 2 ? 4 : 2); }
+// 3D: the index clipper with the P1 sink, one block per SM.  The sink's
+// 4x4 block accumulator and the quadrature raise the register need to about
+// 250: 8 warps (2 per SM sub-partition) can hold them without spilling,
+// while 9-12 warps are capped at 168 registers by the sub-partitions'
+// register files and spill (pool: 256 x 480 B of shared memory).
+#ifndef LSM_IX_P1_BLOCK
+#define LSM_IX_P1_BLOCK 256
+#endif
+constexpr int kIxP1Block = LSM_IX_P1_BLOCK;
+
+size_t p1_smem_bytes() {
+  return (size_t)kIxP1Block * (3 * kIxPoints + IxP1Sink<int32_t, kIxP1Block>::kLaneDoubles) * sizeof(double);
+}
+
+int p1_grid_blocks(int dim) { return sm_count() * (dim == 2 ? 4 : 1); }
 
 cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                            const double* coords_a, const double* tol_a, const double* coords_b,
                            const double* setup_b, const void* enlist_a, const void* enlist_b,
                            int idx_bytes, const double* u_a, const double* v_b, double* blocks,
-                           Partial* partials, cudaStream_t s) {
+                           Partial* partials, cudaStream_t s, int32_t* survivors, unsigned long long* work,
+                           const double* faces_a, const double* screen_b) {
   const int g = p1_grid_blocks(dim);
+  if (dim == 2) {
+    count_launch();
+    if (idx_bytes == 4)
+      k_p1_mass<int32_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+    else
+      k_p1_mass<int64_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+    return cudaGetLastError();
+  }
+  // the early-out pass lists the pairs with output tets (blocks of the
+  // others stay zero), then the index clipper integrates their tets
+  cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
+  if (blocks && npairs > 0) cudaMemsetAsync(blocks, 0, sizeof(double) * 16 * npairs, s);
+  if (npairs > 0) {
+    count_launch();
+    k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, nullptr, pair_a, pair_b, coords_a,
+                                                                     tol_a, setup_b, nullptr, nullptr, survivors,
+                                                                     work, faces_a, screen_b, nullptr);
+  }
+  const int4* list = reinterpret_cast<const int4*>(survivors);
   count_launch();
-  if (dim == 2 && idx_bytes == 4)
-    k_p1_mass<2, int32_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
-  else if (dim == 2)
-    k_p1_mass<2, int64_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
-  else if (idx_bytes == 4)
-    k_p1_mass<3, int32_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
-  else
-    k_p1_mass<3, int64_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
+  if (idx_bytes == 4) {
+    using Sk = IxP1Sink<int32_t, kIxP1Block>;
+    Sk sk{coords_a, coords_b, enlist_a, enlist_b, u_a, v_b, blocks, partials};
+    sk.sum = sk.err = 0.0;
+    sk.ni = 0;
+    k_clip_tets_ix<Sk, kIxP1Block, 1><<<g, kIxP1Block, p1_smem_bytes(), s>>>(list, work, coords_a, tol_a, setup_b,
+                                                                            sk, work + 1);
+  } else {
+    using Sk = IxP1Sink<int64_t, kIxP1Block>;
+    Sk sk{coords_a, coords_b, enlist_a, enlist_b, u_a, v_b, blocks, partials};
+    sk.sum = sk.err = 0.0;
+    sk.ni = 0;
+    k_clip_tets_ix<Sk, kIxP1Block, 1><<<g, kIxP1Block, p1_smem_bytes(), s>>>(list, work, coords_a, tol_a, setup_b,
+                                                                            sk, work + 1);
+  }
   return cudaGetLastError();
+}
+
+cudaError_t init_p1_attributes() {
+  const int smem = (int)p1_smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(k_clip_tets_ix<IxP1Sink<int32_t, kIxP1Block>, kIxP1Block, 1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_clip_tets_ix<IxP1Sink<int64_t, kIxP1Block>, kIxP1Block, 1>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return e;
 }
 
 }  // namespace lsm

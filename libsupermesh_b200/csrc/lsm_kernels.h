@@ -226,11 +226,16 @@ cudaError_t launch_p2_inner(int64_t npairs, const int32_t* pair_a, const int32_t
                             int32_t* pair_n, cudaStream_t s);
 // bad = 1 if any of en[0..n) lies outside [0, limit).
 cudaError_t launch_check_index(int64_t n, const void* en, int idx_bytes, int64_t limit, int* bad, cudaStream_t s);
+// P1-P1 mixed mass: 2D clips every pair; 3D runs the exact early-out pass
+// (survivors: 4 ints per pair, work: two counters, faces_a / screen_b as for
+// launch_clip) and the index clipper with the quadrature on the survivors,
+// with blocks of the other pairs zero-filled.  partials: p1_grid_blocks(dim).
 cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                            const double* coords_a, const double* tol_a, const double* coords_b,
                            const double* setup_b, const void* enlist_a, const void* enlist_b,
                            int idx_bytes, const double* u_a, const double* v_b, double* blocks,
-                           Partial* partials, cudaStream_t s);
+                           Partial* partials, cudaStream_t s, int32_t* survivors, unsigned long long* work,
+                           const double* faces_a, const double* screen_b);
 int p1_grid_blocks(int dim);
 
 // ---- batched (many mesh pairs per launch) --------------------------------
