@@ -71,7 +71,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--kernel-only", action="store_true",
                    help="run only warm-up + timed steps of --op (for profiler launch lists and captures)")
-    p.add_argument("--op", choices=["supermesh", "p1_mass", "p2_inner"], default="supermesh",
+    p.add_argument("--op", choices=["supermesh", "p1_mass", "p2_inner", "pairs", "pairs_mixed"], default="supermesh",
                    help="with --kernel-only: the operation each step runs")
     p.add_argument("--schedule", type=int, default=0,
                    help="with --kernel-only: tet_schedule of the 3D narrow phase (1 needs the trained weights)")
@@ -413,11 +413,16 @@ def kernel_only(args, ctx, dim, A, B, tA, tB, step_device, timed, rank):
     run.  --op supermesh: the whole pipeline (with --schedule for 3D);
     p1_mass: the P1-P1 product u^T M v (u = x on A, v = y on B, device
     meshes and fields); p2_inner: the 2D P2 inner product of P1 fields
-    lifted to P2 (host arrays)."""
+    lifted to P2 (host arrays); pairs: the batched explicit-pair entry
+    (libsupermesh_gpu_intersect_pairs, device memory) on the workload's first
+    2^22 candidate pairs as element coordinates; pairs_mixed: the same pairs
+    with B's element replaced by its bounding box as a hexahedron (3D, tet-hex)
+    or quadrilateral (2D, tri-quad)."""
     import libsupermesh_b200 as lsm
     from libsupermesh_b200 import meshes as M
 
     sp = None
+    units = None  # element pairs per call, where the op has a fixed count
     if args.op == "supermesh":
         if args.schedule:
             from libsupermesh_b200 import scheduler
@@ -435,6 +440,35 @@ def kernel_only(args, ctx, dim, A, B, tA, tB, step_device, timed, rank):
 
         def fn():
             return ctx.p1_mass(tA, tB, du, dv, on_device=True, stream=sp)
+    elif args.op in ("pairs", "pairs_mixed"):
+        import torch
+
+        n_all = ctx.find_candidates(A, B)
+        ip, ind = ctx.get_candidates(len(A[1]), n_all)
+        n = min(n_all, 1 << 22)
+        rows = np.repeat(np.arange(len(ip) - 1), np.diff(ip))[:n]
+        ea = np.ascontiguousarray(A[0][A[1][rows]].reshape(n, -1))
+        eb = B[0][B[1][ind[:n]]]
+        kind = None
+        if args.op == "pairs_mixed":
+            lo, hi = eb.min(axis=1), eb.max(axis=1)
+            if dim == 3:  # Gmsh node order: bottom face 0-3, top face 4-7
+                corner = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                                   [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], dtype=np.float64)
+                kind = lsm.PAIR_TET_HEX
+            else:  # counter-clockwise
+                corner = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], dtype=np.float64)
+                kind = lsm.PAIR_TRI_QUAD
+            eb = lo[:, None, :] + corner[None] * (hi - lo)[:, None, :]
+        eb = np.ascontiguousarray(eb.reshape(n, -1))
+        dev = tA[0].device
+        da, db = torch.from_numpy(ea).to(dev), torch.from_numpy(eb).to(dev)
+        dm = torch.empty(n, dtype=torch.float64, device=dev)
+        dk = torch.empty(n, dtype=torch.int32, device=dev)
+        units = n
+
+        def fn():
+            return ctx.intersect_pairs_device(da, db, dm, dk, dim=dim, kind=kind, stream=sp)
     else:
         if dim != 2:
             raise SystemExit("--op p2_inner needs a 2D workload")
@@ -448,8 +482,11 @@ def kernel_only(args, ctx, dim, A, B, tA, tB, step_device, timed, rank):
     ms, _ = timed(fn, args.steps, args.warmup)
     lsm.set_option("tet_schedule", 0)
     if rank == 0:
-        print(json.dumps({"kernel_only": True, "workload": args.workload, "op": args.op, "schedule": args.schedule,
-                          "ms_per_step": ms / args.steps}), flush=True)
+        line = {"kernel_only": True, "workload": args.workload, "op": args.op, "schedule": args.schedule,
+                "ms_per_step": ms / args.steps}
+        if units:
+            line.update(pairs=units, pairs_per_s=units / (ms / args.steps * 1e-3))
+        print(json.dumps(line), flush=True)
 
 
 def drop_in_per_pair(ctx, dim, A, B, n_cand, n: int = 2000):

@@ -201,7 +201,10 @@ int libsupermesh_gpu_get_pair_results(lsm_gpu_context *ctx, double *measure,
 /* Batched form of the per-pair C API.  tri: a, b [n][3][2]; tet: a, b
  * [n][4][3].  measure[n] = sum of output simplex measures, n_out[n] = number
  * of output simplices; elems (optional) [n][22][3][2] or [n][81][4][3] in
- * the reference's output order.  With on_device = 1 and dim = 3, a and b
+ * the reference's output order (slots past a pair's n_out are left
+ * unspecified).  Tet batches of 2048 pairs or more run through per-pair
+ * setup, the exact early-out pass and the index clipper; smaller ones through
+ * a one-launch clipper (same results).  With on_device = 1 and dim = 3, a and b
  * must be 16-byte aligned (tetrahedra are read with 16-byte loads); other
  * pointers return LSM_ERROR_INVALID_ARGUMENT before any launch. */
 int libsupermesh_gpu_intersect_pairs(lsm_gpu_context *ctx, int dim, int64_t n,

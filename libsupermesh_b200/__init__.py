@@ -363,6 +363,21 @@ class Context:
                                                                     None))
         return m[:n], k[:n], (e[:n] if e is not None else None)
 
+    def intersect_pairs_device(self, a, b, measure, n_out, elems=None, dim: int = 3, kind: int | None = None,
+                               stream: int | None = None):
+        """Explicit element pairs in device memory (CUDA tensors): simplex
+        pairs of dimension dim (kind None) or a mixed kind (PAIR_*); measure
+        [n] f64, n_out [n] int32 and elems (optional) are written on the
+        stream; nothing is copied to the host."""
+        n = int(measure.shape[0])
+        if kind is None:
+            st = self.lib.libsupermesh_gpu_intersect_pairs(self._h, dim, n, _ptr(a), _ptr(b), _ptr(measure),
+                                                           _ptr(n_out), _ptr(elems), 1, stream)
+        else:
+            st = self.lib.libsupermesh_gpu_intersect_pairs_mixed(self._h, kind, n, _ptr(a), _ptr(b), _ptr(measure),
+                                                                 _ptr(n_out), _ptr(elems), 1, stream)
+        self._check(st)
+
     def p1_mass(self, mesh_a, mesh_b, u_a=None, v_b=None, want_blocks: bool = False,
                 on_device: bool = False, stream: int | None = None):
         """Returns (u^T M v or None, blocks or None).  Host meshes and fields,

@@ -78,6 +78,7 @@ struct Ctx {
   DevBuf p1_list;  // survivors of the P1 pass's early-out (kept apart from the narrow phase's)
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
+  DevBuf x_setup, x_tol, x_iota, x_faces, x_screen, x_list;  // explicit tet pairs through the early-out pass
   DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand, bt_indptr;
   // host meshes of a batch staged on the device, one set per dimension (the
   // 3D set is copied on the side stream while the 2D group computes)
@@ -261,7 +262,8 @@ void fini_ctx(Ctx* c) {
                    &c->bvh_work, &c->bvh_leaf, &c->counts, &c->offsets, &c->scan_tmp, &c->pair_a,
                    &c->pair_b, &c->i64_tmp, &c->pair_measure, &c->pair_nout, &c->partials,
                    &c->ovf_list, &c->p1_list, &c->misc, &c->elem_measure, &c->totals, &c->x_a, &c->x_b, &c->x_measure,
-                   &c->x_nout, &c->x_elems, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
+                   &c->x_nout, &c->x_elems, &c->x_setup, &c->x_tol, &c->x_iota, &c->x_faces, &c->x_screen,
+                   &c->x_list, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
                    &c->bt_ncand, &c->bt_stage_pa[0], &c->bt_stage_ea[0], &c->bt_stage_pb[0],
                    &c->bt_stage_eb[0], &c->bt_stage_pa[1], &c->bt_stage_ea[1], &c->bt_stage_pb[1],
@@ -345,6 +347,10 @@ MeshDev upload(Ctx* c, const lsm_gpu_mesh* m, int on_device, DevBuf& pos, DevBuf
 }
 
 int* bad_flag(Ctx* c) { return ensure<int>(c, c->misc, 64); }
+
+// Explicit tet pair batches of at least this many pairs run through the
+// early-out pass and the index clipper (work counters: misc ints 20-23).
+constexpr int64_t kPairsPipelineMin = 2048;
 
 // P1 mass pass (3D): its survivor list and two counters (misc ints 16-19)
 int32_t* p1_survivors(Ctx* c, int dim, int64_t nnz) {
@@ -1827,7 +1833,28 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context* ctx, int dim, int64_t n, c
       dn = n_out ? ensure<int32_t>(c, c->x_nout, n) : nullptr;
       de = elems ? ensure<double>(c, c->x_elems, n * cap * per) : nullptr;
     }
-    CU(lsm::launch_pairs_explicit(dim, n, da, db, dm, dn, de, s));
+    if (dim == 3 && n >= kPairsPipelineMin) {
+      // large batches: per-pair setup, the exact early-outs and the index
+      // clipper (one launch per stage); small ones stay on the one-launch
+      // register clipper below (identical results)
+      double* setup = ensure<double>(c, c->x_setup, n * lsm::kSetup3);
+      double* tol = ensure<double>(c, c->x_tol, n);
+      int32_t* iota = ensure<int32_t>(c, c->x_iota, n);
+      double* faces = g_tet_screen ? ensure<double>(c, c->x_faces, n * lsm::kScreen3) : nullptr;
+      double* screen = g_tet_screen ? ensure<double>(c, c->x_screen, n * lsm::kScreen3) : nullptr;
+      int32_t* list = ensure<int32_t>(c, c->x_list, 4 * n);
+      double* pm = dm ? dm : ensure<double>(c, c->x_measure, n);
+      int32_t* pn = dn ? dn : ensure<int32_t>(c, c->x_nout, n);
+      unsigned long long* work = reinterpret_cast<unsigned long long*>(bad_flag(c) + 20);
+      CU(lsm::launch_setup_pairs3(n, da, db, setup, tol, iota, faces, screen, s));
+      if (de)
+        CU(lsm::launch_clip_elems(n, iota, da, tol, setup, pm, pn, de, list, work, faces, screen, s));
+      else
+        CU(lsm::launch_clip(3, n, iota, iota, da, tol, setup, pm, pn, list, nullptr, work, s, nullptr, nullptr,
+                            nullptr, faces, screen));
+    } else {
+      CU(lsm::launch_pairs_explicit(dim, n, da, db, dm, dn, de, s));
+    }
     if (!on_device) {
       if (measure) CU(cudaMemcpyAsync(measure, dm, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
       if (n_out) CU(cudaMemcpyAsync(n_out, dn, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));

@@ -1488,9 +1488,10 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 // which is settled here (volume test and measure as in the clipper).
 // Survivors are written as {pair, a, b, no-op mask} so that the clipper
 // gets the element numbers and the planes to skip in one load.
-// kSettle false (the P1 mass pass): nothing is written for rejected pairs
-// (their results are zero-filled by the caller) and pairs with all four
-// planes no-op are listed too, for the clipper to integrate A itself.
+// kSettle false (the P1 mass pass, explicit pairs with output tets): pairs
+// with all four planes no-op are listed too, for the clipper to emit A
+// itself; rejected pairs get measure 0 and count 0 where pair_measure is
+// given (the P1 pass passes none and zero-fills its blocks).
 #ifndef LSM_PREFILTER_BPS
 #define LSM_PREFILTER_BPS 2
 #endif
@@ -1583,6 +1584,10 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
       }
       if (!kSettle) {
         live = !reject;
+        if (reject && pair_measure) {
+          pair_measure[i] = 0.0;
+          pair_nout[i] = 0;
+        }
       } else if (reject) {
         pair_measure[i] = 0.0;
         pair_nout[i] = 0;
@@ -1766,6 +1771,45 @@ struct IxMeasureSink {
   __device__ __forceinline__ void finish() {}
 };
 
+// Explicit pairs with their output tets: elems [n][81][4][3] in the
+// reference's order (tets beyond 81 are counted, not stored), measure and
+// count per pair.  The list includes pairs with every plane a no-op.
+struct IxElemSink {
+  static constexpr bool kInside = true;
+  static constexpr int kLaneDoubles = 0;
+  double* pair_measure;
+  int32_t* pair_nout;
+  double* elems;
+  double m;
+  int kept;
+  int pid;
+  __device__ __forceinline__ void bind(double*) {}
+  __device__ __forceinline__ void begin(const int4& r) {
+    m = 0.0;
+    kept = 0;
+    pid = r.x;
+  }
+  __device__ __forceinline__ void tet(const Tet& o, double v1) {
+    if (kept < 81) {
+      double2* e = reinterpret_cast<double2*>(elems + ((int64_t)pid * 81 + kept) * 12);
+      e[0] = make_double2(o.x[0], o.y[0]);
+      e[1] = make_double2(o.z[0], o.x[1]);
+      e[2] = make_double2(o.y[1], o.z[1]);
+      e[3] = make_double2(o.x[2], o.y[2]);
+      e[4] = make_double2(o.z[2], o.x[3]);
+      e[5] = make_double2(o.y[3], o.z[3]);
+    }
+    m = m + v1;
+    ++kept;
+  }
+  __device__ __forceinline__ void end(int64_t p) {
+    pair_measure[p] = m;
+    pair_nout[p] = kept;
+  }
+  template <int NT>
+  __device__ __forceinline__ void finish() {}
+};
+
 template <class Sink, int BLOCK, int BPS>
 __global__ void __launch_bounds__(BLOCK, BPS) k_clip_tets_ix(
     const int4* __restrict__ list, const unsigned long long* __restrict__ nlist, const double* __restrict__ coords_a,
@@ -1918,6 +1962,67 @@ __global__ void __launch_bounds__(BLOCK, BPS) k_clip_tets_ix(
 
 size_t ix_smem_bytes() { return (size_t)kIxBlock * 3 * kIxPoints * sizeof(double); }
 
+// Per-pair setup of explicit tetrahedron pairs (the prep kernel's work for
+// one-element meshes): B's planes and tolerance (setup row), A's tolerance,
+// identity pair indices and, optionally, the rows of the second early-out
+// (A's face planes, B's screen row).
+__global__ void k_setup_pairs3(int64_t n, const double* __restrict__ tet_a, const double* __restrict__ tet_b,
+                               double* setup, double* tol_a, int32_t* iota, double* faces_a, double* screen_b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    Tet a, b;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      a.x[k] = tet_a[12 * i + 3 * k];
+      a.y[k] = tet_a[12 * i + 3 * k + 1];
+      a.z[k] = tet_a[12 * i + 3 * k + 2];
+      b.x[k] = tet_b[12 * i + 3 * k];
+      b.y[k] = tet_b[12 * i + 3 * k + 1];
+      b.z[k] = tet_b[12 * i + 3 * k + 2];
+    }
+    Planes P;
+    tet_planes(b, P);
+    double* o = setup + i * kSetup3;
+#pragma unroll
+    for (int L = 0; L < 4; ++L) {
+      o[4 * L + 0] = P.nx[L];
+      o[4 * L + 1] = P.ny[L];
+      o[4 * L + 2] = P.nz[L];
+      o[4 * L + 3] = P.c[L];
+    }
+    o[16] = 10.0 * spacing(tet_volume_v4(b));
+    o[17] = 0.0;
+    o[18] = 0.0;
+    o[19] = 0.0;
+    tol_a[i] = 10.0 * spacing(tet_volume_v4(a));
+    iota[i] = (int32_t)i;
+    if (screen_b) tet_screen_b(b, P, screen_b + i * kScreen3);
+    if (faces_a) tet_faces_screen(a, faces_a + i * kScreen3);
+  }
+}
+
+cudaError_t launch_setup_pairs3(int64_t n, const double* tet_a, const double* tet_b, double* setup, double* tol_a,
+                                int32_t* iota, double* faces_a, double* screen_b, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launch();
+  k_setup_pairs3<<<grid_for(n, 256, 8), 256, 0, s>>>(n, tet_a, tet_b, setup, tol_a, iota, faces_a, screen_b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_clip_elems(int64_t n, const int32_t* iota, const double* tet_a, const double* tol_a,
+                              const double* setup, double* measure, int32_t* nout, double* elems,
+                              int32_t* survivors, unsigned long long* work, const double* faces_a,
+                              const double* screen_b, cudaStream_t s) {
+  cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
+  if (n <= 0) return cudaGetLastError();
+  count_launch();
+  k_prefilter_tets<false><<<grid_for(n, 256, 8), 256, 0, s>>>(n, nullptr, iota, iota, tet_a, tol_a, setup, measure,
+                                                              nout, survivors, work, faces_a, screen_b, nullptr);
+  count_launch();
+  k_clip_tets_ix<IxElemSink, kIxBlock, kIxBlocksPerSm><<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
+      reinterpret_cast<const int4*>(survivors), work, tet_a, tol_a, setup, IxElemSink{measure, nout, elems}, work + 1);
+  return cudaGetLastError();
+}
+
 
 
 
@@ -1993,6 +2098,9 @@ cudaError_t init_p1_attributes();
 cudaError_t init_device_attributes() {
   cudaError_t e = cudaFuncSetAttribute(k_clip_tets_ix<IxMeasureSink, kIxBlock, kIxBlocksPerSm>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_clip_tets_ix<IxElemSink, kIxBlock, kIxBlocksPerSm>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
   if (e == cudaSuccess) e = init_p1_attributes();
   if (e != cudaSuccess) return e;
   return init_sched_attributes(kSchedMaxWindow);

@@ -182,6 +182,18 @@ cudaError_t launch_i32_to_i64(int64_t n, const int32_t* in, int64_t* out, cudaSt
 // Single-pair style batched intersections over explicit element arrays
 // (tri: [n][3][2]; tet: [n][4][3]).  out_elems optional ([n][22][3][2] or
 // [n][81][4][3]).
+// Explicit tetrahedron pairs through the early-out pass and the index
+// clipper: per-pair setup (setup [n][kSetup3], tol_a [n], iota [n]; faces_a /
+// screen_b [n][kScreen3] optional, for the second early-out), then, for
+// measures and counts, launch_clip(3, n, iota, iota, tet_a, ...), or, with
+// the output tets, launch_clip_elems (elems [n][81][4][3]; survivors: 4 ints
+// per pair; work: two counters).  tet_a must be 16-byte aligned.
+cudaError_t launch_setup_pairs3(int64_t n, const double* tet_a, const double* tet_b, double* setup, double* tol_a,
+                                int32_t* iota, double* faces_a, double* screen_b, cudaStream_t s);
+cudaError_t launch_clip_elems(int64_t n, const int32_t* iota, const double* tet_a, const double* tol_a,
+                              const double* setup, double* measure, int32_t* nout, double* elems,
+                              int32_t* survivors, unsigned long long* work, const double* faces_a,
+                              const double* screen_b, cudaStream_t s);
 cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const double* b,
                                   double* measure, int32_t* nout, double* out_elems,
                                   cudaStream_t s);

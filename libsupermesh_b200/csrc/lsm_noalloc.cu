@@ -52,41 +52,6 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 std::mutex g_mu;
 void* g_addr[64] = {};
 
-// Per-pair setup of an explicit pair list: B's clipping planes and
-// tolerance (exactly as the mesh path's prep kernel computes them), A's
-// tolerance, and the identity pair indices the clipper reads.
-__global__ void k_setup_pairs(int64_t n, const double* __restrict__ tet_a, const double* __restrict__ tet_b,
-                              double* setup, double* tol_a, int32_t* iota) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    lsm::Tet a, b;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      a.x[k] = tet_a[12 * i + 3 * k];
-      a.y[k] = tet_a[12 * i + 3 * k + 1];
-      a.z[k] = tet_a[12 * i + 3 * k + 2];
-      b.x[k] = tet_b[12 * i + 3 * k];
-      b.y[k] = tet_b[12 * i + 3 * k + 1];
-      b.z[k] = tet_b[12 * i + 3 * k + 2];
-    }
-    lsm::Planes P;
-    lsm::tet_planes(b, P);
-    double* o = setup + i * lsm::kSetup3;
-#pragma unroll
-    for (int L = 0; L < 4; ++L) {
-      o[4 * L + 0] = P.nx[L];
-      o[4 * L + 1] = P.ny[L];
-      o[4 * L + 2] = P.nz[L];
-      o[4 * L + 3] = P.c[L];
-    }
-    o[16] = 10.0 * lsm::spacing(lsm::tet_volume_v4(b));
-    o[17] = 0.0;
-    o[18] = 0.0;
-    o[19] = 0.0;
-    tol_a[i] = 10.0 * lsm::spacing(lsm::tet_volume_v4(a));
-    iota[i] = (int32_t)i;
-  }
-}
-
 int scratch_address(void** out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return LSM_ERROR_CUDA;
@@ -140,9 +105,9 @@ extern "C" int libsupermesh_gpu_intersect_tets_noalloc(int64_t n, const double* 
   lsm::Partial* partials = reinterpret_cast<lsm::Partial*>(b + kOffPartials);
   lsm::Partial* tot = reinterpret_cast<lsm::Partial*>(b + kOffTotal);
   if (n > 0) {
-    const int blocks = (int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184);
-    k_setup_pairs<<<blocks, 256, 0, s>>>(n, tet_a, tet_b, setup, tol, iota);
-    if (cudaPeekAtLastError() != cudaSuccess) return LSM_ERROR_CUDA;
+    // B's planes and tolerance, A's tolerance and the identity pair indices
+    if (lsm::launch_setup_pairs3(n, tet_a, tet_b, setup, tol, iota, nullptr, nullptr, s) != cudaSuccess)
+      return LSM_ERROR_CUDA;
     // launch_clip clears the two work counters (survivors, progress) first
     if (lsm::launch_clip(3, n, iota, iota, tet_a, tol, setup, measure, n_out, list, nullptr, work, s) !=
         cudaSuccess)

@@ -300,3 +300,28 @@ def test_mixed_reference_known_answers(gpu_ctx, oracle_mod, ref_meshes, kind, na
     fn = getattr(oracle_mod, _ORACLE_FN[kind])
     for i in range(len(m)):
         assert k[i] == len(fn(s[i], q[i]))
+
+
+def test_device_resident_pairs_equal_host_pairs(gpu_ctx):
+    """The explicit-pair entries with device arrays (on_device = 1, outputs
+    left in device memory) give the host call's measures and counts, simplex
+    and mixed kinds."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(12)
+    n = 4000
+    cases = [(3, None, rng.random((n, 4, 3)), rng.random((n, 4, 3))),
+             (2, None, rng.random((n, 3, 2)), rng.random((n, 3, 2))),
+             (3, lsm.PAIR_TET_HEX, rng.random((n, 4, 3)), _random_hexes(rng, n)),
+             (2, lsm.PAIR_TRI_QUAD, rng.random((n, 3, 2)), _random_quads(rng, n))]
+    for dim, kind, a, b in cases:
+        if kind is None:
+            m, k, _ = gpu_ctx.intersect_pairs(dim, a, b)
+        else:
+            m, k, _ = gpu_ctx.intersect_pairs_mixed(kind, a, b)
+        da = torch.from_numpy(a.reshape(n, -1)).cuda()
+        db = torch.from_numpy(b.reshape(n, -1)).cuda()
+        dm = torch.empty(n, dtype=torch.float64, device="cuda")
+        dk = torch.empty(n, dtype=torch.int32, device="cuda")
+        gpu_ctx.intersect_pairs_device(da, db, dm, dk, dim=dim, kind=kind)
+        torch.cuda.synchronize()
+        assert np.array_equal(dm.cpu().numpy(), m) and np.array_equal(dk.cpu().numpy(), k), (dim, kind)

@@ -367,6 +367,46 @@ def test_intersect_pairs_bitexact(gpu_ctx, oracle_mod, dim):
         assert m[i] == meas
 
 
+def test_intersect_pairs_large_batch_bitexact(gpu_ctx, oracle_mod):
+    """Tet pair batches large enough for the early-out pass + index clipper
+    (the small ones use the one-launch clipper): output tets, counts and
+    measures bit-identical to the oracle and to small batches of the same
+    pairs, with the output tets requested and without, the second early-out
+    on and off.  The pairs include identical and shared-vertex pairs, A well
+    inside B (every plane a no-op), B inside A and far-apart pairs."""
+    a, b = _random_pairs(3, 3200, 31)
+    c = a.mean(axis=1, keepdims=True)
+    b[400:600] = c[400:600] + 3.0 * (a[400:600] - c[400:600])  # A inside B
+    b[600:800] = c[600:800] + 0.2 * (a[600:800] - c[600:800])  # B inside A
+    b[800:1000] += 2.0  # far apart
+    b[1000:1100] = a[1000:1100, ::-1]  # identical, vertices reversed
+    m, k, e = gpu_ctx.intersect_pairs(3, a, b, want_elems=True)
+    for i in range(len(a)):
+        ref = oracle_mod.intersect_tets(a[i], b[i])
+        assert k[i] == len(ref), i
+        assert np.array_equal(e[i, : k[i]], ref), i
+        meas = 0.0
+        for o in ref:
+            meas += oracle_mod.tetrahedron_volume(o)
+        assert m[i] == meas, i
+    assert (k[400:600] == 1).all() and (k[800:1000] == 0).all()
+    m1, k1, _ = gpu_ctx.intersect_pairs(3, a, b)
+    assert np.array_equal(m1, m) and np.array_equal(k1, k)
+    def same_outputs(m2, k2, e2):
+        # slots past a pair's count are unspecified
+        assert np.array_equal(m2, m) and np.array_equal(k2, k)
+        for i in range(len(a)):
+            assert np.array_equal(e2[i, : k[i]], e[i, : k[i]]), i
+
+    small = [gpu_ctx.intersect_pairs(3, a[j:j + 800], b[j:j + 800], want_elems=True) for j in range(0, len(a), 800)]
+    same_outputs(*(np.concatenate([x[q] for x in small]) for q in range(3)))
+    lsm.set_option("tet_screen", 0)
+    try:
+        same_outputs(*gpu_ctx.intersect_pairs(3, a, b, want_elems=True))
+    finally:
+        lsm.set_option("tet_screen", 1)
+
+
 def test_legacy_single_pair_entries(oracle_mod):
     a, b = _random_pairs(2, 16, 3)
     for i in range(len(a)):
