@@ -720,6 +720,7 @@ def run_ours(args, world, rank, local):
         line["cpu_baseline"] = cpu
         line["drop_in_per_pair"] = drop_in_per_pair(ctx, dim, A, B, n_cand)
         line["p1_mass"] = p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush)
+        line["supermesh_elements"] = elements_timing(ctx, dim, tA, tB, n_cand, stream, flush)
         print(json.dumps(line), flush=True)
     ctx.close()
 
@@ -812,6 +813,50 @@ def p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush):
             "e2e_ms": ms_e2e, "e2e_pairs_per_s": n_cand / (ms_e2e * 1e-3),
             "timing": "CUDA events; device-resident meshes and fields, and (e2e) pinned host meshes and "
                       "fields with their copies"}
+
+
+def elements_timing(ctx, dim, tA, tB, n_cand, stream, flush):
+    """The supermesh's simplices themselves (libsupermesh_gpu_supermesh_elements:
+    search, counting narrow phase, offsets, a second clipping pass writing
+    every output simplex with its parents), device-resident meshes and
+    outputs, reported beside the main metric.  CUDA events on the stream, L2
+    flushed before each call, median of 5 after 2 warm-up calls."""
+    import torch
+
+    import libsupermesh_b200 as lsm
+
+    sp = stream.cuda_stream
+    probe = {}
+    try:
+        ctx.supermesh_elements_device(tA, tB, probe, stream=sp)
+    except lsm.LsmError as e:
+        if e.status != 3:
+            raise
+    nc, ne = probe["n_candidates"], probe["n_elements"]
+    per = (3, 2) if dim == 2 else (4, 3)
+    dev = tA[0].device
+    out = {"elem_offset": torch.empty(nc + 1, dtype=torch.int64, device=dev),
+           "elems": torch.empty((max(ne, 1),) + per, dtype=torch.float64, device=dev),
+           "parent_a": torch.empty(max(ne, 1), dtype=torch.int64, device=dev),
+           "parent_b": torch.empty(max(ne, 1), dtype=torch.int64, device=dev),
+           "cand_capacity": nc, "elem_capacity": ne}
+    for _ in range(2):
+        ctx.supermesh_elements_device(tA, tB, out, stream=sp)
+    ms = []
+    for _ in range(5):
+        flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.supermesh_elements_device(tA, tB, out, stream=sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = float(np.median(ms))
+    nbytes = (nc + 1) * 8 + ne * (8 * per[0] * per[1] + 16)
+    del out
+    return {"ms": t, "n_elements": ne, "elements_per_s": ne / (t * 1e-3), "pairs_per_s": n_cand / (t * 1e-3),
+            "output_bytes": nbytes,
+            "timing": "CUDA events; device-resident meshes and outputs (simplices, per-candidate offsets, parents)"}
 
 
 def main():

@@ -179,6 +179,37 @@ int libsupermesh_gpu_supermesh_out(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
                                    const lsm_gpu_mesh *b, int on_device, lsm_gpu_pair_out *out,
                                    lsm_gpu_stats *stats, void *stream);
 
+/* The supermesh itself: every output simplex of every candidate pair of A
+ * and B (what one intersect_tris_real / intersect_tets_real call per
+ * candidate returns, C_bindings.F90:152-174), candidates in the get_output
+ * CSR order and, within a pair, the reference's output order.
+ *   elem_offset  [cand_capacity + 1] (optional): the simplices of candidate k
+ *                are elems[elem_offset[k] .. elem_offset[k+1]-1]
+ *   elems        [elem_capacity][3][2] (triangles) or [elem_capacity][4][3]
+ *                (tets); device arrays 16-byte aligned
+ *   parent_a, parent_b [elem_capacity] (optional): 0-based A and B element of
+ *                each simplex
+ *   n_candidates, n_elements  set by the call
+ * Simplex meshes only.  A counting pass (the narrow phase) sizes the output,
+ * a second pass writes it.  If the candidates do not fit cand_capacity
+ * (with elem_offset given) or the simplices elem_capacity, the call sets both
+ * counts and the stats, writes nothing else and returns LSM_ERROR_CAPACITY;
+ * a retry with those capacities succeeds. */
+typedef struct {
+  int64_t *elem_offset;
+  double *elems;
+  int64_t *parent_a;
+  int64_t *parent_b;
+  int64_t cand_capacity;
+  int64_t elem_capacity;
+  int64_t n_candidates;
+  int64_t n_elements;
+} lsm_gpu_elem_out;
+int libsupermesh_gpu_supermesh_elements(lsm_gpu_context *ctx, const lsm_gpu_mesh *a,
+                                        const lsm_gpu_mesh *b, int on_device,
+                                        lsm_gpu_elem_out *out, lsm_gpu_stats *stats,
+                                        void *stream);
+
 /* Narrow phase alone: intersect and measure every candidate of the last
  * libsupermesh_gpu_find_candidates / libsupermesh_gpu_supermesh call on
  * this context (simplex meshes), as libsupermesh_gpu_supermesh does after

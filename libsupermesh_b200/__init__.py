@@ -93,6 +93,19 @@ class PairOut(ctypes.Structure):
     ]
 
 
+class ElemOut(ctypes.Structure):
+    _fields_ = [
+        ("elem_offset", ctypes.c_void_p),
+        ("elems", ctypes.c_void_p),
+        ("parent_a", ctypes.c_void_p),
+        ("parent_b", ctypes.c_void_p),
+        ("cand_capacity", ctypes.c_int64),
+        ("elem_capacity", ctypes.c_int64),
+        ("n_candidates", ctypes.c_int64),
+        ("n_elements", ctypes.c_int64),
+    ]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("n_candidates", ctypes.c_int64),
@@ -147,6 +160,9 @@ def load() -> ctypes.CDLL:
     L.libsupermesh_gpu_supermesh_out.argtypes = [vp, mp, mp, ctypes.c_int, ctypes.POINTER(PairOut),
                                                  ctypes.POINTER(Stats), vp]
     L.libsupermesh_gpu_supermesh_out.restype = ctypes.c_int
+    L.libsupermesh_gpu_supermesh_elements.argtypes = [vp, mp, mp, ctypes.c_int, ctypes.POINTER(ElemOut),
+                                                      ctypes.POINTER(Stats), vp]
+    L.libsupermesh_gpu_supermesh_elements.restype = ctypes.c_int
     L.libsupermesh_gpu_clip_candidates_ordered.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(Stats), vp]
     L.libsupermesh_gpu_clip_candidates_ordered.restype = ctypes.c_int
     L.libsupermesh_gpu_intersect_pairs.argtypes = [vp, ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp, vp,
@@ -293,6 +309,45 @@ class Context:
                                                             int(on_device), ctypes.byref(o), ctypes.byref(st),
                                                             stream))
         return st, o.n_candidates
+
+    def supermesh_elements(self, mesh_a, mesh_b, parents: bool = True, stream: int | None = None):
+        """The supermesh's simplices (libsupermesh_gpu_supermesh_elements),
+        host meshes: returns (Stats, elem_offset [n_candidates + 1], elems
+        [n][3][2] or [n][4][3], parent_a, parent_b or None).  A first call
+        with no capacity reads the counts; the second fills the arrays."""
+        ma, mb = _mesh(*mesh_a, False), _mesh(*mesh_b, False)
+        dim = ma.dim
+        st = Stats()
+        o = ElemOut(None, None, None, None, 0, 0, 0, 0)
+        r = self.lib.libsupermesh_gpu_supermesh_elements(self._h, ctypes.byref(ma), ctypes.byref(mb), 0,
+                                                         ctypes.byref(o), ctypes.byref(st), stream)
+        if r not in (0, 3):
+            self._check(r)
+        nc, ne = o.n_candidates, o.n_elements
+        off = np.zeros(nc + 1, dtype=np.int64)
+        el = np.zeros((max(ne, 1), 3, 2) if dim == 2 else (max(ne, 1), 4, 3))
+        pa = np.zeros(max(ne, 1), dtype=np.int64) if parents else None
+        pb = np.zeros(max(ne, 1), dtype=np.int64) if parents else None
+        o = ElemOut(_ptr(off), _ptr(el), _ptr(pa), _ptr(pb), nc, ne, 0, 0)
+        self._check(self.lib.libsupermesh_gpu_supermesh_elements(self._h, ctypes.byref(ma), ctypes.byref(mb), 0,
+                                                                 ctypes.byref(o), ctypes.byref(st), stream))
+        return st, off, el[:ne], (pa[:ne] if parents else None), (pb[:ne] if parents else None)
+
+    def supermesh_elements_device(self, mesh_a, mesh_b, out: dict, stream: int | None = None):
+        """Device-resident form: meshes and out's arrays (elem_offset, elems,
+        parent_a, parent_b; CUDA tensors) in device memory, with
+        cand_capacity and elem_capacity.  Returns (Stats, n_candidates,
+        n_elements); raises LsmError (status 3) when the arrays are too small."""
+        ma, mb = _mesh(*mesh_a, True), _mesh(*mesh_b, True)
+        o = ElemOut(_ptr(out.get("elem_offset")), _ptr(out.get("elems")), _ptr(out.get("parent_a")),
+                    _ptr(out.get("parent_b")), int(out.get("cand_capacity", 0)), int(out.get("elem_capacity", 0)),
+                    0, 0)
+        st = Stats()
+        r = self.lib.libsupermesh_gpu_supermesh_elements(self._h, ctypes.byref(ma), ctypes.byref(mb), 1,
+                                                         ctypes.byref(o), ctypes.byref(st), stream)
+        out["n_candidates"], out["n_elements"] = o.n_candidates, o.n_elements
+        self._check(r)
+        return st, o.n_candidates, o.n_elements
 
     def clip_candidates(self, stream: int | None = None) -> Stats:
         """Re-run the narrow phase over the last candidate set."""

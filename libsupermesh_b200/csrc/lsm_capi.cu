@@ -79,6 +79,7 @@ struct Ctx {
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
   DevBuf x_setup, x_tol, x_iota, x_faces, x_screen, x_list;  // explicit tet pairs through the early-out pass
+  DevBuf elem_off, x_pa, x_pb;  // supermesh elements: per-pair offsets, parents
   DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand, bt_indptr;
   // host meshes of a batch staged on the device, one set per dimension (the
   // 3D set is copied on the side stream while the 2D group computes)
@@ -263,7 +264,7 @@ void fini_ctx(Ctx* c) {
                    &c->pair_b, &c->i64_tmp, &c->pair_measure, &c->pair_nout, &c->partials,
                    &c->ovf_list, &c->p1_list, &c->misc, &c->elem_measure, &c->totals, &c->x_a, &c->x_b, &c->x_measure,
                    &c->x_nout, &c->x_elems, &c->x_setup, &c->x_tol, &c->x_iota, &c->x_faces, &c->x_screen,
-                   &c->x_list, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
+                   &c->x_list, &c->elem_off, &c->x_pa, &c->x_pb, &c->u_a, &c->v_b, &c->blocks, &c->bt_tabs, &c->bt_pair_a,
                    &c->bt_pair_b, &c->bt_mort, &c->bt_codes, &c->bt_roots, &c->bt_stops, &c->bt_tot,
                    &c->bt_ncand, &c->bt_stage_pa[0], &c->bt_stage_ea[0], &c->bt_stage_pb[0],
                    &c->bt_stage_eb[0], &c->bt_stage_pa[1], &c->bt_stage_ea[1], &c->bt_stage_pb[1],
@@ -581,7 +582,11 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
 // c->totals (one lsm::Partial).
 // n_dev (optional): the candidate count on the device; c->ncand is then only
 // its upper bound, the capacity of the pair arrays.
-void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_t* n_dev = nullptr) {
+// list_inside (3D): the survivor list also holds the pairs whose every plane
+// is a no-op, for a second pass over the list (the supermesh's elements);
+// no schedule then.
+void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_t* n_dev = nullptr,
+            bool list_inside = false) {
   const int64_t nnz = c->ncand;
   double* pm = ensure<double>(c, c->pair_measure, nnz);
   int32_t* pn = ensure<int32_t>(c, c->pair_nout, nnz);
@@ -606,7 +611,7 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_
   }
   const bool screen = c->dim == 3 && g_tet_screen;
   lsm::SchedBin bin;
-  const bool binned = c->dim == 3 && g_tet_schedule != 0;
+  const bool binned = c->dim == 3 && g_tet_schedule != 0 && !list_inside;
   if (binned) {
     if (g_tet_schedule == 1 && !c->have_sched) {
       set_error(c, "tet_schedule 1 needs scheduler weights (libsupermesh_gpu_sched_set_weights)");
@@ -627,13 +632,22 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_
     bin.out = ensure<int4>(c, c->sched_list, nnz);
     bin.window = g_sched_window;
   }
-  CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+  if (c->dim == 3 && list_inside) {
+    CU(lsm::launch_clip_elems(nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+                              static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
+                              static_cast<double*>(c->b_setup.p), pm, pn, nullptr, ovf, work,
+                              screen ? static_cast<double*>(c->a_faces.p) : nullptr,
+                              screen ? static_cast<double*>(c->b_screen.p) : nullptr, s));
+    c->clip_timed = false;
+  } else {
+    CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                         static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                         static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order,
                         g_time_kernels ? c->clip_ev[0] : nullptr, g_time_kernels ? c->clip_ev[1] : nullptr,
                         screen ? static_cast<double*>(c->a_faces.p) : nullptr,
                         screen ? static_cast<double*>(c->b_screen.p) : nullptr, binned ? &bin : nullptr, n_dev));
-  c->clip_timed = g_time_kernels;
+    c->clip_timed = g_time_kernels;
+  }
   if (c->dim == 3) {
     CU(cudaMemcpyAsync(ensure<unsigned long long>(c, c->surv, 1), work, sizeof(unsigned long long),
                        cudaMemcpyDeviceToDevice, s));
@@ -1755,6 +1769,61 @@ int libsupermesh_gpu_supermesh_out(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, 
   });
 }
 
+int libsupermesh_gpu_supermesh_elements(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const lsm_gpu_mesh* b,
+                                        int on_device, lsm_gpu_elem_out* out, lsm_gpu_stats* stats, void* stream) {
+  Ctx* c = C(ctx);
+  return guarded(c, [&] {
+    REQUIRE(out != nullptr, "NULL output descriptor");
+    REQUIRE(a && (a->dim == 2 || a->dim == 3), "supermesh elements: meshes must be 2D triangles or 3D tets");
+    REQUIRE(!on_device || (((uintptr_t)out->elems) & 15u) == 0, "device elems must be 16-byte aligned");
+    cudaStream_t s = pick(c, stream);
+    find_candidates(c, a, b, on_device, true, false, s);
+    const int64_t n = c->ncand;
+    const int dim = c->dim, per = dim == 2 ? 6 : 12;
+    out->n_candidates = n;
+    // counting pass: the narrow phase (3D: its survivor list kept whole for
+    // the second pass), then the offsets of every pair's simplices
+    narrow(c, s, nullptr, nullptr, true);
+    c->surv_valid = false;  // the list is not the plain narrow phase's
+    int64_t* off = ensure<int64_t>(c, c->elem_off, n + 1);
+    int64_t* tmp = ensure<int64_t>(c, c->scan_tmp, lsm::scan_tmp_entries(n) + 1);
+    CU(lsm::launch_scan(n, static_cast<int*>(c->pair_nout.p), off, tmp, s));
+    int64_t* h = static_cast<int64_t*>(c->host_scalars) + 40;
+    CU(cudaMemcpyAsync(h, off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    read_stats(c, stats, s);  // waits for the stream
+    const int64_t ne = *h;
+    out->n_elements = ne;
+    if (n > out->cand_capacity && out->elem_offset) {
+      set_error(c, "supermesh elements: %lld candidates do not fit elem_offset (capacity %lld)", (long long)n,
+                (long long)out->cand_capacity);
+      throw Fail{LSM_ERROR_CAPACITY};
+    }
+    if (ne > out->elem_capacity) {
+      set_error(c, "supermesh elements: %lld simplices do not fit the element arrays (capacity %lld)",
+                (long long)ne, (long long)out->elem_capacity);
+      throw Fail{LSM_ERROR_CAPACITY};
+    }
+    REQUIRE(ne == 0 || out->elems, "NULL elems");
+    const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (out->elem_offset) CU(cudaMemcpyAsync(out->elem_offset, off, sizeof(int64_t) * (n + 1), k, s));
+    if (ne > 0) {
+      double* de = on_device ? out->elems : ensure<double>(c, c->x_elems, ne * per);
+      int64_t* dpa = !out->parent_a ? nullptr : (on_device ? out->parent_a : ensure<int64_t>(c, c->x_pa, ne));
+      int64_t* dpb = !out->parent_b ? nullptr : (on_device ? out->parent_b : ensure<int64_t>(c, c->x_pb, ne));
+      CU(lsm::launch_emit_elements(dim, n, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
+                                   static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
+                                   static_cast<double*>(c->b_setup.p), static_cast<int32_t*>(c->ovf_list.p),
+                                   reinterpret_cast<unsigned long long*>(bad_flag(c) + 8), off, de, dpa, dpb, s));
+      if (!on_device) {
+        CU(cudaMemcpyAsync(out->elems, de, sizeof(double) * ne * per, k, s));
+        if (dpa) CU(cudaMemcpyAsync(out->parent_a, dpa, sizeof(int64_t) * ne, k, s));
+        if (dpb) CU(cudaMemcpyAsync(out->parent_b, dpb, sizeof(int64_t) * ne, k, s));
+      }
+    }
+    CU(cudaStreamSynchronize(s));
+  });
+}
+
 int libsupermesh_gpu_clip_candidates(lsm_gpu_context* ctx, lsm_gpu_stats* stats, void* stream) {
   Ctx* c = C(ctx);
   return guarded(c, [&] {
@@ -1848,7 +1917,7 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context* ctx, int dim, int64_t n, c
       unsigned long long* work = reinterpret_cast<unsigned long long*>(bad_flag(c) + 20);
       CU(lsm::launch_setup_pairs3(n, da, db, setup, tol, iota, faces, screen, s));
       if (de)
-        CU(lsm::launch_clip_elems(n, iota, da, tol, setup, pm, pn, de, list, work, faces, screen, s));
+        CU(lsm::launch_clip_elems(n, iota, iota, da, tol, setup, pm, pn, de, list, work, faces, screen, s));
       else
         CU(lsm::launch_clip(3, n, iota, iota, da, tol, setup, pm, pn, list, nullptr, work, s, nullptr, nullptr,
                             nullptr, faces, screen));
@@ -1934,7 +2003,9 @@ int libsupermesh_gpu_p1_mass(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const 
                            static_cast<double*>(c->b_coords.p), static_cast<double*>(c->b_setup.p), en_a, en_b,
                            a->index_bytes, du, dv, dbk, part, s, p1_survivors(c, c->dim, nnz), p1_work(c),
                            c->dim == 3 && g_tet_screen ? static_cast<double*>(c->a_faces.p) : nullptr,
-                           c->dim == 3 && g_tet_screen ? static_cast<double*>(c->b_screen.p) : nullptr));
+                           c->dim == 3 && g_tet_screen ? static_cast<double*>(c->b_screen.p) : nullptr,
+                           c->dim == 3 && du && dv ? ensure<double>(c, c->x_measure, std::max<int64_t>(nnz, 1))
+                                                   : nullptr));
     CU(lsm::launch_finalize(part, nblk, tot, s));
     double* h = static_cast<double*>(c->host_scalars) + 64;
     CU(cudaMemcpyAsync(h, tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -1771,9 +1771,10 @@ struct IxMeasureSink {
   __device__ __forceinline__ void finish() {}
 };
 
-// Explicit pairs with their output tets: elems [n][81][4][3] in the
-// reference's order (tets beyond 81 are counted, not stored), measure and
-// count per pair.  The list includes pairs with every plane a no-op.
+// Measure and count per pair and, for explicit pairs, the output tets:
+// elems (optional) [n][81][4][3] in the reference's order (tets beyond 81
+// are counted, not stored).  The list includes pairs with every plane a
+// no-op.
 struct IxElemSink {
   static constexpr bool kInside = true;
   static constexpr int kLaneDoubles = 0;
@@ -1790,7 +1791,7 @@ struct IxElemSink {
     pid = r.x;
   }
   __device__ __forceinline__ void tet(const Tet& o, double v1) {
-    if (kept < 81) {
+    if (elems && kept < 81) {
       double2* e = reinterpret_cast<double2*>(elems + ((int64_t)pid * 81 + kept) * 12);
       e[0] = make_double2(o.x[0], o.y[0]);
       e[1] = make_double2(o.z[0], o.x[1]);
@@ -1806,6 +1807,40 @@ struct IxElemSink {
     pair_measure[p] = m;
     pair_nout[p] = kept;
   }
+  template <int NT>
+  __device__ __forceinline__ void finish() {}
+};
+
+// The supermesh's tets, written where the scan of the per-pair counts puts
+// them: tet j of pair p at elems[pair_off[p] + j], with its parents.
+struct IxEmitSink {
+  static constexpr bool kInside = true;
+  static constexpr int kLaneDoubles = 0;
+  const int64_t* pair_off;
+  double* elems;
+  int64_t* parent_a;
+  int64_t* parent_b;
+  int64_t at;
+  int a, b;
+  __device__ __forceinline__ void bind(double*) {}
+  __device__ __forceinline__ void begin(const int4& r) {
+    at = pair_off[r.x];
+    a = r.y;
+    b = r.z;
+  }
+  __device__ __forceinline__ void tet(const Tet& o, double) {
+    double2* e = reinterpret_cast<double2*>(elems + at * 12);
+    e[0] = make_double2(o.x[0], o.y[0]);
+    e[1] = make_double2(o.z[0], o.x[1]);
+    e[2] = make_double2(o.y[1], o.z[1]);
+    e[3] = make_double2(o.x[2], o.y[2]);
+    e[4] = make_double2(o.z[2], o.x[3]);
+    e[5] = make_double2(o.y[3], o.z[3]);
+    if (parent_a) parent_a[at] = a;
+    if (parent_b) parent_b[at] = b;
+    ++at;
+  }
+  __device__ __forceinline__ void end(int64_t) {}
   template <int NT>
   __device__ __forceinline__ void finish() {}
 };
@@ -2008,15 +2043,16 @@ cudaError_t launch_setup_pairs3(int64_t n, const double* tet_a, const double* te
   return cudaGetLastError();
 }
 
-cudaError_t launch_clip_elems(int64_t n, const int32_t* iota, const double* tet_a, const double* tol_a,
-                              const double* setup, double* measure, int32_t* nout, double* elems,
-                              int32_t* survivors, unsigned long long* work, const double* faces_a,
+cudaError_t launch_clip_elems(int64_t n, const int32_t* pair_a, const int32_t* pair_b, const double* tet_a,
+                              const double* tol_a, const double* setup, double* measure, int32_t* nout,
+                              double* elems, int32_t* survivors, unsigned long long* work, const double* faces_a,
                               const double* screen_b, cudaStream_t s) {
   cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
   if (n <= 0) return cudaGetLastError();
   count_launch();
-  k_prefilter_tets<false><<<grid_for(n, 256, 8), 256, 0, s>>>(n, nullptr, iota, iota, tet_a, tol_a, setup, measure,
-                                                              nout, survivors, work, faces_a, screen_b, nullptr);
+  k_prefilter_tets<false><<<grid_for(n, 256, 8), 256, 0, s>>>(n, nullptr, pair_a, pair_b, tet_a, tol_a, setup,
+                                                              measure, nout, survivors, work, faces_a, screen_b,
+                                                              nullptr);
   count_launch();
   k_clip_tets_ix<IxElemSink, kIxBlock, kIxBlocksPerSm><<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
       reinterpret_cast<const int4*>(survivors), work, tet_a, tol_a, setup, IxElemSink{measure, nout, elems}, work + 1);
@@ -2039,7 +2075,7 @@ __global__ void __launch_bounds__(256) k_reduce_pairs(int64_t npairs, const doub
   unsigned long long ni = 0, no = 0;
   for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     cs_add(sum, err, pm[i]);
-    const int k = pn[i];
+    const int k = pn ? pn[i] : 0;
     ni += k > 0;
     no += k;
   }
@@ -2093,6 +2129,58 @@ cudaError_t launch_reduce_pairs(int64_t npairs, const double* pair_measure, cons
   return cudaGetLastError();
 }
 
+// 2D supermesh triangles: one candidate pair per thread, clipped again with
+// the narrow phase's arithmetic; pairs without output triangles are skipped
+// (their offsets are equal).
+__global__ void __launch_bounds__(128) k_tris_emit(int64_t npairs, const int32_t* __restrict__ pa,
+                                                   const int32_t* __restrict__ pb, const double* __restrict__ coords_a,
+                                                   const double* __restrict__ tol_a, const double* __restrict__ setup_b,
+                                                   const int64_t* __restrict__ pair_off, double* elems,
+                                                   int64_t* parent_a, int64_t* parent_b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npairs;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t at = pair_off[i];
+    if (pair_off[i + 1] == at) continue;
+    const int a = pa[i], b = pb[i];
+    const double* ca = coords_a + (int64_t)a * 6;
+    Lines L;
+    double tolb;
+    load_lines(setup_b + (int64_t)b * kSetup2, L, tolb);
+    const double tol = fmin(tol_a[a], tolb);
+    LocalPoly<kTriWideCap> p, q;
+    double m;
+    clip_tri(ca[0], ca[1], ca[2], ca[3], ca[4], ca[5], L, tol, p, q, kTriWideCap, m,
+             [&](int k, double x0, double y0, double x1, double y1, double x2, double y2) {
+               double2* e = reinterpret_cast<double2*>(elems + (at + k) * 6);
+               e[0] = make_double2(x0, y0);
+               e[1] = make_double2(x1, y1);
+               e[2] = make_double2(x2, y2);
+               if (parent_a) parent_a[at + k] = a;
+               if (parent_b) parent_b[at + k] = b;
+             });
+  }
+}
+
+cudaError_t launch_emit_elements(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
+                                 const double* coords_a, const double* tol_a, const double* setup_b,
+                                 const int32_t* survivors, unsigned long long* work, const int64_t* pair_off,
+                                 double* elems, int64_t* parent_a, int64_t* parent_b, cudaStream_t s) {
+  if (npairs <= 0) return cudaSuccess;
+  count_launch();
+  if (dim == 2) {
+    k_tris_emit<<<grid_for(npairs, 128, 8), 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, setup_b, pair_off,
+                                                         elems, parent_a, parent_b);
+    return cudaGetLastError();
+  }
+  // the survivors of the counting pass again (work[0] holds their number);
+  // only the clipper's pair counter starts over
+  cudaMemsetAsync(work + 1, 0, sizeof(unsigned long long), s);
+  k_clip_tets_ix<IxEmitSink, kIxBlock, kIxBlocksPerSm><<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
+      reinterpret_cast<const int4*>(survivors), work, coords_a, tol_a, setup_b,
+      IxEmitSink{pair_off, elems, parent_a, parent_b}, work + 1);
+  return cudaGetLastError();
+}
+
 cudaError_t init_p1_attributes();
 
 cudaError_t init_device_attributes() {
@@ -2100,6 +2188,9 @@ cudaError_t init_device_attributes() {
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_clip_tets_ix<IxElemSink, kIxBlock, kIxBlocksPerSm>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_clip_tets_ix<IxEmitSink, kIxBlock, kIxBlocksPerSm>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
   if (e == cudaSuccess) e = init_p1_attributes();
   if (e != cudaSuccess) return e;
@@ -3242,7 +3333,8 @@ __device__ __forceinline__ void p1_apply_3d(const double* F, int sw, double x, d
 // P1-P1 mixed mass block of a pair (test_parallel_p1_inner_product_3d.F90:
 // four-point rule, P1 bases of A and B by elimination at each point), per
 // kept output tet in the reference's order; at the end of the pair the block
-// is stored and u^T M v added to a compensated sum.  The per-element part of
+// is stored and u^T M v written per pair (lanes take pairs in a dynamic order;
+// the caller sums them in pair order).  The per-element part of
 // both eliminations is done once per pair (p1_factor_3d) into the lane's
 // slice of shared memory behind the point pool (kLaneDoubles per lane).
 template <typename IDX, int BLOCK>
@@ -3256,12 +3348,10 @@ struct IxP1Sink {
   const double* u_a;
   const double* v_b;
   double* blocks;
-  Partial* partials;
+  double* pair_uv;  // u^T M v per pair (when u_a and v_b are given), summed in pair order afterwards
   double blk[16];
   double* fac;  // this lane's factors: A's at fac, B's at fac + kP1Fac3 * BLOCK
   int a, b, swa, swb;
-  double sum, err;
-  unsigned long long ni;
   __device__ __forceinline__ void bind(double* lane_mem) { fac = lane_mem; }
   __device__ __forceinline__ void begin(const int4& r) {
     a = r.y;
@@ -3306,14 +3396,11 @@ struct IxP1Sink {
 #pragma unroll
         for (int c = 0; c < 4; ++c) sv += ur * blk[r * 4 + c] * v_b[node_of<IDX>(en_b, b, 4, c)];
       }
-      cs_add(sum, err, sv);
+      pair_uv[p] = sv;
     }
-    ++ni;
   }
   template <int NT>
-  __device__ __forceinline__ void finish() {
-    block_reduce_partial<NT>(sum, err, ni, 0ull, &partials[blockIdx.x]);
-  }
+  __device__ __forceinline__ void finish() {}
 };
 
 
@@ -3546,15 +3633,17 @@ size_t p1_smem_bytes() {
   return (size_t)kIxP1Block * (3 * kIxPoints + IxP1Sink<int32_t, kIxP1Block>::kLaneDoubles) * sizeof(double);
 }
 
-int p1_grid_blocks(int dim) { return sm_count() * (dim == 2 ? 4 : 1); }
+// partials written by launch_p1_mass: one per 2D block, or the fixed-order
+// reduction's blocks in 3D
+int p1_grid_blocks(int dim) { return dim == 2 ? sm_count() * 4 : kReduceBlocks; }
 
 cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                            const double* coords_a, const double* tol_a, const double* coords_b,
                            const double* setup_b, const void* enlist_a, const void* enlist_b,
                            int idx_bytes, const double* u_a, const double* v_b, double* blocks,
                            Partial* partials, cudaStream_t s, int32_t* survivors, unsigned long long* work,
-                           const double* faces_a, const double* screen_b) {
-  const int g = p1_grid_blocks(dim);
+                           const double* faces_a, const double* screen_b, double* pair_uv) {
+  const int g = dim == 2 ? p1_grid_blocks(2) : sm_count();
   if (dim == 2) {
     count_launch();
     if (idx_bytes == 4)
@@ -3563,10 +3652,15 @@ cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const
       k_p1_mass<int64_t><<<g, 128, 0, s>>>(npairs, pair_a, pair_b, coords_a, tol_a, coords_b, setup_b, enlist_a, enlist_b, u_a, v_b, blocks, partials);
     return cudaGetLastError();
   }
-  // the early-out pass lists the pairs with output tets (blocks of the
-  // others stay zero), then the index clipper integrates their tets
+  // the early-out pass lists the pairs with output tets (blocks and u^T M v
+  // of the others stay zero), then the index clipper integrates their tets;
+  // u^T M v per pair is summed in pair order (a fixed-order reduction into
+  // reduce_pairs_blocks() partials), so the integral does not depend on the
+  // order in which the lanes took the pairs
+  const bool uv = u_a && v_b;
   cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
   if (blocks && npairs > 0) cudaMemsetAsync(blocks, 0, sizeof(double) * 16 * npairs, s);
+  if (uv && npairs > 0) cudaMemsetAsync(pair_uv, 0, sizeof(double) * npairs, s);
   if (npairs > 0) {
     count_launch();
     k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, nullptr, pair_a, pair_b, coords_a,
@@ -3577,18 +3671,20 @@ cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const
   count_launch();
   if (idx_bytes == 4) {
     using Sk = IxP1Sink<int32_t, kIxP1Block>;
-    Sk sk{coords_a, coords_b, enlist_a, enlist_b, u_a, v_b, blocks, partials};
-    sk.sum = sk.err = 0.0;
-    sk.ni = 0;
+    Sk sk{coords_a, coords_b, enlist_a, enlist_b, u_a, v_b, blocks, pair_uv};
     k_clip_tets_ix<Sk, kIxP1Block, 1><<<g, kIxP1Block, p1_smem_bytes(), s>>>(list, work, coords_a, tol_a, setup_b,
                                                                             sk, work + 1);
   } else {
     using Sk = IxP1Sink<int64_t, kIxP1Block>;
-    Sk sk{coords_a, coords_b, enlist_a, enlist_b, u_a, v_b, blocks, partials};
-    sk.sum = sk.err = 0.0;
-    sk.ni = 0;
+    Sk sk{coords_a, coords_b, enlist_a, enlist_b, u_a, v_b, blocks, pair_uv};
     k_clip_tets_ix<Sk, kIxP1Block, 1><<<g, kIxP1Block, p1_smem_bytes(), s>>>(list, work, coords_a, tol_a, setup_b,
                                                                             sk, work + 1);
+  }
+  if (uv) {
+    count_launch();
+    k_reduce_pairs<<<kReduceBlocks, 256, 0, s>>>(npairs, pair_uv, nullptr, partials, nullptr);
+  } else {
+    cudaMemsetAsync(partials, 0, sizeof(Partial) * kReduceBlocks, s);
   }
   return cudaGetLastError();
 }

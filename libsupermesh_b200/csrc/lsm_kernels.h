@@ -190,10 +190,21 @@ cudaError_t launch_i32_to_i64(int64_t n, const int32_t* in, int64_t* out, cudaSt
 // per pair; work: two counters).  tet_a must be 16-byte aligned.
 cudaError_t launch_setup_pairs3(int64_t n, const double* tet_a, const double* tet_b, double* setup, double* tol_a,
                                 int32_t* iota, double* faces_a, double* screen_b, cudaStream_t s);
-cudaError_t launch_clip_elems(int64_t n, const int32_t* iota, const double* tet_a, const double* tol_a,
-                              const double* setup, double* measure, int32_t* nout, double* elems,
-                              int32_t* survivors, unsigned long long* work, const double* faces_a,
+// launch_clip_elems: the 3D narrow phase whose survivor list also holds the
+// pairs with every plane a no-op (so that a second pass over the list sees
+// every pair with output tets); measure/nout for every pair, elems optional.
+cudaError_t launch_clip_elems(int64_t n, const int32_t* pair_a, const int32_t* pair_b, const double* tet_a,
+                              const double* tol_a, const double* setup, double* measure, int32_t* nout,
+                              double* elems, int32_t* survivors, unsigned long long* work, const double* faces_a,
                               const double* screen_b, cudaStream_t s);
+// The supermesh's simplices: pair p's output simplices (reference order) at
+// elems[pair_off[p] ..] ([3][2] or [4][3] doubles each), parents optional.
+// 3D takes the survivor list and work counters of a launch_clip_elems pass
+// over the same pairs; 2D clips the pairs again.
+cudaError_t launch_emit_elements(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
+                                 const double* coords_a, const double* tol_a, const double* setup_b,
+                                 const int32_t* survivors, unsigned long long* work, const int64_t* pair_off,
+                                 double* elems, int64_t* parent_a, int64_t* parent_b, cudaStream_t s);
 cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const double* b,
                                   double* measure, int32_t* nout, double* out_elems,
                                   cudaStream_t s);
@@ -241,13 +252,15 @@ cudaError_t launch_check_index(int64_t n, const void* en, int idx_bytes, int64_t
 // P1-P1 mixed mass: 2D clips every pair; 3D runs the exact early-out pass
 // (survivors: 4 ints per pair, work: two counters, faces_a / screen_b as for
 // launch_clip) and the index clipper with the quadrature on the survivors,
-// with blocks of the other pairs zero-filled.  partials: p1_grid_blocks(dim).
+// with blocks of the other pairs zero-filled; 3D with u_a and v_b also needs
+// pair_uv [npairs] (u^T M v per pair, summed in pair order).  partials:
+// p1_grid_blocks(dim) entries.
 cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                            const double* coords_a, const double* tol_a, const double* coords_b,
                            const double* setup_b, const void* enlist_a, const void* enlist_b,
                            int idx_bytes, const double* u_a, const double* v_b, double* blocks,
                            Partial* partials, cudaStream_t s, int32_t* survivors, unsigned long long* work,
-                           const double* faces_a, const double* screen_b);
+                           const double* faces_a, const double* screen_b, double* pair_uv = nullptr);
 int p1_grid_blocks(int dim);
 
 // ---- batched (many mesh pairs per launch) --------------------------------

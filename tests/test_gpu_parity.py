@@ -418,10 +418,11 @@ def test_legacy_single_pair_entries(oracle_mod):
         assert lsm.tetrahedron_volume(a[i]) == oracle_mod.tetrahedron_volume(a[i])
 
 
-@pytest.mark.parametrize("name", ["small2d_12x17", "small3d_4x5"])
+@pytest.mark.parametrize("name", ["small2d_12x17", "small3d_4x5", "small3d_20x9"])
 def test_p1_mass_device_inputs(gpu_ctx, name):
     """Device-resident meshes and fields give the host call's u^T M v, bit
-    for bit."""
+    for bit, and repeated calls give the same value (the 3D lanes take pairs
+    in a dynamic order; the sum runs in pair order)."""
     torch = pytest.importorskip("torch")
     dim, A, B = M.config_meshes(name)
     u = np.cos(3 * A[0][:, 0]) + A[0][:, 1]
@@ -434,6 +435,8 @@ def test_p1_mass_device_inputs(gpu_ctx, name):
     torch.cuda.synchronize()
     val, blocks = gpu_ctx.p1_mass(tA, tB, tu, tv, on_device=True)
     assert blocks is None and val == ref
+    for _ in range(3):
+        assert gpu_ctx.p1_mass(tA, tB, tu, tv, on_device=True)[0] == ref
 
 
 def test_p1_mass_reference_answers(gpu_ctx, oracle_mod, ref_meshes):
