@@ -1961,7 +1961,18 @@ int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context* ctx, int kind, int64
       dn = n_out ? ensure<int32_t>(c, c->x_nout, n) : nullptr;
       de = elems ? ensure<double>(c, c->x_elems, n * m.cap * m.per_out) : nullptr;
     }
-    CU(lsm::launch_pairs_mixed(kind, n, da, db, dm, dn, de, s));
+    if (kind == LSM_PAIR_TET_HEX && n >= kPairsPipelineMin) {
+      // large batches: per-pair setup, the exact early-out and the six-plane
+      // index clipper; small ones stay on the one-launch clipper (same results)
+      double* pm = dm ? dm : ensure<double>(c, c->x_measure, n);
+      int32_t* pn = dn ? dn : ensure<int32_t>(c, c->x_nout, n);
+      CU(lsm::launch_tet_hex_pairs(n, da, db, pm, pn, de, ensure<double>(c, c->x_setup, n * 28),
+                                   ensure<double>(c, c->x_tol, n), ensure<int32_t>(c, c->x_iota, n),
+                                   ensure<int32_t>(c, c->x_list, 4 * n),
+                                   reinterpret_cast<unsigned long long*>(bad_flag(c) + 20), s));
+    } else {
+      CU(lsm::launch_pairs_mixed(kind, n, da, db, dm, dn, de, s));
+    }
     if (!on_device) {
       if (measure) CU(cudaMemcpyAsync(measure, dm, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
       if (n_out) CU(cudaMemcpyAsync(n_out, dn, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));

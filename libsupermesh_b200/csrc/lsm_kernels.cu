@@ -1495,7 +1495,13 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 #ifndef LSM_PREFILTER_BPS
 #define LSM_PREFILTER_BPS 2
 #endif
-template <bool kSettle>
+// NP planes per B element in setup rows of clip_row(NP) doubles (4: tets,
+// 6: hexahedra; the second early-out is for tets only).  The margin covers
+// the up to NP-1 nested interpolations of a derived vertex (each within
+// ~7 eps M of an exact convex combination) with room to spare.
+__host__ __device__ constexpr int clip_row(int np) { return 4 * np + 4; }
+
+template <bool kSettle, int NP = 4>
 __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ order,
                                                         const int32_t* __restrict__ pa,
                                                         const int32_t* __restrict__ pb,
@@ -1542,13 +1548,13 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
     if (j < end) {
       Tet t;
       load_tet(coords_a + (int64_t)a * 12, t);
-      const double* pl = setup_b + (int64_t)b * kSetup3;
+      const double* pl = setup_b + (int64_t)b * clip_row(NP);
       double M = 0.0;
 #pragma unroll
       for (int k = 0; k < 4; ++k) M = fmax(M, fmax(fabs(t.x[k]), fmax(fabs(t.y[k]), fabs(t.z[k]))));
       bool reject = false;
 #pragma unroll
-      for (int L = 0; L < 4; ++L) {
+      for (int L = 0; L < NP; ++L) {
         double nx, ny, nz, c;
         load_plane(pl, L, nx, ny, nz, c);
         const double thr = kEps + 64.0 * kEps * (1.0 + 2.0 * fmax(M, fabs(c)));
@@ -1562,7 +1568,7 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
         reject = reject || dmin >= thr;
         noop |= dmax <= -thr ? 1 << L : 0;
       }
-      if (!reject && faces_a) {
+      if (NP == 4 && !reject && faces_a) {
         const double2* sb = reinterpret_cast<const double2*>(screen_b + (int64_t)b * kScreen3);
         const double2 gt = __ldg(sb + 6), mz = __ldg(sb + 7);
         if (gt.x < DBL_MAX) {  // B's planes bound a proper tet
@@ -1591,10 +1597,10 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
       } else if (reject) {
         pair_measure[i] = 0.0;
         pair_nout[i] = 0;
-      } else if (noop == 15) {
-        // A inside all four planes: the reference keeps A as its one tet
+      } else if (noop == (1 << NP) - 1) {
+        // A inside all planes: the reference keeps A as its one tet
         double v1;
-        const bool keep = final_tet_keep(t, fmin(tol_a[a], pl[16]), v1);
+        const bool keep = final_tet_keep(t, fmin(tol_a[a], pl[4 * NP]), v1);
         pair_measure[i] = keep ? v1 : 0.0;
         pair_nout[i] = keep ? 1 : 0;
       } else {
@@ -1772,10 +1778,11 @@ struct IxMeasureSink {
 };
 
 // Measure and count per pair and, for explicit pairs, the output tets:
-// elems (optional) [n][81][4][3] in the reference's order (tets beyond 81
-// are counted, not stored).  The list includes pairs with every plane a
-// no-op.
-struct IxElemSink {
+// elems (optional) [n][kCap][4][3] in the reference's order (tets beyond
+// kCap are counted, not stored: 81 for tet-tet, 729 for tet-hex).  The list
+// includes pairs with every plane a no-op.
+template <int kCap>
+struct IxElemSinkT {
   static constexpr bool kInside = true;
   static constexpr int kLaneDoubles = 0;
   double* pair_measure;
@@ -1791,8 +1798,8 @@ struct IxElemSink {
     pid = r.x;
   }
   __device__ __forceinline__ void tet(const Tet& o, double v1) {
-    if (elems && kept < 81) {
-      double2* e = reinterpret_cast<double2*>(elems + ((int64_t)pid * 81 + kept) * 12);
+    if (elems && kept < kCap) {
+      double2* e = reinterpret_cast<double2*>(elems + ((int64_t)pid * kCap + kept) * 12);
       e[0] = make_double2(o.x[0], o.y[0]);
       e[1] = make_double2(o.z[0], o.x[1]);
       e[2] = make_double2(o.y[1], o.z[1]);
@@ -1810,6 +1817,8 @@ struct IxElemSink {
   template <int NT>
   __device__ __forceinline__ void finish() {}
 };
+
+using IxElemSink = IxElemSinkT<81>;
 
 // The supermesh's tets, written where the scan of the per-pair counts puts
 // them: tet j of pair p at elems[pair_off[p] + j], with its parents.
@@ -1845,16 +1854,26 @@ struct IxEmitSink {
   __device__ __forceinline__ void finish() {}
 };
 
-template <class Sink, int BLOCK, int BPS>
+// Points in a lane's pool for NP planes: A's 4 vertices + 4 per plane.
+__host__ __device__ constexpr int ix_points(int np) { return 4 + 4 * np; }
+
+template <class Sink, int BLOCK, int BPS, int NP = 4>
 __global__ void __launch_bounds__(BLOCK, BPS) k_clip_tets_ix(
     const int4* __restrict__ list, const unsigned long long* __restrict__ nlist, const double* __restrict__ coords_a,
     const double* __restrict__ tol_a, const double* __restrict__ setup_b, Sink sk, unsigned long long* work) {
+  static_assert(ix_points(NP) <= 32, "pool indices are 5 bits");
   extern __shared__ double ix_mem[];
   IxPool<BLOCK> pool{ix_mem + threadIdx.x};
-  sk.bind(ix_mem + 3 * kIxPoints * BLOCK + threadIdx.x);
-  // pending tets: a 120-bit shift register of 20-bit index tuples (stk_hi:
-  // stk_lo, newest in the low bits) and their planes, 2 bits each (stk_lv)
-  unsigned long long stk_lo = 0, stk_hi = 0;
+  sk.bind(ix_mem + 3 * ix_points(NP) * BLOCK + threadIdx.x);
+  // pending tets (at most 2 per plane but the last): a shift register of
+  // 20-bit index tuples over kW words (stk[kW-1]:...:stk[0], newest in the
+  // low bits) and their planes, kLB bits each (stk_lv)
+  constexpr int kW = NP <= 4 ? 2 : 4;
+  constexpr int kLB = NP <= 4 ? 2 : 3;
+  static_assert(2 * (NP - 1) * 20 <= 64 * kW && 2 * (NP - 1) * kLB <= 32, "pending-tet stack too small");
+  unsigned long long stk[kW];
+#pragma unroll
+  for (int w = 0; w < kW; ++w) stk[w] = 0;
   unsigned stk_lv = 0;
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -1877,29 +1896,31 @@ __global__ void __launch_bounds__(BLOCK, BPS) k_clip_tets_ix(
   int L = 0, sp = 0;
   // planes this pair clips at (bit L; the prefilter's no-op planes are
   // skipped) and the last of them
-  unsigned act = 15u;
-  int lastL = 3;
+  constexpr unsigned kAll = (1u << NP) - 1u;
+  unsigned act = kAll;
+  int lastL = NP - 1;
   for (;;) {
     // ---- prefetch pipeline
     if (nstage == 1) {
       load_tet(coords_a + (int64_t)nrec.y * 12, nt);
-      ntol = fmin(tol_a[nrec.y], setup_b[(int64_t)nrec.z * kSetup3 + 16]);
+      ntol = fmin(tol_a[nrec.y], setup_b[(int64_t)nrec.z * clip_row(NP) + 4 * NP]);
       nstage = 2;
     }
     if (p < 0 && nstage == 2) {
       p = nrec.x;
 #pragma unroll
       for (int v = 0; v < 4; ++v) pool.put(v, V3{nt.x[v], nt.y[v], nt.z[v]});
-      planes = setup_b + (int64_t)nrec.z * kSetup3;
+      planes = setup_b + (int64_t)nrec.z * clip_row(NP);
       tol = ntol;
       cur = ix_pack(0, 1, 2, 3);
       sk.begin(nrec);
-      act = ~(unsigned)nrec.w & 15u;  // never 0 unless Sink::kInside
+      act = ~(unsigned)nrec.w & kAll;  // never 0 unless Sink::kInside
       L = __ffs(act) - 1;
       lastL = 31 - __clz(act);
       sp = 0;
       nstage = 0;
-      stk_lo = stk_hi = 0;
+#pragma unroll
+      for (int w = 0; w < kW; ++w) stk[w] = 0;
       stk_lv = 0;
       if (Sink::kInside && act == 0u) {
         // A inside all four planes: the reference keeps A as its one tet
@@ -1965,15 +1986,17 @@ __global__ void __launch_bounds__(BLOCK, BPS) k_clip_tets_ix(
     if (k > 0) {
       const unsigned lv = (unsigned)(__ffs(act & (~0u << (L + 1))) - 1);  // next plane clipped at
       if (k == 3) {
-        stk_hi = (stk_hi << 20) | (stk_lo >> 44);
-        stk_lo = (stk_lo << 20) | c2;
-        stk_lv = (stk_lv << 2) | lv;
+#pragma unroll
+        for (int w = kW - 1; w > 0; --w) stk[w] = (stk[w] << 20) | (stk[w - 1] >> 44);
+        stk[0] = (stk[0] << 20) | c2;
+        stk_lv = (stk_lv << kLB) | lv;
         ++sp;
       }
       if (k >= 2) {
-        stk_hi = (stk_hi << 20) | (stk_lo >> 44);
-        stk_lo = (stk_lo << 20) | c1;
-        stk_lv = (stk_lv << 2) | lv;
+#pragma unroll
+        for (int w = kW - 1; w > 0; --w) stk[w] = (stk[w] << 20) | (stk[w - 1] >> 44);
+        stk[0] = (stk[0] << 20) | c1;
+        stk_lv = (stk_lv << kLB) | lv;
         ++sp;
       }
       cur = c0;
@@ -1981,11 +2004,12 @@ __global__ void __launch_bounds__(BLOCK, BPS) k_clip_tets_ix(
       continue;
     }
     if (sp > 0) {
-      cur = (unsigned)(stk_lo & 0xfffffull);
-      L = (int)(stk_lv & 3u);
-      stk_lo = (stk_lo >> 20) | (stk_hi << 44);
-      stk_hi >>= 20;
-      stk_lv >>= 2;
+      cur = (unsigned)(stk[0] & 0xfffffull);
+      L = (int)(stk_lv & ((1u << kLB) - 1u));
+#pragma unroll
+      for (int w = 0; w < kW - 1; ++w) stk[w] = (stk[w] >> 20) | (stk[w + 1] << 44);
+      stk[kW - 1] >>= 20;
+      stk_lv >>= kLB;
       --sp;
       continue;
     }
@@ -2040,6 +2064,65 @@ cudaError_t launch_setup_pairs3(int64_t n, const double* tet_a, const double* te
   if (n <= 0) return cudaSuccess;
   count_launch();
   k_setup_pairs3<<<grid_for(n, 256, 8), 256, 0, s>>>(n, tet_a, tet_b, setup, tol_a, iota, faces_a, screen_b);
+  return cudaGetLastError();
+}
+
+// Explicit tet-hexahedron pairs through the same pipeline with six planes
+// (Supermesh.F90:262-280 planes, tolerance from the tet alone): per-pair
+// setup rows of clip_row(6) doubles (planes, +inf in the tolerance slot so
+// that fmin keeps A's), the first early-out and the no-op planes, then the
+// index clipper with a pool of 28 points.  320 threads per SM: 672 B of pool
+// per lane.
+constexpr int kIxHexBlock = 320;
+
+size_t ix_hex_smem_bytes() { return (size_t)kIxHexBlock * 3 * ix_points(6) * sizeof(double); }
+
+__global__ void k_setup_hex_pairs(int64_t n, const double* __restrict__ tet_a, const double* __restrict__ hex_b,
+                                  double* setup, double* tol_a, int32_t* iota) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double nx[6], ny[6], nz[6], c[6];
+    hex_planes(hex_b + 24 * i, nx, ny, nz, c);
+    double* o = setup + i * clip_row(6);
+#pragma unroll
+    for (int L = 0; L < 6; ++L) {
+      o[4 * L + 0] = nx[L];
+      o[4 * L + 1] = ny[L];
+      o[4 * L + 2] = nz[L];
+      o[4 * L + 3] = c[L];
+    }
+    o[24] = pos_inf();
+    o[25] = 0.0;
+    o[26] = 0.0;
+    o[27] = 0.0;
+    Tet a;
+    load_tet(tet_a + 12 * i, a);
+    tol_a[i] = 10.0 * spacing(tet_volume_v4(a));
+    iota[i] = (int32_t)i;
+  }
+}
+
+cudaError_t launch_tet_hex_pairs(int64_t n, const double* tet_a, const double* hex_b, double* measure, int32_t* nout,
+                                 double* elems, double* setup, double* tol_a, int32_t* iota, int32_t* survivors,
+                                 unsigned long long* work, cudaStream_t s) {
+  cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
+  if (n <= 0) return cudaGetLastError();
+  count_launch(3);
+  k_setup_hex_pairs<<<grid_for(n, 256, 8), 256, 0, s>>>(n, tet_a, hex_b, setup, tol_a, iota);
+  const int4* list = reinterpret_cast<const int4*>(survivors);
+  const int g = sm_count();
+  if (elems) {
+    k_prefilter_tets<false, 6><<<grid_for(n, 256, 8), 256, 0, s>>>(n, nullptr, iota, iota, tet_a, tol_a, setup,
+                                                                   measure, nout, survivors, work, nullptr, nullptr,
+                                                                   nullptr);
+    k_clip_tets_ix<IxElemSinkT<729>, kIxHexBlock, 1, 6><<<g, kIxHexBlock, ix_hex_smem_bytes(), s>>>(
+        list, work, tet_a, tol_a, setup, IxElemSinkT<729>{measure, nout, elems}, work + 1);
+  } else {
+    k_prefilter_tets<true, 6><<<grid_for(n, 256, 8), 256, 0, s>>>(n, nullptr, iota, iota, tet_a, tol_a, setup,
+                                                                  measure, nout, survivors, work, nullptr, nullptr,
+                                                                  nullptr);
+    k_clip_tets_ix<IxMeasureSink, kIxHexBlock, 1, 6><<<g, kIxHexBlock, ix_hex_smem_bytes(), s>>>(
+        list, work, tet_a, tol_a, setup, IxMeasureSink{measure, nout, 0.0, 0}, work + 1);
+  }
   return cudaGetLastError();
 }
 
@@ -2192,6 +2275,12 @@ cudaError_t init_device_attributes() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_clip_tets_ix<IxEmitSink, kIxBlock, kIxBlocksPerSm>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_clip_tets_ix<IxMeasureSink, kIxHexBlock, 1, 6>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_hex_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_clip_tets_ix<IxElemSinkT<729>, kIxHexBlock, 1, 6>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_hex_smem_bytes());
   if (e == cudaSuccess) e = init_p1_attributes();
   if (e != cudaSuccess) return e;
   return init_sched_attributes(kSchedMaxWindow);

@@ -205,6 +205,14 @@ cudaError_t launch_emit_elements(int dim, int64_t npairs, const int32_t* pair_a,
                                  const double* coords_a, const double* tol_a, const double* setup_b,
                                  const int32_t* survivors, unsigned long long* work, const int64_t* pair_off,
                                  double* elems, int64_t* parent_a, int64_t* parent_b, cudaStream_t s);
+// Explicit tet-hexahedron pairs (a [n][4][3] 16-byte aligned, hex_b
+// [n][8][3]) through per-pair setup (setup [n][28], tol_a [n], iota [n]), the
+// first early-out with the no-op planes, and the six-plane index clipper:
+// measure/nout per pair and, optionally, elems [n][729][4][3]; survivors 4
+// ints per pair, work two counters.
+cudaError_t launch_tet_hex_pairs(int64_t n, const double* tet_a, const double* hex_b, double* measure, int32_t* nout,
+                                 double* elems, double* setup, double* tol_a, int32_t* iota, int32_t* survivors,
+                                 unsigned long long* work, cudaStream_t s);
 cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const double* b,
                                   double* measure, int32_t* nout, double* out_elems,
                                   cudaStream_t s);

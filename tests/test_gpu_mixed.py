@@ -325,3 +325,38 @@ def test_device_resident_pairs_equal_host_pairs(gpu_ctx):
         gpu_ctx.intersect_pairs_device(da, db, dm, dk, dim=dim, kind=kind)
         torch.cuda.synchronize()
         assert np.array_equal(dm.cpu().numpy(), m) and np.array_equal(dk.cpu().numpy(), k), (dim, kind)
+
+
+def test_tet_hex_large_batch_bitexact(gpu_ctx, oracle_mod):
+    """Tet-hex batches large enough for the early-out pass + six-plane index
+    clipper: output tets, counts and measures bit-identical to the oracle and
+    to small batches (one-launch clipper), with and without the output
+    tets.  Includes tets well inside their hexahedron (every plane a no-op),
+    hexahedra inside tets, far-apart pairs and Kuhn tets of unit cubes."""
+    rng = np.random.default_rng(41)
+    n = 2600
+    t = rng.random((n, 4, 3))
+    h = _random_hexes(rng, n)
+    unit = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                     [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], dtype=np.float64)
+    h[:64] = unit
+    t[:64] = unit[[0, 1, 2, 6]]
+    ch = h[64:300].mean(axis=1, keepdims=True)
+    t[64:300] = ch + 0.05 * (rng.random((236, 4, 3)) - 0.5)  # tet inside the hexahedron
+    t[300:400] = rng.random((100, 4, 3)) * 4.0 - 1.5  # large tets around the hexahedron
+    t[400:500] += 3.0  # far apart
+    m, k, e = gpu_ctx.intersect_pairs_mixed(lsm.PAIR_TET_HEX, t, h, want_elems=True)
+    for i in range(n):
+        ref = oracle_mod.intersect_tet_hex(t[i], h[i])
+        assert k[i] == len(ref), i
+        assert np.array_equal(e[i, : k[i]], ref), i
+        meas = 0.0
+        for o in ref:
+            meas += oracle_mod.tetrahedron_volume(o)
+        assert m[i] == meas, i
+    assert (k[400:500] == 0).all()
+    m1, k1, _ = gpu_ctx.intersect_pairs_mixed(lsm.PAIR_TET_HEX, t, h)
+    assert np.array_equal(m1, m) and np.array_equal(k1, k)
+    parts = [gpu_ctx.intersect_pairs_mixed(lsm.PAIR_TET_HEX, t[j:j + 650], h[j:j + 650]) for j in range(0, n, 650)]
+    assert np.array_equal(np.concatenate([x[0] for x in parts]), m)
+    assert np.array_equal(np.concatenate([x[1] for x in parts]), k)
