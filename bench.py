@@ -720,6 +720,8 @@ def run_ours(args, world, rank, local):
         line["cpu_baseline"] = cpu
         line["drop_in_per_pair"] = drop_in_per_pair(ctx, dim, A, B, n_cand)
         line["p1_mass"] = p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush)
+        if not args.no_cpu_baseline:
+            line["p1_mass"]["cpu_baseline"] = p1_mass_cpu(dim, A, B)
         line["supermesh_elements"] = elements_timing(ctx, dim, tA, tB, n_cand, stream, flush)
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -813,6 +815,22 @@ def p1_mass_timing(ctx, tA, tB, hA, hB, n_cand, stream, flush):
             "e2e_ms": ms_e2e, "e2e_pairs_per_s": n_cand / (ms_e2e * 1e-3),
             "timing": "CUDA events; device-resident meshes and fields, and (e2e) pinned host meshes and "
                       "fields with their copies"}
+
+
+def p1_mass_cpu(dim, A, B):
+    """The oracle's P1-P1 product (the reference's per-candidate clipping
+    and quadrature, 1 host thread) on a corner-box sample of the workload
+    with 1/64 of A's elements: candidate pairs per second, the search
+    included."""
+    import oracle
+
+    As, Bs, desc = corner_sample(dim, A, B, frac=1.0 / 64)
+    t0 = time.perf_counter()
+    ip, ind = oracle.tree_finder(dim, As, Bs)
+    oracle.p1_mass(dim, As, Bs, ip, ind, As[0][:, 0], Bs[0][:, 1])
+    dt = time.perf_counter() - t0
+    return {"value": len(ind) / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
+            "sample": f"{desc} ({len(ind)} candidates), oracle tree finder + P1 product, 1 thread, {dt:.2f} s"}
 
 
 def elements_timing(ctx, dim, tA, tB, n_cand, stream, flush):
