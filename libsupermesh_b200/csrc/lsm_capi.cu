@@ -96,6 +96,7 @@ struct Ctx {
   // pinned staging of the single-pair entries (inputs and the whole output
   // buffer travel through it, one host wait per call)
   void* pair_io = nullptr;
+  void* pair_io_dev = nullptr;  // the same pinned buffer as seen by kernels (mapped), or null
   // events around the clip kernel of the last narrow phase (option time_kernels)
   cudaEvent_t clip_ev[2] = {nullptr, nullptr};
   // side stream for mesh A's upload and prep (overlaps B's tree build) and
@@ -1082,18 +1083,28 @@ void legacy_check(Ctx* c, int st) {
 // and the output simplices after them.
 constexpr size_t kPairIoBytes = 16384;
 char* pair_io(Ctx* c) {
-  if (!c->pair_io && cudaMallocHost(&c->pair_io, kPairIoBytes) != cudaSuccess) {
-    (void)cudaGetLastError();
-    c->pair_io = nullptr;
-    set_error(c, "pinned host allocation of %zu bytes failed", kPairIoBytes);
-    throw Fail{LSM_ERROR_OUT_OF_MEMORY};
+  if (!c->pair_io) {
+    if (cudaMallocHost(&c->pair_io, kPairIoBytes) != cudaSuccess) {
+      (void)cudaGetLastError();
+      c->pair_io = nullptr;
+      set_error(c, "pinned host allocation of %zu bytes failed", kPairIoBytes);
+      throw Fail{LSM_ERROR_OUT_OF_MEMORY};
+    }
+    // page-locked memory is mapped for the device under unified addressing:
+    // the per-pair kernels then read their inputs and write their outputs
+    // there directly (no copy calls); without a mapping the copies stay
+    if (cudaHostGetDevicePointer(&c->pair_io_dev, c->pair_io, 0) != cudaSuccess) {
+      (void)cudaGetLastError();
+      c->pair_io_dev = nullptr;
+    }
   }
   return static_cast<char*>(c->pair_io);
 }
 
-// One pair through the batched kernels: inputs copied into pinned staging
-// and sent in one copy, the kernel, then the count and the whole output
-// buffer (at most cap simplices) back in one copy, one host wait.
+// One pair through the batched kernels: inputs staged in a pinned buffer
+// that the kernel reads and writes directly (mapped), or, without a mapping,
+// sent in one copy with the count and the output buffer back in one copy;
+// one host wait.
 void single_pair(int dim, const double* a, const double* b, double* out_elems, int* n_out) {
   std::lock_guard<std::mutex> lk(g_mutex);
   Ctx* c = legacy_ctx();
@@ -1105,14 +1116,23 @@ void single_pair(int dim, const double* a, const double* b, double* out_elems, i
     double* hin = reinterpret_cast<double*>(io);
     memcpy(hin, a, sizeof(double) * per);
     memcpy(hin + per, b, sizeof(double) * per);
-    double* din = ensure<double>(c, c->x_a, 2 * per);
-    const size_t out_bytes = 16 + sizeof(double) * (size_t)cap * per;
-    char* dout = ensure<char>(c, c->x_elems, (int64_t)out_bytes);
-    CU(cudaMemcpyAsync(din, hin, sizeof(double) * 2 * per, cudaMemcpyHostToDevice, s));
-    CU(lsm::launch_pairs_explicit(dim, 1, din, din + per, nullptr, reinterpret_cast<int32_t*>(dout),
-                                  reinterpret_cast<double*>(dout + 16), s));
     char* hout = io + 1024;
-    CU(cudaMemcpyAsync(hout, dout, out_bytes, cudaMemcpyDeviceToHost, s));
+    if (c->pair_io_dev) {
+      // the kernel reads the pair from the pinned buffer and writes the count
+      // and the simplices back into it: one launch, one wait
+      char* dio = static_cast<char*>(c->pair_io_dev);
+      const double* din = reinterpret_cast<const double*>(dio);
+      CU(lsm::launch_pairs_explicit(dim, 1, din, din + per, nullptr, reinterpret_cast<int32_t*>(dio + 1024),
+                                    reinterpret_cast<double*>(dio + 1024 + 16), s));
+    } else {
+      double* din = ensure<double>(c, c->x_a, 2 * per);
+      const size_t out_bytes = 16 + sizeof(double) * (size_t)cap * per;
+      char* dout = ensure<char>(c, c->x_elems, (int64_t)out_bytes);
+      CU(cudaMemcpyAsync(din, hin, sizeof(double) * 2 * per, cudaMemcpyHostToDevice, s));
+      CU(lsm::launch_pairs_explicit(dim, 1, din, din + per, nullptr, reinterpret_cast<int32_t*>(dout),
+                                    reinterpret_cast<double*>(dout + 16), s));
+      CU(cudaMemcpyAsync(hout, dout, out_bytes, cudaMemcpyDeviceToHost, s));
+    }
     CU(cudaStreamSynchronize(s));
     const int k = *reinterpret_cast<int32_t*>(hout);
     *n_out = k;
