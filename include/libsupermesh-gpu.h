@@ -235,9 +235,10 @@ int libsupermesh_gpu_get_pair_results(lsm_gpu_context *ctx, double *measure,
  * the reference's output order (slots past a pair's n_out are left
  * unspecified).  Tet batches of 2048 pairs or more run through per-pair
  * setup, the exact early-out pass and the index clipper; smaller ones through
- * a one-launch clipper (same results).  With on_device = 1 and dim = 3, a and b
- * must be 16-byte aligned (tetrahedra are read with 16-byte loads); other
- * pointers return LSM_ERROR_INVALID_ARGUMENT before any launch. */
+ * a one-launch clipper (same results).  With on_device = 1 and dim = 3, a, b
+ * and elems must be 16-byte aligned (tetrahedra are read and written with
+ * 16-byte accesses); other pointers return LSM_ERROR_INVALID_ARGUMENT before
+ * any launch. */
 int libsupermesh_gpu_intersect_pairs(lsm_gpu_context *ctx, int dim, int64_t n,
                                      const double *a, const double *b,
                                      double *measure, int32_t *n_out,
@@ -255,7 +256,7 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context *ctx, int dim, int64_t n,
  *                       Supermesh.F90:303-334: A sliced into five tets)
  * measure[n] = sum of output measures, n_out[n] = number of outputs, elems
  * optional, in the reference's output order.  With on_device = 1 and kind
- * LSM_PAIR_TET_HEX, a must be 16-byte aligned (as for
+ * LSM_PAIR_TET_HEX, a and elems must be 16-byte aligned (as for
  * libsupermesh_gpu_intersect_pairs). */
 enum {
   LSM_PAIR_INTERVALS = 0,

@@ -1904,6 +1904,9 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context* ctx, int dim, int64_t n, c
     REQUIRE(a && b, "NULL element arrays");
     REQUIRE(!on_device || dim == 2 || ((((uintptr_t)a | (uintptr_t)b) & 15u) == 0),
             "device tetrahedron arrays must be 16-byte aligned (a %p, b %p)", (const void*)a, (const void*)b);
+    // output tets are written with 16-byte stores
+    REQUIRE(!on_device || dim == 2 || ((uintptr_t)elems & 15u) == 0,
+            "device elems must be 16-byte aligned (%p)", (const void*)elems);
     cudaStream_t s = pick(c, stream);
     const int per = dim == 2 ? 6 : 12;
     const int64_t cap = dim == 2 ? 22 : 81;
@@ -1962,8 +1965,9 @@ int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context* ctx, int kind, int64
     REQUIRE(n >= 0, "negative pair count");
     if (n == 0) return;
     REQUIRE(a && b, "NULL element arrays");
-    REQUIRE(!on_device || kind != LSM_PAIR_TET_HEX || (((uintptr_t)a & 15u) == 0),
-            "device tetrahedron array a must be 16-byte aligned (%p)", (const void*)a);
+    REQUIRE(!on_device || kind != LSM_PAIR_TET_HEX || ((((uintptr_t)a | (uintptr_t)elems) & 15u) == 0),
+            "device tetrahedron array a and elems must be 16-byte aligned (a %p, elems %p)", (const void*)a,
+            (const void*)elems);
     cudaStream_t s = pick(c, stream);
     const MixedShape m = mixed_shape(kind);
     const double *da = a, *db = b;

@@ -64,6 +64,13 @@ def test_misaligned_device_tets_are_refused(gpu_ctx):
                                                   ctypes.c_void_p(meas.data_ptr()),
                                                   ctypes.c_void_p(nout.data_ptr()), None, 1, None)
     assert st == LSM_ERROR_INVALID_ARGUMENT
+    # aligned inputs, output tets at an odd double offset (16-byte stores)
+    elems = torch.zeros(n * 81 * 12 + 2, dtype=torch.float64, device="cuda")
+    st = L.libsupermesh_gpu_intersect_pairs(gpu_ctx._h, 3, n, ctypes.c_void_p(da.data_ptr()),
+                                            ctypes.c_void_p(db.data_ptr()), ctypes.c_void_p(meas.data_ptr()),
+                                            ctypes.c_void_p(nout.data_ptr()), ctypes.c_void_p(elems.data_ptr() + 8),
+                                            1, None)
+    assert st == LSM_ERROR_INVALID_ARGUMENT
     # the context is untouched: the aligned copies give the host results
     ga = da[1:].clone()
     gb = db[1:].clone()
