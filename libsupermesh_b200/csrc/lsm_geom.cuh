@@ -260,13 +260,17 @@ __device__ __forceinline__ void tet_faces_screen(const Tet& t, double* o) {
   const double drift = 128.0 * kEps * (1.0 + max_abs_tet(t));
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
+    // a face of a degenerate A (a repeated vertex: zero cross product, NaN
+    // normal) proves nothing: (0, 0, 0, +inf) never rejects.  fmax would
+    // skip the NaN products and leave h at -inf, which rejects every B.
+    const bool ok = isfinite(P.nx[i]) && isfinite(P.ny[i]) && isfinite(P.nz[i]);
     double h = -pos_inf();
 #pragma unroll
     for (int k = 0; k < 4; ++k) h = fmax(h, (P.nx[i] * t.x[k] + P.ny[i] * t.y[k]) + P.nz[i] * t.z[k]);
-    o[4 * i + 0] = P.nx[i];
-    o[4 * i + 1] = P.ny[i];
-    o[4 * i + 2] = P.nz[i];
-    o[4 * i + 3] = h + drift;
+    o[4 * i + 0] = ok ? P.nx[i] : 0.0;
+    o[4 * i + 1] = ok ? P.ny[i] : 0.0;
+    o[4 * i + 2] = ok ? P.nz[i] : 0.0;
+    o[4 * i + 3] = ok && isfinite(h) ? h + drift : pos_inf();
   }
 }
 

@@ -680,3 +680,39 @@ def test_batched_device_inputs_and_empty_mesh(gpu_ctx):
     torch.cuda.synchronize()
     t, nc, ni = gpu_ctx.supermesh_batched(tdev, on_device=True)
     assert np.array_equal(nc, nc_ref) and np.array_equal(ni, ni_ref) and np.array_equal(t, t_ref)
+
+
+def _with_degenerate(dim, mesh, seed, count=40):
+    """The mesh plus `count` zero-measure elements over its nodes: half with
+    a repeated node, half flat (the last node replaced by a new node at the
+    midpoint of the first two)."""
+    pos, en = mesh
+    rng = np.random.default_rng(seed)
+    extra = en[rng.choice(len(en), count, replace=False)].copy()
+    h = count // 2
+    extra[:h, 1] = extra[:h, 0]
+    mid = 0.5 * (pos[extra[h:, 0]] + pos[extra[h:, 1]])
+    extra[h:, -1] = np.arange(len(pos), len(pos) + len(mid))
+    return np.vstack([pos, mid]), np.vstack([en, extra]).astype(en.dtype)
+
+
+@pytest.mark.parametrize("name", ["small2d_9x11", "small3d_5x6"])
+def test_identical_and_degenerate_meshes(gpu_ctx, oracle_mod, name):
+    """A mesh against itself (every element meets its copy exactly, its
+    neighbours along shared faces), and meshes with zero-measure elements
+    (repeated or collinear/coplanar nodes: NaN planes and zero tolerances)
+    on either side: per-pair results equal the oracle's."""
+    dim, A, B = M.config_meshes(name)
+    check_pipeline(gpu_ctx, oracle_mod, dim, A, A, domain=1.0)
+    Ad, Bd = _with_degenerate(dim, A, 3), _with_degenerate(dim, B, 4)
+    check_pipeline(gpu_ctx, oracle_mod, dim, Ad, B)
+    check_pipeline(gpu_ctx, oracle_mod, dim, A, Bd)
+    check_pipeline(gpu_ctx, oracle_mod, dim, Ad, Bd)
+    # the supermesh's simplices of the degenerate pairs too
+    st, off, el, pa, pb = gpu_ctx.supermesh_elements(Ad, Bd)
+    ip, ind = gpu_ctx.get_candidates(len(Ad[1]), st.n_candidates)
+    rws = np.repeat(np.arange(len(ip) - 1), np.diff(ip))
+    for k in range(st.n_candidates):
+        ea, eb = Ad[0][Ad[1][rws[k]]], Bd[0][Bd[1][ind[k]]]
+        ref = oracle_mod.intersect_tris(ea, eb) if dim == 2 else oracle_mod.intersect_tets(ea, eb)
+        assert np.array_equal(el[off[k]:off[k + 1]], np.asarray(ref).reshape((-1,) + el.shape[1:])), k
