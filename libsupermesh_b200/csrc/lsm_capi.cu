@@ -350,6 +350,17 @@ MeshDev upload(Ctx* c, const lsm_gpu_mesh* m, int on_device, DevBuf& pos, DevBuf
 
 int* bad_flag(Ctx* c) { return ensure<int>(c, c->misc, 64); }
 
+// The narrow phase's work lists carry candidate indices as 32-bit ints
+// (survivor records, overflow lists): more candidates than that are refused
+// (the search alone, with its 64-bit offsets, has no such limit).
+void require_pair_index(Ctx* c, int64_t n) {
+  if (n > INT32_MAX) {
+    set_error(c, "%lld candidate pairs: the narrow phase takes at most 2^31-1 per call (split the meshes)",
+              (long long)n);
+    throw Fail{LSM_ERROR_CAPACITY};
+  }
+}
+
 // Explicit tet pair batches of at least this many pairs run through the
 // early-out pass and the index clipper (work counters: misc ints 20-23).
 constexpr int64_t kPairsPipelineMin = 2048;
@@ -589,6 +600,7 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
 void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_t* n_dev = nullptr,
             bool list_inside = false) {
   const int64_t nnz = c->ncand;
+  require_pair_index(c, nnz);
   double* pm = ensure<double>(c, c->pair_measure, nnz);
   int32_t* pn = ensure<int32_t>(c, c->pair_nout, nnz);
   const int nred = lsm::reduce_pairs_blocks();
@@ -1925,7 +1937,7 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context* ctx, int dim, int64_t n, c
       dn = n_out ? ensure<int32_t>(c, c->x_nout, n) : nullptr;
       de = elems ? ensure<double>(c, c->x_elems, n * cap * per) : nullptr;
     }
-    if (dim == 3 && n >= kPairsPipelineMin) {
+    if (dim == 3 && n >= kPairsPipelineMin && n <= INT32_MAX) {
       // large batches: per-pair setup, the exact early-outs and the index
       // clipper (one launch per stage); small ones stay on the one-launch
       // register clipper below (identical results)
@@ -1985,7 +1997,7 @@ int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context* ctx, int kind, int64
       dn = n_out ? ensure<int32_t>(c, c->x_nout, n) : nullptr;
       de = elems ? ensure<double>(c, c->x_elems, n * m.cap * m.per_out) : nullptr;
     }
-    if (kind == LSM_PAIR_TET_HEX && n >= kPairsPipelineMin) {
+    if (kind == LSM_PAIR_TET_HEX && n >= kPairsPipelineMin && n <= INT32_MAX) {
       // large batches: per-pair setup, the exact early-out and the six-plane
       // index clipper; small ones stay on the one-launch clipper (same results)
       double* pm = dm ? dm : ensure<double>(c, c->x_measure, n);
@@ -2016,6 +2028,7 @@ int libsupermesh_gpu_p1_mass(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const 
     REQUIRE(a->dim == 2 || a->dim == 3, "P1 mass matrix: Invalid dimension %d", a->dim);
     find_candidates(c, a, b, on_device, true, true, s);
     const int64_t nnz = c->ncand;
+    require_pair_index(c, nnz);
     const int loc = c->dim + 1;
     const double *du = u_a, *dv = v_b;
     if (!on_device && u_a && v_b) {
