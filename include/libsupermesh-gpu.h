@@ -18,6 +18,10 @@
  *     of the last failure (libsupermesh_gpu_last_error).
  *   - stream: a cudaStream_t (NULL = the context's own stream).  Calls are
  *     synchronous with respect to the host unless stated otherwise.
+ *   - a call that clips (supermesh, P1, elements, batched groups) takes at
+ *     most 2^31-1 candidate pairs (per dimension group for the batched
+ *     entries); beyond that it returns LSM_ERROR_CAPACITY before clipping
+ *     (the candidate search alone has no such limit).
  */
 #ifndef LIBSUPERMESH_GPU_H
 #define LIBSUPERMESH_GPU_H
