@@ -716,3 +716,28 @@ def test_identical_and_degenerate_meshes(gpu_ctx, oracle_mod, name):
         ea, eb = Ad[0][Ad[1][rws[k]]], Bd[0][Bd[1][ind[k]]]
         ref = oracle_mod.intersect_tris(ea, eb) if dim == 2 else oracle_mod.intersect_tets(ea, eb)
         assert np.array_equal(el[off[k]:off[k + 1]], np.asarray(ref).reshape((-1,) + el.shape[1:])), k
+
+
+@pytest.mark.parametrize("name", ["small2d_3x4", "small3d_2x3"])
+def test_empty_meshes_through_every_entry(gpu_ctx, name):
+    """An empty A (or B) through the supermesh, its simplices, the P1-P1
+    product and the per-candidate outputs: no candidates, zero results, no
+    error; the context then serves a normal call."""
+    dim, A, B = M.config_meshes(name)
+    loc = dim + 1
+    emptyA = (A[0], np.zeros((0, loc), dtype=A[1].dtype))
+    emptyB = (B[0], np.zeros((0, loc), dtype=B[1].dtype))
+    for X, Y in ((emptyA, B), (A, emptyB), (emptyA, emptyB)):
+        st, off, el, pa, pb = gpu_ctx.supermesh_elements(X, Y)
+        assert st.n_candidates == 0 and len(el) == 0 and np.array_equal(off, [0])
+        val, blocks = gpu_ctx.p1_mass(X, Y, X[0][:, 0], Y[0][:, 1], want_blocks=True)
+        assert val == 0.0 and len(blocks) == 0
+        out = {"elem_measure": np.zeros(len(X[1])), "ind_ptr": np.zeros(len(X[1]) + 1, dtype=np.int64),
+               "indices": np.zeros(1, dtype=np.int64), "pair_measure": np.zeros(1),
+               "pair_n_out": np.zeros(1, dtype=np.int32), "capacity": 0}
+        st2, n = gpu_ctx.supermesh_out(X, Y, out)
+        assert n == 0 and st2.total_measure == 0.0 and (out["ind_ptr"] == 0).all()
+    m, k, _ = gpu_ctx.intersect_pairs(dim, np.zeros((0, loc, dim)), np.zeros((0, loc, dim)))
+    assert len(m) == 0 and len(k) == 0
+    st, _ = gpu_ctx.supermesh(A, B)
+    assert abs(st.total_measure - 1.0) <= REL_TOL
