@@ -439,6 +439,7 @@ lsm::BVH build_tree(Ctx* c, const MeshDev& b, cudaStream_t s) {
   bvh.hi_esc = bvh.lo_left + 1;
   bvh.leaf = ensure<double>(c, c->bvh_leaf, 8 * n);
   int* work = ensure<int>(c, c->bvh_work, 8 * n);
+  bvh.bucket = lsm::tree_bucket((int)n, true);
   CU(lsm::launch_bvh_build(dim, (int)n, keys, vals, static_cast<float*>(c->b_box32.p), bvh, work, s,
                            static_cast<double*>(c->b_box64.p)));
   return bvh;

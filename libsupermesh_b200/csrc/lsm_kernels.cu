@@ -59,6 +59,11 @@ int query_block() { return g_query_block; }
 void set_query_block(int v) { g_query_block = v; }
 int leaf_bucket() { return g_leaf_bucket; }
 void set_leaf_bucket(int v) { g_leaf_bucket = v; }
+int tree_bucket(int n, bool leaf_records) {
+  // buckets need the leaf records and fit the node encoding (first leaf
+  // below 2^27, at most 8 leaves)
+  return leaf_records && g_leaf_bucket > 1 && n < (1 << 27) ? g_leaf_bucket : 1;
+}
 
 void count_launch(int n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 
@@ -859,7 +864,7 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
   // leaf buckets need the leaf records (box64) and fit the node encoding
   // (first leaf below 2^27, at most 8 leaves)
   int* first_leaf = right + n;
-  const bool buckets = box64 && g_leaf_bucket > 1 && n < (1 << 27);
+  const bool buckets = tree_bucket(n, box64 != nullptr) > 1;
   if (n > 1) {
     k_bvh_internal<<<(n - 1 + 255) / 256, 256, 0, s>>>(n, sorted_keys, parent, rope, last, left, right,
                                                        buckets ? first_leaf : nullptr);
@@ -919,7 +924,7 @@ __device__ __forceinline__ void cache_put(int32_t* cache, int cap, const Spill& 
 // leaf visit is one load that gives the exact box test and the next node;
 // without them it reads the leaf's FP32 node and then the element's FP64
 // box, two dependent loads.  Both give the same candidates in the same order.
-template <int DIM, bool FILL>
+template <int DIM, bool FILL, bool BUCKET>
 __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __restrict__ box64_a,
                                                const float4* __restrict__ lo_left,
                                                const float4* __restrict__ hi_esc, int n,
@@ -979,7 +984,7 @@ __global__ void __launch_bounds__(256) k_query(int64_t nel_a, const double* __re
       if (DIM == 3) ov = ov && H.z > ql[2] && L.z < qh[2];
       if (ov) {
         const int w = __float_as_int(L.w);
-        if (node < n - 1 && w < 0) {
+        if (BUCKET && node < n - 1 && w < 0) {
           // leaf bucket: its sorted leaves in order, exact FP64 test each
           // (independent loads), then on past the subtree
           const int f = w & 0x07ffffff, nl = ((w >> 27) & 7) + 1;
@@ -1104,16 +1109,19 @@ cudaError_t launch_query(int dim, bool fill, int64_t nel_a, const double* box64_
 #define LSM_QUERY_ARGS                                                                                    \
   nel_a, box64_a, bvh.lo_left, bvh.hi_esc, bvh.n, box64_b, counts, offsets, pair_a, pair_b, cc, cap, rows, \
       over_rows, bvh.leaf, pair_cap
+  // the bucket scan is compiled in only where the hierarchy has buckets:
+  // without them its branch alone slows the walk (2D count pass +27%)
+  const bool bk = bvh.bucket > 1;
   if (dim == 2) {
     if (fill)
-      k_query<2, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
+      bk ? k_query<2, true, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS) : k_query<2, true, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
     else
-      k_query<2, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
+      bk ? k_query<2, false, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS) : k_query<2, false, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
   } else {
     if (fill)
-      k_query<3, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
+      bk ? k_query<3, true, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS) : k_query<3, true, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
     else
-      k_query<3, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
+      bk ? k_query<3, false, true><<<g, B, 0, s>>>(LSM_QUERY_ARGS) : k_query<3, false, false><<<g, B, 0, s>>>(LSM_QUERY_ARGS);
   }
 #undef LSM_QUERY_ARGS
   return cudaGetLastError();

@@ -51,6 +51,9 @@ void set_query_block(int v);
 // records instead of being walked.
 int leaf_bucket();
 void set_leaf_bucket(int v);
+// The bucket size launch_bvh_build uses for n leaves (1 = none); BVH::bucket
+// must carry it to the search.
+int tree_bucket(int n, bool leaf_records);
 
 struct BVH {
   int n = 0;                 // leaves
@@ -61,6 +64,9 @@ struct BVH {
   // optional [n][8] f64 leaf records in sorted order: lo (3), hi (3),
   // {element, escape} as two ints, pad
   double* leaf = nullptr;
+  // internal nodes of at most `bucket` leaves carry a leaf-bucket code in
+  // place of their left child (1: none)
+  int bucket = 1;
 };
 
 // Mesh prep: gather coordinates, boxes, measures/tolerances, B clip setup.
