@@ -792,6 +792,7 @@ __device__ __forceinline__ int bvh_escape(int n, int node, const int* __restrict
   return r == n - 1 ? -1 : rope[r + 1];
 }
 
+template <bool BUCKET>
 __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, const float4* __restrict__ box32,
                             const int* __restrict__ parent, const int* __restrict__ rope,
                             const int* __restrict__ last, const int* __restrict__ left,
@@ -831,7 +832,7 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
     l.y = fminf(a0.y, b0.y);
     l.z = fminf(a0.z, b0.z);
     l.w = __int_as_float(lc);
-    if (first_leaf) {
+    if (BUCKET) {
       // a subtree of at most `bucket` leaves becomes a bucket: the node
       // records its first sorted leaf and leaf count instead of its left
       // child, and the search scans those leaf records in order
@@ -870,10 +871,14 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
                                                        buckets ? first_leaf : nullptr);
   }
   cudaMemsetAsync(parent, 0xff, sizeof(int), s);  // parent[root] = -1
-  k_bvh_refit<<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
-                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim, box64,
-                                              box64 ? bvh.leaf : nullptr, buckets ? first_leaf : nullptr,
-                                              g_leaf_bucket);
+  if (buckets)
+    k_bvh_refit<true><<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
+                                                      rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim,
+                                                      box64, bvh.leaf, first_leaf, g_leaf_bucket);
+  else
+    k_bvh_refit<false><<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
+                                                       rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim,
+                                                       box64, box64 ? bvh.leaf : nullptr, nullptr, 1);
   return cudaGetLastError();
 }
 
@@ -1063,18 +1068,23 @@ __global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const in
       const int c = __shfl_sync(0xffffffffu, cnt, r);
       const int64_t o = __shfl_sync(0xffffffffu, off, r);
       const int64_t row = base + r;
+      // entries of this row that fit the pair arrays (all of them unless a
+      // capacity-mode call outgrew its arrays)
+      const int64_t room = pair_cap - o;
+      const int lim = room >= c ? c : (room > 0 ? (int)room : 0);
       if (c > cap) {
         // the cached head, then the row's chain of spill chunks; rows that
         // lost theirs (-2) are filled by the traversal over the listed rows
         const int first = sp.row_chunk ? sp.row_chunk[row] : -2;
         if (first < 0) continue;
-        for (int k = lane; k < cap && o + k < pair_cap; k += 32) {
+        const int head = lim < cap ? lim : cap;
+        for (int k = lane; k < head; k += 32) {
           pair_a[o + k] = (int32_t)row;
           pair_b[o + k] = cache[row * cap + k];
         }
         int ch = first;
         for (int k0 = cap; k0 < c; k0 += kSpillChunk) {
-          for (int k = lane; k < kSpillChunk && k0 + k < c && o + k0 + k < pair_cap; k += 32) {
+          for (int k = lane; k < kSpillChunk && k0 + k < lim; k += 32) {
             pair_a[o + k0 + k] = (int32_t)row;
             pair_b[o + k0 + k] = sp.pool[(int64_t)ch * kSpillChunk + k];
           }
@@ -1082,7 +1092,7 @@ __global__ void __launch_bounds__(256) k_fill_from_cache(int64_t nel_a, const in
         }
         continue;
       }
-      for (int k = lane; k < c && o + k < pair_cap; k += 32) {
+      for (int k = lane; k < lim; k += 32) {
         pair_a[o + k] = (int32_t)row;
         pair_b[o + k] = cache[row * cap + k];
       }
@@ -2471,9 +2481,9 @@ cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const
   if (n > 1) k_bvh_internal64<<<(n - 1 + 255) / 256, 256, 0, s>>>(n, codes, parent, rope, last, left, right, mesh_off_b, roots);
   cudaMemsetAsync(parent, 0xff, sizeof(int), s);
   k_mesh_roots<<<(nm + 255) / 256, 256, 0, s>>>(nm, n, mesh_off_b, rope, last, roots, stops);
-  k_bvh_refit<<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
-                                              rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim, box64,
-                                              box64 ? bvh.leaf : nullptr, nullptr, 1);
+  k_bvh_refit<false><<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
+                                                     rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim,
+                                                     box64, box64 ? bvh.leaf : nullptr, nullptr, 1);
   return cudaGetLastError();
 }
 
