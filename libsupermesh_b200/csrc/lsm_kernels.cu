@@ -16,7 +16,11 @@
 //                       memory, FP64 Sutherland-Hodgman
 //   K6  k_prefilter_tets two exact early-outs and the no-op plane mask;
 //                       k_clip_tets_ix depth-first clipping over point
-//                       indices with a refill pipeline
+//                       indices with a refill pipeline, templated on what it
+//                       does with the kept tets (measures; explicit pairs'
+//                       output tets; the supermesh's tets at their offsets;
+//                       the P1 quadrature) and on the plane count (4: tets,
+//                       6: hexahedra)
 //   K7  compensated reductions (per-block (sum, err), then final; per mesh
 //                       pair for the batched path)
 //   K8  P1-P1 mixed mass blocks + u^T M v: 2D k_p1_mass; 3D the early-out
@@ -25,7 +29,10 @@
 //   K9  1D sort finder  k_prep_1d, 64-bit stable sort, max segment tree,
 //                       k_rows_1d, k_sweep_1d, k_emit_1d;  k_clip_intervals
 //   K10 explicit pairs  k_pairs_tris / _tets and the mixed element pairs
-//                       (intervals, tri-quad, quad-quad, tet-hex, hex-hex)
+//                       (intervals, tri-quad, quad-quad, tet-hex, hex-hex);
+//                       large tet-tet / tet-hex batches: k_setup_pairs3 /
+//                       k_setup_hex_pairs, then K6
+//   K13 supermesh elements  K6's emit pass (3D), k_tris_emit (2D)
 //
 // Everything FP64 is compiled with -fmad=false so that each +,-,*,/ is a
 // separately rounded IEEE operation, matching libsupermesh's gfortran build.
