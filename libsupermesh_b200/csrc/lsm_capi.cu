@@ -103,6 +103,11 @@ struct Ctx {
   // the events that order it with the caller's stream
   cudaStream_t side = nullptr;
   cudaEvent_t side_ev[2] = {nullptr, nullptr};
+  // large host meshes: element lists copied in chunks on their own stream,
+  // each chunk's prep waiting for its copy (events: B's chunks, A's chunks,
+  // and the copy stream's waits for earlier work)
+  cudaStream_t copy = nullptr;
+  cudaEvent_t chunk_ev[10] = {};
   bool clip_timed = false;
   bool surv_valid = false;  // surv holds the clipper's pair count of the last 3D narrow phase
   // bumped whenever a device buffer is (re)allocated: a captured graph holds
@@ -168,12 +173,13 @@ void set_error(Ctx* c, const char* fmt, ...) {
 // failed call returns with no copy or kernel of its own still reading the
 // caller's meshes.
 struct SyncOnThrow {
-  cudaStream_t s0, s1;
+  cudaStream_t s0, s1, s2 = nullptr;
   int depth = std::uncaught_exceptions();
   ~SyncOnThrow() {
     if (std::uncaught_exceptions() > depth) {
       cudaStreamSynchronize(s0);
       cudaStreamSynchronize(s1);
+      if (s2) cudaStreamSynchronize(s2);
     }
   }
 };
@@ -248,9 +254,15 @@ int init_ctx(int device, Ctx* c) {
       cudaEventCreate(&c->clip_ev[0]) != cudaSuccess || cudaEventCreate(&c->clip_ev[1]) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->side_ev[0], cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->side_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&c->side_ev[1], cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
     (void)cudaGetLastError();
     return LSM_ERROR_CUDA;
+  }
+  for (cudaEvent_t& e : c->chunk_ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return LSM_ERROR_CUDA;
   }
   return LSM_SUCCESS;
 }
@@ -285,6 +297,16 @@ void fini_ctx(Ctx* c) {
       cudaEventDestroy(e);
       e = nullptr;
     }
+  for (cudaEvent_t& e : c->chunk_ev)
+    if (e) {
+      cudaEventDestroy(e);
+      e = nullptr;
+    }
+  if (c->copy) {
+    cudaStreamSynchronize(c->copy);
+    cudaStreamDestroy(c->copy);
+    c->copy = nullptr;
+  }
   if (c->side) {
     cudaStreamSynchronize(c->side);
     cudaStreamDestroy(c->side);
@@ -398,24 +420,67 @@ lsm::Spill make_spill(Ctx* c, int64_t nel, int cap) {
 
 // prep of the query mesh A: coords (simplices only), box64, tol; tets also
 // get their face planes for the clipper's separation screen
-void prep_a(Ctx* c, const MeshDev& a, bool simplex, cudaStream_t s) {
+// Prep of elements [e0, e0 + n) of A or B (every per-element output at its
+// element's offset); the buffers are sized for the whole mesh first.
+void prep_a_range(Ctx* c, const MeshDev& a, bool simplex, int64_t e0, int64_t n, cudaStream_t s) {
   double* coords = simplex ? ensure<double>(c, c->a_coords, a.nel * a.loc * a.dim) : nullptr;
   double* box = ensure<double>(c, c->a_box64, a.nel * 2 * a.dim);
   double* tol = simplex ? ensure<double>(c, c->a_tol, a.nel) : nullptr;
   double* faces = simplex && a.dim == 3 ? ensure<double>(c, c->a_faces, a.nel * lsm::kScreen3) : nullptr;
-  CU(lsm::launch_prep(a.dim, a.loc, a.nel, a.pos, a.en, a.idx_bytes, coords, box, nullptr, tol, nullptr,
-                      bad_flag(c), a.nnodes, s, faces));
+  if (n <= 0) return;
+  const char* en = static_cast<const char*>(a.en) + e0 * a.loc * a.idx_bytes;
+  CU(lsm::launch_prep(a.dim, a.loc, n, a.pos, en, a.idx_bytes, coords ? coords + e0 * a.loc * a.dim : nullptr,
+                      box + e0 * 2 * a.dim, nullptr, tol ? tol + e0 : nullptr, nullptr, bad_flag(c), a.nnodes, s,
+                      faces ? faces + e0 * lsm::kScreen3 : nullptr));
 }
 
-void prep_b(Ctx* c, const MeshDev& b, bool simplex, bool want_coords, cudaStream_t s) {
+void prep_b_range(Ctx* c, const MeshDev& b, bool simplex, bool want_coords, int64_t e0, int64_t n, cudaStream_t s) {
   double* coords = want_coords ? ensure<double>(c, c->b_coords, b.nel * b.loc * b.dim) : nullptr;
   double* box = ensure<double>(c, c->b_box64, b.nel * 2 * b.dim);
   float* box32 = ensure<float>(c, c->b_box32, b.nel * 8);
-  double* setup = nullptr;
-  if (simplex) setup = ensure<double>(c, c->b_setup, b.nel * (b.dim == 2 ? lsm::kSetup2 : lsm::kSetup3));
+  const int srow = b.dim == 2 ? lsm::kSetup2 : lsm::kSetup3;
+  double* setup = simplex ? ensure<double>(c, c->b_setup, b.nel * srow) : nullptr;
   double* screen = simplex && b.dim == 3 ? ensure<double>(c, c->b_screen, b.nel * lsm::kScreen3) : nullptr;
-  CU(lsm::launch_prep(b.dim, b.loc, b.nel, b.pos, b.en, b.idx_bytes, coords, box, box32, nullptr, setup,
-                      bad_flag(c), b.nnodes, s, nullptr, screen));
+  if (n <= 0) return;
+  const char* en = static_cast<const char*>(b.en) + e0 * b.loc * b.idx_bytes;
+  CU(lsm::launch_prep(b.dim, b.loc, n, b.pos, en, b.idx_bytes, coords ? coords + e0 * b.loc * b.dim : nullptr,
+                      box + e0 * 2 * b.dim, box32 + e0 * 8, nullptr, setup ? setup + e0 * srow : nullptr,
+                      bad_flag(c), b.nnodes, s, nullptr, screen ? screen + e0 * lsm::kScreen3 : nullptr));
+}
+
+// Large host meshes: the element list is copied in kPrepChunks pieces on the
+// context's copy stream (after the node positions), and the prep of each
+// piece, on the mesh's own stream, waits only for that piece's copy, so the
+// copies and the prep overlap.  ev[k] marks piece k's copy.
+constexpr int64_t kPrepChunkMin = 1 << 18;
+constexpr int kPrepChunks = 4;
+
+MeshDev upload_chunks(Ctx* c, const lsm_gpu_mesh* m, DevBuf& pos, DevBuf& en, int chunks, cudaEvent_t* ev) {
+  MeshDev d{m->dim, m->loc, m->index_bytes, m->nnodes, m->nelements, m->positions, m->enlist};
+  double* p = ensure<double>(c, pos, m->nnodes * m->dim);
+  char* e = ensure<char>(c, en, m->nelements * m->loc * m->index_bytes);
+  d.pos = p;
+  d.en = e;
+  if (m->nelements > 0)
+    CU(cudaMemcpyAsync(p, m->positions, sizeof(double) * m->nnodes * m->dim, cudaMemcpyHostToDevice, c->copy));
+  const size_t row = (size_t)m->loc * m->index_bytes;
+  for (int k = 0; k < chunks; ++k) {
+    const int64_t e0 = m->nelements * k / chunks, e1 = m->nelements * (k + 1) / chunks;
+    if (e1 > e0)
+      CU(cudaMemcpyAsync(e + e0 * row, static_cast<const char*>(m->enlist) + e0 * row, (size_t)(e1 - e0) * row,
+                         cudaMemcpyHostToDevice, c->copy));
+    CU(cudaEventRecord(ev[k], c->copy));
+  }
+  return d;
+}
+
+template <class Prep>
+void prep_chunks(Ctx* c, const MeshDev& d, int chunks, const cudaEvent_t* ev, cudaStream_t s, Prep prep) {
+  for (int k = 0; k < chunks; ++k) {
+    const int64_t e0 = d.nel * k / chunks, e1 = d.nel * (k + 1) / chunks;
+    CU(cudaStreamWaitEvent(s, ev[k], 0));
+    prep(e0, e1 - e0);
+  }
 }
 
 lsm::BVH build_tree(Ctx* c, const MeshDev& b, cudaStream_t s) {
@@ -531,16 +596,37 @@ void find_candidates(Ctx* c, const lsm_gpu_mesh* ma, const lsm_gpu_mesh* mb, int
   simplex = simplex || (ma->loc == ma->dim + 1 && mb->loc == mb->dim + 1);
   // A's upload and prep run on the side stream, overlapping B's prep and
   // tree build on s; s waits for them before the search.  A's copies start
-  // once B's are done, so B's (on the critical path) get the whole link.
+  // once B's are done, so B's (on the critical path) get the whole link;
+  // large host meshes come in chunks whose prep overlaps the next copy.
   SyncOnThrow sync_on_throw{s, c->side};
   CU(cudaMemsetAsync(bad_flag(c), 0, sizeof(int) * 64, s));
-  MeshDev b = upload(c, mb, on_device, c->b_pos, c->b_en, s);
-  CU(cudaEventRecord(c->side_ev[0], s));
-  CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
-  MeshDev a = upload(c, ma, on_device, c->a_pos, c->a_en, c->side);
-  prep_a(c, a, simplex, c->side);
+  MeshDev a, b;
+  if (!on_device && std::max(ma->nelements, mb->nelements) >= kPrepChunkMin) {
+    // chunked copies on the copy stream (B's first: B is on the critical
+    // path), once earlier work that may still read these buffers is done
+    sync_on_throw.s2 = c->copy;
+    cudaEvent_t* ev = c->chunk_ev;
+    CU(cudaEventRecord(ev[8], s));
+    CU(cudaEventRecord(ev[9], c->side));
+    CU(cudaStreamWaitEvent(c->copy, ev[8], 0));
+    CU(cudaStreamWaitEvent(c->copy, ev[9], 0));
+    const int kb = mb->nelements >= kPrepChunkMin ? kPrepChunks : 1;
+    const int ka = ma->nelements >= kPrepChunkMin ? kPrepChunks : 1;
+    b = upload_chunks(c, mb, c->b_pos, c->b_en, kb, ev);
+    a = upload_chunks(c, ma, c->a_pos, c->a_en, ka, ev + 4);
+    prep_chunks(c, b, kb, ev, s,
+                [&](int64_t e0, int64_t n) { prep_b_range(c, b, simplex, want_b_coords, e0, n, s); });
+    prep_chunks(c, a, ka, ev + 4, c->side,
+                [&](int64_t e0, int64_t n) { prep_a_range(c, a, simplex, e0, n, c->side); });
+  } else {
+    b = upload(c, mb, on_device, c->b_pos, c->b_en, s);
+    CU(cudaEventRecord(c->side_ev[0], s));
+    CU(cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
+    a = upload(c, ma, on_device, c->a_pos, c->a_en, c->side);
+    prep_a_range(c, a, simplex, 0, a.nel, c->side);
+    prep_b_range(c, b, simplex, want_b_coords, 0, b.nel, s);
+  }
   CU(cudaEventRecord(c->side_ev[1], c->side));
-  prep_b(c, b, simplex, want_b_coords, s);
   const int64_t nel_a = a.nel;
   int64_t* offsets = ensure<int64_t>(c, c->offsets, nel_a + 1);
   int* counts = ensure<int>(c, c->counts, nel_a);
