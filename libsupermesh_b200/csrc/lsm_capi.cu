@@ -76,6 +76,9 @@ struct Ctx {
   // narrow phase
   DevBuf pair_measure, pair_nout, partials, ovf_list, misc, elem_measure, totals;
   DevBuf p1_list;  // survivors of the P1 pass's early-out (kept apart from the narrow phase's)
+  // 3D narrow phase: per-block survivor segment lengths, the clipper's chunk
+  // table, and the compacted list for the consumers that index survivors
+  DevBuf seg_cnt, seg_tab, surv_list;
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
   DevBuf x_setup, x_tol, x_iota, x_faces, x_screen, x_list;  // explicit tet pairs through the early-out pass
@@ -110,6 +113,8 @@ struct Ctx {
   cudaEvent_t chunk_ev[10] = {};
   bool clip_timed = false;
   bool surv_valid = false;  // surv holds the clipper's pair count of the last 3D narrow phase
+  bool surv_seg = false;    // ... and ovf_list holds its survivors as segments (seg_tab)
+  int64_t surv_npairs = 0;  // the pair count that narrow phase was sized for
   // bumped whenever a device buffer is (re)allocated: a captured graph holds
   // buffer addresses and is only replayed while this is unchanged
   uint64_t gen = 0;
@@ -126,6 +131,8 @@ struct Ctx {
     size_t res_off[2] = {0, 0};
     int last_dim = 0, last_loc = 0;
     int64_t last_na = 0, last_nb = 0;
+    bool last_seg = false;
+    int64_t last_surv_npairs = 0;
   } bg;
 
   // state of the last candidate search
@@ -285,7 +292,7 @@ void fini_ctx(Ctx* c) {
                    &c->d1_keyhi, &c->d1_perm_a, &c->d1_perm_b, &c->d1_lo_a, &c->d1_hi_a, &c->d1_lo_b,
                    &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over, &c->q_pool, &c->q_next, &c->q_first,
                    &c->a_faces, &c->b_screen, &c->surv, &c->sched_w, &c->sched_list, &c->sched_cls,
-                   &c->sched_adam, &c->bt_indptr};
+                   &c->sched_adam, &c->bt_indptr, &c->seg_cnt, &c->seg_tab, &c->surv_list};
   for (DevBuf* b : all) free_buf(*b);
   for (cudaEvent_t& e : c->clip_ev)
     if (e) {
@@ -739,14 +746,22 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_
                               screen ? static_cast<double*>(c->a_faces.p) : nullptr,
                               screen ? static_cast<double*>(c->b_screen.p) : nullptr, s));
     c->clip_timed = false;
+    c->surv_seg = false;
   } else {
+    // 3D plain order: survivors as per-block segments, taken by chunks
+    const bool seg = c->dim == 3 && !binned;
+    int* seg_cnt = seg ? ensure<int>(c, c->seg_cnt, lsm::seg_blocks(nnz)) : nullptr;
+    int4* seg_tab = seg ? ensure<int4>(c, c->seg_tab, lsm::seg_table_entries(nnz)) : nullptr;
     CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                         static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                         static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order,
                         g_time_kernels ? c->clip_ev[0] : nullptr, g_time_kernels ? c->clip_ev[1] : nullptr,
                         screen ? static_cast<double*>(c->a_faces.p) : nullptr,
-                        screen ? static_cast<double*>(c->b_screen.p) : nullptr, binned ? &bin : nullptr, n_dev));
+                        screen ? static_cast<double*>(c->b_screen.p) : nullptr, binned ? &bin : nullptr, n_dev,
+                        seg_cnt, seg_tab));
     c->clip_timed = g_time_kernels;
+    c->surv_seg = seg;
+    c->surv_npairs = nnz;
   }
   if (c->dim == 3) {
     CU(cudaMemcpyAsync(ensure<unsigned long long>(c, c->surv, 1), work, sizeof(unsigned long long),
@@ -1380,6 +1395,8 @@ bool replay_batch_graph(Ctx* c, const std::vector<uint64_t>& sig, cudaStream_t s
   c->simplex_prep = true;
   c->have_pairs = true;
   c->surv_valid = g.last_dim == 3;
+  c->surv_seg = g.last_seg;
+  c->surv_npairs = g.last_surv_npairs;
   return true;
 }
 
@@ -1459,6 +1476,8 @@ void capture_batch_graph(Ctx* c, std::vector<uint64_t> sig, const std::vector<in
   g.last_loc = c->loc_a;
   g.last_na = c->nel_a;
   g.last_nb = c->nel_b;
+  g.last_seg = c->surv_seg;
+  g.last_surv_npairs = c->surv_npairs;
 }
 
 // Both batched entries.
@@ -2245,7 +2264,14 @@ int libsupermesh_gpu_sched_samples(lsm_gpu_context* ctx, int64_t cap, void* feat
     }
     cudaStream_t s = pick(c, stream);
     const unsigned long long* nl = reinterpret_cast<const unsigned long long*>(bad_flag(c) + 8);
-    CU(lsm::launch_sched_samples(static_cast<const int4*>(c->ovf_list.p), nl, cap, static_cast<double*>(c->a_coords.p),
+    const int4* list = static_cast<const int4*>(c->ovf_list.p);
+    if (c->surv_seg) {
+      // the survivors in the clipper's order, as one list
+      int4* flat = ensure<int4>(c, c->surv_list, std::max<int64_t>(c->surv_npairs, 1));
+      CU(lsm::launch_seg_compact(c->surv_npairs, nl + 2, static_cast<const int4*>(c->seg_tab.p), list, flat, s));
+      list = flat;
+    }
+    CU(lsm::launch_sched_samples(list, nl, cap, static_cast<double*>(c->a_coords.p),
                                  static_cast<double*>(c->b_screen.p), static_cast<int32_t*>(c->pair_nout.p), features,
                                  classes, s));
     unsigned long long* h = reinterpret_cast<unsigned long long*>(static_cast<char*>(c->host_scalars) + 512);

@@ -1526,7 +1526,14 @@ __device__ __forceinline__ void load_tet(const double* __restrict__ v, Tet& t) {
 // ~7 eps M of an exact convex combination) with room to spare.
 __host__ __device__ constexpr int clip_row(int np) { return 4 * np + 4; }
 
-template <bool kSettle, int NP = 4>
+// Pairs per block of the early-out pass (256 threads): one contiguous range
+// each, a multiple of the block size.
+constexpr int kSegChunk = 64;
+__host__ __device__ inline int64_t seg_per(int64_t npairs, int grid) {
+  return ((npairs + grid - 1) / grid + 255) / 256 * 256;
+}
+
+template <bool kSettle, int NP = 4, bool kSeg = false>
 __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64_t npairs, const int32_t* __restrict__ order,
                                                         const int32_t* __restrict__ pa,
                                                         const int32_t* __restrict__ pb,
@@ -1537,14 +1544,19 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
                                                         int32_t* survivors, unsigned long long* nsurv,
                                                         const double* __restrict__ faces_a,
                                                         const double* __restrict__ screen_b,
-                                                        const int64_t* __restrict__ n_dev) {
+                                                        const int64_t* __restrict__ n_dev, int* seg_count = nullptr) {
   // n_dev (optional): the pair count on the device, npairs its upper bound
   if (n_dev && *n_dev < npairs) npairs = *n_dev;
+  __shared__ unsigned s_cnt;
+  if (kSeg) {
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+  }
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   // each block takes one contiguous range of pairs (consecutive iterations
   // then share A rows and most B elements in L1)
-  const int64_t per = ((npairs + gridDim.x - 1) / gridDim.x + blockDim.x - 1) / blockDim.x * blockDim.x;
+  const int64_t per = seg_per(npairs, gridDim.x);  // a multiple of the block size (256)
   const int64_t beg = (int64_t)blockIdx.x * per;
   const int64_t end = beg + per < npairs ? beg + per : npairs;
   // the pair indices stream from DRAM: each iteration loads the next one's
@@ -1636,7 +1648,9 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
     if (mask) {
       const int leader = __ffs(mask) - 1;
       unsigned long long off = 0;
-      if (lane == leader) off = atomicAdd(nsurv, (unsigned long long)__popc(mask));
+      if (lane == leader)
+        off = kSeg ? (unsigned long long)beg + atomicAdd(&s_cnt, (unsigned)__popc(mask))
+                   : atomicAdd(nsurv, (unsigned long long)__popc(mask));
       off = __shfl_sync(0xffffffffu, off, leader);
       if (live) {
         const int64_t o = (int64_t)off + __popc(mask & lt);
@@ -1644,6 +1658,84 @@ __global__ void __launch_bounds__(256, LSM_PREFILTER_BPS) k_prefilter_tets(int64
       }
     }
   }
+  if (kSeg) {
+    __syncthreads();
+    if (threadIdx.x == 0) seg_count[blockIdx.x] = (int)s_cnt;
+  }
+}
+
+// Segmented survivor lists.  With kSeg the early-out pass takes no global
+// atomic per warp: block k appends its survivors at k * per (per = the pairs
+// a block takes, so a segment never outgrows its range) through a counter
+// in shared memory and writes the segment's length to seg_count[k].  The
+// clipper then claims whole chunks of at most kIxChunk records that lie in
+// one segment from a table, in segment order: {first, end, position in the
+// compacted list, 0}.  The table kernel runs one block per segment (the
+// early-out pass's grid) and writes the survivor count (work[0]) and the
+// chunk count (work[2]).
+int64_t seg_table_entries(int64_t npairs) { return npairs / kSegChunk + (int64_t)sm_count() * 8 + 1; }
+int seg_blocks(int64_t npairs) { return grid_for(npairs, 256, 8); }
+
+__global__ void __launch_bounds__(256) k_seg_chunks(int64_t npairs, const int64_t* __restrict__ n_dev,
+                                                    const int* __restrict__ seg_count, int4* table,
+                                                    unsigned long long* work) {
+  if (n_dev && *n_dev < npairs) npairs = *n_dev;
+  const int64_t per = seg_per(npairs, gridDim.x);
+  __shared__ long long part[2][8];
+  long long sn = 0, sc = 0;
+  for (int k = threadIdx.x; k < (int)blockIdx.x; k += blockDim.x) {
+    const int c = seg_count[k];
+    sn += c;
+    sc += (c + kSegChunk - 1) / kSegChunk;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sn += __shfl_xor_sync(0xffffffffu, sn, o);
+    sc += __shfl_xor_sync(0xffffffffu, sc, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    part[0][threadIdx.x >> 5] = sn;
+    part[1][threadIdx.x >> 5] = sc;
+  }
+  __syncthreads();
+  long long pn = 0, pc = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    pn += part[0][w];
+    pc += part[1][w];
+  }
+  const int cnt = seg_count[blockIdx.x];
+  const int nch = (cnt + kSegChunk - 1) / kSegChunk;
+  const int64_t first = (int64_t)blockIdx.x * per;
+  for (int j = threadIdx.x; j < nch; j += blockDim.x) {
+    const int lo = j * kSegChunk, hi = lo + kSegChunk < cnt ? lo + kSegChunk : cnt;
+    table[pc + j] = make_int4((int)(first + lo), (int)(first + hi), (int)(pn + lo), 0);
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+    work[0] = (unsigned long long)(pn + cnt);
+    work[2] = (unsigned long long)(pc + nch);
+  }
+}
+
+// The segmented list gathered into one compacted list (in table order): for
+// consumers that index survivors directly.  One warp per chunk.
+__global__ void __launch_bounds__(256) k_seg_compact(int64_t max_chunks, const unsigned long long* __restrict__ nchunks,
+                                                     const int4* __restrict__ table, const int4* __restrict__ seg,
+                                                     int4* out) {
+  const int64_t nc = (int64_t)*nchunks < max_chunks ? (int64_t)*nchunks : max_chunks;
+  const int lane = threadIdx.x & 31;
+  for (int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc;
+       c += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int4 t = table[c];
+    for (int k = lane; k < t.y - t.x; k += 32) out[(int64_t)t.z + k] = seg[(int64_t)t.x + k];
+  }
+}
+
+cudaError_t launch_seg_compact(int64_t npairs, const unsigned long long* nchunks, const int4* table,
+                               const int4* seg, int4* out, cudaStream_t s) {
+  const int64_t maxc = seg_table_entries(npairs);
+  count_launch();
+  k_seg_compact<<<grid_for(maxc * 32, 256, 8), 256, 0, s>>>(maxc, nchunks, table, seg, out);
+  return cudaGetLastError();
 }
 
 // ----------------------------------------------------------------------
@@ -1885,7 +1977,10 @@ __host__ __device__ constexpr int ix_points(int np) { return 4 + 4 * np; }
 template <class Sink, int BLOCK, int BPS, int NP = 4>
 __global__ void __launch_bounds__(BLOCK, BPS) k_clip_tets_ix(
     const int4* __restrict__ list, const unsigned long long* __restrict__ nlist, const double* __restrict__ coords_a,
-    const double* __restrict__ tol_a, const double* __restrict__ setup_b, Sink sk, unsigned long long* work) {
+    const double* __restrict__ tol_a, const double* __restrict__ setup_b, Sink sk, unsigned long long* work,
+    const int4* __restrict__ chunks = nullptr) {
+  // chunks (optional): the list is segmented; nlist then counts the table's
+  // chunks and work counts the chunks taken
   static_assert(ix_points(NP) <= 32, "pool indices are 5 bits");
   extern __shared__ double ix_mem[];
   IxPool<BLOCK> pool{ix_mem + threadIdx.x};
@@ -1963,13 +2058,19 @@ __global__ void __launch_bounds__(BLOCK, BPS) k_clip_tets_ix(
       while (wm) {
         if (cbeg >= cend) {
           unsigned long long base = 0;
-          if (lane == 0) base = atomicAdd(work, (unsigned long long)kIxChunk);
+          if (lane == 0) base = atomicAdd(work, chunks ? 1ull : (unsigned long long)kIxChunk);
           base = __shfl_sync(full, base, 0);
-          cbeg = (int64_t)base;
-          cend = cbeg + kIxChunk < npairs ? cbeg + kIxChunk : npairs;
-          if (cbeg >= npairs) {
+          if ((int64_t)base >= npairs) {
             exhausted = true;
             break;
+          }
+          if (chunks) {
+            const int4 ch = chunks[base];
+            cbeg = ch.x;
+            cend = ch.y;
+          } else {
+            cbeg = (int64_t)base;
+            cend = cbeg + kIxChunk < npairs ? cbeg + kIxChunk : npairs;
           }
         }
         const int navail = (int)(cend - cbeg);
@@ -2197,7 +2298,8 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
                         const int32_t* order, cudaEvent_t ev_begin, cudaEvent_t ev_end, const double* faces_a,
-                        const double* screen_b, const SchedBin* bin, const int64_t* n_dev) {
+                        const double* screen_b, const SchedBin* bin, const int64_t* n_dev, int* seg_count,
+                        int4* chunk_table) {
   const int g = clip_grid_blocks(dim);
   count_launch();
   if (dim == 2) {
@@ -2211,9 +2313,19 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     if (ev_begin) cudaEventRecord(ev_begin, s);
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
     count_launch();
-    k_prefilter_tets<true><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, tol_a,
-                                                              setup_b, pair_measure, pair_nout, overflow_list, work,
-                                                              faces_a, screen_b, n_dev);
+    const bool seg = seg_count && chunk_table && !bin;
+    if (seg) {
+      const int gp = seg_blocks(npairs);
+      k_prefilter_tets<true, 4, true><<<gp, 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, tol_a, setup_b,
+                                                        pair_measure, pair_nout, overflow_list, work, faces_a,
+                                                        screen_b, n_dev, seg_count);
+      count_launch();
+      k_seg_chunks<<<gp, 256, 0, s>>>(npairs, n_dev, seg_count, chunk_table, work);
+    } else {
+      k_prefilter_tets<true><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, tol_a,
+                                                                setup_b, pair_measure, pair_nout, overflow_list,
+                                                                work, faces_a, screen_b, n_dev);
+    }
     const int4* list = reinterpret_cast<const int4*>(overflow_list);
     if (bin) {
       // the survivors reordered into class-uniform runs within windows
@@ -2222,7 +2334,8 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
       list = bin->out;
     }
     k_clip_tets_ix<IxMeasureSink, kIxBlock, kIxBlocksPerSm><<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
-        list, work, coords_a, tol_a, setup_b, IxMeasureSink{pair_measure, pair_nout, 0.0, 0}, work + 1);
+        list, seg ? work + 2 : work, coords_a, tol_a, setup_b, IxMeasureSink{pair_measure, pair_nout, 0.0, 0},
+        work + 1, seg ? chunk_table : nullptr);
   }
   if (ev_end) cudaEventRecord(ev_end, s);
   return cudaGetLastError();

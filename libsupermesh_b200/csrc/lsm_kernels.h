@@ -148,8 +148,18 @@ cudaError_t launch_scan(int64_t n, const int* counts, int64_t* offsets, int64_t*
 // second exact early-out (B beyond a face of A).
 // bin (3D, optional): the learned scheduler's reordering of the survivors
 // between the early-out pass and the clipper (lsm_sched.h).
+// seg_count (seg_blocks(npairs) ints) and chunk_table
+// (seg_table_entries(npairs) entries), 3D, optional, not with bin: the
+// survivors are written as per-block segments of overflow_list (no global
+// counter), and the clipper takes them by chunks from the table; `work`
+// then holds four counters (survivors, chunks taken, chunks, unused).
+// launch_seg_compact gathers such a list into a compacted one.
 struct SchedBin;
 int clip_grid_blocks(int dim);
+int seg_blocks(int64_t npairs);
+int64_t seg_table_entries(int64_t npairs);
+cudaError_t launch_seg_compact(int64_t npairs, const unsigned long long* nchunks, const int4* table,
+                               const int4* seg, int4* out, cudaStream_t s);
 cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                         const double* coords_a, const double* tol_a, const double* setup_b,
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
@@ -157,7 +167,8 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         const int32_t* order = nullptr, cudaEvent_t ev_begin = nullptr,
                         cudaEvent_t ev_end = nullptr, const double* faces_a = nullptr,
                         const double* screen_b = nullptr, const SchedBin* bin = nullptr,
-                        const int64_t* n_dev = nullptr);
+                        const int64_t* n_dev = nullptr, int* seg_count = nullptr,
+                        int4* chunk_table = nullptr);
 // Opt-in shared-memory limits for the clip kernels on the current device.
 cudaError_t init_device_attributes();
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
