@@ -79,6 +79,7 @@ struct Ctx {
   // 3D narrow phase: per-block survivor segment lengths, the clipper's chunk
   // table, and the compacted list for the consumers that index survivors
   DevBuf seg_cnt, seg_tab, surv_list;
+  DevBuf p1_seg_cnt, p1_seg_tab, x_seg_cnt, x_seg_tab;  // the same for the P1 pass and explicit pairs
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
   DevBuf x_setup, x_tol, x_iota, x_faces, x_screen, x_list;  // explicit tet pairs through the early-out pass
@@ -292,7 +293,8 @@ void fini_ctx(Ctx* c) {
                    &c->d1_keyhi, &c->d1_perm_a, &c->d1_perm_b, &c->d1_lo_a, &c->d1_hi_a, &c->d1_lo_b,
                    &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over, &c->q_pool, &c->q_next, &c->q_first,
                    &c->a_faces, &c->b_screen, &c->surv, &c->sched_w, &c->sched_list, &c->sched_cls,
-                   &c->sched_adam, &c->bt_indptr, &c->seg_cnt, &c->seg_tab, &c->surv_list};
+                   &c->sched_adam, &c->bt_indptr, &c->seg_cnt, &c->seg_tab, &c->surv_list,
+                   &c->p1_seg_cnt, &c->p1_seg_tab, &c->x_seg_cnt, &c->x_seg_tab};
   for (DevBuf* b : all) free_buf(*b);
   for (cudaEvent_t& e : c->clip_ev)
     if (e) {
@@ -391,14 +393,25 @@ void require_pair_index(Ctx* c, int64_t n) {
 }
 
 // Explicit tet pair batches of at least this many pairs run through the
-// early-out pass and the index clipper (work counters: misc ints 20-23).
+// early-out pass and the index clipper (work counters: misc ints 24-29).
 constexpr int64_t kPairsPipelineMin = 2048;
+unsigned long long* pairs_work(Ctx* c) { return reinterpret_cast<unsigned long long*>(bad_flag(c) + 24); }
 
-// P1 mass pass (3D): its survivor list and two counters (misc ints 16-19)
+// Survivor segments of a 3D early-out pass over n pairs (lengths and chunk
+// table) in the given buffers.
+lsm::SegList seg_list(Ctx* c, DevBuf& cnt, DevBuf& tab, int64_t n) {
+  return lsm::SegList{ensure<int>(c, cnt, lsm::seg_blocks(n)), ensure<int4>(c, tab, lsm::seg_table_entries(n))};
+}
+
+// P1 mass pass (3D): its survivor list, segments and three counters (misc
+// ints 16-21)
 int32_t* p1_survivors(Ctx* c, int dim, int64_t nnz) {
   return dim == 3 ? ensure<int32_t>(c, c->p1_list, 4 * std::max<int64_t>(nnz, 1)) : nullptr;
 }
 unsigned long long* p1_work(Ctx* c) { return reinterpret_cast<unsigned long long*>(bad_flag(c) + 16); }
+lsm::SegList p1_seg(Ctx* c, int dim, int64_t nnz) {
+  return dim == 3 ? seg_list(c, c->p1_seg_cnt, c->p1_seg_tab, nnz) : lsm::SegList{};
+}
 
 // Device memory the candidate-row cache of the search may hold: min(4 GiB,
 // 1/32 of the device).  Only rows' actual candidates are written (4 B each);
@@ -740,25 +753,25 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_
     bin.window = g_sched_window;
   }
   if (c->dim == 3 && list_inside) {
+    const lsm::SegList sg = seg_list(c, c->seg_cnt, c->seg_tab, nnz);
     CU(lsm::launch_clip_elems(nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                               static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                               static_cast<double*>(c->b_setup.p), pm, pn, nullptr, ovf, work,
                               screen ? static_cast<double*>(c->a_faces.p) : nullptr,
-                              screen ? static_cast<double*>(c->b_screen.p) : nullptr, s));
+                              screen ? static_cast<double*>(c->b_screen.p) : nullptr, s, &sg));
     c->clip_timed = false;
     c->surv_seg = false;
   } else {
     // 3D plain order: survivors as per-block segments, taken by chunks
     const bool seg = c->dim == 3 && !binned;
-    int* seg_cnt = seg ? ensure<int>(c, c->seg_cnt, lsm::seg_blocks(nnz)) : nullptr;
-    int4* seg_tab = seg ? ensure<int4>(c, c->seg_tab, lsm::seg_table_entries(nnz)) : nullptr;
+    const lsm::SegList sg = seg ? seg_list(c, c->seg_cnt, c->seg_tab, nnz) : lsm::SegList{};
     CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                         static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                         static_cast<double*>(c->b_setup.p), pm, pn, ovf, ovf_count, work, s, order,
                         g_time_kernels ? c->clip_ev[0] : nullptr, g_time_kernels ? c->clip_ev[1] : nullptr,
                         screen ? static_cast<double*>(c->a_faces.p) : nullptr,
                         screen ? static_cast<double*>(c->b_screen.p) : nullptr, binned ? &bin : nullptr, n_dev,
-                        seg_cnt, seg_tab));
+                        &sg));
     c->clip_timed = g_time_kernels;
     c->surv_seg = seg;
     c->surv_npairs = nnz;
@@ -1145,9 +1158,11 @@ bool run_batch_group(Ctx* c, int dim, const std::vector<int>& idx, const lsm_gpu
         double* dst = on_device ? o->p1_blocks + bo->p1_next : ensure<double>(c, c->blocks, p1_need);
         lsm::Partial* pp = ensure<lsm::Partial>(c, c->partials, std::max<int64_t>(lsm::p1_grid_blocks(dim),
                                                                                   lsm::mesh_totals_pieces(nm)));
+        const lsm::SegList p1sg = p1_seg(c, dim, nnz);
         CU(lsm::launch_p1_mass(dim, nnz, pa, pb, a_coords, a_tol, b_coords, b_setup, nullptr, nullptr, ib, nullptr,
                                nullptr, dst, pp, s, p1_survivors(c, dim, nnz), p1_work(c),
-                               g_tet_screen ? a_faces : nullptr, g_tet_screen ? b_screen : nullptr));
+                               g_tet_screen ? a_faces : nullptr, g_tet_screen ? b_screen : nullptr, nullptr,
+                               &p1sg));
         if (!on_device)
           CU(cudaMemcpyAsync(o->p1_blocks + bo->p1_next, dst, sizeof(double) * p1_need, cudaMemcpyDeviceToHost, s));
       }
@@ -1948,10 +1963,14 @@ int libsupermesh_gpu_supermesh_elements(lsm_gpu_context* ctx, const lsm_gpu_mesh
       double* de = on_device ? out->elems : ensure<double>(c, c->x_elems, ne * per);
       int64_t* dpa = !out->parent_a ? nullptr : (on_device ? out->parent_a : ensure<int64_t>(c, c->x_pa, ne));
       int64_t* dpb = !out->parent_b ? nullptr : (on_device ? out->parent_b : ensure<int64_t>(c, c->x_pb, ne));
+      // the counting pass's survivor segments (3D)
+      const lsm::SegList esg = dim == 3 ? lsm::SegList{static_cast<int*>(c->seg_cnt.p), static_cast<int4*>(c->seg_tab.p)}
+                                        : lsm::SegList{};
       CU(lsm::launch_emit_elements(dim, n, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                                    static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                                    static_cast<double*>(c->b_setup.p), static_cast<int32_t*>(c->ovf_list.p),
-                                   reinterpret_cast<unsigned long long*>(bad_flag(c) + 8), off, de, dpa, dpb, s));
+                                   reinterpret_cast<unsigned long long*>(bad_flag(c) + 8), off, de, dpa, dpb, s,
+                                   &esg));
       if (!on_device) {
         CU(cudaMemcpyAsync(out->elems, de, sizeof(double) * ne * per, k, s));
         if (dpa) CU(cudaMemcpyAsync(out->parent_a, dpa, sizeof(int64_t) * ne, k, s));
@@ -2055,13 +2074,14 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context* ctx, int dim, int64_t n, c
       int32_t* list = ensure<int32_t>(c, c->x_list, 4 * n);
       double* pm = dm ? dm : ensure<double>(c, c->x_measure, n);
       int32_t* pn = dn ? dn : ensure<int32_t>(c, c->x_nout, n);
-      unsigned long long* work = reinterpret_cast<unsigned long long*>(bad_flag(c) + 20);
+      unsigned long long* work = pairs_work(c);
+      const lsm::SegList sg = seg_list(c, c->x_seg_cnt, c->x_seg_tab, n);
       CU(lsm::launch_setup_pairs3(n, da, db, setup, tol, iota, faces, screen, s));
       if (de)
-        CU(lsm::launch_clip_elems(n, iota, iota, da, tol, setup, pm, pn, de, list, work, faces, screen, s));
+        CU(lsm::launch_clip_elems(n, iota, iota, da, tol, setup, pm, pn, de, list, work, faces, screen, s, &sg));
       else
         CU(lsm::launch_clip(3, n, iota, iota, da, tol, setup, pm, pn, list, nullptr, work, s, nullptr, nullptr,
-                            nullptr, faces, screen));
+                            nullptr, faces, screen, nullptr, nullptr, &sg));
     } else {
       CU(lsm::launch_pairs_explicit(dim, n, da, db, dm, dn, de, s));
     }
@@ -2108,10 +2128,10 @@ int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context* ctx, int kind, int64
       // index clipper; small ones stay on the one-launch clipper (same results)
       double* pm = dm ? dm : ensure<double>(c, c->x_measure, n);
       int32_t* pn = dn ? dn : ensure<int32_t>(c, c->x_nout, n);
+      const lsm::SegList hsg = seg_list(c, c->x_seg_cnt, c->x_seg_tab, n);
       CU(lsm::launch_tet_hex_pairs(n, da, db, pm, pn, de, ensure<double>(c, c->x_setup, n * 28),
                                    ensure<double>(c, c->x_tol, n), ensure<int32_t>(c, c->x_iota, n),
-                                   ensure<int32_t>(c, c->x_list, 4 * n),
-                                   reinterpret_cast<unsigned long long*>(bad_flag(c) + 20), s));
+                                   ensure<int32_t>(c, c->x_list, 4 * n), pairs_work(c), s, &hsg));
     } else {
       CU(lsm::launch_pairs_mixed(kind, n, da, db, dm, dn, de, s));
     }
@@ -2152,6 +2172,7 @@ int libsupermesh_gpu_p1_mass(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const 
     lsm::Partial* tot = ensure<lsm::Partial>(c, c->totals, 1);
     const void* en_a = on_device ? a->enlist : c->a_en.p;
     const void* en_b = on_device ? b->enlist : c->b_en.p;
+    const lsm::SegList p1sg = p1_seg(c, c->dim, nnz);
     CU(lsm::launch_p1_mass(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                            static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),
                            static_cast<double*>(c->b_coords.p), static_cast<double*>(c->b_setup.p), en_a, en_b,
@@ -2159,7 +2180,8 @@ int libsupermesh_gpu_p1_mass(lsm_gpu_context* ctx, const lsm_gpu_mesh* a, const 
                            c->dim == 3 && g_tet_screen ? static_cast<double*>(c->a_faces.p) : nullptr,
                            c->dim == 3 && g_tet_screen ? static_cast<double*>(c->b_screen.p) : nullptr,
                            c->dim == 3 && du && dv ? ensure<double>(c, c->x_measure, std::max<int64_t>(nnz, 1))
-                                                   : nullptr));
+                                                   : nullptr,
+                           &p1sg));
     CU(lsm::launch_finalize(part, nblk, tot, s));
     double* h = static_cast<double*>(c->host_scalars) + 64;
     CU(cudaMemcpyAsync(h, tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -1738,6 +1738,35 @@ cudaError_t launch_seg_compact(int64_t npairs, const unsigned long long* nchunks
   return cudaGetLastError();
 }
 
+// The early-out pass over n pairs into `survivors`: one list counted in
+// work[0], or, with seg, per-block segments and their chunk table (work[0]
+// survivors, work[2] chunks).  The clipper then takes seg_nlist(seg, work)
+// and seg_table(seg).
+namespace {
+inline bool seg_on(const SegList* seg) { return seg && seg->count && seg->table; }
+inline const unsigned long long* seg_nlist(const SegList* seg, const unsigned long long* work) {
+  return seg_on(seg) ? work + 2 : work;
+}
+inline const int4* seg_table(const SegList* seg) { return seg_on(seg) ? seg->table : nullptr; }
+template <bool kSettle, int NP>
+void run_prefilter(int64_t n, const int32_t* order, const int32_t* pa, const int32_t* pb, const double* coords_a,
+                   const double* tol_a, const double* setup, double* measure, int32_t* nout, int32_t* survivors,
+                   unsigned long long* work, const double* faces_a, const double* screen_b, const int64_t* n_dev,
+                   const SegList* seg, cudaStream_t s) {
+  const int gp = grid_for(n, 256, 8);
+  if (seg_on(seg)) {
+    count_launch(2);
+    k_prefilter_tets<kSettle, NP, true><<<gp, 256, 0, s>>>(n, order, pa, pb, coords_a, tol_a, setup, measure, nout,
+                                                           survivors, work, faces_a, screen_b, n_dev, seg->count);
+    k_seg_chunks<<<gp, 256, 0, s>>>(n, n_dev, seg->count, seg->table, work);
+  } else {
+    count_launch();
+    k_prefilter_tets<kSettle, NP><<<gp, 256, 0, s>>>(n, order, pa, pb, coords_a, tol_a, setup, measure, nout,
+                                                     survivors, work, faces_a, screen_b, n_dev);
+  }
+}
+}  // namespace
+
 // ----------------------------------------------------------------------
 // K6: depth-first tet clipper over point indices
 // ----------------------------------------------------------------------
@@ -2229,25 +2258,25 @@ __global__ void k_setup_hex_pairs(int64_t n, const double* __restrict__ tet_a, c
 
 cudaError_t launch_tet_hex_pairs(int64_t n, const double* tet_a, const double* hex_b, double* measure, int32_t* nout,
                                  double* elems, double* setup, double* tol_a, int32_t* iota, int32_t* survivors,
-                                 unsigned long long* work, cudaStream_t s) {
+                                 unsigned long long* work, cudaStream_t s, const SegList* seg) {
   cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
   if (n <= 0) return cudaGetLastError();
-  count_launch(3);
+  count_launch(2);
   k_setup_hex_pairs<<<grid_for(n, 256, 8), 256, 0, s>>>(n, tet_a, hex_b, setup, tol_a, iota);
   const int4* list = reinterpret_cast<const int4*>(survivors);
   const int g = sm_count();
   if (elems) {
-    k_prefilter_tets<false, 6><<<grid_for(n, 256, 8), 256, 0, s>>>(n, nullptr, iota, iota, tet_a, tol_a, setup,
-                                                                   measure, nout, survivors, work, nullptr, nullptr,
-                                                                   nullptr);
+    run_prefilter<false, 6>(n, nullptr, iota, iota, tet_a, tol_a, setup, measure, nout, survivors, work, nullptr,
+                            nullptr, nullptr, seg, s);
     k_clip_tets_ix<IxElemSinkT<729>, kIxHexBlock, 1, 6><<<g, kIxHexBlock, ix_hex_smem_bytes(), s>>>(
-        list, work, tet_a, tol_a, setup, IxElemSinkT<729>{measure, nout, elems}, work + 1);
+        list, seg_nlist(seg, work), tet_a, tol_a, setup, IxElemSinkT<729>{measure, nout, elems}, work + 1,
+        seg_table(seg));
   } else {
-    k_prefilter_tets<true, 6><<<grid_for(n, 256, 8), 256, 0, s>>>(n, nullptr, iota, iota, tet_a, tol_a, setup,
-                                                                  measure, nout, survivors, work, nullptr, nullptr,
-                                                                  nullptr);
+    run_prefilter<true, 6>(n, nullptr, iota, iota, tet_a, tol_a, setup, measure, nout, survivors, work, nullptr,
+                           nullptr, nullptr, seg, s);
     k_clip_tets_ix<IxMeasureSink, kIxHexBlock, 1, 6><<<g, kIxHexBlock, ix_hex_smem_bytes(), s>>>(
-        list, work, tet_a, tol_a, setup, IxMeasureSink{measure, nout, 0.0, 0}, work + 1);
+        list, seg_nlist(seg, work), tet_a, tol_a, setup, IxMeasureSink{measure, nout, 0.0, 0}, work + 1,
+        seg_table(seg));
   }
   return cudaGetLastError();
 }
@@ -2255,16 +2284,15 @@ cudaError_t launch_tet_hex_pairs(int64_t n, const double* tet_a, const double* h
 cudaError_t launch_clip_elems(int64_t n, const int32_t* pair_a, const int32_t* pair_b, const double* tet_a,
                               const double* tol_a, const double* setup, double* measure, int32_t* nout,
                               double* elems, int32_t* survivors, unsigned long long* work, const double* faces_a,
-                              const double* screen_b, cudaStream_t s) {
+                              const double* screen_b, cudaStream_t s, const SegList* seg) {
   cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
   if (n <= 0) return cudaGetLastError();
-  count_launch();
-  k_prefilter_tets<false><<<grid_for(n, 256, 8), 256, 0, s>>>(n, nullptr, pair_a, pair_b, tet_a, tol_a, setup,
-                                                              measure, nout, survivors, work, faces_a, screen_b,
-                                                              nullptr);
+  run_prefilter<false, 4>(n, nullptr, pair_a, pair_b, tet_a, tol_a, setup, measure, nout, survivors, work, faces_a,
+                          screen_b, nullptr, seg, s);
   count_launch();
   k_clip_tets_ix<IxElemSink, kIxBlock, kIxBlocksPerSm><<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
-      reinterpret_cast<const int4*>(survivors), work, tet_a, tol_a, setup, IxElemSink{measure, nout, elems}, work + 1);
+      reinterpret_cast<const int4*>(survivors), seg_nlist(seg, work), tet_a, tol_a, setup,
+      IxElemSink{measure, nout, elems}, work + 1, seg_table(seg));
   return cudaGetLastError();
 }
 
@@ -2298,8 +2326,7 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         double* pair_measure, int32_t* pair_nout, int32_t* overflow_list,
                         int* overflow_count, unsigned long long* work, cudaStream_t s,
                         const int32_t* order, cudaEvent_t ev_begin, cudaEvent_t ev_end, const double* faces_a,
-                        const double* screen_b, const SchedBin* bin, const int64_t* n_dev, int* seg_count,
-                        int4* chunk_table) {
+                        const double* screen_b, const SchedBin* bin, const int64_t* n_dev, const SegList* seg) {
   const int g = clip_grid_blocks(dim);
   count_launch();
   if (dim == 2) {
@@ -2312,20 +2339,9 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     // they settle every candidate
     if (ev_begin) cudaEventRecord(ev_begin, s);
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
-    count_launch();
-    const bool seg = seg_count && chunk_table && !bin;
-    if (seg) {
-      const int gp = seg_blocks(npairs);
-      k_prefilter_tets<true, 4, true><<<gp, 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, tol_a, setup_b,
-                                                        pair_measure, pair_nout, overflow_list, work, faces_a,
-                                                        screen_b, n_dev, seg_count);
-      count_launch();
-      k_seg_chunks<<<gp, 256, 0, s>>>(npairs, n_dev, seg_count, chunk_table, work);
-    } else {
-      k_prefilter_tets<true><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, order, pair_a, pair_b, coords_a, tol_a,
-                                                                setup_b, pair_measure, pair_nout, overflow_list,
-                                                                work, faces_a, screen_b, n_dev);
-    }
+    const SegList sg = bin ? SegList{} : (seg ? *seg : SegList{});
+    run_prefilter<true, 4>(npairs, order, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure, pair_nout,
+                           overflow_list, work, faces_a, screen_b, n_dev, &sg, s);
     const int4* list = reinterpret_cast<const int4*>(overflow_list);
     if (bin) {
       // the survivors reordered into class-uniform runs within windows
@@ -2334,8 +2350,8 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
       list = bin->out;
     }
     k_clip_tets_ix<IxMeasureSink, kIxBlock, kIxBlocksPerSm><<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
-        list, seg ? work + 2 : work, coords_a, tol_a, setup_b, IxMeasureSink{pair_measure, pair_nout, 0.0, 0},
-        work + 1, seg ? chunk_table : nullptr);
+        list, seg_nlist(&sg, work), coords_a, tol_a, setup_b, IxMeasureSink{pair_measure, pair_nout, 0.0, 0},
+        work + 1, seg_table(&sg));
   }
   if (ev_end) cudaEventRecord(ev_end, s);
   return cudaGetLastError();
@@ -2385,7 +2401,8 @@ __global__ void __launch_bounds__(128) k_tris_emit(int64_t npairs, const int32_t
 cudaError_t launch_emit_elements(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                                  const double* coords_a, const double* tol_a, const double* setup_b,
                                  const int32_t* survivors, unsigned long long* work, const int64_t* pair_off,
-                                 double* elems, int64_t* parent_a, int64_t* parent_b, cudaStream_t s) {
+                                 double* elems, int64_t* parent_a, int64_t* parent_b, cudaStream_t s,
+                                 const SegList* seg) {
   if (npairs <= 0) return cudaSuccess;
   count_launch();
   if (dim == 2) {
@@ -2397,8 +2414,8 @@ cudaError_t launch_emit_elements(int dim, int64_t npairs, const int32_t* pair_a,
   // only the clipper's pair counter starts over
   cudaMemsetAsync(work + 1, 0, sizeof(unsigned long long), s);
   k_clip_tets_ix<IxEmitSink, kIxBlock, kIxBlocksPerSm><<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
-      reinterpret_cast<const int4*>(survivors), work, coords_a, tol_a, setup_b,
-      IxEmitSink{pair_off, elems, parent_a, parent_b}, work + 1);
+      reinterpret_cast<const int4*>(survivors), seg_nlist(seg, work), coords_a, tol_a, setup_b,
+      IxEmitSink{pair_off, elems, parent_a, parent_b}, work + 1, seg_table(seg));
   return cudaGetLastError();
 }
 
@@ -3869,7 +3886,7 @@ cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const
                            const double* setup_b, const void* enlist_a, const void* enlist_b,
                            int idx_bytes, const double* u_a, const double* v_b, double* blocks,
                            Partial* partials, cudaStream_t s, int32_t* survivors, unsigned long long* work,
-                           const double* faces_a, const double* screen_b, double* pair_uv) {
+                           const double* faces_a, const double* screen_b, double* pair_uv, const SegList* seg) {
   const int g = dim == 2 ? p1_grid_blocks(2) : sm_count();
   if (dim == 2) {
     count_launch();
@@ -3888,24 +3905,22 @@ cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const
   cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
   if (blocks && npairs > 0) cudaMemsetAsync(blocks, 0, sizeof(double) * 16 * npairs, s);
   if (uv && npairs > 0) cudaMemsetAsync(pair_uv, 0, sizeof(double) * npairs, s);
-  if (npairs > 0) {
-    count_launch();
-    k_prefilter_tets<false><<<grid_for(npairs, 256, 8), 256, 0, s>>>(npairs, nullptr, pair_a, pair_b, coords_a,
-                                                                     tol_a, setup_b, nullptr, nullptr, survivors,
-                                                                     work, faces_a, screen_b, nullptr);
-  }
+  if (npairs > 0)
+    run_prefilter<false, 4>(npairs, nullptr, pair_a, pair_b, coords_a, tol_a, setup_b, nullptr, nullptr, survivors,
+                            work, faces_a, screen_b, nullptr, seg, s);
+  const bool sg = seg_on(seg) && npairs > 0;
   const int4* list = reinterpret_cast<const int4*>(survivors);
   count_launch();
   if (idx_bytes == 4) {
     using Sk = IxP1Sink<int32_t, kIxP1Block>;
     Sk sk{coords_a, coords_b, enlist_a, enlist_b, u_a, v_b, blocks, pair_uv};
-    k_clip_tets_ix<Sk, kIxP1Block, 1><<<g, kIxP1Block, p1_smem_bytes(), s>>>(list, work, coords_a, tol_a, setup_b,
-                                                                            sk, work + 1);
+    k_clip_tets_ix<Sk, kIxP1Block, 1><<<g, kIxP1Block, p1_smem_bytes(), s>>>(
+        list, sg ? work + 2 : work, coords_a, tol_a, setup_b, sk, work + 1, sg ? seg->table : nullptr);
   } else {
     using Sk = IxP1Sink<int64_t, kIxP1Block>;
     Sk sk{coords_a, coords_b, enlist_a, enlist_b, u_a, v_b, blocks, pair_uv};
-    k_clip_tets_ix<Sk, kIxP1Block, 1><<<g, kIxP1Block, p1_smem_bytes(), s>>>(list, work, coords_a, tol_a, setup_b,
-                                                                            sk, work + 1);
+    k_clip_tets_ix<Sk, kIxP1Block, 1><<<g, kIxP1Block, p1_smem_bytes(), s>>>(
+        list, sg ? work + 2 : work, coords_a, tol_a, setup_b, sk, work + 1, sg ? seg->table : nullptr);
   }
   if (uv) {
     count_launch();

@@ -148,13 +148,19 @@ cudaError_t launch_scan(int64_t n, const int* counts, int64_t* offsets, int64_t*
 // second exact early-out (B beyond a face of A).
 // bin (3D, optional): the learned scheduler's reordering of the survivors
 // between the early-out pass and the clipper (lsm_sched.h).
-// seg_count (seg_blocks(npairs) ints) and chunk_table
-// (seg_table_entries(npairs) entries), 3D, optional, not with bin: the
-// survivors are written as per-block segments of overflow_list (no global
-// counter), and the clipper takes them by chunks from the table; `work`
-// then holds four counters (survivors, chunks taken, chunks, unused).
-// launch_seg_compact gathers such a list into a compacted one.
+// seg (3D, optional, ignored with bin): the survivors are written as
+// per-block segments of overflow_list (no global counter) and the clipper
+// takes them by chunks from seg->table; `work` then holds three counters
+// (survivors, chunks taken, chunks).  launch_seg_compact gathers such a list
+// into a compacted one.
 struct SchedBin;
+// Per-block survivor segments of the early-out pass over npairs pairs:
+// count [seg_blocks(npairs)] segment lengths, table
+// [seg_table_entries(npairs)] chunks {first, end, compacted position, 0}.
+struct SegList {
+  int* count = nullptr;
+  int4* table = nullptr;
+};
 int clip_grid_blocks(int dim);
 int seg_blocks(int64_t npairs);
 int64_t seg_table_entries(int64_t npairs);
@@ -167,8 +173,7 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
                         const int32_t* order = nullptr, cudaEvent_t ev_begin = nullptr,
                         cudaEvent_t ev_end = nullptr, const double* faces_a = nullptr,
                         const double* screen_b = nullptr, const SchedBin* bin = nullptr,
-                        const int64_t* n_dev = nullptr, int* seg_count = nullptr,
-                        int4* chunk_table = nullptr);
+                        const int64_t* n_dev = nullptr, const SegList* seg = nullptr);
 // Opt-in shared-memory limits for the clip kernels on the current device.
 cudaError_t init_device_attributes();
 cudaError_t launch_clip_tris_wide(const int32_t* overflow_list, const int* overflow_count, int64_t cap,
@@ -204,32 +209,35 @@ cudaError_t launch_i32_to_i64(int64_t n, const int32_t* in, int64_t* out, cudaSt
 // screen_b [n][kScreen3] optional, for the second early-out), then, for
 // measures and counts, launch_clip(3, n, iota, iota, tet_a, ...), or, with
 // the output tets, launch_clip_elems (elems [n][81][4][3]; survivors: 4 ints
-// per pair; work: two counters).  tet_a must be 16-byte aligned.
+// per pair; work: two counters, three with seg).  tet_a must be 16-byte
+// aligned.
 cudaError_t launch_setup_pairs3(int64_t n, const double* tet_a, const double* tet_b, double* setup, double* tol_a,
                                 int32_t* iota, double* faces_a, double* screen_b, cudaStream_t s);
 // launch_clip_elems: the 3D narrow phase whose survivor list also holds the
 // pairs with every plane a no-op (so that a second pass over the list sees
-// every pair with output tets); measure/nout for every pair, elems optional.
+// every pair with output tets); measure/nout for every pair, elems optional;
+// seg (optional) as for launch_clip.
 cudaError_t launch_clip_elems(int64_t n, const int32_t* pair_a, const int32_t* pair_b, const double* tet_a,
                               const double* tol_a, const double* setup, double* measure, int32_t* nout,
                               double* elems, int32_t* survivors, unsigned long long* work, const double* faces_a,
-                              const double* screen_b, cudaStream_t s);
+                              const double* screen_b, cudaStream_t s, const SegList* seg = nullptr);
 // The supermesh's simplices: pair p's output simplices (reference order) at
 // elems[pair_off[p] ..] ([3][2] or [4][3] doubles each), parents optional.
-// 3D takes the survivor list and work counters of a launch_clip_elems pass
-// over the same pairs; 2D clips the pairs again.
+// 3D takes the survivor list, work counters and seg of a launch_clip_elems
+// pass over the same pairs; 2D clips the pairs again.
 cudaError_t launch_emit_elements(int dim, int64_t npairs, const int32_t* pair_a, const int32_t* pair_b,
                                  const double* coords_a, const double* tol_a, const double* setup_b,
                                  const int32_t* survivors, unsigned long long* work, const int64_t* pair_off,
-                                 double* elems, int64_t* parent_a, int64_t* parent_b, cudaStream_t s);
+                                 double* elems, int64_t* parent_a, int64_t* parent_b, cudaStream_t s,
+                                 const SegList* seg = nullptr);
 // Explicit tet-hexahedron pairs (a [n][4][3] 16-byte aligned, hex_b
 // [n][8][3]) through per-pair setup (setup [n][28], tol_a [n], iota [n]), the
 // first early-out with the no-op planes, and the six-plane index clipper:
 // measure/nout per pair and, optionally, elems [n][729][4][3]; survivors 4
-// ints per pair, work two counters.
+// ints per pair, work two counters (three with seg, as for launch_clip).
 cudaError_t launch_tet_hex_pairs(int64_t n, const double* tet_a, const double* hex_b, double* measure, int32_t* nout,
                                  double* elems, double* setup, double* tol_a, int32_t* iota, int32_t* survivors,
-                                 unsigned long long* work, cudaStream_t s);
+                                 unsigned long long* work, cudaStream_t s, const SegList* seg = nullptr);
 cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const double* b,
                                   double* measure, int32_t* nout, double* out_elems,
                                   cudaStream_t s);
@@ -275,8 +283,8 @@ cudaError_t launch_p2_inner(int64_t npairs, const int32_t* pair_a, const int32_t
 // bad = 1 if any of en[0..n) lies outside [0, limit).
 cudaError_t launch_check_index(int64_t n, const void* en, int idx_bytes, int64_t limit, int* bad, cudaStream_t s);
 // P1-P1 mixed mass: 2D clips every pair; 3D runs the exact early-out pass
-// (survivors: 4 ints per pair, work: two counters, faces_a / screen_b as for
-// launch_clip) and the index clipper with the quadrature on the survivors,
+// (survivors: 4 ints per pair, work: two counters (three with seg),
+// faces_a / screen_b / seg as for launch_clip) and the index clipper with the quadrature on the survivors,
 // with blocks of the other pairs zero-filled; 3D with u_a and v_b also needs
 // pair_uv [npairs] (u^T M v per pair, summed in pair order).  partials:
 // p1_grid_blocks(dim) entries.
@@ -285,7 +293,8 @@ cudaError_t launch_p1_mass(int dim, int64_t npairs, const int32_t* pair_a, const
                            const double* setup_b, const void* enlist_a, const void* enlist_b,
                            int idx_bytes, const double* u_a, const double* v_b, double* blocks,
                            Partial* partials, cudaStream_t s, int32_t* survivors, unsigned long long* work,
-                           const double* faces_a, const double* screen_b, double* pair_uv = nullptr);
+                           const double* faces_a, const double* screen_b, double* pair_uv = nullptr,
+                           const SegList* seg = nullptr);
 int p1_grid_blocks(int dim);
 
 // ---- batched (many mesh pairs per launch) --------------------------------
