@@ -254,6 +254,12 @@ __device__ __forceinline__ double max_abs_tet(const Tet& t) {
 
 __device__ __forceinline__ double pos_inf() { return __longlong_as_double(0x7ff0000000000000ll); }
 
+// Two doubles in one 16-byte store (p 16-byte aligned: every per-element row
+// the prep writes holds an even number of doubles).
+__device__ __forceinline__ void st2(double* p, double a, double b) {
+  *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+
 __device__ __forceinline__ void tet_faces_screen(const Tet& t, double* o) {
   Planes P;
   tet_planes(t, P);
@@ -267,10 +273,8 @@ __device__ __forceinline__ void tet_faces_screen(const Tet& t, double* o) {
     double h = -pos_inf();
 #pragma unroll
     for (int k = 0; k < 4; ++k) h = fmax(h, (P.nx[i] * t.x[k] + P.ny[i] * t.y[k]) + P.nz[i] * t.z[k]);
-    o[4 * i + 0] = ok ? P.nx[i] : 0.0;
-    o[4 * i + 1] = ok ? P.ny[i] : 0.0;
-    o[4 * i + 2] = ok ? P.nz[i] : 0.0;
-    o[4 * i + 3] = ok && isfinite(h) ? h + drift : pos_inf();
+    st2(o + 4 * i, ok ? P.nx[i] : 0.0, ok ? P.ny[i] : 0.0);
+    st2(o + 4 * i + 2, ok ? P.nz[i] : 0.0, ok && isfinite(h) ? h + drift : pos_inf());
   }
 }
 
@@ -307,16 +311,14 @@ __device__ __forceinline__ void tet_screen_b(const Tet& t, const Planes& P, doub
   const bool neg = D[0] < -kDetErr && D[1] < -kDetErr && D[2] < -kDetErr && D[3] < -kDetErr;
   const double dmin = fmin(fmin(fabs(D[0]), fabs(D[1])), fmin(fabs(D[2]), fabs(D[3])));
   const double g = (pos || neg) ? 3.02 / (dmin - kDetErr) : pos_inf();
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    o[3 * k + 0] = t.x[k];
-    o[3 * k + 1] = t.y[k];
-    o[3 * k + 2] = t.z[k];
-  }
-  o[12] = g;
-  o[13] = tau + 16.0 * kEps * (1.0 + 2.0 * M);
-  o[14] = M;
-  o[15] = 0.0;
+  st2(o + 0, t.x[0], t.y[0]);
+  st2(o + 2, t.z[0], t.x[1]);
+  st2(o + 4, t.y[1], t.z[1]);
+  st2(o + 6, t.x[2], t.y[2]);
+  st2(o + 8, t.z[2], t.x[3]);
+  st2(o + 10, t.y[3], t.z[3]);
+  st2(o + 12, g, tau + 16.0 * kEps * (1.0 + 2.0 * M));
+  st2(o + 14, M, 0.0);
 }
 
 // Face planes of a hexahedron in Gmsh node order (Supermesh.F90:262-280):

@@ -172,8 +172,9 @@ __device__ __forceinline__ void prep_element(int64_t e, const double* __restrict
   }
   if (!ok) atomicExch(bad, 1);
   if (coords) {
+    static_assert((LOC * DIM) % 2 == 0, "element rows of an even number of doubles");
 #pragma unroll
-    for (int j = 0; j < LOC * DIM; ++j) coords[e * LOC * DIM + j] = v[j];
+    for (int j = 0; j < LOC * DIM; j += 2) st2(coords + e * LOC * DIM + j, v[j], v[j + 1]);
   }
   double lo[DIM], hi[DIM];
 #pragma unroll
@@ -186,10 +187,14 @@ __device__ __forceinline__ void prep_element(int64_t e, const double* __restrict
       hi[c] = fmax(hi[c], v[k * DIM + c]);
     }
   if (box64) {
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-      box64[e * 2 * DIM + c] = lo[c];
-      box64[e * 2 * DIM + DIM + c] = hi[c];
+    double* o = box64 + e * 2 * DIM;
+    if (DIM == 3) {
+      st2(o, lo[0], lo[1]);
+      st2(o + 2, lo[DIM - 1], hi[0]);
+      st2(o + 4, hi[1], hi[DIM - 1]);
+    } else {
+      st2(o, lo[0], lo[1]);
+      st2(o + 2, hi[0], hi[1]);
     }
   }
   if (box32) {
@@ -228,28 +233,21 @@ __device__ __forceinline__ void prep_element(int64_t e, const double* __restrict
       double* o = setup + e * kSetup2;
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        o[4 * i + 0] = L.nx[i];
-        o[4 * i + 1] = L.ny[i];
-        o[4 * i + 2] = L.px[i];
-        o[4 * i + 3] = L.py[i];
+        st2(o + 4 * i, L.nx[i], L.ny[i]);
+        st2(o + 4 * i + 2, L.px[i], L.py[i]);
       }
-      o[12] = tol;
-      o[13] = 0.0;
+      st2(o + 12, tol, 0.0);
     } else {
       Planes P;
       tet_planes(t, P);
       double* o = setup + e * kSetup3;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        o[4 * i + 0] = P.nx[i];
-        o[4 * i + 1] = P.ny[i];
-        o[4 * i + 2] = P.nz[i];
-        o[4 * i + 3] = P.c[i];
+        st2(o + 4 * i, P.nx[i], P.ny[i]);
+        st2(o + 4 * i + 2, P.nz[i], P.c[i]);
       }
-      o[16] = tol;
-      o[17] = 0.0;
-      o[18] = 0.0;
-      o[19] = 0.0;
+      st2(o + 16, tol, 0.0);
+      st2(o + 18, 0.0, 0.0);
       if (screen) tet_screen_b(t, P, screen + e * kScreen3);
     }
   }
