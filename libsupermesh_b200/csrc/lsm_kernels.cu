@@ -1280,15 +1280,18 @@ struct NoEmit {
   __device__ __forceinline__ void operator()(int, double, double, double, double, double, double) const {}
 };
 
+// A setup row of kSetup2 doubles (16-byte aligned) in seven 16-byte loads.
 __device__ __forceinline__ void load_lines(const double* __restrict__ o, Lines& L, double& tol) {
+  const double2* q = reinterpret_cast<const double2*>(o);
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    L.nx[i] = o[4 * i + 0];
-    L.ny[i] = o[4 * i + 1];
-    L.px[i] = o[4 * i + 2];
-    L.py[i] = o[4 * i + 3];
+    const double2 n = __ldg(q + 2 * i), pt = __ldg(q + 2 * i + 1);
+    L.nx[i] = n.x;
+    L.ny[i] = n.y;
+    L.px[i] = pt.x;
+    L.py[i] = pt.y;
   }
-  tol = o[12];
+  tol = __ldg(q + 6).x;
 }
 
 __global__ void __launch_bounds__(kTriBlock) k_clip_tris(int64_t npairs, const int32_t* __restrict__ pa,
@@ -1322,13 +1325,14 @@ __global__ void __launch_bounds__(kTriBlock) k_clip_tris(int64_t npairs, const i
       na = pa[ni];
       nb = pb[ni];
     }
-    const double* va = coords_a + (int64_t)a * 6;
+    const double2* va = reinterpret_cast<const double2*>(coords_a + (int64_t)a * 6);
+    const double2 v0 = __ldg(va), v1 = __ldg(va + 1), v2 = __ldg(va + 2);
     Lines L;
     double tolb;
     load_lines(setup_b + (int64_t)b * kSetup2, L, tolb);
     const double tol = fmin(tol_a[a], tolb);
     double m;
-    const int n = clip_tri(va[0], va[1], va[2], va[3], va[4], va[5], L, tol, p, q, kTriCap, m, NoEmit{});
+    const int n = clip_tri(v0.x, v0.y, v1.x, v1.y, v2.x, v2.y, L, tol, p, q, kTriCap, m, NoEmit{});
     if (n < 0) {
       const int k = atomicAdd(ovf_count, 1);
       ovf_list[k] = (int32_t)i;
@@ -2181,30 +2185,20 @@ size_t ix_smem_bytes() { return (size_t)kIxBlock * 3 * kIxPoints * sizeof(double
 __global__ void k_setup_pairs3(int64_t n, const double* __restrict__ tet_a, const double* __restrict__ tet_b,
                                double* setup, double* tol_a, int32_t* iota, double* faces_a, double* screen_b) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    // both pair arrays are 16-byte aligned (checked by the entry points)
     Tet a, b;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      a.x[k] = tet_a[12 * i + 3 * k];
-      a.y[k] = tet_a[12 * i + 3 * k + 1];
-      a.z[k] = tet_a[12 * i + 3 * k + 2];
-      b.x[k] = tet_b[12 * i + 3 * k];
-      b.y[k] = tet_b[12 * i + 3 * k + 1];
-      b.z[k] = tet_b[12 * i + 3 * k + 2];
-    }
+    load_tet(tet_a + 12 * i, a);
+    load_tet(tet_b + 12 * i, b);
     Planes P;
     tet_planes(b, P);
     double* o = setup + i * kSetup3;
 #pragma unroll
     for (int L = 0; L < 4; ++L) {
-      o[4 * L + 0] = P.nx[L];
-      o[4 * L + 1] = P.ny[L];
-      o[4 * L + 2] = P.nz[L];
-      o[4 * L + 3] = P.c[L];
+      st2(o + 4 * L, P.nx[L], P.ny[L]);
+      st2(o + 4 * L + 2, P.nz[L], P.c[L]);
     }
-    o[16] = 10.0 * spacing(tet_volume_v4(b));
-    o[17] = 0.0;
-    o[18] = 0.0;
-    o[19] = 0.0;
+    st2(o + 16, 10.0 * spacing(tet_volume_v4(b)), 0.0);
+    st2(o + 18, 0.0, 0.0);
     tol_a[i] = 10.0 * spacing(tet_volume_v4(a));
     iota[i] = (int32_t)i;
     if (screen_b) tet_screen_b(b, P, screen_b + i * kScreen3);
@@ -2238,15 +2232,11 @@ __global__ void k_setup_hex_pairs(int64_t n, const double* __restrict__ tet_a, c
     double* o = setup + i * clip_row(6);
 #pragma unroll
     for (int L = 0; L < 6; ++L) {
-      o[4 * L + 0] = nx[L];
-      o[4 * L + 1] = ny[L];
-      o[4 * L + 2] = nz[L];
-      o[4 * L + 3] = c[L];
+      st2(o + 4 * L, nx[L], ny[L]);
+      st2(o + 4 * L + 2, nz[L], c[L]);
     }
-    o[24] = pos_inf();
-    o[25] = 0.0;
-    o[26] = 0.0;
-    o[27] = 0.0;
+    st2(o + 24, pos_inf(), 0.0);
+    st2(o + 26, 0.0, 0.0);
     Tet a;
     load_tet(tet_a + 12 * i, a);
     tol_a[i] = 10.0 * spacing(tet_volume_v4(a));
