@@ -2224,11 +2224,25 @@ constexpr int kIxHexBlock = 320;
 
 size_t ix_hex_smem_bytes() { return (size_t)kIxHexBlock * 3 * ix_points(6) * sizeof(double); }
 
+// kVec: hex_b is 16-byte aligned, each hexahedron is read in 12 16-byte loads
+template <bool kVec>
 __global__ void k_setup_hex_pairs(int64_t n, const double* __restrict__ tet_a, const double* __restrict__ hex_b,
                                   double* setup, double* tol_a, int32_t* iota) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double nx[6], ny[6], nz[6], c[6];
-    hex_planes(hex_b + 24 * i, nx, ny, nz, c);
+    if (kVec) {
+      double h[24];
+      const double2* q = reinterpret_cast<const double2*>(hex_b + 24 * i);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) {
+        const double2 v = __ldg(q + k);
+        h[2 * k] = v.x;
+        h[2 * k + 1] = v.y;
+      }
+      hex_planes(h, nx, ny, nz, c);
+    } else {
+      hex_planes(hex_b + 24 * i, nx, ny, nz, c);
+    }
     double* o = setup + i * clip_row(6);
 #pragma unroll
     for (int L = 0; L < 6; ++L) {
@@ -2250,7 +2264,10 @@ cudaError_t launch_tet_hex_pairs(int64_t n, const double* tet_a, const double* h
   cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
   if (n <= 0) return cudaGetLastError();
   count_launch(2);
-  k_setup_hex_pairs<<<grid_for(n, 256, 8), 256, 0, s>>>(n, tet_a, hex_b, setup, tol_a, iota);
+  if ((reinterpret_cast<uintptr_t>(hex_b) & 15u) == 0)
+    k_setup_hex_pairs<true><<<grid_for(n, 256, 8), 256, 0, s>>>(n, tet_a, hex_b, setup, tol_a, iota);
+  else
+    k_setup_hex_pairs<false><<<grid_for(n, 256, 8), 256, 0, s>>>(n, tet_a, hex_b, setup, tol_a, iota);
   const int4* list = reinterpret_cast<const int4*>(survivors);
   const int g = sm_count();
   if (elems) {
