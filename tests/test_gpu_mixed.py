@@ -327,6 +327,31 @@ def test_device_resident_pairs_equal_host_pairs(gpu_ctx):
         assert np.array_equal(dm.cpu().numpy(), m) and np.array_equal(dk.cpu().numpy(), k), (dim, kind)
 
 
+def test_tet_hex_device_hexahedra_any_alignment(gpu_ctx):
+    """Device hexahedra of a large tet-hex batch are read in 16-byte loads
+    when the array is 16-byte aligned and in 8-byte loads otherwise (a view
+    at an odd double offset): both give the host call's measures and
+    counts."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(17)
+    n = 3000
+    a = rng.random((n, 4, 3))
+    b = _random_hexes(rng, n)
+    m, k, _ = gpu_ctx.intersect_pairs_mixed(lsm.PAIR_TET_HEX, a, b)
+    da = torch.from_numpy(a.reshape(n, -1)).cuda()
+    flat = torch.from_numpy(b.reshape(-1)).cuda()
+    for off in (0, 1):
+        buf = torch.zeros(flat.numel() + 2, dtype=torch.float64, device="cuda")
+        buf[off:off + flat.numel()] = flat
+        db = buf[off:off + flat.numel()].view(n, 24)
+        assert (db.data_ptr() % 16 == 0) == (off == 0)
+        dm = torch.empty(n, dtype=torch.float64, device="cuda")
+        dk = torch.empty(n, dtype=torch.int32, device="cuda")
+        gpu_ctx.intersect_pairs_device(da, db, dm, dk, kind=lsm.PAIR_TET_HEX)
+        torch.cuda.synchronize()
+        assert np.array_equal(dm.cpu().numpy(), m) and np.array_equal(dk.cpu().numpy(), k), off
+
+
 def test_tet_hex_large_batch_bitexact(gpu_ctx, oracle_mod):
     """Tet-hex batches large enough for the early-out pass + six-plane index
     clipper: output tets, counts and measures bit-identical to the oracle and
