@@ -797,14 +797,26 @@ __device__ __forceinline__ int bvh_escape(int n, int node, const int* __restrict
   return r == n - 1 ? -1 : rope[r + 1];
 }
 
+constexpr int kRefitBlock = 256;
+
 template <bool BUCKET>
-__global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, const float4* __restrict__ box32,
+__global__ void __launch_bounds__(kRefitBlock) k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, const float4* __restrict__ box32,
                             const int* __restrict__ parent, const int* __restrict__ rope,
                             const int* __restrict__ last, const int* __restrict__ left,
                             const int* __restrict__ right, int* visit, float4* lo_left, float4* hi_esc,
                             int dim, const double* __restrict__ box64, double* leaf,
                             const int* __restrict__ first_leaf, int bucket) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  // Nodes whose leaf range lies within this block's 256 leaves are merged
+  // through shared memory (block-scope counters and boxes) when first_leaf
+  // is given; the climb above them uses the device-scope counters.  Node i
+  // is an end of its own range, so an in-block node i has i - L in [0, 256).
+  __shared__ float4 s_lo[2 * kRefitBlock], s_hi[2 * kRefitBlock];  // leaves, then internal nodes
+  __shared__ int s_vis[kRefitBlock];
+  const int L = blockIdx.x * kRefitBlock;
+  const int R = (L + kRefitBlock < n ? L + kRefitBlock : n) - 1;
+  s_vis[threadIdx.x] = 0;
+  __syncthreads();
+  const int k = L + threadIdx.x;
   if (k >= n) return;
   const int elem = sorted_vals[k];
   int node = (n - 1) + k;
@@ -813,6 +825,8 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
   hi.w = __int_as_float(bvh_escape(n, node, rope, last));
   lo_left[2 * node] = lo;
   hi_esc[2 * node] = hi;
+  s_lo[threadIdx.x] = lo;
+  s_hi[threadIdx.x] = hi;
   if (leaf) {
     // leaf record in sorted order: FP64 box (lo at 0.., hi at 3..), element, escape
     double* o = leaf + (int64_t)k * 8;
@@ -825,7 +839,41 @@ __global__ void k_bvh_refit(int n, const int32_t* __restrict__ sorted_vals, cons
   }
   if (n == 1) return;
   int p = parent[node];
+  bool local = first_leaf != nullptr;
   for (int guard = 0; guard < 128 && p >= 0; ++guard) {
+    if (local) {
+      if (first_leaf[p] >= L && last[p] <= R) {
+        // block scope: this thread's boxes out, the sibling's in
+        __threadfence_block();
+        if (atomicAdd_block(&s_vis[p - L], 1) == 0) return;  // sibling not done yet
+        __threadfence_block();
+        const int lc = left[p], rc = right[p];
+        const int ia = lc >= n - 1 ? lc - (n - 1) - L : kRefitBlock + lc - L;
+        const int ib = rc >= n - 1 ? rc - (n - 1) - L : kRefitBlock + rc - L;
+        const float4 a0 = s_lo[ia], a1 = s_hi[ia], b0 = s_lo[ib], b1 = s_hi[ib];
+        float4 l, h;
+        l.x = fminf(a0.x, b0.x);
+        l.y = fminf(a0.y, b0.y);
+        l.z = fminf(a0.z, b0.z);
+        l.w = __int_as_float(lc);
+        if (BUCKET) {
+          const int f = first_leaf[p], cnt = last[p] - f + 1;
+          if (cnt <= bucket) l.w = __int_as_float((int)(0x80000000u | ((unsigned)(cnt - 1) << 27) | (unsigned)f));
+        }
+        h.x = fmaxf(a1.x, b1.x);
+        h.y = fmaxf(a1.y, b1.y);
+        h.z = fmaxf(a1.z, b1.z);
+        h.w = __int_as_float(bvh_escape(n, p, rope, last));
+        lo_left[2 * p] = l;
+        hi_esc[2 * p] = h;
+        s_lo[kRefitBlock + p - L] = l;
+        s_hi[kRefitBlock + p - L] = h;
+        if (p == 0) return;
+        p = parent[p];
+        continue;
+      }
+      local = false;  // above the block's subtrees: device scope from here on
+    }
     // release: this thread's node boxes; acquire: the sibling's
     cuda::atomic_ref<int, cuda::thread_scope_device> vis(visit[p]);
     if (vis.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;  // sibling not done yet
@@ -873,17 +921,17 @@ cudaError_t launch_bvh_build(int dim, int n, const uint32_t* sorted_keys, const 
   const bool buckets = tree_bucket(n, box64 != nullptr) > 1;
   if (n > 1) {
     k_bvh_internal<<<(n - 1 + 255) / 256, 256, 0, s>>>(n, sorted_keys, parent, rope, last, left, right,
-                                                       buckets ? first_leaf : nullptr);
+                                                       first_leaf);
   }
   cudaMemsetAsync(parent, 0xff, sizeof(int), s);  // parent[root] = -1
   if (buckets)
-    k_bvh_refit<true><<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
-                                                      rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim,
-                                                      box64, bvh.leaf, first_leaf, g_leaf_bucket);
+    k_bvh_refit<true><<<(n + kRefitBlock - 1) / kRefitBlock, kRefitBlock, 0, s>>>(
+        n, sorted_vals, reinterpret_cast<const float4*>(box32), parent, rope, last, left, right, visit, bvh.lo_left,
+        bvh.hi_esc, dim, box64, bvh.leaf, n > 1 ? first_leaf : nullptr, g_leaf_bucket);
   else
-    k_bvh_refit<false><<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
-                                                       rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim,
-                                                       box64, box64 ? bvh.leaf : nullptr, nullptr, 1);
+    k_bvh_refit<false><<<(n + kRefitBlock - 1) / kRefitBlock, kRefitBlock, 0, s>>>(
+        n, sorted_vals, reinterpret_cast<const float4*>(box32), parent, rope, last, left, right, visit, bvh.lo_left,
+        bvh.hi_esc, dim, box64, box64 ? bvh.leaf : nullptr, n > 1 ? first_leaf : nullptr, 1);
   return cudaGetLastError();
 }
 
@@ -2623,7 +2671,7 @@ cudaError_t launch_batched_tree(int n, int nm, const int32_t* sorted_vals, const
   if (n > 1) k_bvh_internal64<<<(n - 1 + 255) / 256, 256, 0, s>>>(n, codes, parent, rope, last, left, right, mesh_off_b, roots);
   cudaMemsetAsync(parent, 0xff, sizeof(int), s);
   k_mesh_roots<<<(nm + 255) / 256, 256, 0, s>>>(nm, n, mesh_off_b, rope, last, roots, stops);
-  k_bvh_refit<false><<<(n + 255) / 256, 256, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
+  k_bvh_refit<false><<<(n + kRefitBlock - 1) / kRefitBlock, kRefitBlock, 0, s>>>(n, sorted_vals, reinterpret_cast<const float4*>(box32), parent,
                                                      rope, last, left, right, visit, bvh.lo_left, bvh.hi_esc, dim,
                                                      box64, box64 ? bvh.leaf : nullptr, nullptr, 1);
   return cudaGetLastError();
