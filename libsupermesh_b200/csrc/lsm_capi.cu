@@ -83,6 +83,7 @@ struct Ctx {
   // explicit pairs / p1 / batched
   DevBuf x_a, x_b, x_measure, x_nout, x_elems, u_a, v_b, blocks;
   DevBuf x_setup, x_tol, x_iota, x_faces, x_screen, x_list;  // explicit tet pairs through the early-out pass
+  DevBuf x_sub;  // hexahedron pairs: A's five tets
   DevBuf elem_off, x_pa, x_pb;  // supermesh elements: per-pair offsets, parents
   DevBuf bt_tabs, bt_pair_a, bt_pair_b, bt_mort, bt_codes, bt_roots, bt_stops, bt_tot, bt_ncand, bt_indptr;
   // host meshes of a batch staged on the device, one set per dimension (the
@@ -294,7 +295,7 @@ void fini_ctx(Ctx* c) {
                    &c->d1_hi_b, &c->d1_tree, &c->d1_e, &c->d1_l, &c->d1_js, &c->q_cache, &c->q_over, &c->q_pool, &c->q_next, &c->q_first,
                    &c->a_faces, &c->b_screen, &c->surv, &c->sched_w, &c->sched_list, &c->sched_cls,
                    &c->sched_adam, &c->bt_indptr, &c->seg_cnt, &c->seg_tab, &c->surv_list,
-                   &c->p1_seg_cnt, &c->p1_seg_tab, &c->x_seg_cnt, &c->x_seg_tab};
+                   &c->p1_seg_cnt, &c->p1_seg_tab, &c->x_seg_cnt, &c->x_seg_tab, &c->x_sub};
   for (DevBuf* b : all) free_buf(*b);
   for (cudaEvent_t& e : c->clip_ev)
     if (e) {
@@ -2132,6 +2133,19 @@ int libsupermesh_gpu_intersect_pairs_mixed(lsm_gpu_context* ctx, int kind, int64
       CU(lsm::launch_tet_hex_pairs(n, da, db, pm, pn, de, ensure<double>(c, c->x_setup, n * 28),
                                    ensure<double>(c, c->x_tol, n), ensure<int32_t>(c, c->x_iota, n),
                                    ensure<int32_t>(c, c->x_list, 4 * n), pairs_work(c), s, &hsg));
+    } else if (kind == LSM_PAIR_HEX_HEX && n >= kPairsPipelineMin && n <= INT32_MAX / 5 &&
+               (((uintptr_t)de) & 15u) == 0) {
+      // large batches: A's five tets clipped by the six-plane index clipper,
+      // one launch per tet, each pair's results carried in order (output tets
+      // written with 16-byte stores: device elems off a 16-byte boundary
+      // stay on the one-launch clipper below, same results)
+      double* pm = dm ? dm : ensure<double>(c, c->x_measure, n);
+      int32_t* pn = dn ? dn : ensure<int32_t>(c, c->x_nout, n);
+      const lsm::SegList hsg = seg_list(c, c->x_seg_cnt, c->x_seg_tab, n);
+      CU(lsm::launch_hex_hex_pairs(n, da, db, pm, pn, de, ensure<double>(c, c->x_setup, n * 28),
+                                   ensure<double>(c, c->x_sub, 5 * n * 12), ensure<double>(c, c->x_tol, 5 * n),
+                                   ensure<int32_t>(c, c->x_iota, n), ensure<int32_t>(c, c->x_list, 4 * n),
+                                   pairs_work(c), s, &hsg));
     } else {
       CU(lsm::launch_pairs_mixed(kind, n, da, db, dm, dn, de, s));
     }

@@ -2016,6 +2016,48 @@ struct IxElemSinkT {
 
 using IxElemSink = IxElemSinkT<81>;
 
+// As IxElemSinkT, but a pair's sum, count and output tets continue from
+// what an earlier launch left in pair_measure / pair_nout / elems: the
+// hexahedron-hexahedron pairs clip A's five tets in five launches, and the
+// reference sums and lists all their output tets in one running order.
+template <int kCap>
+struct IxCarrySinkT {
+  static constexpr bool kInside = true;
+  static constexpr int kLaneDoubles = 0;
+  double* pair_measure;
+  int32_t* pair_nout;
+  double* elems;
+  double m;
+  int kept;
+  int pid;
+  __device__ __forceinline__ void bind(double*) {}
+  __device__ __forceinline__ void begin(const int4& r) {
+    pid = r.x;
+    m = pair_measure[pid];
+    kept = pair_nout[pid];
+  }
+  __device__ __forceinline__ void tet(const Tet& o, double v1) {
+    if (elems && kept < kCap) {
+      double2* e = reinterpret_cast<double2*>(elems + ((int64_t)pid * kCap + kept) * 12);
+      e[0] = make_double2(o.x[0], o.y[0]);
+      e[1] = make_double2(o.z[0], o.x[1]);
+      e[2] = make_double2(o.y[1], o.z[1]);
+      e[3] = make_double2(o.x[2], o.y[2]);
+      e[4] = make_double2(o.z[2], o.x[3]);
+      e[5] = make_double2(o.y[3], o.z[3]);
+    }
+    m = m + v1;
+    ++kept;
+  }
+  __device__ __forceinline__ void end(int64_t p) {
+    pair_measure[p] = m;
+    pair_nout[p] = kept;
+  }
+  template <int NT>
+  __device__ __forceinline__ void finish() {}
+};
+constexpr int kHexHexCap = 5 * 729;  // output tets per hexahedron pair
+
 // The supermesh's tets, written where the scan of the per-pair counts puts
 // them: tet j of pair p at elems[pair_off[p] + j], with its parents.
 struct IxEmitSink {
@@ -2334,6 +2376,72 @@ cudaError_t launch_tet_hex_pairs(int64_t n, const double* tet_a, const double* h
   return cudaGetLastError();
 }
 
+// Hexahedron-hexahedron pairs: B's six face planes (setup rows of
+// clip_row(6) doubles with +inf in the tolerance slot), and A's five tets
+// in the reference's slicing order (Supermesh.F90 intersect_elements), tet k
+// of pair i at sub[(k * n + i) * 12] with its tolerance at tol[k * n + i].
+__global__ void k_setup_hex_hex(int64_t n, const double* __restrict__ hex_a, const double* __restrict__ hex_b,
+                                double* setup, double* sub, double* tol, int32_t* iota) {
+  const int T[5][4] = {{2, 5, 6, 7}, {0, 2, 3, 7}, {0, 4, 5, 7}, {0, 1, 2, 5}, {0, 2, 5, 7}};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double nx[6], ny[6], nz[6], c[6];
+    hex_planes(hex_b + 24 * i, nx, ny, nz, c);
+    double* o = setup + i * clip_row(6);
+#pragma unroll
+    for (int L = 0; L < 6; ++L) {
+      st2(o + 4 * L, nx[L], ny[L]);
+      st2(o + 4 * L + 2, nz[L], c[L]);
+    }
+    st2(o + 24, pos_inf(), 0.0);
+    st2(o + 26, 0.0, 0.0);
+    const double* h = hex_a + 24 * i;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      Tet t;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        t.x[v] = h[3 * T[k][v]];
+        t.y[v] = h[3 * T[k][v] + 1];
+        t.z[v] = h[3 * T[k][v] + 2];
+      }
+      double* q = sub + ((int64_t)k * n + i) * 12;
+      st2(q + 0, t.x[0], t.y[0]);
+      st2(q + 2, t.z[0], t.x[1]);
+      st2(q + 4, t.y[1], t.z[1]);
+      st2(q + 6, t.x[2], t.y[2]);
+      st2(q + 8, t.z[2], t.x[3]);
+      st2(q + 10, t.y[3], t.z[3]);
+      tol[(int64_t)k * n + i] = 10.0 * spacing(tet_volume_v4(t));
+    }
+    iota[i] = (int32_t)i;
+  }
+}
+
+cudaError_t launch_hex_hex_pairs(int64_t n, const double* hex_a, const double* hex_b, double* measure, int32_t* nout,
+                                 double* elems, double* setup, double* sub, double* tol, int32_t* iota,
+                                 int32_t* survivors, unsigned long long* work, cudaStream_t s, const SegList* seg) {
+  if (n <= 0) return cudaSuccess;
+  count_launch();
+  k_setup_hex_hex<<<grid_for(n, 256, 8), 256, 0, s>>>(n, hex_a, hex_b, setup, sub, tol, iota);
+  cudaMemsetAsync(measure, 0, sizeof(double) * n, s);
+  cudaMemsetAsync(nout, 0, sizeof(int32_t) * n, s);
+  const int4* list = reinterpret_cast<const int4*>(survivors);
+  for (int k = 0; k < 5; ++k) {
+    // tet k of every pair: rejected pairs keep their carried results, the
+    // others (A's tet inside all six planes included) add to them
+    const double* tk = sub + (int64_t)k * n * 12;
+    const double* lk = tol + (int64_t)k * n;
+    cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
+    run_prefilter<false, 6>(n, nullptr, iota, iota, tk, lk, setup, nullptr, nullptr, survivors, work, nullptr,
+                            nullptr, nullptr, seg, s);
+    count_launch();
+    k_clip_tets_ix<IxCarrySinkT<kHexHexCap>, kIxHexBlock, 1, 6><<<sm_count(), kIxHexBlock, ix_hex_smem_bytes(), s>>>(
+        list, seg_nlist(seg, work), tk, lk, setup, IxCarrySinkT<kHexHexCap>{measure, nout, elems}, work + 1,
+        seg_table(seg));
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_clip_elems(int64_t n, const int32_t* pair_a, const int32_t* pair_b, const double* tet_a,
                               const double* tol_a, const double* setup, double* measure, int32_t* nout,
                               double* elems, int32_t* survivors, unsigned long long* work, const double* faces_a,
@@ -2485,6 +2593,9 @@ cudaError_t init_device_attributes() {
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_smem_bytes());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_clip_tets_ix<IxMeasureSink, kIxHexBlock, 1, 6>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_hex_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_clip_tets_ix<IxCarrySinkT<kHexHexCap>, kIxHexBlock, 1, 6>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ix_hex_smem_bytes());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_clip_tets_ix<IxElemSinkT<729>, kIxHexBlock, 1, 6>,

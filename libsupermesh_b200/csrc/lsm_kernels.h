@@ -238,6 +238,17 @@ cudaError_t launch_emit_elements(int dim, int64_t npairs, const int32_t* pair_a,
 cudaError_t launch_tet_hex_pairs(int64_t n, const double* tet_a, const double* hex_b, double* measure, int32_t* nout,
                                  double* elems, double* setup, double* tol_a, int32_t* iota, int32_t* survivors,
                                  unsigned long long* work, cudaStream_t s, const SegList* seg = nullptr);
+// Explicit hexahedron-hexahedron pairs (hex_a, hex_b [n][8][3]) through the
+// six-plane index clipper: A sliced into its five tets (sub [5][n][12] and
+// tol [5][n], 16-byte aligned scratch), each clipped against B's planes
+// (setup [n][28]) in one launch per tet, every pair's measure, count and
+// output tets (elems optional, [n][5*729][4][3]) carried from tet to tet in
+// the reference's order; survivors 4 ints per pair, work and seg as for
+// launch_tet_hex_pairs.
+cudaError_t launch_hex_hex_pairs(int64_t n, const double* hex_a, const double* hex_b, double* measure, int32_t* nout,
+                                 double* elems, double* setup, double* sub, double* tol, int32_t* iota,
+                                 int32_t* survivors, unsigned long long* work, cudaStream_t s,
+                                 const SegList* seg = nullptr);
 cudaError_t launch_pairs_explicit(int dim, int64_t n, const double* a, const double* b,
                                   double* measure, int32_t* nout, double* out_elems,
                                   cudaStream_t s);

@@ -352,6 +352,53 @@ def test_tet_hex_device_hexahedra_any_alignment(gpu_ctx):
         assert np.array_equal(dm.cpu().numpy(), m) and np.array_equal(dk.cpu().numpy(), k), off
 
 
+def test_hex_hex_large_batch_bitexact(gpu_ctx, oracle_mod):
+    """Hexahedron pairs in a batch large enough for the six-plane index
+    clipper (A's five tets in five launches, each pair's sum, count and
+    output tets carried from tet to tet): measures and counts bit-identical
+    to the oracle and to small batches (one-launch clipper), output tets of
+    a sample of pairs to the oracle's.  Includes identical unit cubes, A
+    inside B, B inside A and far-apart pairs."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(43)
+    n = 2300
+    a = _random_hexes(rng, n)
+    b = _random_hexes(rng, n)
+    unit = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                     [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], dtype=np.float64)
+    a[:40] = unit
+    b[:40] = unit
+    c = b[40:200].mean(axis=1, keepdims=True)
+    a[40:120] = c[:80] + 0.1 * (a[40:120] - a[40:120].mean(axis=1, keepdims=True))  # A inside B
+    b[120:200] = a[120:200].mean(axis=1, keepdims=True) + 0.1 * (b[120:200] - c[80:])  # B inside A
+    a[200:260] += 3.0  # far apart
+    m, k, _ = gpu_ctx.intersect_pairs_mixed(lsm.PAIR_HEX_HEX, a, b)
+    parts = [gpu_ctx.intersect_pairs_mixed(lsm.PAIR_HEX_HEX, a[j:j + 500], b[j:j + 500]) for j in range(0, n, 500)]
+    assert np.array_equal(np.concatenate([x[0] for x in parts]), m)
+    assert np.array_equal(np.concatenate([x[1] for x in parts]), k)
+    assert (k[200:260] == 0).all()
+    for i in range(n):
+        ref = oracle_mod.intersect_hexes(a[i], b[i])
+        assert k[i] == len(ref), i
+        meas = 0.0
+        for o in ref:
+            meas += oracle_mod.tetrahedron_volume(o)
+        assert m[i] == meas, i
+    # output tets (device arrays: [n][5*729][4][3] does not fit a host test)
+    da = torch.from_numpy(a.reshape(n, -1)).cuda()
+    db = torch.from_numpy(b.reshape(n, -1)).cuda()
+    dm = torch.empty(n, dtype=torch.float64, device="cuda")
+    dk = torch.empty(n, dtype=torch.int32, device="cuda")
+    de = torch.empty((n, 5 * 729, 4, 3), dtype=torch.float64, device="cuda")
+    gpu_ctx.intersect_pairs_device(da, db, dm, dk, de, kind=lsm.PAIR_HEX_HEX)
+    torch.cuda.synchronize()
+    assert np.array_equal(dm.cpu().numpy(), m) and np.array_equal(dk.cpu().numpy(), k)
+    for i in list(range(0, 260, 7)) + list(range(260, n, 97)):
+        ref = oracle_mod.intersect_hexes(a[i], b[i])
+        assert np.array_equal(de[i, : k[i]].cpu().numpy(), ref), i
+    del de
+
+
 def test_tet_hex_large_batch_bitexact(gpu_ctx, oracle_mod):
     """Tet-hex batches large enough for the early-out pass + six-plane index
     clipper: output tets, counts and measures bit-identical to the oracle and

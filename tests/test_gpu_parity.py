@@ -407,6 +407,25 @@ def test_intersect_pairs_large_batch_bitexact(gpu_ctx, oracle_mod):
         lsm.set_option("tet_screen", 1)
 
 
+@pytest.mark.parametrize("n", [2047, 2048, 2049, 70001])
+def test_intersect_pairs_batch_sizes_agree(gpu_ctx, n):
+    """Tet pair batches just below, at and above the size where the early-out
+    pass + index clipper take over (its survivors go to per-block segments
+    that the clipper takes by chunks; 70001 pairs give partial blocks and
+    segments of every length), against the same pairs in batches of 1000
+    (one-launch clipper): measures, counts and output tets identical."""
+    a, b = _random_pairs(3, n, 100 + n % 97)
+    m, k, e = gpu_ctx.intersect_pairs(3, a, b, want_elems=n < 10000)
+    parts = [gpu_ctx.intersect_pairs(3, a[j:j + 1000], b[j:j + 1000], want_elems=n < 10000)
+             for j in range(0, n, 1000)]
+    assert np.array_equal(m, np.concatenate([x[0] for x in parts]))
+    assert np.array_equal(k, np.concatenate([x[1] for x in parts]))
+    if e is not None:
+        e2 = np.concatenate([x[2] for x in parts])
+        for i in range(n):
+            assert np.array_equal(e[i, : k[i]], e2[i, : k[i]]), i
+
+
 def test_legacy_single_pair_entries(oracle_mod):
     a, b = _random_pairs(2, 16, 3)
     for i in range(len(a)):
