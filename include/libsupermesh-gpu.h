@@ -261,7 +261,11 @@ int libsupermesh_gpu_intersect_pairs(lsm_gpu_context *ctx, int dim, int64_t n,
  * measure[n] = sum of output measures, n_out[n] = number of outputs, elems
  * optional, in the reference's output order.  With on_device = 1 and kind
  * LSM_PAIR_TET_HEX, a and elems must be 16-byte aligned (as for
- * libsupermesh_gpu_intersect_pairs). */
+ * libsupermesh_gpu_intersect_pairs).  Batches of 2048 pairs or more of
+ * LSM_PAIR_TET_HEX and LSM_PAIR_HEX_HEX (the latter when elems is NULL or
+ * 16-byte aligned) run through the exact early-out pass and the six-plane
+ * index clipper; smaller ones through a one-launch clipper, with identical
+ * results. */
 enum {
   LSM_PAIR_INTERVALS = 0,
   LSM_PAIR_TRI_QUAD = 1,
