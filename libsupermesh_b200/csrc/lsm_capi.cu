@@ -751,6 +751,7 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_
     }
     bin.screen_b = static_cast<double*>(c->b_screen.p);
     bin.out = ensure<int4>(c, c->sched_list, nnz);
+    bin.flat = ensure<int4>(c, c->surv_list, std::max<int64_t>(nnz, 1));
     bin.window = g_sched_window;
   }
   if (c->dim == 3 && list_inside) {
@@ -763,8 +764,9 @@ void narrow(Ctx* c, cudaStream_t s, const int32_t* order = nullptr, const int64_
     c->clip_timed = false;
     c->surv_seg = false;
   } else {
-    // 3D plain order: survivors as per-block segments, taken by chunks
-    const bool seg = c->dim == 3 && !binned;
+    // 3D: survivors as per-block segments, taken by chunks (the binned
+    // orders gather them into one list first)
+    const bool seg = c->dim == 3;
     const lsm::SegList sg = seg ? seg_list(c, c->seg_cnt, c->seg_tab, nnz) : lsm::SegList{};
     CU(lsm::launch_clip(c->dim, nnz, static_cast<int32_t*>(c->pair_a.p), static_cast<int32_t*>(c->pair_b.p),
                         static_cast<double*>(c->a_coords.p), static_cast<double*>(c->a_tol.p),

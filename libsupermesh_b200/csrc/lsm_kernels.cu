@@ -2376,13 +2376,16 @@ cudaError_t launch_tet_hex_pairs(int64_t n, const double* tet_a, const double* h
   return cudaGetLastError();
 }
 
+// A hexahedron (Gmsh node order) as five tets, in the order and with the
+// vertex order of the reference's slicing (Supermesh.F90:303-334).
+__device__ constexpr int kHexTets[5][4] = {{2, 5, 6, 7}, {0, 2, 3, 7}, {0, 4, 5, 7}, {0, 1, 2, 5}, {0, 2, 5, 7}};
+
 // Hexahedron-hexahedron pairs: B's six face planes (setup rows of
 // clip_row(6) doubles with +inf in the tolerance slot), and A's five tets
-// in the reference's slicing order (Supermesh.F90 intersect_elements), tet k
+// in the reference's slicing order (Supermesh.F90:303-334), tet k
 // of pair i at sub[(k * n + i) * 12] with its tolerance at tol[k * n + i].
 __global__ void k_setup_hex_hex(int64_t n, const double* __restrict__ hex_a, const double* __restrict__ hex_b,
                                 double* setup, double* sub, double* tol, int32_t* iota) {
-  const int T[5][4] = {{2, 5, 6, 7}, {0, 2, 3, 7}, {0, 4, 5, 7}, {0, 1, 2, 5}, {0, 2, 5, 7}};
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double nx[6], ny[6], nz[6], c[6];
     hex_planes(hex_b + 24 * i, nx, ny, nz, c);
@@ -2400,9 +2403,9 @@ __global__ void k_setup_hex_hex(int64_t n, const double* __restrict__ hex_a, con
       Tet t;
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        t.x[v] = h[3 * T[k][v]];
-        t.y[v] = h[3 * T[k][v] + 1];
-        t.z[v] = h[3 * T[k][v] + 2];
+        t.x[v] = h[3 * kHexTets[k][v]];
+        t.y[v] = h[3 * kHexTets[k][v] + 1];
+        t.z[v] = h[3 * kHexTets[k][v] + 2];
       }
       double* q = sub + ((int64_t)k * n + i) * 12;
       st2(q + 0, t.x[0], t.y[0]);
@@ -2500,19 +2503,26 @@ cudaError_t launch_clip(int dim, int64_t npairs, const int32_t* pair_a, const in
     // they settle every candidate
     if (ev_begin) cudaEventRecord(ev_begin, s);
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), s);
-    const SegList sg = bin ? SegList{} : (seg ? *seg : SegList{});
+    // the binned orders read one list: with bin->flat the segments are
+    // gathered into it first
+    const SegList sg = (bin && !bin->flat) ? SegList{} : (seg ? *seg : SegList{});
     run_prefilter<true, 4>(npairs, order, pair_a, pair_b, coords_a, tol_a, setup_b, pair_measure, pair_nout,
                            overflow_list, work, faces_a, screen_b, n_dev, &sg, s);
     const int4* list = reinterpret_cast<const int4*>(overflow_list);
     if (bin) {
+      if (seg_on(&sg)) {
+        cudaError_t e = launch_seg_compact(npairs, work + 2, sg.table, list, bin->flat, s);
+        if (e != cudaSuccess) return e;
+        list = bin->flat;
+      }
       // the survivors reordered into class-uniform runs within windows
       cudaError_t e = launch_sched_bin(*bin, list, work, bin->out, coords_a, s);
       if (e != cudaSuccess) return e;
       list = bin->out;
     }
     k_clip_tets_ix<IxMeasureSink, kIxBlock, kIxBlocksPerSm><<<sm_count() * kIxBlocksPerSm, kIxBlock, ix_smem_bytes(), s>>>(
-        list, seg_nlist(&sg, work), coords_a, tol_a, setup_b, IxMeasureSink{pair_measure, pair_nout, 0.0, 0},
-        work + 1, seg_table(&sg));
+        list, bin ? work : seg_nlist(&sg, work), coords_a, tol_a, setup_b,
+        IxMeasureSink{pair_measure, pair_nout, 0.0, 0}, work + 1, bin ? nullptr : seg_table(&sg));
   }
   if (ev_end) cudaEventRecord(ev_end, s);
   return cudaGetLastError();
@@ -3241,7 +3251,6 @@ __global__ void k_pairs_quad_quad(int64_t n, const double* __restrict__ A, const
 __global__ void __launch_bounds__(64) k_pairs_hex_hex(int64_t n, const double* __restrict__ A,
                                                       const double* __restrict__ B, double* measure,
                                                       int32_t* nout, double* out_elems) {
-  const int T[5][4] = {{2, 5, 6, 7}, {0, 2, 3, 7}, {0, 4, 5, 7}, {0, 1, 2, 5}, {0, 2, 5, 7}};
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double* h = A + 24 * i;
     ArrPlanes<6> P;
@@ -3253,9 +3262,9 @@ __global__ void __launch_bounds__(64) k_pairs_hex_hex(int64_t n, const double* _
       Tet ta;
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        ta.x[v] = h[3 * T[s][v]];
-        ta.y[v] = h[3 * T[s][v] + 1];
-        ta.z[v] = h[3 * T[s][v] + 2];
+        ta.x[v] = h[3 * kHexTets[s][v]];
+        ta.y[v] = h[3 * kHexTets[s][v] + 1];
+        ta.z[v] = h[3 * kHexTets[s][v] + 2];
       }
       const double tol = 10.0 * spacing(tet_volume_v4(ta));
       TetStackN<10> stk;

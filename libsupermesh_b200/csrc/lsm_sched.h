@@ -45,6 +45,7 @@ struct SchedBin {
   int8_t* pred_of_pair = nullptr;
   const double* screen_b = nullptr;  // B's vertices (kScreen3 rows)
   int4* out = nullptr;               // binned list, as many entries as the survivors
+  int4* flat = nullptr;              // (optional) the survivor segments gathered into one list first
   int window = 1024;
 };
 
